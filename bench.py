@@ -1,0 +1,395 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 symmetric-deletion neighbour search.
+
+One step = one full nearest-neighbour search (pack, variant generation, key sort,
+grouping, candidate emission, pair sort, verification, compaction) over the workload's
+sequences, inputs resident in HBM (`value`); `e2e` is the same search through the C ABI's
+host-buffer entry point (xtn_context_perform) with the host->device copy of the sequences
+and the device->host copy of the result pairs inside the timed region.
+
+Workload (default): 1,000,000 synthetic CDR3 sequences, 20% in mutant clusters, 2% exact
+duplicates, Levenshtein d = 2, seeded generator (xtn.synth_clusters).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--workload NAME]
+
+With N > 1 (under torchrun) every rank runs an independent replica of the workload on its
+own GPU (the search does not shard); `value` is the sum over ranks divided by the slowest
+rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "xt-neighbor_b200")
+sys.path.insert(0, PKG)
+
+WORKLOADS = {
+    "nn_1m_leven_d2": dict(kind="clusters", n=1_000_000, d=2, measure=0, seed=20241),
+    "nn_10k_leven_d1": dict(kind="mutants", n=10_000, d=1, measure=0, seed=20240),
+    "nn_10m_leven_d2": dict(kind="clusters", n=10_000_000, d=2, measure=0, seed=20242),
+    "nn_10m_hamming_d2": dict(kind="clusters", n=10_000_000, d=2, measure=1, seed=20242),
+}
+DEFAULT_WORKLOAD = "nn_1m_leven_d2"
+METRIC = "seqs/s (symmetric-deletion NN search, whole job)"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def gen_workload(w):
+    import xtn
+
+    if w["kind"] == "clusters":
+        return xtn.synth_clusters(w["seed"], w["n"], 0.20, 0.02)
+    return xtn.synth_mutants(w["seed"], w["n"], 0.10)
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | None:
+    """Compulsory bytes one launch of `kernel` must move (per-launch average over a step)."""
+    V, G, Pc = st["n_variants"], st["n_groups"], st["n_candidates"]
+    if kernel == "key_sort_downsweep":
+        return 16.0 * V  # read + write each 8-byte record once
+    if kernel == "key_sort_upsweep":
+        return 8.0 * V
+    if kernel == "gen":
+        return 8.0 * V + 25.0 * n  # records out; key, length, offset in
+    if kernel == "find_groups":
+        return 8.0 * V + 12.0 * G
+    if kernel == "pack":
+        return n_chars + 8.0 * n + 21.0 * n
+    if kernel == "verify":
+        return 8.0 * Pc + 2.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args, w):
+    import datetime
+
+    import numpy as np
+    import torch
+
+    import xtn
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    chars, offs = gen_workload(w)
+    n = len(offs) - 1
+    ctx = xtn.Context(local)
+    ctx.set_profiling(True)
+    d_chars = torch.from_numpy(chars).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ext = torch.cuda.ExternalStream(ctx.stream())
+    torch.cuda.synchronize()
+
+    def step():
+        return ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(local)
+    if rank == 0:
+        sampler.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    times, ktimes, launches, n_out, stats = [], {}, 0, 0, None
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between steps (outside the timed window)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        n_out = step()
+        e1.record(ext)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        for k, (ms, cnt) in ctx.kernel_times().items():
+            a, b = ktimes.get(k, (0.0, 0))
+            ktimes[k] = (a + ms, b + cnt)
+        stats = ctx.stats()
+        launches += stats["n_launches"]
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop() if rank == 0 else None
+    ms_step = sum(times) / len(times)
+
+    # end to end through the host-buffer entry point: H2D + search + D2H each step
+    pin_c = torch.from_numpy(chars).pin_memory()
+    pin_o = torch.from_numpy(offs.view(np.int32)).pin_memory()
+    hc, ho = pin_c.numpy(), pin_o.numpy().view(np.uint32)
+    e2e_times = []
+    res = None
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        res = ctx.perform(hc, ho, distance=w["d"], measure=w["measure"])
+        e1.record(ext)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+    assert len(res.pairs) == n_out
+
+    if pg:
+        t = torch.tensor([ms_step, e2e_ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_step, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        ctx.close()
+        if pg:
+            pg.destroy_process_group()
+        return None
+
+    peak, peak_kind = measured_peak_hbm()
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_launches) = dom
+    per_launch_ms = dom_ms / dom_launches
+    launches_per_step = dom_launches / args.steps
+    ab = algorithmic_bytes(dom_name, stats, n, len(chars))
+    achieved = (ab / launches_per_step) / (per_launch_ms / 1e3) / 1e9 if ab else None
+    total_kernel_ms = sum(v[0] for v in ktimes.values())
+    line = {
+        "metric": METRIC,
+        "value": world * n / (ms_step / 1e3),
+        "unit": "seqs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded CDR3 generator)",
+        "config": {
+            "workload": args.workload,
+            "n_seqs": n,
+            "distance": w["d"],
+            "measure": "hamming" if w["measure"] else "leven",
+            "parallelism": f"replicas x{world}",
+            "l2": "flushed between steps (256 MiB write)",
+        },
+        "pairs_per_s": world * n_out / (ms_step / 1e3),
+        "verified_pairs": n_out,
+        "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_out")},
+        "e2e": {
+            "value": world * n / (e2e_ms / 1e3),
+            "unit": "seqs/s",
+            "ms_per_step": e2e_ms,
+            "h2d_bytes_per_step": int(len(chars) + 4 * len(offs)),
+            "d2h_bytes_per_step": int(n_out * 9),
+        },
+        "gpu_launches": int(launches),
+        "roofline": {
+            "kernel": dom_name,
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "traffic": None,
+            "algorithmic_bytes_per_launch": (ab / launches_per_step) if ab else None,
+            "launch_ms": per_launch_ms,
+            "share_of_kernel_time": dom_ms / total_kernel_ms,
+        },
+        "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][0])},
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(chars, offs, w)
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return line
+
+
+def cpu_baseline(chars, offs, w, max_seconds=30.0):
+    """The CPU oracle (multithreaded restatement of the reference algorithm) on the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    n = len(offs) - 1
+    sample = n
+    t0 = time.perf_counter()
+    orc.nn_search(chars, offs, w["d"], w["measure"])
+    dt = time.perf_counter() - t0
+    return {
+        "value": sample / dt,
+        "unit": "seqs/s",
+        "cores": orc.threads(),
+        "kind": "port",
+        "sample": f"whole workload ({sample} seqs), one search",
+        "seconds": dt,
+    }
+
+
+def write_csv(chars, offs, path):
+    import numpy as np
+
+    b = chars.tobytes()
+    with open(path, "wb") as f:
+        f.write(b"cdr3\n")
+        out = bytearray()
+        for i in range(len(offs) - 1):
+            out += b[offs[i] : offs[i + 1]]
+            out += b"\n"
+        f.write(out)
+
+
+def run_reference(args, w):
+    """The reference XTNeighbor-streaming (oracle/_ref/xt_neighbor_ref, its own CUDA CLI built
+    for sm_100a) on the same workload, timed as the reference's harness does: wall clock
+    around the whole process, no output file."""
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return None
+    ref = os.path.join(ROOT, "oracle", "_ref", "xt_neighbor_ref")
+    chars, offs = gen_workload(w)
+    n = len(offs) - 1
+    if not os.path.exists(ref):
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/xt_neighbor_ref missing"}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "seqs.csv")
+        write_csv(chars, offs, path)
+        cmd = [ref, "-i", path, "-n", str(n), "-d", str(w["d"])]
+        if w["measure"]:
+            cmd += ["-m", "hamming"]
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+            dt = time.perf_counter() - t0
+            if p.returncode != 0 or "Cuda error" in p.stdout:
+                return {"impl": "reference", "unavailable": f"reference exited {p.returncode}: {(p.stderr or p.stdout)[-200:]}"}
+            if i >= args.warmup:
+                times.append(dt)
+    s = sum(times) / len(times)
+    v = n / s
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "seqs/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded CDR3 generator)",
+        "config": {"workload": args.workload, "n_seqs": n, "distance": w["d"],
+                   "measure": "hamming" if w["measure"] else "leven", "parallelism": "single process"},
+        "cpu_baseline": {"value": v, "unit": "seqs/s", "cores": 1, "kind": "reference",
+                         "sample": "reference xt_neighbor (CUDA build, sm_100a) on this GPU; whole process: "
+                                   "parse + search, no -o, wall clock"},
+        "e2e": {"value": v, "unit": "seqs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * xtn_b200 - C ABI of the B200 (sm_100a) symmetric-deletion neighbour search.
+ *
+ * This is the drop-in boundary for the hot path of XTNeighbor-streaming
+ * (heartnetkung/XT-neighbor, xtneighbor_streaming/, abbreviated S/ below). The
+ * reference exposes the path as one C++ function,
+ *     void xtn_perform(XTNArgs, SeqArray*, SeqInfo*, void callback(XTNOutput))
+ * (S/src/xtn.cu:267, declared S/src/xtn.h:124), called only by its CLI (S/src/cli.cu:267-271).
+ * This header restates that interface with plain pointers and sizes so that any FFI
+ * (ctypes, cgo, JNI, N-API) can bind it, and adds a reusable context, device-resident
+ * entry points and status codes. All calls are synchronous with respect to the host
+ * unless stated otherwise; a context may be used by one host thread at a time.
+ */
+#ifndef XTN_B200_H
+#define XTN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Distance measures; same values as LEVENSHTEIN / HAMMING in S/src/xtn.h:12-14. */
+#define XTN_LEVENSHTEIN 0
+#define XTN_HAMMING 1
+
+/* Return codes. 0..2 are the reference's ReturnCode {SUCCESS, ERROR, EXIT}
+ * (S/src/xtn.h:93); the reference reports CUDA failures by printing and carrying on
+ * (S/src/util.cu:5-11), this library returns one of the codes below instead. */
+#define XTN_SUCCESS 0
+#define XTN_ERROR 1
+#define XTN_EXIT 2
+#define XTN_ERR_CUDA 3      /* a CUDA call failed; xtn_last_error() has the text */
+#define XTN_ERR_NOMEM 4     /* device or pinned-host allocation failed */
+#define XTN_ERR_ARG 5       /* invalid argument (sizes, distance, measure, null pointers) */
+#define XTN_ERR_NODEV 6     /* no usable CUDA device */
+#define XTN_ERR_LIMIT 7     /* input exceeds a documented limit of this build */
+
+/* Pair of sequence indexes; layout of Int2 (S/src/xtn.h:30-36). */
+typedef struct xtn_int2 {
+    int32_t x, y;
+} xtn_int2;
+
+/* Per-sequence information in overlap mode; layout of SeqInfo (S/src/xtn.h:41-45).
+ * frequency: the row's count (non-zero int); repertoire: 0-based repertoire id, non-decreasing
+ * over rows; original_index: the row's own index (the reference sets it, S/src/cli.cu:178-181). */
+typedef struct xtn_seq_info {
+    int32_t frequency, repertoire, original_index;
+} xtn_seq_info;
+
+/* Arguments; the fields of XTNArgs (S/src/xtn.h:50-60) that reach the algorithm.
+ * The reference selects overlap mode with infoPath != NULL (S/src/xtn.cu:281); here a
+ * non-null `info` argument does. */
+typedef struct xtn_args {
+    int32_t distance; /* >= 1 (S/src/cli.cu:53-57) */
+    int32_t measure;  /* XTN_LEVENSHTEIN or XTN_HAMMING */
+    int32_t verbose;  /* non-zero: print stage sizes and timings to stdout */
+    int32_t info_len; /* overlap mode: number of repertoires (the -N value) */
+} xtn_args;
+
+/* One chunk of output; layout of XTNOutput (S/src/xtn.h:83-88).
+ * NN mode: index_pairs[i] = (x, y), x < y, globally sorted by (x, y); pairwise_distances[i]
+ * is the reference's `char` distance. Overlap mode: index_pairs[i] = (rep_x, rep_y) with
+ * rep_x <= rep_y, sorted, and pairwise_frequencies[i] the summed count products (mod 2^64).
+ * The arrays are owned by the library and valid only during the callback, as in the
+ * reference (S/src/xtn.cu:458-459,479). */
+typedef struct xtn_output {
+    const xtn_int2* index_pairs;
+    const int8_t* pairwise_distances;
+    const uint64_t* pairwise_frequencies;
+    int64_t len;
+} xtn_output;
+
+typedef void (*xtn_callback)(const xtn_output* output, void* user);
+
+/* Opaque reusable state: device, stream and device buffers that grow on demand. */
+typedef struct xtn_context xtn_context;
+
+/* Counters and stage timings of the last run on a context. */
+typedef struct xtn_stats {
+    int64_t n_seqs;            /* sequences searched (unique sequences in overlap mode) */
+    int64_t n_variants;        /* deletion variants generated */
+    int64_t n_groups;          /* groups of equal variant hashes with >= 2 members */
+    int64_t n_candidates;      /* candidate pairs emitted (with repeats and self-pairs) */
+    int64_t n_unique;          /* distinct candidate pairs */
+    int64_t n_out;             /* verified pairs (NN) or matrix entries (overlap) */
+    int64_t n_verified_pairs;  /* verified sequence pairs (overlap mode) */
+    int64_t n_launches;        /* kernel launches of the last run */
+    int32_t id_bits;           /* bits used for a sequence id in packed records */
+    int32_t n_rounds;          /* key-space rounds the search ran in */
+    double ms_total;           /* device time of the last run, milliseconds */
+    double ms_stage[8];        /* pack, gen, key sort, group, emit, pair sort, verify, output */
+} xtn_stats;
+
+/* ------------------------------------------------------------------ reference interface */
+
+/* xtn_perform: the whole search on host buffers; replaces S/src/xtn.cu:267-509.
+ * seqs/offsets: CSR store of n_seqs sequences (what SeqArray holds after parsing,
+ *   S/src/codec.cu:168-243): sequence i is seqs[offsets[i] .. offsets[i+1]), residues in
+ *   'A'..'Y' minus B,J,O,U,X, length 1..500.
+ * info: NULL for nearest-neighbour mode; in overlap mode one entry per row (row order).
+ * callback is called one or more times with consecutive chunks of the sorted output.
+ * Uses a library-owned context on device 0. Returns XTN_SUCCESS or an error code. */
+int xtn_perform(const xtn_args* args, const char* seqs, const uint32_t* offsets, int32_t n_seqs,
+                const xtn_seq_info* info, xtn_callback callback, void* user);
+
+/* ------------------------------------------------------------------ context API */
+
+int xtn_context_create(int device, xtn_context** out);
+void xtn_context_destroy(xtn_context* ctx);
+
+/* xtn_perform on an explicit context. */
+int xtn_context_perform(xtn_context* ctx, const xtn_args* args, const char* seqs, const uint32_t* offsets,
+                        int32_t n_seqs, const xtn_seq_info* info, xtn_callback callback, void* user);
+
+/* Nearest-neighbour search on inputs already in device memory (d_seqs, d_offsets as in
+ * xtn_perform). The result stays on the device; *n_out receives its length. Read it with
+ * xtn_context_fetch or xtn_context_result_device. */
+int xtn_context_nn_device(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                          int32_t n_seqs, int64_t* n_out);
+
+/* Copies up to `cap` entries of the last result to host memory (either pointer may be NULL). */
+int xtn_context_fetch(xtn_context* ctx, xtn_int2* pairs, int8_t* distances, uint64_t* frequencies, int64_t cap);
+
+/* Device pointers of the last result (valid until the next run on the context). */
+int xtn_context_result_device(xtn_context* ctx, const xtn_int2** d_pairs, const int8_t** d_distances, int64_t* n_out);
+
+/* The CUDA stream the context launches on (as a cudaStream_t cast to void*). */
+void* xtn_context_stream(xtn_context* ctx);
+
+int xtn_context_stats(const xtn_context* ctx, xtn_stats* out);
+
+/* Per-kernel device time. With profiling on, every kernel launch of a run is bracketed by
+ * CUDA events on the context stream; xtn_context_kernel_times then reports, per kernel
+ * name, the summed duration (ms) and launch count of the last run. Returns the number of
+ * distinct kernels (entries written: at most cap). */
+int xtn_context_set_profiling(xtn_context* ctx, int on);
+int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double* ms, int64_t* launches, int cap);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char* xtn_last_error(void);
+
+/* Library version string ("2.0.0" like the reference CLI, S/src/cli.cu:9, plus a build tag). */
+const char* xtn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XTN_B200_H */

@@ -1,0 +1,24 @@
+#!/usr/bin/env bash
+# Builds the reference XTNeighbor-streaming from its own sources (read in place, never
+# copied) into oracle/_ref/, for use as a checker only:
+#   _ref/xt_neighbor_ref - the reference CLI (S/src/cli.cu, one translation unit), sm_100a
+#   _ref/ref_harness     - host harness around the reference's variant generator and codec
+# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+set -euo pipefail
+REF=${1:-/root/reference}
+SRC="$REF/xtneighbor_streaming/src"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+if [ ! -f "$SRC/cli.cu" ]; then
+    echo "build_ref: reference sources not found under $SRC; skipping" >&2
+    exit 0
+fi
+mkdir -p "$OUT"
+NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
+if [ ! -x "$OUT/ref_harness" ] || [ "$HERE/ref_harness.cu" -nt "$OUT/ref_harness" ]; then
+    "$NVCC" -O2 -w -gencode arch=compute_100a,code=sm_100a -I "$SRC" -o "$OUT/ref_harness" "$HERE/ref_harness.cu"
+fi
+if [ ! -x "$OUT/xt_neighbor_ref" ]; then
+    "$NVCC" -O3 -w -gencode arch=compute_100a,code=sm_100a -o "$OUT/xt_neighbor_ref" "$SRC/cli.cu"
+fi
+echo "build_ref: ok ($OUT)"

@@ -1,0 +1,71 @@
+// Test helper: the library's host+device helpers (key packing, run-prefix variant
+// enumeration, Myers/Hamming distances, prefix-variant test) compiled for the CPU, so the
+// test suite can compare them with the oracle without a GPU. Not part of the product.
+#include <cstdint>
+#include <cstring>
+
+#include "../../xt-neighbor_b200/csrc/xtn_common.cuh"
+
+using namespace xtn;
+
+static u128 pack(const char* s, int L) {
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    u128 v = 0;
+    for (int j = 0; j < Lk; j++) v = key_put(v, j, (unsigned)code_of((uint8_t)s[j]));
+    return v;
+}
+
+static void unpack(u128 v, char* out) {
+    int i = 0;
+    for (; i < kKeyLen; i++) {
+        int c = key_get(v, i);
+        if (!c) break;
+        out[i] = (char)('A' - 1 + c);
+    }
+    out[i] = '\0';
+}
+
+extern "C" {
+
+// Variants of the first 18 residues of s (length L) with at most d deletions: count, and
+// when out != NULL the decoded strings (19 bytes each) and hashes.
+int hc_variants(const char* s, int L, int d, char* out, uint64_t* hashes, int cap) {
+    u128 key = pack(s, L);
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    int n = 0;
+    for_each_variant(key, Lk, d, [&](u128 k) {
+        if (n < cap) {
+            if (out) unpack(k, out + 19 * n);
+            if (hashes) hashes[n] = key_hash(k);
+        }
+        n++;
+    });
+    return n;
+}
+
+int hc_variant_count(const char* s, int L, int d) {
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    return variant_count(pack(s, L), Lk, d);
+}
+
+void hc_key_del(const char* s, int L, int p, char* out) { unpack(key_del(pack(s, L), p), out); }
+
+int hc_lev_myers(const char* a, int la, const char* b, int lb) {
+    return lev_myers64((const uint8_t*)a, la, (const uint8_t*)b, lb);
+}
+
+int hc_lev_dp(const char* a, int la, const char* b, int lb, int cap) {
+    int col[kMaxInputLength + 2];
+    return lev_dp((const uint8_t*)a, la, (const uint8_t*)b, lb, col, cap);
+}
+
+int hc_hamming(const char* a, int la, const char* b, int lb, int* raw) {
+    return hamming_ref((const uint8_t*)a, la, (const uint8_t*)b, lb, raw);
+}
+
+int hc_share_variant(const char* a, int la, const char* b, int lb, int d) {
+    return prefixes_share_variant((const uint8_t*)a, la, (const uint8_t*)b, lb, d) ? 1 : 0;
+}
+
+uint64_t hc_tri_row_start(uint64_t i, uint64_t s) { return tri_row_start(i, s); }
+}

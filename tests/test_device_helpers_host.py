@@ -1,0 +1,122 @@
+"""The product's shared host/device helpers (xt-neighbor_b200/csrc/xtn_common.cuh), compiled
+for the CPU into tests/hostcheck/libhostcheck.so, against the oracle and brute force.
+
+Covers: run-prefix variant enumeration gives exactly the set of distinct strings of the
+reference's variant multiset; the closed-form variant count; Myers' bit-vector Levenshtein
+and the banded-exit DP; the reference's Hamming (77 sentinel, signed-char wrap); and the
+prefix-shares-a-variant predicate.
+"""
+import ctypes
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+
+HC = os.path.join(os.path.dirname(__file__), "hostcheck", "libhostcheck.so")
+pytestmark = pytest.mark.skipif(not os.path.exists(HC), reason="hostcheck helper not built")
+
+
+@pytest.fixture(scope="module")
+def hc():
+    lib = ctypes.CDLL(HC)
+    lib.hc_variants.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.hc_tri_row_start.restype = ctypes.c_uint64
+    lib.hc_tri_row_start.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+    return lib
+
+
+def variants(hc, s, d):
+    n = hc.hc_variants(s.encode(), len(s), d, None, None, 0)
+    buf = ctypes.create_string_buffer(19 * n)
+    hs = np.zeros(n, np.uint64)
+    hc.hc_variants(s.encode(), len(s), d, buf, hs.ctypes.data_as(ctypes.c_void_p), n)
+    raw = buf.raw
+    out = [raw[19 * i : 19 * i + 19].split(b"\0")[0].decode() for i in range(n)]
+    return out, hs
+
+
+def rand_seqs(rng, n, lo=1, hi=26, alpha="ACDEFGHIKLMNPQRSTVWY"):
+    out = []
+    for _ in range(n):
+        L = int(rng.integers(lo, hi))
+        sub = alpha[: int(rng.integers(2, len(alpha) + 1))]
+        out.append("".join(rng.choice(list(sub), L)))
+    return out
+
+
+def test_variant_set_equals_reference_multiset(hc):
+    rng = np.random.default_rng(3)
+    for s in rand_seqs(rng, 500):
+        for d in (1, 2, 3, 4):
+            got, hashes = variants(hc, s, d)
+            ref = orc.expand_keys(s, d)
+            assert set(got) == set(ref), (s, d)
+            assert hc.hc_variant_count(s.encode(), len(s), d) == len(got), (s, d)
+            # equal strings hash equally
+            hm = {}
+            for g, h in zip(got, hashes):
+                assert hm.setdefault(g, int(h)) == int(h)
+
+
+def test_key_delete(hc):
+    rng = np.random.default_rng(5)
+    for s in rand_seqs(rng, 200, 1, 19):
+        for p in range(len(s)):
+            buf = ctypes.create_string_buffer(20)
+            hc.hc_key_del(s.encode(), len(s), p, buf)
+            assert buf.value.decode() == s[:p] + s[p + 1 :]
+
+
+def test_levenshtein_myers_and_dp(hc):
+    rng = np.random.default_rng(9)
+    seqs = rand_seqs(rng, 400, 1, 70, "ACDEF")
+    for a, b in zip(seqs[::2], seqs[1::2]):
+        ref = orc.levenshtein(a, b)
+        if len(a) <= 64:
+            assert hc.hc_lev_myers(a.encode(), len(a), b.encode(), len(b)) == ref, (a, b)
+        assert hc.hc_lev_dp(a.encode(), len(a), b.encode(), len(b), 1000) == ref
+        got = hc.hc_lev_dp(a.encode(), len(a), b.encode(), len(b), 2)
+        assert (got == ref) if ref <= 2 else got > 2
+
+
+def test_levenshtein_long(hc):
+    rng = np.random.default_rng(10)
+    for _ in range(20):
+        a = "".join(rng.choice(list("ACD"), int(rng.integers(100, 500))))
+        b = list(a)
+        for _ in range(int(rng.integers(0, 4))):
+            b[int(rng.integers(0, len(b)))] = "E"
+        b = "".join(b)
+        assert hc.hc_lev_dp(a.encode(), len(a), b.encode(), len(b), 1000) == orc.levenshtein(a, b)
+
+
+def test_hamming_reference(hc):
+    raw = ctypes.c_int()
+    assert hc.hc_hamming(b"CAAA", 4, b"CAA", 3, ctypes.byref(raw)) == 77
+    a, b = "A" * 200, "AC" * 100
+    v = hc.hc_hamming(a.encode(), 200, b.encode(), 200, ctypes.byref(raw))
+    assert raw.value == 100 and v == orc.hamming(a, b)
+    a, b = "A" * 300, "C" * 300
+    v = hc.hc_hamming(a.encode(), 300, b.encode(), 300, ctypes.byref(raw))
+    assert raw.value == 300 and v == orc.hamming(a, b) == 44
+
+
+def test_prefix_share_variant(hc):
+    rng = np.random.default_rng(12)
+    seqs = rand_seqs(rng, 600, 1, 24, "ACDE")
+    for a, b in zip(seqs[::2], seqs[1::2]):
+        for d in (1, 2, 3):
+            va = set(orc.expand_keys(a, d))
+            vb = set(orc.expand_keys(b, d))
+            assert hc.hc_share_variant(a.encode(), len(a), b.encode(), len(b), d) == (1 if va & vb else 0), (a, b, d)
+
+
+def test_triangle_rows(hc):
+    for s in range(2, 40):
+        l = 0
+        for i in range(s - 1):
+            assert hc.hc_tri_row_start(i, s) == l
+            l += s - 1 - i

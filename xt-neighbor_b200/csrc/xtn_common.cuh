@@ -1,0 +1,253 @@
+// Host+device helpers shared by the sm_100a kernels and the CPU self-test.
+//
+// Key format. The reference keys a sequence by its first 18 residues, 5 bits each
+// (S/src/codec.cu:43-60, S/src/kernel.cu:594-610, MAX_COMPRESSED_LENGTH S/src/xtn.h:8).
+// Here the same 90 bits live in one unsigned 128-bit word, residue i in bits
+// [123-5i, 128-5i) (MSB first) and zeros after the last residue, so a deletion is one
+// masked shift and equal strings are equal words.
+//
+// Variant enumeration. The reference emits every deletion set of at most min(d, L)
+// positions, duplicates included (S/src/generate_combination.cu:42-141). Deleting any c
+// residues of one run of equal residues gives the same string as deleting the first c of
+// that run, so enumerating only "run-prefix" deletion sets yields the same set of distinct
+// strings with far fewer repeats. The set of key-sharing sequence pairs is unchanged; only
+// repeated emissions of the same pair disappear.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define XTN_HD __host__ __device__ __forceinline__
+#else
+#define XTN_HD inline
+#endif
+
+namespace xtn {
+
+typedef unsigned __int128 u128;
+
+constexpr int kKeyLen = 18;          // S/src/xtn.h:8
+constexpr int kLevenshtein = 0;      // S/src/xtn.h:12
+constexpr int kHamming = 1;          // S/src/xtn.h:14
+constexpr int kHammingLenMismatch = 77;  // S/src/kernel.cu:292-293
+constexpr int kMaxInputLength = 500;     // S/src/codec.cu:18
+
+// 'A'..'Y' -> 1..25 (S/src/codec.cu:25-38); inputs are validated by the parser.
+XTN_HD int code_of(uint8_t c) { return (int)c - ('A' - 1); }
+
+XTN_HD u128 key_put(u128 v, int i, unsigned code) { return v | ((u128)code << (123 - 5 * i)); }
+XTN_HD int key_get(u128 v, int i) { return (int)((v >> (123 - 5 * i)) & 31u); }
+
+// Delete residue p of a packed key (p < 18).
+XTN_HD u128 key_del(u128 v, int p) {
+    if (p == 0) return v << 5;
+    u128 hi = ~(u128)0 << (128 - 5 * p);
+    return (v & hi) | ((v << 5) & ~hi);
+}
+
+// Bit i set when residue i starts a run of equal residues (i < L).
+XTN_HD uint32_t key_run_starts(u128 v, int L) {
+    u128 x = v ^ (v >> 5);
+    uint32_t m = 0;
+    for (int i = 0; i < L; i++)
+        if (key_get(x, i)) m |= 1u << i;
+    return m;
+}
+
+// MurmurHash3's 64-bit finaliser (Appleby, public domain).
+XTN_HD uint64_t fmix64(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
+}
+
+// Hash of a packed key. Only equality of keys matters for correctness: two sequences
+// that share a key always share its hash, and pairs that share only a hash are removed
+// by exact verification.
+XTN_HD uint64_t key_hash(u128 v) {
+    uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;
+    return fmix64(hi ^ fmix64(lo + 0x9e3779b97f4a7c15ULL));
+}
+
+// Calls f(key) once per run-prefix deletion set of at most min(d, L) positions
+// (the empty set included). Returns the number of calls.
+template <class F>
+XTN_HD int for_each_variant(u128 key, int L, int d, F&& f) {
+    f(key);
+    int e = d < L ? d : L;
+    if (e <= 0) return 1;
+    uint32_t rs = key_run_starts(key, L);
+    int count = 1;
+    if (e <= 2) {
+        for (int p = 0; p < L; p++) {
+            if (!((rs >> p) & 1u)) continue;
+            u128 v1 = key_del(key, p);
+            f(v1);
+            count++;
+            if (e == 2)
+                for (int q = p + 1; q < L; q++) {
+                    if (!(((rs >> q) & 1u) || q == p + 1)) continue;
+                    f(key_del(v1, q - 1));
+                    count++;
+                }
+        }
+        return count;
+    }
+    // general depth: iterative DFS over ascending run-prefix deletion sets
+    int pos[kKeyLen];
+    u128 val[kKeyLen + 1];
+    val[0] = key;
+    int depth = 0, q = 0;
+    while (true) {
+        if (depth < e && q < L) {
+            bool ok = ((rs >> q) & 1u) || (depth > 0 && pos[depth - 1] == q - 1);
+            if (ok) {
+                pos[depth] = q;
+                val[depth + 1] = key_del(val[depth], q - depth);
+                f(val[depth + 1]);
+                count++;
+                depth++;
+                q = q + 1;
+            } else {
+                q++;
+            }
+            continue;
+        }
+        if (depth == 0) break;
+        depth--;
+        q = pos[depth] + 1;
+    }
+    return count;
+}
+
+struct CountOnly {
+    XTN_HD void operator()(u128) const {}
+};
+
+XTN_HD int popc32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __popc(x);
+#else
+    return __builtin_popcount(x);
+#endif
+}
+
+// Number of calls for_each_variant makes, in closed form for d <= 2.
+XTN_HD int variant_count(u128 key, int L, int d) {
+    int e = d < L ? d : L;
+    if (e <= 0) return 1;
+    if (e <= 2) {
+        uint32_t rs = key_run_starts(key, L);
+        int R = popc32(rs);
+        if (e == 1) return 1 + R;
+        uint32_t cont = ~rs & ((L >= 32) ? 0xffffffffu : ((1u << L) - 1u));
+        int R2 = popc32(rs & (cont >> 1));
+        return 1 + R + R * (R - 1) / 2 + R2;
+    }
+    return for_each_variant(key, L, d, CountOnly{});
+}
+
+// Row i of a group of size s owns pairs (i, i+1..s-1); it starts at local index r(i).
+XTN_HD uint64_t tri_row_start(uint64_t i, uint64_t s) { return i * (2 * s - i - 1) / 2; }
+
+// ------------------------------------------------------------------ distances
+// Levenshtein distance by Myers' bit-vector algorithm in Hyyro's global form
+// (G. Myers, J. ACM 46(3) 1999; H. Hyyro, 2001). `a` is the pattern (1 <= m <= 64).
+XTN_HD int lev_myers64(const uint8_t* a, int m, const uint8_t* b, int n) {
+    uint64_t p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0;  // bit-sliced residue codes of a
+    for (int i = 0; i < m; i++) {
+        unsigned c = (unsigned)code_of(a[i]);
+        uint64_t bit = 1ull << i;
+        if (c & 1u) p0 |= bit;
+        if (c & 2u) p1 |= bit;
+        if (c & 4u) p2 |= bit;
+        if (c & 8u) p3 |= bit;
+        if (c & 16u) p4 |= bit;
+    }
+    const uint64_t mask = m == 64 ? ~0ull : ((1ull << m) - 1);
+    const uint64_t high = 1ull << (m - 1);
+    uint64_t pv = mask, mv = 0;
+    int score = m;
+    for (int j = 0; j < n; j++) {
+        unsigned c = (unsigned)code_of(b[j]);
+        uint64_t eq = mask;
+        eq &= (c & 1u) ? p0 : ~p0;
+        eq &= (c & 2u) ? p1 : ~p1;
+        eq &= (c & 4u) ? p2 : ~p2;
+        eq &= (c & 8u) ? p3 : ~p3;
+        eq &= (c & 16u) ? p4 : ~p4;
+        uint64_t xv = eq | mv;
+        uint64_t xh = (((eq & pv) + pv) ^ pv) | eq;
+        uint64_t ph = mv | ~(xh | pv);
+        uint64_t mh = pv & xh;
+        if (ph & high) score++;
+        else if (mh & high) score--;
+        ph = (ph << 1) | 1ull;
+        mh = mh << 1;
+        pv = mh | ~(xv | ph);
+        mv = ph & xv;
+    }
+    return score;
+}
+
+// Exact Levenshtein with the column held in `col` (>= m+1 ints), stopping early once every
+// cell of a column exceeds `cap` (the result is then some value > cap).
+XTN_HD int lev_dp(const uint8_t* a, int m, const uint8_t* b, int n, int* col, int cap) {
+    for (int y = 0; y <= m; y++) col[y] = y;
+    for (int x = 1; x <= n; x++) {
+        int lastdiag = col[0];
+        col[0] = x;
+        int best = x;
+        for (int y = 1; y <= m; y++) {
+            int old = col[y];
+            int v = col[y] + 1, w = col[y - 1] + 1, z = lastdiag + (a[y - 1] == b[x - 1] ? 0 : 1);
+            int r = v < w ? v : w;
+            r = r < z ? r : z;
+            col[y] = r;
+            lastdiag = old;
+            best = best < r ? best : r;
+        }
+        if (best > cap) return cap + 1;
+    }
+    return col[m];
+}
+
+// Hamming as the reference computes it (S/src/kernel.cu:290-300): 77 for unequal
+// lengths, and the mismatch count held in a signed char (wraps past 127). Also returns the
+// unwrapped count through *raw.
+XTN_HD int hamming_ref(const uint8_t* a, int la, const uint8_t* b, int lb, int* raw) {
+    if (la != lb) {
+        *raw = kHammingLenMismatch;
+        return kHammingLenMismatch;
+    }
+    int m = 0;
+    for (int i = 0; i < la; i++) m += a[i] != b[i];
+    *raw = m;
+    return (int)(int8_t)(uint8_t)(m & 0xFF);
+}
+
+// True when the first-18-residue keys of a and b share a deletion variant of at most d
+// deletions each, i.e. when LCS(A, B) >= max(|A|, |B|) - d for the prefixes A, B. This is
+// the reference's candidate condition; the verify step needs it only where the reference's
+// wrapped Hamming counter accepts a pair whose true distance exceeds d.
+XTN_HD bool prefixes_share_variant(const uint8_t* a, int la, const uint8_t* b, int lb, int d) {
+    int A = la < kKeyLen ? la : kKeyLen, B = lb < kKeyLen ? lb : kKeyLen;
+    int need = (A > B ? A : B) - d;
+    if (need <= 0) return true;
+    int row[kKeyLen + 1];
+    for (int j = 0; j <= B; j++) row[j] = 0;
+    for (int i = 1; i <= A; i++) {
+        int diag = 0;
+        for (int j = 1; j <= B; j++) {
+            int up = row[j];
+            int v = a[i - 1] == b[j - 1] ? diag + 1 : (row[j] > row[j - 1] ? row[j] : row[j - 1]);
+            diag = up;
+            row[j] = v;
+        }
+    }
+    return row[B] >= need;
+}
+
+}  // namespace xtn

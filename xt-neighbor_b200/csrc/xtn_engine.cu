@@ -1,0 +1,1017 @@
+// B200 (sm_100a) symmetric-deletion neighbour search: kernels, host orchestration and the
+// C ABI declared in include/xtn_b200.h.
+//
+// Pipeline for nearest-neighbour mode (reference stages in S/src/xtn.cu:311-473):
+//   pack     k_pack          first 18 residues -> 128-bit key, variant count per sequence
+//   scan                     variant offsets
+//   gen      k_gen           one 64-bit record per deletion variant: hash bits | sequence id
+//   sort     radix_sort_u64  records by their hash bits (equal variants become adjacent)
+//   group    k_find_groups   runs of >= 2 equal hashes
+//   emit     k_emit          every id pair of every run, packed (min << b) | max
+//   sort     radix_sort_u64  candidate pairs
+//   verify   k_verify        unique pairs, x != y, Levenshtein (Myers) / Hamming on the full
+//                            strings, keep dist <= d (S/src/kernel.cu:359-392)
+//   compact  k_compact       sorted (x, y, dist) output
+// Everything stays in device memory; the host reads four scalars to size buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/xtn_b200.h"
+#include "xtn_common.cuh"
+#include "xtn_prims.cuh"
+
+namespace xtn {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_err;
+static void set_err(const std::string& s) { t_err = s; }
+
+#define XTN_CK(call)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            set_err(std::string(#call) + " failed: " + cudaGetErrorString(e_));                 \
+            return e_ == cudaErrorMemoryAllocation ? XTN_ERR_NOMEM : XTN_ERR_CUDA;                \
+        }                                                                                         \
+    } while (0)
+
+#define XTN_TRY(expr)             \
+    do {                          \
+        int r_ = (expr);          \
+        if (r_ != XTN_SUCCESS) return r_; \
+    } while (0)
+
+// ------------------------------------------------------------------ kernels
+constexpr int kThreads = 256;
+
+__global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
+                       const int32_t* __restrict__ rows, int n, int d, u128* __restrict__ keys,
+                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int r = rows ? rows[i] : i;
+    uint32_t s = offs[r];
+    int L = (int)(offs[r + 1] - s);
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    u128 v = 0;
+    for (int j = 0; j < Lk; j++) v = key_put(v, j, (unsigned)code_of(chars[s + j]));
+    keys[i] = v;
+    klen[i] = (uint8_t)Lk;
+    vcnt[i] = (uint32_t)variant_count(v, Lk, d);
+}
+
+__global__ void k_gen(const u128* __restrict__ keys, const uint8_t* __restrict__ klen,
+                      const uint64_t* __restrict__ voff, int n, int d, int idbits, uint64_t* __restrict__ recs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
+    uint64_t o = voff[i];
+    const uint64_t id = (uint64_t)i;
+    for_each_variant(keys[i], klen[i], d, [&](u128 k) { recs[o++] = (key_hash(k) & hi_mask) | id; });
+}
+
+// Heads of runs of >= 2 equal hashes; appended in any order through a warp-aggregated cursor.
+__global__ void k_find_groups(const uint64_t* __restrict__ recs, int64_t V, int idbits, uint64_t* __restrict__ gstart,
+                              uint32_t* __restrict__ gsize, unsigned long long* __restrict__ counter, int64_t cap) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool head = false;
+    uint64_t k = 0;
+    if (i < V) {
+        k = recs[i] >> idbits;
+        head = (i == 0 || (recs[i - 1] >> idbits) != k) && (i + 1 < V && (recs[i + 1] >> idbits) == k);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, head);
+    if (m == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!head) return;
+    unsigned long long slot = base + __popc(m & ((1u << lane) - 1u));
+    int64_t j = i + 2;
+    while (j < V && (recs[j] >> idbits) == k) j++;
+    if ((int64_t)slot < cap) {
+        gstart[slot] = (uint64_t)i;
+        gsize[slot] = (uint32_t)(j - i);
+    }
+}
+
+__global__ void k_pair_counts(const uint32_t* __restrict__ gsize, int64_t G, uint64_t* __restrict__ cnt) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    uint64_t s = gsize[g];
+    cnt[g] = s * (s - 1) / 2;
+}
+
+constexpr int kEmitPer = 8;
+
+
+__global__ void k_emit(const uint64_t* __restrict__ recs, const uint64_t* __restrict__ gstart,
+                       const uint32_t* __restrict__ gsize, const uint64_t* __restrict__ goff, int64_t G, uint64_t P,
+                       int idbits, uint64_t* __restrict__ pairs) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t p = t * kEmitPer;
+    if (p >= P) return;
+    uint64_t pend = p + kEmitPer < P ? p + kEmitPer : P;
+    int64_t lo = 0, hi = G - 1;
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (goff[mid] <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    int64_t g = lo;
+    uint64_t s = gsize[g];
+    uint64_t base = gstart[g];
+    uint64_t l = p - goff[g];
+    double b2 = (double)(2 * s - 1);
+    int64_t ii = (int64_t)floor((b2 - sqrt(b2 * b2 - 8.0 * (double)l)) * 0.5);
+    if (ii < 0) ii = 0;
+    uint64_t i = (uint64_t)ii;
+    while (i + 1 < s && tri_row_start(i + 1, s) <= l) i++;
+    while (i > 0 && tri_row_start(i, s) > l) i--;
+    uint64_t j = i + 1 + (l - tri_row_start(i, s));
+    const uint64_t idmask = (1ull << idbits) - 1ull;
+    for (; p < pend; p++) {
+        uint64_t a = recs[base + i] & idmask, b = recs[base + j] & idmask;
+        uint64_t x = a < b ? a : b, y = a < b ? b : a;
+        pairs[p] = (x << idbits) | y;
+        if (++j == s) {
+            ++i;
+            j = i + 1;
+            if (i + 1 >= s) {
+                if (++g >= G) break;
+                s = gsize[g];
+                base = gstart[g];
+                i = 0;
+                j = 1;
+            }
+        }
+    }
+}
+
+// Distance of two full-length sequences as the reference reports it
+// (S/src/kernel.cu:235-300,359-392); *keep says whether the pair is output.
+__device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb, int d, int measure, bool* keep) {
+    if (measure == kHamming) {
+        int raw;
+        int dv = hamming_ref(a, la, b, lb, &raw);
+        bool k = dv <= d;
+        // a wrapped counter (lengths >= 128) can accept a far pair: the reference outputs it
+        // only when it was a candidate, i.e. when the 18-residue prefixes share a variant
+        if (k && raw > d) k = prefixes_share_variant(a, la, b, lb, d);
+        *keep = k;
+        return dv;
+    }
+    int diff = la > lb ? la - lb : lb - la;
+    if (diff > d) {
+        *keep = false;
+        return diff;
+    }
+    int dv;
+    if (la <= 64 && la <= lb) dv = lev_myers64(a, la, b, lb);
+    else if (lb <= 64) dv = lev_myers64(b, lb, a, la);
+    else {
+        int col[kMaxInputLength + 1];
+        dv = lev_dp(a, la, b, lb, col, d);
+    }
+    *keep = dv <= d;
+    return dv;
+}
+
+__global__ void k_verify(const uint64_t* __restrict__ pairs, int64_t P, int idbits, const uint8_t* __restrict__ chars,
+                         const uint32_t* __restrict__ offs, const int32_t* __restrict__ rows, int d, int measure,
+                         int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    uint64_t p = pairs[i];
+    bool keep = false;
+    int dv = 0;
+    if (i == 0 || pairs[i - 1] != p) {
+        const uint64_t idmask = (1ull << idbits) - 1ull;
+        uint32_t x = (uint32_t)(p >> idbits), y = (uint32_t)(p & idmask);
+        if (x != y) {
+            int rx = rows ? rows[x] : (int)x, ry = rows ? rows[y] : (int)y;
+            uint32_t sa = offs[rx], sb = offs[ry];
+            dv = pair_distance(chars + sa, (int)(offs[rx + 1] - sa), chars + sb, (int)(offs[ry + 1] - sb), d, measure,
+                               &keep);
+        }
+    }
+    dist[i] = (int8_t)dv;
+    flag[i] = keep ? 1 : 0;
+}
+
+__global__ void k_compact(const uint64_t* __restrict__ pairs, int64_t P, int idbits, const int8_t* __restrict__ dist,
+                          const uint8_t* __restrict__ flag, const uint32_t* __restrict__ pos, xtn_int2* __restrict__ out,
+                          int8_t* __restrict__ out_dist) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P || !flag[i]) return;
+    uint64_t p = pairs[i];
+    uint32_t o = pos[i];
+    out[o] = xtn_int2{(int32_t)(p >> idbits), (int32_t)(p & ((1ull << idbits) - 1ull))};
+    out_dist[o] = dist[i];
+}
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+static int ensure(DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return XTN_SUCCESS;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t nb = bytes + bytes / 8;
+    nb = (nb + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc(&b.p, nb);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        set_err(std::string("device allocation of ") + std::to_string(nb) + " bytes failed: " + cudaGetErrorString(e));
+        return XTN_ERR_NOMEM;
+    }
+    b.cap = nb;
+    return XTN_SUCCESS;
+}
+
+static void release(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+template <typename T>
+static T* P(DevBuf& b) {
+    return reinterpret_cast<T*>(b.p);
+}
+
+static inline unsigned blocks_for(int64_t n, int per_block = kThreads) {
+    int64_t b = (n + per_block - 1) / per_block;
+    return (unsigned)(b > 0 ? b : 1);
+}
+
+static int id_bits_for(int64_t n) {
+    int b = 1;
+    while ((int64_t(1) << b) < n) b++;
+    return b;
+}
+
+}  // namespace xtn
+
+using namespace xtn;
+
+enum { S_PACK, S_GEN, S_KSORT, S_GROUP, S_EMIT, S_PSORT, S_VERIFY, S_OUT, S_COUNT };
+
+struct xtn_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[S_COUNT + 1] = {};
+    // inputs (host-buffer API)
+    DevBuf chars, offs;
+    // pipeline
+    DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
+    DevBuf scratch64, scratch32, counter;
+    // results
+    DevBuf out_pairs, out_dist, out_freq;
+    uint64_t* h_scalar = nullptr;  // pinned
+    void* h_stage = nullptr;       // pinned output staging
+    size_t h_stage_cap = 0;
+    int64_t n_out = 0;
+    bool overlap_result = false;
+    xtn_stats stats{};
+    void* overlap_bufs = nullptr;
+    KernelProfiler prof;
+    std::vector<std::string> kt_names;
+    std::vector<double> kt_ms;
+    std::vector<int64_t> kt_launches;
+};
+
+namespace xtn {
+
+static int read_scalar(xtn_context* c, const void* dptr, size_t bytes, uint64_t* out) {
+    *c->h_scalar = 0;
+    XTN_CK(cudaMemcpyAsync(c->h_scalar, dptr, bytes, cudaMemcpyDeviceToHost, c->stream));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    *out = *c->h_scalar;
+    return XTN_SUCCESS;
+}
+
+static void begin_run(xtn_context* c) {
+    c->prof.reset(c->stream);
+    current_profiler() = &c->prof;
+}
+
+// After the stream has drained: per-kernel totals (profiling on) and the launch count.
+static void end_run(xtn_context* c) {
+    current_profiler() = nullptr;
+    c->stats.n_launches = c->prof.launches;
+    c->kt_names.clear();
+    c->kt_ms.clear();
+    c->kt_launches.clear();
+    if (!c->prof.on) return;
+    cudaStreamSynchronize(c->stream);
+    for (size_t i = 0; i < c->prof.used; i++) {
+        const KernelProfiler::Rec& r = c->prof.recs[i];
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        size_t k = 0;
+        while (k < c->kt_names.size() && c->kt_names[k] != r.name) k++;
+        if (k == c->kt_names.size()) {
+            c->kt_names.push_back(r.name);
+            c->kt_ms.push_back(0);
+            c->kt_launches.push_back(0);
+        }
+        c->kt_ms[k] += ms;
+        c->kt_launches[k]++;
+    }
+}
+
+static int scan_u32_to_u64(xtn_context* c, const uint32_t* in, uint64_t* out, int64_t n) {
+    XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(n)));
+    scan_exclusive<uint32_t, uint64_t>(in, out, n, P<uint64_t>(c->scratch64), c->stream);
+    return XTN_SUCCESS;
+}
+
+static int scan_u64(xtn_context* c, const uint64_t* in, uint64_t* out, int64_t n) {
+    XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(n)));
+    scan_exclusive<uint64_t, uint64_t>(in, out, n, P<uint64_t>(c->scratch64), c->stream);
+    return XTN_SUCCESS;
+}
+
+static int sort_u64(xtn_context* c, DevBuf& a, DevBuf& b, int64_t n, int lo, int hi, uint64_t** result, const char* up,
+                    const char* down) {
+    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
+    *result = radix_sort_u64(P<uint64_t>(a), P<uint64_t>(b), n, lo, hi, P<uint32_t>(c->scratch32), c->stream, up, down);
+    return XTN_SUCCESS;
+}
+
+// The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
+// -> CSR row. On success the result is in c->out_pairs / c->out_dist, c->n_out entries; the
+// verified pair list in sorted (x, y) order of search indexes.
+static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n, int d,
+                  int measure) {
+    xtn_stats& st = c->stats;
+    memset(&st, 0, sizeof st);
+    st.n_seqs = n;
+    st.n_rounds = 1;
+    const int idbits = id_bits_for(n);
+    st.id_bits = idbits;
+    cudaStream_t s = c->stream;
+    XTN_CK(cudaEventRecord(c->ev[0], s));
+
+    // pack + variant counts
+    XTN_TRY(ensure(c->keys, sizeof(u128) * n));
+    XTN_TRY(ensure(c->klen, (size_t)n));
+    XTN_TRY(ensure(c->vcnt, sizeof(uint32_t) * n));
+    XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (n + 1)));
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen),
+                                             P<uint32_t>(c->vcnt)));
+    XTN_CK(cudaGetLastError());
+    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n));
+    XTN_CK(cudaEventRecord(c->ev[1], s));
+    uint64_t V = 0;
+    XTN_TRY(read_scalar(c, P<uint64_t>(c->voff) + n, 8, &V));
+    st.n_variants = (int64_t)V;
+    if (V >= (uint64_t)UINT32_MAX) {
+        set_err("too many deletion variants for one round (" + std::to_string(V) + ")");
+        return XTN_ERR_LIMIT;
+    }
+
+    // generate + sort records
+    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V));
+    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->voff), n, d, idbits,
+                                            P<uint64_t>(c->recA)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaEventRecord(c->ev[2], s));
+    uint64_t* recs = nullptr;
+    XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, "key_sort_upsweep", "key_sort_downsweep"));
+    XTN_CK(cudaEventRecord(c->ev[3], s));
+
+    // groups of equal hashes
+    XTN_TRY(ensure(c->counter, 64));
+    int64_t gcap = std::max<int64_t>(1 << 16, (int64_t)(V / 8));
+    uint64_t G = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        XTN_TRY(ensure(c->gstart, sizeof(uint64_t) * gcap));
+        XTN_TRY(ensure(c->gsize, sizeof(uint32_t) * gcap));
+        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 8, s));
+        XTN_LAUNCH("find_groups", k_find_groups<<<blocks_for((int64_t)V), kThreads, 0, s>>>(recs, (int64_t)V, idbits, P<uint64_t>(c->gstart),
+                                                                   P<uint32_t>(c->gsize),
+                                                                   P<unsigned long long>(c->counter), gcap));
+        XTN_CK(cudaGetLastError());
+        XTN_TRY(read_scalar(c, c->counter.p, 8, &G));
+        if ((int64_t)G <= gcap) break;
+        gcap = (int64_t)G;
+    }
+    st.n_groups = (int64_t)G;
+    XTN_TRY(ensure(c->gcnt, sizeof(uint64_t) * (G + 1)));
+    XTN_TRY(ensure(c->goff, sizeof(uint64_t) * (G + 1)));
+    uint64_t Pc = 0;
+    if (G > 0) {
+        XTN_LAUNCH("pair_counts", k_pair_counts<<<blocks_for((int64_t)G), kThreads, 0, s>>>(P<uint32_t>(c->gsize), (int64_t)G,
+                                                                   P<uint64_t>(c->gcnt)));
+        XTN_CK(cudaGetLastError());
+        XTN_TRY(scan_u64(c, P<uint64_t>(c->gcnt), P<uint64_t>(c->goff), (int64_t)G));
+        XTN_TRY(read_scalar(c, P<uint64_t>(c->goff) + G, 8, &Pc));
+    }
+    XTN_CK(cudaEventRecord(c->ev[4], s));
+    st.n_candidates = (int64_t)Pc;
+    if (Pc >= (uint64_t)UINT32_MAX) {
+        set_err("too many candidate pairs for one round (" + std::to_string(Pc) + ")");
+        return XTN_ERR_LIMIT;
+    }
+
+    // candidate pairs
+    XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Pc));
+    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc));
+    if (Pc > 0) {
+        uint64_t threads = (Pc + kEmitPer - 1) / kEmitPer;
+        XTN_LAUNCH("emit", k_emit<<<blocks_for((int64_t)threads), kThreads, 0, s>>>(recs, P<uint64_t>(c->gstart), P<uint32_t>(c->gsize),
+                                                                 P<uint64_t>(c->goff), (int64_t)G, Pc, idbits,
+                                                                 P<uint64_t>(c->pairA)));
+        XTN_CK(cudaGetLastError());
+    }
+    XTN_CK(cudaEventRecord(c->ev[5], s));
+    uint64_t* pairs = P<uint64_t>(c->pairA);
+    if (Pc > 1)
+        XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, 2 * idbits, &pairs, "pair_sort_upsweep",
+                         "pair_sort_downsweep"));
+    XTN_CK(cudaEventRecord(c->ev[6], s));
+
+    // verify + compact
+    XTN_TRY(ensure(c->dist, (size_t)Pc));
+    XTN_TRY(ensure(c->flag, (size_t)Pc));
+    XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Pc + 1)));
+    uint64_t nout = 0;
+    if (Pc > 0) {
+        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
+                                                              P<int8_t>(c->dist), P<uint8_t>(c->flag)));
+        XTN_CK(cudaGetLastError());
+        XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * scan_scratch_elems((int64_t)Pc)));
+        scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc,
+                                          P<uint32_t>(c->scratch32), s);
+        XTN_CK(cudaEventRecord(c->ev[7], s));
+        XTN_TRY(read_scalar(c, P<uint32_t>(c->fpos) + Pc, 4, &nout));
+    } else {
+        XTN_CK(cudaEventRecord(c->ev[7], s));
+    }
+    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * nout));
+    XTN_TRY(ensure(c->out_dist, (size_t)nout));
+    if (nout > 0)
+        XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, P<int8_t>(c->dist),
+                                                               P<uint8_t>(c->flag), P<uint32_t>(c->fpos),
+                                                               P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaEventRecord(c->ev[8], s));
+    XTN_CK(cudaStreamSynchronize(s));
+    c->n_out = (int64_t)nout;
+    c->overlap_result = false;
+    st.n_out = (int64_t)nout;
+    // unique candidates = number of distinct pairs; counted from the verify flags' input side
+    float ms = 0;
+    for (int k = 0; k < S_COUNT; k++) {
+        cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+        st.ms_stage[k] = ms;
+    }
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[S_COUNT]);
+    st.ms_total = ms;
+    return XTN_SUCCESS;
+}
+
+static int check_args(const xtn_args* a) {
+    if (!a) {
+        set_err("null args");
+        return XTN_ERR_ARG;
+    }
+    if (a->distance < 1) {
+        set_err("distance must be a valid number larger than 0");
+        return XTN_ERR_ARG;
+    }
+    if (a->measure != XTN_LEVENSHTEIN && a->measure != XTN_HAMMING) {
+        set_err("invalid measure option");
+        return XTN_ERR_ARG;
+    }
+    return XTN_SUCCESS;
+}
+
+static int check_offsets(const uint32_t* offs, int n) {
+    for (int i = 0; i < n; i++) {
+        if (offs[i + 1] <= offs[i] || offs[i + 1] - offs[i] > (uint32_t)kMaxInputLength) {
+            set_err("sequence " + std::to_string(i) + " has an invalid length");
+            return XTN_ERR_ARG;
+        }
+    }
+    return XTN_SUCCESS;
+}
+
+static int upload(xtn_context* c, const char* seqs, const uint32_t* offsets, int n) {
+    size_t nch = offsets[n];
+    XTN_TRY(ensure(c->chars, nch + 16));
+    XTN_TRY(ensure(c->offs, sizeof(uint32_t) * (n + 1)));
+    XTN_CK(cudaMemcpyAsync(c->chars.p, seqs, nch, cudaMemcpyHostToDevice, c->stream));
+    XTN_CK(cudaMemcpyAsync(c->offs.p, offsets, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+    return XTN_SUCCESS;
+}
+
+static int stage_host(xtn_context* c, size_t bytes) {
+    if (c->h_stage_cap >= bytes) return XTN_SUCCESS;
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    size_t nb = bytes + bytes / 8 + 4096;
+    XTN_CK(cudaMallocHost(&c->h_stage, nb));
+    c->h_stage_cap = nb;
+    return XTN_SUCCESS;
+}
+
+// Hands the device result to the callback in chunks of at most kChunk entries.
+static int deliver(xtn_context* c, xtn_callback cb, void* user) {
+    const int64_t kChunk = int64_t(1) << 24;
+    int64_t n = c->n_out;
+    if (!cb) return XTN_SUCCESS;
+    int64_t chunk = std::min<int64_t>(std::max<int64_t>(n, 1), kChunk);
+    size_t per = sizeof(xtn_int2) + (c->overlap_result ? sizeof(uint64_t) : 1);
+    XTN_TRY(stage_host(c, per * chunk));
+    xtn_int2* hp = reinterpret_cast<xtn_int2*>(c->h_stage);
+    void* hv = reinterpret_cast<char*>(c->h_stage) + sizeof(xtn_int2) * chunk;
+    if (n == 0) {
+        xtn_output out{hp, c->overlap_result ? nullptr : reinterpret_cast<int8_t*>(hv),
+                       c->overlap_result ? reinterpret_cast<uint64_t*>(hv) : nullptr, 0};
+        cb(&out, user);
+        return XTN_SUCCESS;
+    }
+    for (int64_t o = 0; o < n; o += chunk) {
+        int64_t m = std::min(chunk, n - o);
+        XTN_CK(cudaMemcpyAsync(hp, P<xtn_int2>(c->out_pairs) + o, sizeof(xtn_int2) * m, cudaMemcpyDeviceToHost, c->stream));
+        if (c->overlap_result)
+            XTN_CK(cudaMemcpyAsync(hv, P<uint64_t>(c->out_freq) + o, sizeof(uint64_t) * m, cudaMemcpyDeviceToHost,
+                                   c->stream));
+        else
+            XTN_CK(cudaMemcpyAsync(hv, P<int8_t>(c->out_dist) + o, (size_t)m, cudaMemcpyDeviceToHost, c->stream));
+        XTN_CK(cudaStreamSynchronize(c->stream));
+        xtn_output out{hp, c->overlap_result ? nullptr : reinterpret_cast<int8_t*>(hv),
+                       c->overlap_result ? reinterpret_cast<uint64_t*>(hv) : nullptr, m};
+        cb(&out, user);
+    }
+    return XTN_SUCCESS;
+}
+
+// ------------------------------------------------------------------ overlap mode
+// Repertoire overlap (S/src/xtn_overlap_inner.cu:57-245, S/src/kernel.cu:405-435,565-584):
+//   1. rows with identical full strings are merged (hash sort + exact string check); the
+//      occurrences of a unique string keep row order, as the reference's stable sort does;
+//   2. diagonal term: for occurrences a <= b of one unique string, f_a*f_b is added to
+//      (rep_a, rep_b);
+//   3. the nearest-neighbour pipeline runs on one representative row per unique string;
+//   4. cross term: for a verified unique pair (u, v) and occurrences a of u, b of v,
+//      f_a*f_b (x2 when rep_a == rep_b) is added to (min rep, max rep);
+//   5. the R x R matrix of sums (u64, wrapping like the reference's size_t) is emitted in
+//      (x, y) order for every entry that received a contribution.
+
+__global__ void k_row_hash(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs, int n, int idbits,
+                           uint64_t* __restrict__ recs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = offs[i];
+    int L = (int)(offs[i + 1] - s);
+    uint64_t h = 0x84222325cbf29ce4ULL ^ (uint64_t)L;
+    for (int j = 0; j < L; j++) h = (h ^ chars[s + j]) * 0x100000001b3ULL;
+    h = fmix64(h);
+    recs[i] = (h & ~((1ull << idbits) - 1ull)) | (uint64_t)i;
+}
+
+__device__ __forceinline__ int cmp_rows(const uint8_t* chars, const uint32_t* offs, uint32_t a, uint32_t b) {
+    uint32_t sa = offs[a], sb = offs[b];
+    int la = (int)(offs[a + 1] - sa), lb = (int)(offs[b + 1] - sb);
+    int m = la < lb ? la : lb;
+    for (int k = 0; k < m; k++) {
+        int x = chars[sa + k], y = chars[sb + k];
+        if (x != y) return x < y ? -1 : 1;
+    }
+    return la == lb ? 0 : (la < lb ? -1 : 1);
+}
+
+// A run of equal hashes that holds different strings (a hash collision) is re-ordered by
+// (string, row) so that equal strings are contiguous again with rows ascending.
+__global__ void k_run_fix(uint64_t* __restrict__ recs, int n, int idbits, const uint8_t* __restrict__ chars,
+                          const uint32_t* __restrict__ offs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t idmask = (1ull << idbits) - 1ull;
+    uint64_t k = recs[i] >> idbits;
+    if (i > 0 && (recs[i - 1] >> idbits) == k) return;
+    int j = i + 1;
+    bool mixed = false;
+    while (j < n && (recs[j] >> idbits) == k) {
+        if (cmp_rows(chars, offs, (uint32_t)(recs[i] & idmask), (uint32_t)(recs[j] & idmask)) != 0) mixed = true;
+        j++;
+    }
+    if (!mixed) return;
+    for (int a = i + 1; a < j; a++) {
+        uint64_t v = recs[a];
+        int b = a - 1;
+        while (b >= i) {
+            int c = cmp_rows(chars, offs, (uint32_t)(recs[b] & idmask), (uint32_t)(v & idmask));
+            if (c < 0 || (c == 0 && (recs[b] & idmask) < (v & idmask))) break;
+            recs[b + 1] = recs[b];
+            b--;
+        }
+        recs[b + 1] = v;
+    }
+}
+
+__global__ void k_uniq_flags(const uint64_t* __restrict__ recs, int n, int idbits, const uint8_t* __restrict__ chars,
+                             const uint32_t* __restrict__ offs, uint8_t* __restrict__ head) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t idmask = (1ull << idbits) - 1ull;
+    bool h = i == 0 || (recs[i] >> idbits) != (recs[i - 1] >> idbits) ||
+             cmp_rows(chars, offs, (uint32_t)(recs[i - 1] & idmask), (uint32_t)(recs[i] & idmask)) != 0;
+    head[i] = h ? 1 : 0;
+}
+
+__global__ void k_uniq_build(const uint64_t* __restrict__ recs, const uint8_t* __restrict__ head,
+                             const uint32_t* __restrict__ uidx, int n, int idbits, int32_t* __restrict__ rep_row,
+                             uint32_t* __restrict__ occ_start, uint32_t* __restrict__ srow) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t row = (uint32_t)(recs[i] & ((1ull << idbits) - 1ull));
+    srow[i] = row;
+    if (head[i]) {
+        uint32_t u = uidx[i];
+        occ_start[u] = (uint32_t)i;
+        rep_row[u] = (int32_t)row;
+    }
+    if (i == n - 1) occ_start[uidx[n]] = (uint32_t)n;
+}
+
+__device__ __forceinline__ uint64_t freq_product(int32_t a, int32_t b) {
+    return (uint64_t)(int64_t)a * (uint64_t)(int64_t)b;
+}
+
+__global__ void k_diag(const uint32_t* __restrict__ occ_start, const uint32_t* __restrict__ srow, int U,
+                       const int32_t* __restrict__ freq, const int32_t* __restrict__ rep, int R,
+                       unsigned long long* __restrict__ M, uint8_t* __restrict__ present) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    uint32_t s = occ_start[u], e = occ_start[u + 1];
+    for (uint32_t a = s; a < e; a++) {
+        uint32_t ra = srow[a];
+        for (uint32_t b = a; b < e; b++) {
+            uint32_t rb = srow[b];
+            size_t cell = (size_t)rep[ra] * R + rep[rb];
+            atomicAdd(&M[cell], (unsigned long long)freq_product(freq[ra], freq[rb]));
+            present[cell] = 1;
+        }
+    }
+}
+
+// Cross term; with R <= kSmemReps the block accumulates into shared memory first.
+constexpr int kSmemReps = 96;
+
+__global__ void k_cross(const xtn_int2* __restrict__ pairs, int64_t np, const uint32_t* __restrict__ occ_start,
+                        const uint32_t* __restrict__ srow, const int32_t* __restrict__ freq,
+                        const int32_t* __restrict__ rep, int R, unsigned long long* __restrict__ M,
+                        uint8_t* __restrict__ present) {
+    extern __shared__ unsigned long long s_m[];
+    const bool local = R <= kSmemReps;
+    uint8_t* s_p = reinterpret_cast<uint8_t*>(s_m + (local ? R * R : 0));
+    if (local) {
+        for (int k = threadIdx.x; k < R * R; k += blockDim.x) {
+            s_m[k] = 0;
+            s_p[k] = 0;
+        }
+        __syncthreads();
+    }
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        xtn_int2 pr = pairs[t];
+        uint32_t s1 = occ_start[pr.x], e1 = occ_start[pr.x + 1];
+        uint32_t s2 = occ_start[pr.y], e2 = occ_start[pr.y + 1];
+        for (uint32_t a = s1; a < e1; a++) {
+            uint32_t ra = srow[a];
+            int qa = rep[ra];
+            int32_t fa = freq[ra];
+            for (uint32_t b = s2; b < e2; b++) {
+                uint32_t rb = srow[b];
+                int qb = rep[rb];
+                uint64_t f = freq_product(fa, freq[rb]);
+                if (qa == qb) f *= 2;
+                int x = qa < qb ? qa : qb, y = qa < qb ? qb : qa;
+                size_t cell = (size_t)x * R + y;
+                if (local) {
+                    atomicAdd(&s_m[cell], (unsigned long long)f);
+                    s_p[cell] = 1;
+                } else {
+                    atomicAdd(&M[cell], (unsigned long long)f);
+                    present[cell] = 1;
+                }
+            }
+        }
+    }
+    if (local) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < R * R; k += blockDim.x)
+            if (s_p[k]) {
+                atomicAdd(&M[k], s_m[k]);
+                present[k] = 1;
+            }
+    }
+}
+
+__global__ void k_matrix_compact(const unsigned long long* __restrict__ M, const uint8_t* __restrict__ present,
+                                 const uint32_t* __restrict__ pos, int R, xtn_int2* __restrict__ out,
+                                 uint64_t* __restrict__ out_freq) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)R * R || !present[k]) return;
+    uint32_t o = pos[k];
+    out[o] = xtn_int2{(int32_t)(k / R), (int32_t)(k % R)};
+    out_freq[o] = M[k];
+}
+
+}  // namespace xtn
+
+struct xtn_overlap_bufs {
+    DevBuf freq, rep, recA, recB, head, uidx, rep_row, occ_start, srow, M, present, mpos, scratch;
+};
+
+namespace xtn {
+
+constexpr int kMaxRepertoires = 8192;
+
+int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* h_info, int n, int d,
+                int measure, int R) {
+    if (R > kMaxRepertoires) {
+        set_err("overlap mode supports at most " + std::to_string(kMaxRepertoires) + " repertoires");
+        return XTN_ERR_LIMIT;
+    }
+    for (int i = 0; i < n; i++)
+        if (h_info[i].repertoire < 0 || h_info[i].repertoire >= R) {
+            set_err("repertoire id out of range at row " + std::to_string(i));
+            return XTN_ERR_ARG;
+        }
+    cudaStream_t s = c->stream;
+    xtn_overlap_bufs& b = *reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
+    const int idbits = id_bits_for(n);
+    // frequencies and repertoires, de-interleaved on the host
+    std::vector<int32_t> hf(n), hr(n);
+    for (int i = 0; i < n; i++) {
+        hf[i] = h_info[i].frequency;
+        hr[i] = h_info[i].repertoire;
+    }
+    XTN_TRY(ensure(b.freq, sizeof(int32_t) * n));
+    XTN_TRY(ensure(b.rep, sizeof(int32_t) * n));
+    XTN_CK(cudaMemcpyAsync(b.freq.p, hf.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    XTN_CK(cudaMemcpyAsync(b.rep.p, hr.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+
+    // 1. merge identical strings
+    XTN_TRY(ensure(b.recA, sizeof(uint64_t) * n));
+    XTN_TRY(ensure(b.recB, sizeof(uint64_t) * n));
+    XTN_LAUNCH("row_hash", k_row_hash<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, n, idbits, P<uint64_t>(b.recA)));
+    XTN_CK(cudaGetLastError());
+    uint64_t* recs = nullptr;
+    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
+    recs = radix_sort_u64(P<uint64_t>(b.recA), P<uint64_t>(b.recB), n, idbits, 64, P<uint32_t>(c->scratch32), s,
+                          "row_sort_upsweep", "row_sort_downsweep");
+    XTN_LAUNCH("run_fix", k_run_fix<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs));
+    XTN_TRY(ensure(b.head, (size_t)n));
+    XTN_TRY(ensure(b.uidx, sizeof(uint32_t) * (n + 1)));
+    XTN_LAUNCH("uniq_flags", k_uniq_flags<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs, P<uint8_t>(b.head)));
+    XTN_TRY(ensure(b.scratch, sizeof(uint32_t) * scan_scratch_elems(n)));
+    scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, P<uint32_t>(b.scratch), s);
+    uint64_t U = 0;
+    XTN_TRY(read_scalar(c, P<uint32_t>(b.uidx) + n, 4, &U));
+    XTN_TRY(ensure(b.rep_row, sizeof(int32_t) * U));
+    XTN_TRY(ensure(b.occ_start, sizeof(uint32_t) * (U + 1)));
+    XTN_TRY(ensure(b.srow, sizeof(uint32_t) * n));
+    XTN_LAUNCH("uniq_build", k_uniq_build<<<blocks_for(n), kThreads, 0, s>>>(recs, P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, idbits,
+                                                    P<int32_t>(b.rep_row), P<uint32_t>(b.occ_start), P<uint32_t>(b.srow)));
+    XTN_CK(cudaGetLastError());
+
+    // 2. diagonal term
+    size_t RR = (size_t)R * R;
+    XTN_TRY(ensure(b.M, sizeof(unsigned long long) * RR));
+    XTN_TRY(ensure(b.present, RR));
+    XTN_CK(cudaMemsetAsync(b.M.p, 0, sizeof(unsigned long long) * RR, s));
+    XTN_CK(cudaMemsetAsync(b.present.p, 0, RR, s));
+    XTN_LAUNCH("diag", k_diag<<<blocks_for((int64_t)U), kThreads, 0, s>>>(P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), (int)U,
+                                                       P<int32_t>(b.freq), P<int32_t>(b.rep), R,
+                                                       P<unsigned long long>(b.M), P<uint8_t>(b.present)));
+    XTN_CK(cudaGetLastError());
+
+    // 3. neighbours among the unique strings
+    XTN_TRY(run_nn(c, chars, offs, P<int32_t>(b.rep_row), (int)U, d, measure));
+    const int64_t nverified = c->n_out;
+
+    // 4. cross term
+    if (nverified > 0) {
+        size_t smem = R <= kSmemReps ? RR * (sizeof(unsigned long long) + 1) : 0;
+        if (smem > 48 * 1024) XTN_CK(cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int64_t blocks = std::min<int64_t>((nverified + kThreads - 1) / kThreads, 148 * 4);
+        XTN_LAUNCH("cross", k_cross<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, smem, s>>>(
+            P<xtn_int2>(c->out_pairs), nverified, P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), P<int32_t>(b.freq),
+            P<int32_t>(b.rep), R, P<unsigned long long>(b.M), P<uint8_t>(b.present)));
+        XTN_CK(cudaGetLastError());
+    }
+
+    // 5. matrix -> sorted entries
+    XTN_TRY(ensure(b.mpos, sizeof(uint32_t) * (RR + 1)));
+    XTN_TRY(ensure(b.scratch, sizeof(uint32_t) * scan_scratch_elems((int64_t)RR)));
+    scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.present), P<uint32_t>(b.mpos), (int64_t)RR, P<uint32_t>(b.scratch), s);
+    uint64_t nent = 0;
+    XTN_TRY(read_scalar(c, P<uint32_t>(b.mpos) + RR, 4, &nent));
+    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * nent));
+    XTN_TRY(ensure(c->out_freq, sizeof(uint64_t) * nent));
+    XTN_LAUNCH("matrix_compact", k_matrix_compact<<<blocks_for((int64_t)RR), kThreads, 0, s>>>(P<unsigned long long>(b.M), P<uint8_t>(b.present),
+                                                                 P<uint32_t>(b.mpos), R, P<xtn_int2>(c->out_pairs),
+                                                                 P<uint64_t>(c->out_freq)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaStreamSynchronize(s));
+    c->n_out = (int64_t)nent;
+    c->overlap_result = true;
+    c->stats.n_verified_pairs = nverified;
+    c->stats.n_out = (int64_t)nent;
+    c->stats.n_seqs = (int64_t)U;
+    return XTN_SUCCESS;
+}
+
+}  // namespace xtn
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* xtn_last_error(void) { return t_err.c_str(); }
+
+const char* xtn_version(void) { return "2.0.0 (xtn_b200 sm_100a)"; }
+
+int xtn_context_create(int device, xtn_context** out) {
+    if (!out) {
+        set_err("null output pointer");
+        return XTN_ERR_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_err(std::string("no CUDA device: ") + cudaGetErrorString(e));
+        return XTN_ERR_NODEV;
+    }
+    if (device < 0 || device >= ndev) {
+        set_err("device index out of range");
+        return XTN_ERR_ARG;
+    }
+    XTN_CK(cudaSetDevice(device));
+    xtn_context* c = new xtn_context();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&c->h_scalar, 64) != cudaSuccess) {
+        set_err("stream or pinned scalar allocation failed");
+        delete c;
+        return XTN_ERR_CUDA;
+    }
+    for (auto& ev : c->ev) cudaEventCreate(&ev);
+    c->overlap_bufs = new xtn_overlap_bufs();
+    *out = c;
+    return XTN_SUCCESS;
+}
+
+void xtn_context_destroy(xtn_context* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->chars, &c->offs, &c->keys, &c->klen, &c->vcnt, &c->voff, &c->recA, &c->recB,
+                      &c->gstart, &c->gsize, &c->gcnt, &c->goff, &c->pairA, &c->pairB, &c->dist, &c->flag,
+                      &c->fpos, &c->scratch64, &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq};
+    for (DevBuf* b : bufs) release(*b);
+    if (c->overlap_bufs) {
+        xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
+        DevBuf* obufs[] = {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
+                           &ob->occ_start, &ob->srow, &ob->M, &ob->present, &ob->mpos, &ob->scratch};
+        for (DevBuf* b : obufs) release(*b);
+        delete ob;
+    }
+    for (auto& ev : c->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->h_scalar) cudaFreeHost(c->h_scalar);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+void* xtn_context_stream(xtn_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int xtn_context_stats(const xtn_context* c, xtn_stats* out) {
+    if (!c || !out) return XTN_ERR_ARG;
+    *out = c->stats;
+    return XTN_SUCCESS;
+}
+
+int xtn_context_nn_device(xtn_context* c, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                          int32_t n, int64_t* n_out) {
+    if (!c || !d_seqs || !d_offsets || n < 1) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    XTN_CK(cudaSetDevice(c->device));
+    begin_run(c);
+    int r = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance, args->measure);
+    end_run(c);
+    if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
+    return r;
+}
+
+int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, const uint32_t* offsets, int32_t n,
+                        const xtn_seq_info* info, xtn_callback cb, void* user) {
+    if (!c || !seqs || !offsets || n < 1) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    XTN_TRY(check_offsets(offsets, n));
+    XTN_CK(cudaSetDevice(c->device));
+    XTN_TRY(upload(c, seqs, offsets, n));
+    const uint8_t* dch = P<uint8_t>(c->chars);
+    const uint32_t* dof = P<uint32_t>(c->offs);
+    int r;
+    begin_run(c);
+    if (info) {
+        if (args->info_len < 1) {
+            set_err("invalid info length");
+            return XTN_ERR_ARG;
+        }
+        r = run_overlap(c, dch, dof, info, n, args->distance, args->measure, args->info_len);
+    } else {
+        r = run_nn(c, dch, dof, nullptr, n, args->distance, args->measure);
+    }
+    end_run(c);
+    if (r != XTN_SUCCESS) return r;
+    if (args->verbose) {
+        const xtn_stats& st = c->stats;
+        printf("xtn_b200: seqs %lld variants %lld groups %lld candidates %lld output %lld (%.3f ms device)\n",
+               (long long)st.n_seqs, (long long)st.n_variants, (long long)st.n_groups, (long long)st.n_candidates,
+               (long long)st.n_out, st.ms_total);
+    }
+    return deliver(c, cb, user);
+}
+
+int xtn_context_set_profiling(xtn_context* c, int on) {
+    if (!c) return XTN_ERR_ARG;
+    c->prof.on = on != 0;
+    return XTN_SUCCESS;
+}
+
+int xtn_context_kernel_times(const xtn_context* c, const char** names, double* ms, int64_t* launches, int cap) {
+    if (!c) return -XTN_ERR_ARG;
+    int n = (int)c->kt_names.size();
+    for (int i = 0; i < n && i < cap; i++) {
+        if (names) names[i] = c->kt_names[i].c_str();
+        if (ms) ms[i] = c->kt_ms[i];
+        if (launches) launches[i] = c->kt_launches[i];
+    }
+    return n;
+}
+
+int xtn_context_fetch(xtn_context* c, xtn_int2* pairs, int8_t* distances, uint64_t* freqs, int64_t cap) {
+    if (!c || cap < 0) return XTN_ERR_ARG;
+    int64_t m = std::min(cap, c->n_out);
+    if (m <= 0) return XTN_SUCCESS;
+    if (pairs) XTN_CK(cudaMemcpyAsync(pairs, c->out_pairs.p, sizeof(xtn_int2) * m, cudaMemcpyDeviceToHost, c->stream));
+    if (distances && !c->overlap_result)
+        XTN_CK(cudaMemcpyAsync(distances, c->out_dist.p, (size_t)m, cudaMemcpyDeviceToHost, c->stream));
+    if (freqs && c->overlap_result)
+        XTN_CK(cudaMemcpyAsync(freqs, c->out_freq.p, sizeof(uint64_t) * m, cudaMemcpyDeviceToHost, c->stream));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    return XTN_SUCCESS;
+}
+
+int xtn_context_result_device(xtn_context* c, const xtn_int2** d_pairs, const int8_t** d_dist, int64_t* n_out) {
+    if (!c) return XTN_ERR_ARG;
+    if (d_pairs) *d_pairs = P<xtn_int2>(c->out_pairs);
+    if (d_dist) *d_dist = P<int8_t>(c->out_dist);
+    if (n_out) *n_out = c->n_out;
+    return XTN_SUCCESS;
+}
+
+static std::mutex g_default_mu;
+static xtn_context* g_default = nullptr;
+
+int xtn_perform(const xtn_args* args, const char* seqs, const uint32_t* offsets, int32_t n, const xtn_seq_info* info,
+                xtn_callback cb, void* user) {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (!g_default) XTN_TRY(xtn_context_create(0, &g_default));
+    return xtn_context_perform(g_default, args, seqs, offsets, n, info, cb, user);
+}
+
+}  // extern "C"

@@ -1,0 +1,307 @@
+// Device-wide primitives written for this library: exclusive prefix sums and a stable LSD
+// radix sort of 64-bit keys. They replace the CUB calls of the reference
+// (S/src/cub.cu:80-104,116-124,136-173) on this path.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace xtn {
+
+// ------------------------------------------------------------------ launch accounting
+// Every kernel launch of the library goes through XTN_LAUNCH, which counts it and, when
+// profiling is on, brackets it with a pair of CUDA events on the launching stream so the
+// caller can read per-kernel device time after the run.
+struct KernelProfiler {
+    bool on = false;
+    int64_t launches = 0;
+    struct Rec {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    size_t used = 0;
+    cudaStream_t stream = nullptr;
+    void reset(cudaStream_t s) {
+        stream = s;
+        used = 0;
+        launches = 0;
+    }
+    void begin(const char* name) {
+        launches++;
+        if (!on) return;
+        if (used == recs.size()) {
+            Rec r{name, nullptr, nullptr};
+            cudaEventCreate(&r.a);
+            cudaEventCreate(&r.b);
+            recs.push_back(r);
+        }
+        recs[used].name = name;
+        cudaEventRecord(recs[used].a, stream);
+    }
+    void end() {
+        if (!on) return;
+        cudaEventRecord(recs[used].b, stream);
+        used++;
+    }
+    ~KernelProfiler() {
+        for (auto& r : recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+};
+
+inline KernelProfiler*& current_profiler() {
+    static thread_local KernelProfiler* p = nullptr;
+    return p;
+}
+
+#define XTN_LAUNCH(name, ...)                                  \
+    do {                                                       \
+        ::xtn::KernelProfiler* pr_ = ::xtn::current_profiler(); \
+        if (pr_) pr_->begin(name);                             \
+        __VA_ARGS__;                                           \
+        if (pr_) pr_->end();                                   \
+    } while (0)
+
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive scan of one value per thread across the block; returns the block total in *total.
+template <typename T, int BLOCK>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* total) {
+    __shared__ T warp_sums[BLOCK / 32 + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = warp_inclusive_scan(v);
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < BLOCK / 32 ? warp_sums[lane] : T(0);
+        T winc = warp_inclusive_scan(w);
+        if (lane < BLOCK / 32) warp_sums[lane] = winc - w;
+        if (lane == BLOCK / 32 - 1) warp_sums[BLOCK / 32] = winc;
+    }
+    __syncthreads();
+    T r = inc - v + warp_sums[warp];
+    *total = warp_sums[BLOCK / 32];
+    __syncthreads();
+    return r;
+}
+
+template <typename In, typename Out>
+__global__ void __launch_bounds__(kScanBlock) k_scan_reduce(const In* __restrict__ in, Out* __restrict__ sums, int64_t n) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    Out s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + (int64_t)k * kScanBlock + threadIdx.x;
+        if (i < n) s += (Out)in[i];
+    }
+    __shared__ Out red[kScanBlock / 32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        Out t = threadIdx.x < kScanBlock / 32 ? red[threadIdx.x] : Out(0);
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = t;
+    }
+}
+
+// out[i] = offset[tile] + sum(in[0..i) within the tile); out[n] = grand total when the
+// caller passes n_out = n + 1 (the last tile writes it).
+template <typename In, typename Out>
+__global__ void __launch_bounds__(kScanBlock) k_scan_tiles(const In* __restrict__ in, Out* __restrict__ out,
+                                                           const Out* __restrict__ tile_offsets, int64_t n, bool write_total) {
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    Out v[kScanItems];
+    Out s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + k;
+        v[k] = i < n ? (Out)in[i] : Out(0);
+        s += v[k];
+    }
+    Out total;
+    Out ex = block_exclusive_scan<Out, kScanBlock>(s, &total);
+    Out off = tile_offsets ? tile_offsets[blockIdx.x] : Out(0);
+    Out run = off + ex;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (write_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = off + total;
+}
+
+// Scratch requirement (in Out elements) for scan_exclusive over n items.
+inline int64_t scan_scratch_elems(int64_t n) {
+    int64_t total = 0;
+    while (n > kScanTile) {
+        int64_t t = (n + kScanTile - 1) / kScanTile;
+        total += 2 * t + 1;
+        n = t;
+    }
+    return total + 1;
+}
+
+// Exclusive scan of n items into out[0..n), with out[n] = total. `scratch` holds
+// scan_scratch_elems(n) Out elements. Asynchronous on `stream`.
+template <typename In, typename Out>
+void scan_exclusive(const In* in, Out* out, int64_t n, Out* scratch, cudaStream_t stream) {
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, sizeof(Out), stream);
+        return;
+    }
+    int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        XTN_LAUNCH("scan_tiles", (k_scan_tiles<In, Out><<<1, kScanBlock, 0, stream>>>(in, out, nullptr, n, true)));
+        return;
+    }
+    Out* sums = scratch;
+    Out* offs = scratch + tiles;
+    XTN_LAUNCH("scan_reduce", (k_scan_reduce<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, sums, n)));
+    scan_exclusive<Out, Out>(sums, offs, tiles, scratch + 2 * tiles + 1, stream);
+    XTN_LAUNCH("scan_tiles", (k_scan_tiles<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, offs, n, true)));
+}
+
+// ------------------------------------------------------------------ LSD radix sort (u64 keys)
+// One pass = upsweep (per-tile digit counts) + exclusive scan over the digit-major count
+// matrix + downsweep (stable rank inside the tile with warp match, reorder in shared
+// memory, coalesced write of each digit run). Keys carry their payload in the low bits.
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(const uint64_t* __restrict__ keys, int64_t n, int shift,
+                                                                uint32_t* __restrict__ counts, int64_t ntiles) {
+    __shared__ uint32_t hist[kRadix];
+    hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int k = 0; k < kSortItems; k++) {
+        int64_t i = base + (int64_t)k * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = hist[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_downsweep(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                                                  int64_t n, int shift, const uint32_t* __restrict__ offsets,
+                                                                  int64_t ntiles) {
+    __shared__ uint64_t s_keys[kSortTile];
+    __shared__ uint32_t s_cnt[kSortWarps][kRadix + 1];
+    __shared__ uint32_t s_start[kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&s_cnt[0][0])[i] = 0;
+    __syncthreads();
+
+    const int64_t tile_base = (int64_t)blockIdx.x * kSortTile;
+    const int64_t valid64 = n - tile_base;
+    const int valid = valid64 > kSortTile ? kSortTile : (int)valid64;
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t key[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        int pos = warp * (32 * kSortItems) + k * 32 + lane;  // warp-contiguous tile order
+        bool ok = pos < valid;
+        uint64_t kv = ok ? in[tile_base + pos] : 0ull;
+        unsigned dg = ok ? (unsigned)((kv >> shift) & (kRadix - 1)) : (unsigned)kRadix;
+        unsigned peers = __match_any_sync(0xffffffffu, dg);
+        int leader = __ffs(peers) - 1;
+        uint32_t before = 0;
+        if (lane == leader) {
+            before = s_cnt[warp][dg];
+            s_cnt[warp][dg] = before + __popc(peers);
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        key[k] = kv;
+        rank[k] = before + __popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps; then exclusive scan over digits
+    uint32_t tot = 0;
+    {
+        const int d = threadIdx.x;  // kSortThreads == kRadix
+#pragma unroll
+        for (int w = 0; w < kSortWarps; w++) {
+            uint32_t c = s_cnt[w][d];
+            s_cnt[w][d] = tot;
+            tot += c;
+        }
+    }
+    uint32_t all;
+    uint32_t start = block_exclusive_scan<uint32_t, kSortThreads>(tot, &all);
+    s_start[threadIdx.x] = start;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        int pos = warp * (32 * kSortItems) + k * 32 + lane;
+        if (pos < valid) {
+            unsigned dg = (unsigned)((key[k] >> shift) & (kRadix - 1));
+            s_keys[s_start[dg] + s_cnt[warp][dg] + rank[k]] = key[k];
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < valid; i += kSortThreads) {
+        uint64_t kv = s_keys[i];
+        unsigned dg = (unsigned)((kv >> shift) & (kRadix - 1));
+        out[(int64_t)offsets[(int64_t)dg * ntiles + blockIdx.x] + (i - s_start[dg])] = kv;
+    }
+}
+
+inline int64_t radix_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+// Scratch (u32 elements) for radix_sort_u64 over n keys.
+inline int64_t radix_scratch_elems(int64_t n) {
+    int64_t m = radix_tiles(n) * kRadix;
+    return 2 * (m + 1) + scan_scratch_elems(m + 1);
+}
+
+// Sorts keys[0..n) by bits [lo_bit, hi_bit), stable. Ping-pongs between `keys` and `alt`;
+// returns the buffer that holds the result.
+inline uint64_t* radix_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int hi_bit, uint32_t* scratch,
+                                cudaStream_t stream, const char* up_name = "radix_upsweep",
+                                const char* down_name = "radix_downsweep") {
+    if (n <= 1 || hi_bit <= lo_bit) return keys;
+    const int64_t ntiles = radix_tiles(n);
+    const int64_t m = ntiles * kRadix;
+    uint32_t* counts = scratch;
+    uint32_t* offsets = scratch + (m + 1);
+    uint32_t* sscratch = scratch + 2 * (m + 1);
+    uint64_t* src = keys;
+    uint64_t* dst = alt;
+    for (int shift = lo_bit; shift < hi_bit; shift += kRadixBits) {
+        XTN_LAUNCH(up_name, k_radix_upsweep<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(src, n, shift, counts, ntiles));
+        scan_exclusive<uint32_t, uint32_t>(counts, offsets, m, sscratch, stream);
+        XTN_LAUNCH(down_name, k_radix_downsweep<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(src, dst, n, shift, offsets, ntiles));
+        uint64_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+}  // namespace xtn

@@ -1,0 +1,327 @@
+"""ctypes binding of the xtn_b200 C ABI (include/xtn_b200.h).
+
+This is the Python mirror of the reference's library entry point
+``xtn_perform(XTNArgs, SeqArray*, SeqInfo*, callback)`` (xtneighbor_streaming/src/xtn.cu:267):
+``Context.perform`` takes the CSR sequence store the reference's SeqArray holds, an optional
+per-row SeqInfo table (overlap mode) and returns the concatenated XTNOutput chunks.
+The compute path is the CUDA library ``lib/libxtn_b200.so``; there is no CPU fallback:
+loading fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libxtn_b200.so")
+SYNTH_PATH = os.path.join(HERE, "lib", "libxtn_synth.so")
+CLI_PATH = os.path.join(HERE, "bin", "xt_neighbor")
+
+LEVENSHTEIN = 0  # xtneighbor_streaming/src/xtn.h:12
+HAMMING = 1  # xtneighbor_streaming/src/xtn.h:14
+
+SUCCESS, ERROR, EXIT = 0, 1, 2
+ERR_CUDA, ERR_NOMEM, ERR_ARG, ERR_NODEV, ERR_LIMIT = 3, 4, 5, 6, 7
+
+SYMBOLS = (
+    "xtn_perform",
+    "xtn_context_create",
+    "xtn_context_destroy",
+    "xtn_context_perform",
+    "xtn_context_nn_device",
+    "xtn_context_fetch",
+    "xtn_context_result_device",
+    "xtn_context_stream",
+    "xtn_context_stats",
+    "xtn_context_set_profiling",
+    "xtn_context_kernel_times",
+    "xtn_last_error",
+    "xtn_version",
+)
+
+
+class Int2(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_int32), ("y", ctypes.c_int32)]
+
+
+class SeqInfo(ctypes.Structure):
+    _fields_ = [("frequency", ctypes.c_int32), ("repertoire", ctypes.c_int32), ("original_index", ctypes.c_int32)]
+
+
+class Args(ctypes.Structure):
+    _fields_ = [
+        ("distance", ctypes.c_int32),
+        ("measure", ctypes.c_int32),
+        ("verbose", ctypes.c_int32),
+        ("info_len", ctypes.c_int32),
+    ]
+
+
+class Output(ctypes.Structure):
+    _fields_ = [
+        ("index_pairs", ctypes.POINTER(Int2)),
+        ("pairwise_distances", ctypes.POINTER(ctypes.c_int8)),
+        ("pairwise_frequencies", ctypes.POINTER(ctypes.c_uint64)),
+        ("len", ctypes.c_int64),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_seqs", ctypes.c_int64),
+        ("n_variants", ctypes.c_int64),
+        ("n_groups", ctypes.c_int64),
+        ("n_candidates", ctypes.c_int64),
+        ("n_unique", ctypes.c_int64),
+        ("n_out", ctypes.c_int64),
+        ("n_verified_pairs", ctypes.c_int64),
+        ("n_launches", ctypes.c_int64),
+        ("id_bits", ctypes.c_int32),
+        ("n_rounds", ctypes.c_int32),
+        ("ms_total", ctypes.c_double),
+        ("ms_stage", ctypes.c_double * 8),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "ms_stage"}
+        d["ms_stage"] = list(self.ms_stage)
+        return d
+
+
+CALLBACK = ctypes.CFUNCTYPE(None, ctypes.POINTER(Output), ctypes.c_void_p)
+
+_lib = None
+
+
+class XtnError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"xtn_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Loads lib/libxtn_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA library not built: {LIB_PATH} is missing (run __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    lib.xtn_last_error.restype = ctypes.c_char_p
+    lib.xtn_version.restype = ctypes.c_char_p
+    lib.xtn_context_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+    lib.xtn_context_destroy.argtypes = [P]
+    lib.xtn_context_destroy.restype = None
+    lib.xtn_context_perform.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P, CALLBACK, P]
+    lib.xtn_perform.argtypes = [ctypes.POINTER(Args), P, P, ctypes.c_int32, P, CALLBACK, P]
+    lib.xtn_context_nn_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_context_fetch.argtypes = [P, P, P, P, ctypes.c_int64]
+    lib.xtn_context_result_device.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_context_stream.argtypes = [P]
+    lib.xtn_context_stream.restype = P
+    lib.xtn_context_stats.argtypes = [P, ctypes.POINTER(Stats)]
+    lib.xtn_context_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.xtn_context_kernel_times.argtypes = [P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+    _lib = lib
+    return lib
+
+
+def _check(code: int):
+    if code != SUCCESS:
+        raise XtnError(code, load().xtn_last_error().decode(errors="replace"))
+
+
+def pack_sequences(seqs) -> tuple[np.ndarray, np.ndarray]:
+    """List of strings -> (chars uint8, offsets uint32) CSR store, as SeqArray keeps it."""
+    enc = [s.encode() for s in seqs]
+    offs = np.zeros(len(enc) + 1, dtype=np.uint32)
+    if enc:
+        offs[1:] = np.cumsum([len(e) for e in enc])
+    chars = np.frombuffer(b"".join(enc), dtype=np.uint8).copy()
+    return chars, offs
+
+
+def unpack_sequences(chars: np.ndarray, offs: np.ndarray) -> list[str]:
+    b = chars.tobytes()
+    return [b[offs[i] : offs[i + 1]].decode() for i in range(len(offs) - 1)]
+
+
+@dataclass
+class Result:
+    pairs: np.ndarray  # (n, 2) int32
+    distances: np.ndarray | None  # (n,) int8, NN mode
+    frequencies: np.ndarray | None  # (n,) uint64, overlap mode
+
+
+class Context:
+    """Reusable device context (stream + growing device buffers)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.h = ctypes.c_void_p()
+        _check(self.lib.xtn_context_create(device, ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            self.lib.xtn_context_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def perform(self, chars, offsets, distance=1, measure=LEVENSHTEIN, info=None, n_reps=0, verbose=0) -> Result:
+        """The whole search on host buffers (xtn_context_perform)."""
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        n = len(offsets) - 1
+        args = Args(distance, measure, verbose, n_reps)
+        chunks_p, chunks_v = [], []
+        overlap = info is not None
+
+        def cb(out_ptr, _user):
+            o = out_ptr.contents
+            m = o.len
+            if m <= 0:
+                return
+            pp = ctypes.cast(o.index_pairs, ctypes.POINTER(ctypes.c_int32))
+            chunks_p.append(np.ctypeslib.as_array(pp, shape=(m, 2)).copy())
+            if overlap:
+                chunks_v.append(np.ctypeslib.as_array(o.pairwise_frequencies, shape=(m,)).copy())
+            else:
+                chunks_v.append(np.ctypeslib.as_array(o.pairwise_distances, shape=(m,)).copy())
+
+        ccb = CALLBACK(cb)
+        info_arr = None
+        if overlap:
+            info_arr = np.ascontiguousarray(info, dtype=np.int32).reshape(-1, 3)
+        rc = self.lib.xtn_context_perform(
+            self.h,
+            ctypes.byref(args),
+            chars.ctypes.data_as(ctypes.c_void_p),
+            offsets.ctypes.data_as(ctypes.c_void_p),
+            n,
+            info_arr.ctypes.data_as(ctypes.c_void_p) if overlap else None,
+            ccb,
+            None,
+        )
+        _check(rc)
+        pairs = np.concatenate(chunks_p) if chunks_p else np.zeros((0, 2), np.int32)
+        if overlap:
+            vals = np.concatenate(chunks_v) if chunks_v else np.zeros(0, np.uint64)
+            return Result(pairs, None, vals)
+        vals = np.concatenate(chunks_v) if chunks_v else np.zeros(0, np.int8)
+        return Result(pairs, vals, None)
+
+    def nn_device(self, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN) -> int:
+        """Search on device pointers; returns the number of output pairs (kept on device)."""
+        args = Args(distance, measure, 0, 0)
+        nout = ctypes.c_int64()
+        _check(
+            self.lib.xtn_context_nn_device(
+                self.h, ctypes.byref(args), ctypes.c_void_p(d_chars), ctypes.c_void_p(d_offsets), n, ctypes.byref(nout)
+            )
+        )
+        return nout.value
+
+    def fetch(self, n: int) -> Result:
+        pairs = np.zeros((n, 2), np.int32)
+        dist = np.zeros(n, np.int8)
+        _check(
+            self.lib.xtn_context_fetch(
+                self.h, pairs.ctypes.data_as(ctypes.c_void_p), dist.ctypes.data_as(ctypes.c_void_p), None, n
+            )
+        )
+        return Result(pairs, dist, None)
+
+    def stream(self) -> int:
+        return self.lib.xtn_context_stream(self.h) or 0
+
+    def set_profiling(self, on: bool):
+        _check(self.lib.xtn_context_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total ms, launches)} of the last run (profiling on)."""
+        cap = 64
+        names = (ctypes.c_char_p * cap)()
+        ms = (ctypes.c_double * cap)()
+        ln = (ctypes.c_int64 * cap)()
+        n = self.lib.xtn_context_kernel_times(self.h, names, ms, ln, cap)
+        return {names[i].decode(): (ms[i], ln[i]) for i in range(min(n, cap))}
+
+    def stats(self) -> dict:
+        st = Stats()
+        _check(self.lib.xtn_context_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+
+# ---------------------------------------------------------------- synthetic data (host)
+_synth = None
+
+
+def _load_synth():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise RuntimeError(f"generator library not built: {SYNTH_PATH}")
+        s = ctypes.CDLL(SYNTH_PATH)
+        s.synth_nn.restype = ctypes.c_void_p
+        s.synth_nn.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        s.synth_overlap.restype = ctypes.c_void_p
+        s.synth_overlap.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        for f in ("synth_n", "synth_total_chars"):
+            getattr(s, f).restype = ctypes.c_int64
+            getattr(s, f).argtypes = [ctypes.c_void_p]
+        s.synth_n_reps.restype = ctypes.c_int32
+        s.synth_n_reps.argtypes = [ctypes.c_void_p]
+        s.synth_copy.argtypes = [ctypes.c_void_p] * 5
+        s.synth_free.argtypes = [ctypes.c_void_p]
+        _synth = s
+    return _synth
+
+
+def _take(h, with_info=False):
+    s = _load_synth()
+    n, nc, nr = s.synth_n(h), s.synth_total_chars(h), s.synth_n_reps(h)
+    chars = np.zeros(nc, np.uint8)
+    offs = np.zeros(n + 1, np.uint32)
+    freq = np.zeros(n if with_info else 0, np.int32)
+    reps = np.zeros(nr, np.int32)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a.size else None
+    s.synth_copy(h, ptr(chars), ptr(offs), ptr(freq), ptr(reps))
+    s.synth_free(h)
+    return chars, offs, freq, reps
+
+
+def synth_mutants(seed: int, n: int, mutant_frac: float = 0.10):
+    """n generator sequences, a fraction of them 1-2 edit mutants of earlier rows."""
+    chars, offs, _, _ = _take(_load_synth().synth_nn(seed, n, 0, mutant_frac, 0.0))
+    return chars, offs
+
+
+def synth_clusters(seed: int, n: int, cluster_frac: float = 0.20, dup_frac: float = 0.02):
+    """n generator sequences with mutant clusters and exact duplicates, shuffled."""
+    chars, offs, _, _ = _take(_load_synth().synth_nn(seed, n, 1, cluster_frac, dup_frac))
+    return chars, offs
+
+
+def synth_repertoires(seed: int, n_reps: int, min_size: float, max_size: float, shared: float = 0.05):
+    """Repertoire-overlap input: (chars, offsets, info (n,3) int32, rep_sizes)."""
+    chars, offs, freq, reps = _take(_load_synth().synth_overlap(seed, n_reps, min_size, max_size, shared), True)
+    n = len(offs) - 1
+    rep_of = np.repeat(np.arange(len(reps), dtype=np.int32), reps)
+    info = np.stack([freq, rep_of, np.arange(n, dtype=np.int32)], axis=1).astype(np.int32)
+    return chars, offs, info, reps
