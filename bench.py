@@ -157,7 +157,7 @@ def run_ours(args, w):
         pg = dist
     chars, offs = gen_workload(w)
     n = len(offs) - 1
-    ctx = xtn.Context(local)
+    ctx = xtn.Context(local, engine=1 if args.engine == "sort" else 0)
     ctx.set_profiling(True)
     d_chars = torch.from_numpy(chars).cuda()
     d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
@@ -253,6 +253,7 @@ def run_ours(args, w):
             "distance": w["d"],
             "measure": "hamming" if w["measure"] else "leven",
             "parallelism": f"replicas x{world}",
+            "engine": args.engine,
             "l2": "flushed between steps (256 MiB write)",
         },
         "pairs_per_s": world * n_out / (ms_step / 1e3),
@@ -282,6 +283,8 @@ def run_ours(args, w):
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][0])},
         "clocks": clocks,
     }
+    if world == 1 and not args.no_cli:
+        line["cli_process"] = cli_process(args, w, chars, offs)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(chars, offs, w)
     ctx.close()
@@ -308,6 +311,30 @@ def cpu_baseline(chars, offs, w, max_seconds=30.0):
         "sample": f"whole workload ({sample} seqs), one search",
         "seconds": dt,
     }
+
+
+def cli_process(args, w, chars, offs):
+    """The xt_neighbor CLI as a whole process on the workload file (parse + search, no -o),
+    timed like the reference's published harness: wall clock around the process."""
+    import xtn
+
+    n = len(offs) - 1
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "seqs.csv")
+        write_csv(chars, offs, path)
+        cmd = [xtn.CLI_PATH, "-i", path, "-n", str(n), "-d", str(w["d"])] + (["-m", "hamming"] if w["measure"] else [])
+        times = []
+        for i in range(2 + 3):
+            t0 = time.perf_counter()
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            dt = time.perf_counter() - t0
+            if p.returncode != 0:
+                return {"error": p.stderr[-200:]}
+            if i >= 2:
+                times.append(dt)
+    s = sum(times) / len(times)
+    return {"value": n / s, "unit": "seqs/s", "ms_per_run": s * 1e3, "runs": len(times),
+            "what": "xt_neighbor CLI process: CSV parse + search, no -o, wall clock"}
 
 
 def write_csv(chars, offs, path):
@@ -379,11 +406,14 @@ def run_reference(args, w):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--engine", choices=["bucket", "sort"], default="bucket",
+                    help="key grouping: shared-memory hash buckets (default) or full radix sort")
+    ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)

@@ -138,6 +138,16 @@ int xtn_context_stats(const xtn_context* ctx, xtn_stats* out);
 int xtn_context_set_profiling(xtn_context* ctx, int on);
 int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double* ms, int64_t* launches, int cap);
 
+/* Tuning and engine options of a context (0 on success, XTN_ERR_ARG for an unknown name or
+ * a value out of range):
+ *   "engine"          0 = hash-bucket grouping in shared memory (default),
+ *                     1 = full radix sort of the variant records (the plain comparison form)
+ *   "bucket_bits_max" 1..15: upper bound on log2(number of first-level buckets) (default 15)
+ *   "group_cap"       2..8192: largest bucket grouped in shared memory; larger ones are split
+ *                     by further hash bits, and what still does not fit is grouped by sorting
+ *                     (default 8192) */
+int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
+
 /* Text of the last error on the calling thread ("" if none). */
 const char* xtn_last_error(void);
 

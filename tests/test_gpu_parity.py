@@ -13,9 +13,18 @@ from conftest import assert_same_pairs, csr
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def ctx():
-    c = xtn.Context(0)
+ENGINES = {
+    "bucket": {},
+    "sort": {"engine": 1},
+    # tiny first-level table and shared-memory cap: exercises the bucket split and the
+    # sort-based fallback for oversized buckets on small inputs
+    "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64},
+}
+
+
+@pytest.fixture(scope="module", params=sorted(ENGINES))
+def ctx(request):
+    c = xtn.Context(0, **ENGINES[request.param])
     yield c
     c.close()
 

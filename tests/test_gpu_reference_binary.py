@@ -1,0 +1,120 @@
+"""Byte-for-byte parity of the xt_neighbor CLI with the reference XTNeighbor-streaming binary.
+
+oracle/build_ref.sh builds the reference's own CLI (xtneighbor_streaming/src/cli.cu,
+sm_100a) into oracle/_ref/xt_neighbor_ref. On a GPU box both binaries run on the same
+seeded input files with -o, and their output files must be identical. The CPU oracle's
+output, formatted the reference's way, is checked too, so the oracle is pinned to the real
+reference on these inputs. Skipped where the reference build is absent.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import xtn
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not os.path.exists(orc.REF_CLI), reason="reference build absent")]
+
+
+def write_nn_csv(path, chars, offs):
+    b = chars.tobytes()
+    with open(path, "wb") as f:
+        f.write(b"cdr3\n")
+        f.write(b"".join(b[offs[i] : offs[i + 1]] + b"\n" for i in range(len(offs) - 1)))
+
+
+def run_both(tmp_path, args):
+    outs = []
+    for name, exe in (("ours", xtn.CLI_PATH), ("ref", orc.REF_CLI)):
+        out = tmp_path / f"{name}.txt"
+        p = subprocess.run([exe] + args + ["-o", str(out)], capture_output=True, text=True, timeout=900,
+                           env=dict(os.environ, LC_ALL="C"))
+        assert p.returncode == 0, f"{name}: rc={p.returncode} {p.stderr[-500:]}"
+        outs.append(out.read_bytes())
+    return outs
+
+
+def oracle_nn_text(chars, offs, d, m):
+    pairs, dist, _ = orc.nn_search(chars, offs, d, m)
+    return "".join(f"{x} {y} {v}\n" for (x, y), v in zip(pairs.tolist(), dist.tolist())).encode()
+
+
+@pytest.mark.parametrize(
+    "kind,n,d,measure",
+    [("mutants", 10_000, 1, "leven"), ("mutants", 10_000, 2, "hamming"), ("clusters", 100_000, 2, "leven"),
+     ("clusters", 100_000, 1, "hamming"), ("mutants", 3_000, 3, "leven")],
+)
+def test_nn_output_identical(tmp_path, kind, n, d, measure):
+    if kind == "mutants":
+        chars, offs = xtn.synth_mutants(seed=n + d, n=n, mutant_frac=0.10)
+    else:
+        chars, offs = xtn.synth_clusters(seed=n + d, n=n)
+    f = tmp_path / "in.csv"
+    write_nn_csv(f, chars, offs)
+    args = ["-i", str(f), "-n", str(n), "-d", str(d)] + (["-m", "hamming"] if measure == "hamming" else [])
+    ours, ref = run_both(tmp_path, args)
+    assert len(ref) > 0
+    assert ours == ref
+    assert oracle_nn_text(chars, offs, d, 1 if measure == "hamming" else 0) == ref
+
+
+def test_long_sequences_identical(tmp_path):
+    """Lengths 19..100: verification on the full strings beyond the 18-residue key."""
+    rng = np.random.default_rng(4)
+    seqs = []
+    for _ in range(1500):
+        L = int(rng.integers(19, 101))
+        seqs.append("".join(rng.choice(list("CASSLGTEF"), L)))
+    for i in range(0, 1500, 2):
+        s = list(seqs[i])
+        s[int(rng.integers(0, len(s)))] = "W"
+        seqs.append("".join(s))
+    chars, offs = xtn.pack_sequences(seqs)
+    f = tmp_path / "in.csv"
+    write_nn_csv(f, chars, offs)
+    ours, ref = run_both(tmp_path, ["-i", str(f), "-n", str(len(seqs)), "-d", "2"])
+    assert ours == ref and len(ref) > 0
+
+
+def test_overlap_output_identical(tmp_path):
+    chars, offs, info, reps = xtn.synth_repertoires(seed=8, n_reps=6, min_size=300, max_size=3000, shared=0.2)
+    n = len(offs) - 1
+    b = chars.tobytes()
+    f = tmp_path / "seq.csv"
+    with open(f, "wb") as fh:
+        fh.write(b"cdr3,count\n")
+        fh.write(b"".join(b[offs[i] : offs[i + 1]] + b"," + str(int(info[i, 0])).encode() + b"\n" for i in range(n)))
+    fi = tmp_path / "info.csv"
+    fi.write_text("size\n" + "".join(f"{int(r)}\n" for r in reps))
+    ours, ref = run_both(tmp_path, ["-i", str(f), "-n", str(n), "-I", str(fi), "-N", str(len(reps)), "-d", "1"])
+    assert ours == ref and len(ref) > 0
+    pairs, sums = orc.overlap_search(chars, offs, info, 1, 0)
+    assert "".join(f"{x} {y} {int(s)}\n" for (x, y), s in zip(pairs.tolist(), sums)).encode() == ref
+
+
+def test_airr_input_identical(tmp_path):
+    chars, offs = xtn.synth_mutants(seed=77, n=2000)
+    b = chars.tobytes()
+    f = tmp_path / "in.tsv"
+    with open(f, "wb") as fh:
+        fh.write(b"sequence_id\tv_call\tcdr3_aa\tduplicate_count\n")
+        for i in range(len(offs) - 1):
+            fh.write(b"s%d\tTRBV1\t" % i + b[offs[i] : offs[i + 1]] + b"\t%d\n" % (i % 7 + 1))
+    ours, ref = run_both(tmp_path, ["-a", "-i", str(f), "-n", str(len(offs) - 1), "-d", "1"])
+    assert ours == ref and len(ref) > 0
+
+
+@pytest.mark.parametrize(
+    "content,args",
+    [("cdr3\nCAAA\nCAXA\n", ["-n", "2"]), ("cdr3\nCAAA\n", ["-n", "2"]), ("cdr3\nCAAA\nCAAA\n", ["-n", "1"])],
+)
+def test_error_messages_identical(tmp_path, content, args):
+    f = tmp_path / "bad.csv"
+    f.write_text(content)
+    res = []
+    for exe in (xtn.CLI_PATH, orc.REF_CLI):
+        p = subprocess.run([exe, "-i", str(f)] + args, capture_output=True, text=True, timeout=120)
+        res.append((p.returncode, p.stderr))
+    assert res[0] == res[1]

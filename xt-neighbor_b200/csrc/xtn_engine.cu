@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,7 @@
 #include "../../include/xtn_b200.h"
 #include "xtn_common.cuh"
 #include "xtn_prims.cuh"
+#include "xtn_bucket.cuh"
 
 namespace xtn {
 
@@ -281,6 +283,13 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
+    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB;
+    int sms = 148;
+    int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
+    bool attrs_set = false;
+    int bucket_bits_max = 15;
+    uint32_t group_cap = kGroupCap;
+    uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
     // results
     DevBuf out_pairs, out_dist, out_freq;
     uint64_t* h_scalar = nullptr;  // pinned
@@ -355,6 +364,182 @@ static int sort_u64(xtn_context* c, DevBuf& a, DevBuf& b, int64_t n, int lo, int
     return XTN_SUCCESS;
 }
 
+
+// Grows a buffer keeping its first `used` bytes.
+static int ensure_keep(xtn_context* c, DevBuf& b, size_t bytes, size_t used) {
+    if (b.cap >= bytes) return XTN_SUCCESS;
+    DevBuf nb;
+    XTN_TRY(ensure(nb, bytes));
+    if (used) XTN_CK(cudaMemcpyAsync(nb.p, b.p, used, cudaMemcpyDeviceToDevice, c->stream));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    release(b);
+    b = nb;
+    return XTN_SUCCESS;
+}
+
+// Candidate pairs of a record array sorted by hash: runs of equal hash, every id pair of every
+// run appended to c->pairA at index `base`. *count receives the number appended.
+static int group_sorted(xtn_context* c, const uint64_t* recs, int64_t V, int idbits, uint64_t base, uint64_t* count) {
+    cudaStream_t s = c->stream;
+    XTN_TRY(ensure(c->counter, 64));
+    int64_t gcap = std::max<int64_t>(1 << 16, V / 8);
+    uint64_t G = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        XTN_TRY(ensure(c->gstart, sizeof(uint64_t) * gcap));
+        XTN_TRY(ensure(c->gsize, sizeof(uint32_t) * gcap));
+        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 8, s));
+        XTN_LAUNCH("find_groups", k_find_groups<<<blocks_for(V), kThreads, 0, s>>>(
+                                      recs, V, idbits, P<uint64_t>(c->gstart), P<uint32_t>(c->gsize),
+                                      P<unsigned long long>(c->counter), gcap));
+        XTN_CK(cudaGetLastError());
+        XTN_TRY(read_scalar(c, c->counter.p, 8, &G));
+        if ((int64_t)G <= gcap) break;
+        gcap = (int64_t)G;
+    }
+    c->stats.n_groups += (int64_t)G;
+    *count = 0;
+    if (G == 0) return XTN_SUCCESS;
+    XTN_TRY(ensure(c->gcnt, sizeof(uint64_t) * (G + 1)));
+    XTN_TRY(ensure(c->goff, sizeof(uint64_t) * (G + 1)));
+    XTN_LAUNCH("pair_counts", k_pair_counts<<<blocks_for((int64_t)G), kThreads, 0, s>>>(P<uint32_t>(c->gsize),
+                                                                                       (int64_t)G, P<uint64_t>(c->gcnt)));
+    XTN_CK(cudaGetLastError());
+    XTN_TRY(scan_u64(c, P<uint64_t>(c->gcnt), P<uint64_t>(c->goff), (int64_t)G));
+    uint64_t Pc = 0;
+    XTN_TRY(read_scalar(c, P<uint64_t>(c->goff) + G, 8, &Pc));
+    if (Pc == 0) return XTN_SUCCESS;
+    XTN_TRY(ensure_keep(c, c->pairA, sizeof(uint64_t) * (base + Pc) + 64, sizeof(uint64_t) * base));
+    uint64_t threads = (Pc + kEmitPer - 1) / kEmitPer;
+    XTN_LAUNCH("emit", k_emit<<<blocks_for((int64_t)threads), kThreads, 0, s>>>(
+                           recs, P<uint64_t>(c->gstart), P<uint32_t>(c->gsize), P<uint64_t>(c->goff), (int64_t)G, Pc,
+                           idbits, P<uint64_t>(c->pairA) + base));
+    XTN_CK(cudaGetLastError());
+    *count = Pc;
+    return XTN_SUCCESS;
+}
+
+// Sort engine: every record materialised in sequence order, radix-sorted by hash, grouped.
+static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t V, uint64_t* Pc) {
+    cudaStream_t s = c->stream;
+    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
+    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(P<u128>(c->keys), P<uint8_t>(c->klen),
+                                                              P<uint64_t>(c->voff), n, d, idbits, P<uint64_t>(c->recA)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaEventRecord(c->ev[2], s));
+    uint64_t* recs = nullptr;
+    XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, "key_sort_upsweep", "key_sort_downsweep"));
+    XTN_CK(cudaEventRecord(c->ev[3], s));
+    XTN_TRY(group_sorted(c, recs, (int64_t)V, idbits, 0, Pc));
+    XTN_CK(cudaEventRecord(c->ev[4], s));
+    return XTN_SUCCESS;
+}
+
+// Bucket engine (xtn_bucket.cuh).
+static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_t V, uint64_t* Pc) {
+    cudaStream_t s = c->stream;
+    int b1 = 1;
+    while (b1 < c->bucket_bits_max && (V >> b1) > 3000) b1++;
+    const int nb = 1 << b1;
+    const int ntiles = c->sms * (int)std::max<int64_t>(1, ((int64_t)n + (int64_t)c->sms * 8192 - 1) / ((int64_t)c->sms * 8192));
+    const int tile = (n + ntiles - 1) / ntiles;
+    const size_t hist_smem = sizeof(uint32_t) * nb;
+    XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)ntiles * nb));
+    XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)ntiles * nb));
+    XTN_TRY(ensure(c->btotals, sizeof(uint32_t) * (nb + 1)));
+    XTN_TRY(ensure(c->bstart, sizeof(uint64_t) * (nb + 1)));
+    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
+    if (!c->attrs_set) {
+        XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
+        c->attrs_set = true;
+    }
+    XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
+                                   P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, P<uint32_t>(c->bcounts)));
+    XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
+                                     P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
+    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
+    XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
+                                     P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
+                                     P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaEventRecord(c->ev[2], s));
+
+    // plan: buckets that fit go to grouping, the rest are split by the next hash bits
+    const size_t desc_cap = (size_t)nb * 3 + 4 * V / c->group_cap + 2048;
+    XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
+    XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
+    XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * nb));
+    XTN_TRY(ensure(c->bcnt, 64));
+    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
+    XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
+                                  P<uint64_t>(c->bstart), nb, c->group_cap, P<BucketDesc>(c->bdesc),
+                                  P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
+    XTN_CK(cudaGetLastError());
+    uint32_t cnt[8] = {0};
+    XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaStreamSynchronize(s));
+    memcpy(cnt, c->h_scalar, 32);
+    if (cnt[1] > 0) {
+        XTN_LAUNCH("bucket_split", k_bucket_split<<<cnt[1], 1024, 0, s>>>(
+                                       P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                                       P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
+        XTN_CK(cudaGetLastError());
+        XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        memcpy(cnt, c->h_scalar, 32);
+    }
+    XTN_CK(cudaEventRecord(c->ev[3], s));
+    const uint32_t ndesc = cnt[0], nfall = cnt[3];
+
+    // group every listed bucket in shared memory
+    uint64_t cap = std::max<uint64_t>({c->last_pc + c->last_pc / 4, V / 16, (uint64_t)1 << 20});
+    uint64_t total = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * cap + 64));
+        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
+        if (ndesc > 0)
+            XTN_LAUNCH("bucket_group", k_bucket_group<<<ndesc, kGroupThreads, sizeof(GroupSmem), s>>>(
+                                           P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
+                                           P<uint64_t>(c->pairA), cap, P<unsigned long long>(c->counter),
+                                           P<unsigned int>(c->counter) + 2));
+        XTN_CK(cudaGetLastError());
+        XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        total = c->h_scalar[0];
+        if ((c->h_scalar[1] & 0xffffffffu) != 0) {
+            set_err("bucket grouping: a shared-memory bulk copy did not complete in time");
+            return XTN_ERR_CUDA;
+        }
+        if (total <= cap) break;
+        cap = total;
+    }
+    c->stats.n_groups = ndesc;
+    XTN_CK(cudaEventRecord(c->ev[4], s));
+
+    // buckets too large for shared memory: sorted and grouped in global memory
+    if (nfall > 0) {
+        std::vector<BucketDesc> fl(nfall);
+        XTN_CK(cudaMemcpy(fl.data(), c->bfall.p, sizeof(BucketDesc) * nfall, cudaMemcpyDeviceToHost));
+        for (const BucketDesc& f : fl) {
+            XTN_TRY(ensure(c->fbA, sizeof(uint64_t) * f.size + 64));
+            XTN_TRY(ensure(c->fbB, sizeof(uint64_t) * f.size + 64));
+            XTN_CK(cudaMemcpyAsync(c->fbA.p, P<uint64_t>(c->recB) + f.start, sizeof(uint64_t) * f.size,
+                                   cudaMemcpyDeviceToDevice, s));
+            uint64_t* sorted = nullptr;
+            XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, "fallback_sort_upsweep",
+                             "fallback_sort_downsweep"));
+            uint64_t more = 0;
+            XTN_TRY(group_sorted(c, sorted, f.size, idbits, total, &more));
+            total += more;
+        }
+    }
+    *Pc = total;
+    return XTN_SUCCESS;
+}
+
 // The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
 // -> CSR row. On success the result is in c->out_pairs / c->out_dist, c->n_out entries; the
 // verified pair list in sorted (x, y) order of search indexes.
@@ -387,61 +572,19 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         return XTN_ERR_LIMIT;
     }
 
-    // generate + sort records
-    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V));
-    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V));
-    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->voff), n, d, idbits,
-                                            P<uint64_t>(c->recA)));
-    XTN_CK(cudaGetLastError());
-    XTN_CK(cudaEventRecord(c->ev[2], s));
-    uint64_t* recs = nullptr;
-    XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, "key_sort_upsweep", "key_sort_downsweep"));
-    XTN_CK(cudaEventRecord(c->ev[3], s));
-
-    // groups of equal hashes
-    XTN_TRY(ensure(c->counter, 64));
-    int64_t gcap = std::max<int64_t>(1 << 16, (int64_t)(V / 8));
-    uint64_t G = 0;
-    for (int attempt = 0; attempt < 2; attempt++) {
-        XTN_TRY(ensure(c->gstart, sizeof(uint64_t) * gcap));
-        XTN_TRY(ensure(c->gsize, sizeof(uint32_t) * gcap));
-        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 8, s));
-        XTN_LAUNCH("find_groups", k_find_groups<<<blocks_for((int64_t)V), kThreads, 0, s>>>(recs, (int64_t)V, idbits, P<uint64_t>(c->gstart),
-                                                                   P<uint32_t>(c->gsize),
-                                                                   P<unsigned long long>(c->counter), gcap));
-        XTN_CK(cudaGetLastError());
-        XTN_TRY(read_scalar(c, c->counter.p, 8, &G));
-        if ((int64_t)G <= gcap) break;
-        gcap = (int64_t)G;
-    }
-    st.n_groups = (int64_t)G;
-    XTN_TRY(ensure(c->gcnt, sizeof(uint64_t) * (G + 1)));
-    XTN_TRY(ensure(c->goff, sizeof(uint64_t) * (G + 1)));
+    // candidate pairs: every (min id, max id) of every group of equal variant hashes
     uint64_t Pc = 0;
-    if (G > 0) {
-        XTN_LAUNCH("pair_counts", k_pair_counts<<<blocks_for((int64_t)G), kThreads, 0, s>>>(P<uint32_t>(c->gsize), (int64_t)G,
-                                                                   P<uint64_t>(c->gcnt)));
-        XTN_CK(cudaGetLastError());
-        XTN_TRY(scan_u64(c, P<uint64_t>(c->gcnt), P<uint64_t>(c->goff), (int64_t)G));
-        XTN_TRY(read_scalar(c, P<uint64_t>(c->goff) + G, 8, &Pc));
-    }
-    XTN_CK(cudaEventRecord(c->ev[4], s));
+    XTN_TRY(ensure(c->counter, 64));
+    if (c->engine == 1) XTN_TRY(candidates_sorted(c, n, d, idbits, V, &Pc));
+    else XTN_TRY(candidates_bucketed(c, n, d, idbits, V, &Pc));
+    c->last_pc = Pc;
     st.n_candidates = (int64_t)Pc;
     if (Pc >= (uint64_t)UINT32_MAX) {
         set_err("too many candidate pairs for one round (" + std::to_string(Pc) + ")");
         return XTN_ERR_LIMIT;
     }
-
-    // candidate pairs
-    XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Pc));
-    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc));
-    if (Pc > 0) {
-        uint64_t threads = (Pc + kEmitPer - 1) / kEmitPer;
-        XTN_LAUNCH("emit", k_emit<<<blocks_for((int64_t)threads), kThreads, 0, s>>>(recs, P<uint64_t>(c->gstart), P<uint32_t>(c->gsize),
-                                                                 P<uint64_t>(c->goff), (int64_t)G, Pc, idbits,
-                                                                 P<uint64_t>(c->pairA)));
-        XTN_CK(cudaGetLastError());
-    }
+    XTN_TRY(ensure_keep(c, c->pairA, sizeof(uint64_t) * Pc + 64, sizeof(uint64_t) * Pc));
+    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc + 64));
     XTN_CK(cudaEventRecord(c->ev[5], s));
     uint64_t* pairs = P<uint64_t>(c->pairA);
     if (Pc > 1)
@@ -882,6 +1025,8 @@ int xtn_context_create(int device, xtn_context** out) {
     }
     for (auto& ev : c->ev) cudaEventCreate(&ev);
     c->overlap_bufs = new xtn_overlap_bufs();
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (const char* e = getenv("XTN_ENGINE")) c->engine = (strcmp(e, "sort") == 0) ? 1 : 0;
     *out = c;
     return XTN_SUCCESS;
 }
@@ -890,9 +1035,12 @@ void xtn_context_destroy(xtn_context* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->chars, &c->offs, &c->keys, &c->klen, &c->vcnt, &c->voff, &c->recA, &c->recB,
-                      &c->gstart, &c->gsize, &c->gcnt, &c->goff, &c->pairA, &c->pairB, &c->dist, &c->flag,
-                      &c->fpos, &c->scratch64, &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq};
+    DevBuf* bufs[] = {&c->chars,   &c->offs,     &c->keys,      &c->klen,      &c->vcnt,     &c->voff,
+                      &c->recA,    &c->recB,     &c->gstart,    &c->gsize,     &c->gcnt,     &c->goff,
+                      &c->pairA,   &c->pairB,    &c->dist,      &c->flag,      &c->fpos,     &c->scratch64,
+                      &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
+                      &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
+                      &c->bcnt,    &c->fbA,      &c->fbB};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -964,6 +1112,18 @@ int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, 
                (long long)st.n_out, st.ms_total);
     }
     return deliver(c, cb, user);
+}
+
+int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
+    if (!c || !name) return XTN_ERR_ARG;
+    if (!strcmp(name, "engine") && (v == 0 || v == 1)) c->engine = (int)v;
+    else if (!strcmp(name, "bucket_bits_max") && v >= 1 && v <= 15) c->bucket_bits_max = (int)v;
+    else if (!strcmp(name, "group_cap") && v >= 2 && v <= kGroupCap) c->group_cap = (uint32_t)v;
+    else {
+        set_err(std::string("unknown option or value out of range: ") + name);
+        return XTN_ERR_ARG;
+    }
+    return XTN_SUCCESS;
 }
 
 int xtn_context_set_profiling(xtn_context* c, int on) {

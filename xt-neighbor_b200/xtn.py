@@ -36,6 +36,7 @@ SYMBOLS = (
     "xtn_context_result_device",
     "xtn_context_stream",
     "xtn_context_stats",
+    "xtn_context_set_option",
     "xtn_context_set_profiling",
     "xtn_context_kernel_times",
     "xtn_last_error",
@@ -125,6 +126,7 @@ def load():
     lib.xtn_context_stream.restype = P
     lib.xtn_context_stats.argtypes = [P, ctypes.POINTER(Stats)]
     lib.xtn_context_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.xtn_context_set_option.argtypes = [P, ctypes.c_char_p, ctypes.c_int64]
     lib.xtn_context_kernel_times.argtypes = [P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
     _lib = lib
@@ -161,10 +163,15 @@ class Result:
 class Context:
     """Reusable device context (stream + growing device buffers)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, **options):
         self.lib = load()
         self.h = ctypes.c_void_p()
         _check(self.lib.xtn_context_create(device, ctypes.byref(self.h)))
+        for k, v in options.items():
+            self.set_option(k, v)
+
+    def set_option(self, name: str, value: int):
+        _check(self.lib.xtn_context_set_option(self.h, name.encode(), int(value)))
 
     def close(self):
         if self.h:
