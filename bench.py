@@ -115,20 +115,27 @@ class ClockSampler:
 
 
 def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | None:
-    """Compulsory bytes one launch of `kernel` must move (per-launch average over a step)."""
-    V, G, Pc = st["n_variants"], st["n_groups"], st["n_candidates"]
+    """Compulsory HBM bytes of all launches of `kernel` in one step (divided by the launch count
+    by the caller). V = deletion variants, P = candidate pairs, n = sequences."""
+    V, Pc = st["n_variants"], st["n_candidates"]
+    if kernel == "bucket_scatter":
+        return 8.0 * V + 48.0 * n  # each 8-byte record written once; key, run info, offsets read
+    if kernel == "bucket_group":
+        return 8.0 * V + 8.0 * Pc  # each record read once; candidate pairs written
+    if kernel == "bucket_split":
+        return 16.0 * V  # records of split buckets read once and written once
+    if kernel == "bucket_count":
+        return 17.0 * n  # key and length of each sequence
     if kernel == "key_sort_downsweep":
-        return 16.0 * V  # read + write each 8-byte record once
+        return 16.0 * V  # sort engine: read + write each 8-byte record once
     if kernel == "key_sort_upsweep":
         return 8.0 * V
     if kernel == "gen":
-        return 8.0 * V + 25.0 * n  # records out; key, length, offset in
+        return 8.0 * V + 25.0 * n
     if kernel == "find_groups":
-        return 8.0 * V + 12.0 * G
-    if kernel == "pack":
-        return n_chars + 8.0 * n + 21.0 * n
+        return 8.0 * V
     if kernel == "verify":
-        return 8.0 * Pc + 2.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
+        return 10.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
     return None
 
 
@@ -157,7 +164,9 @@ def run_ours(args, w):
         pg = dist
     chars, offs = gen_workload(w)
     n = len(offs) - 1
-    ctx = xtn.Context(local, engine=1 if args.engine == "sort" else 0)
+    opts = {k: int(v) for k, v in (o.split("=", 1) for o in args.opt)}
+    opts.setdefault("engine", 1 if args.engine == "sort" else 0)
+    ctx = xtn.Context(local, **opts)
     ctx.set_profiling(True)
     d_chars = torch.from_numpy(chars).cuda()
     d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
@@ -254,6 +263,7 @@ def run_ours(args, w):
             "measure": "hamming" if w["measure"] else "leven",
             "parallelism": f"replicas x{world}",
             "engine": args.engine,
+            "options": {o.split("=", 1)[0]: int(o.split("=", 1)[1]) for o in args.opt},
             "l2": "flushed between steps (256 MiB write)",
         },
         "pairs_per_s": world * n_out / (ms_step / 1e3),
@@ -414,6 +424,8 @@ def main():
     ap.add_argument("--engine", choices=["bucket", "sort"], default="bucket",
                     help="key grouping: shared-memory hash buckets (default) or full radix sort")
     ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
+    ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
+                    help="context option (xtn_context_set_option), repeatable")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)

@@ -43,6 +43,16 @@ int hc_variants(const char* s, int L, int d, char* out, uint64_t* hashes, int ca
     return n;
 }
 
+// Variants by flat index v = 0..count-1 (decoded strings, 19 bytes each); d <= 2.
+int hc_variants_flat(const char* s, int L, int d, char* out, int cap) {
+    u128 key = pack(s, L);
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    int n = variant_count(key, Lk, d);
+    const uint64_t info = key_run_info(key, Lk);
+    for (int v = 0; v < n && v < cap; v++) unpack(variant_at(key, info, v), out + 19 * v);
+    return n;
+}
+
 int hc_variant_count(const char* s, int L, int d) {
     int Lk = L < kKeyLen ? L : kKeyLen;
     return variant_count(pack(s, L), Lk, d);

@@ -61,6 +61,20 @@ def test_variant_set_equals_reference_multiset(hc):
                 assert hm.setdefault(g, int(h)) == int(h)
 
 
+def test_flat_variant_index_matches_enumeration(hc):
+    """variant_at(v), v = 0..count-1 (the staged scatter's parallel decode) yields exactly the
+    multiset for_each_variant enumerates, for d = 1, 2."""
+    rng = np.random.default_rng(21)
+    for s in rand_seqs(rng, 600, 1, 26):
+        for d in (1, 2):
+            ref, _ = variants(hc, s, d)
+            n = hc.hc_variant_count(s.encode(), len(s), d)
+            buf = ctypes.create_string_buffer(19 * n)
+            assert hc.hc_variants_flat(s.encode(), len(s), d, buf, n) == n
+            flat = [buf.raw[19 * i : 19 * i + 19].split(b"\0")[0].decode() for i in range(n)]
+            assert sorted(flat) == sorted(ref), (s, d)
+
+
 def test_key_delete(hc):
     rng = np.random.default_rng(5)
     for s in rand_seqs(rng, 200, 1, 19):

@@ -19,6 +19,8 @@ ENGINES = {
     # tiny first-level table and shared-memory cap: exercises the bucket split and the
     # sort-based fallback for oversized buckets on small inputs
     "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64},
+    # buckets loaded into shared memory by plain loads instead of a TMA bulk copy
+    "bucket_plain_loads": {"group_tma": 0, "scatter_ctas_per_sm": 1},
 }
 
 

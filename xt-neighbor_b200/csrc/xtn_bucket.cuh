@@ -2,17 +2,26 @@
 //
 // The sort-based engine orders all V variant records by hash with a multi-pass radix sort
 // (about 24 bytes of HBM traffic per record per 8-bit digit). Grouping only needs equal
-// hashes to meet, not a global order, so this engine moves each record through HBM once:
-//   count    k_bucket_count    per tile of sequences: histogram of the top B1 hash bits
-//                              (variants are generated, hashed and counted, not stored)
+// hashes to meet, not a global order, so this engine moves each 8-byte record through HBM a
+// fixed small number of times:
+//   count    k_bucket_count    per tile of sequences: histogram of the top b1 hash bits
+//                              (variants generated and hashed, not stored)
 //   offsets  k_bucket_colscan  per bucket: exclusive prefix over tiles, bucket totals
-//   scatter  k_bucket_scatter  the same variants again, each written once as a 64-bit
-//                              record (next hash bits | sequence id) into its bucket's range
+//   scatter  k_bucket_scatter_staged
+//                              the variants again, 8192 at a time in shared memory (one
+//                              variant per thread from a flat index), counting-sorted by
+//                              bucket there and written out as contiguous runs: every
+//                              global store is part of a coalesced run, so L2 receives
+//                              whole sectors instead of read-modify-writing partial ones
 //   plan     k_bucket_plan     buckets that fit in shared memory go straight to grouping;
-//                              larger ones are split by the next hash bits (k_bucket_split)
-//   group    k_bucket_group    one CTA per bucket: TMA bulk copy of the bucket into shared
-//                              memory, counting sort on 12 hash bits, runs of equal hashes,
-//                              every id pair of every run appended to the candidate list
+//                              larger ones are split by their next hash bits
+//   split    k_bucket_split_staged
+//                              the same staged partition, per bucket, into sub-buckets
+//   group    k_bucket_group    one CTA per (sub-)bucket: TMA bulk copy into shared memory,
+//                              a bitmap filter that drops records without a partner, a
+//                              counting sort of the rest, runs of equal hashes, then every id
+//                              pair of every run, spread evenly over the CTA's threads and
+//                              written with coalesced stores
 // Buckets that still exceed shared memory after the split (one variant shared by very many
 // sequences) are grouped by the sort-based path instead.
 #pragma once
@@ -22,13 +31,23 @@
 
 namespace xtn {
 
-constexpr int kBucketThreads = 1024;   // count/scatter CTAs (one per SM: up to 128 KB of counters)
+constexpr int kBucketThreads = 512;    // k_bucket_count and the direct scatter (d > 2)
+constexpr int kStageThreads = 1024;    // staged scatter / split
+constexpr int kStageChunk = 8192;      // records per staged chunk
+constexpr int kMaxFan = 1024;          // fan-out of one staged partition
+// First-level fan-out: each staged chunk of 8192 records then leaves runs of ~16 records per
+// bucket (128 bytes), enough for whole-sector writes.
+constexpr int kMaxFirstLevelBits = 9;
 constexpr int kGroupThreads = 512;
-constexpr int kGroupCap = 8192;        // records a grouping CTA holds in shared memory
-constexpr int kDigitBits = 12;
+constexpr int kGroupCap = 6144;        // records a grouping CTA holds in shared memory
+constexpr int kBitmapLog = 17;         // hash bits of the "seen" / "seen twice" bitmaps
+constexpr int kBitmapBits = 1 << kBitmapLog;
+constexpr int kBitmapWords = kBitmapBits / 32;
+constexpr int kDigitBits = 11;         // hash bits of the candidates' counting sort
 constexpr int kDigits = 1 << kDigitBits;
-constexpr int kBigGroup = 48;          // runs at least this long are emitted by the whole CTA
-constexpr int kMaxBigGroups = 64;
+// Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to 3072;
+// buckets with more than this go to the sort-based fallback).
+constexpr int kMaxRuns = 2048;
 constexpr uint32_t kWaitLimit = 1u << 26;  // bound on mbarrier polls
 
 // Descriptor of one bucket (or sub-bucket) handed to the grouping kernel.
@@ -47,6 +66,37 @@ struct SplitJob {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Exclusive scan of one value per thread across a block of THREADS threads.
+template <typename T, int THREADS>
+__device__ __forceinline__ T block_scan_ex(T v, T* total, T* warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < THREADS / 32 ? warp_sums[lane] : T(0);
+        T winc = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T t = __shfl_up_sync(0xffffffffu, winc, o);
+            if (lane >= o) winc += t;
+        }
+        if (lane < THREADS / 32) warp_sums[lane] = winc - w;
+        if (lane == THREADS / 32 - 1) warp_sums[THREADS / 32] = winc;
+    }
+    __syncthreads();
+    T r = inc - v + warp_sums[warp];
+    *total = warp_sums[THREADS / 32];
+    __syncthreads();
+    return r;
+}
+
+// ------------------------------------------------------------------ count
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const u128* __restrict__ keys,
                                                                  const uint8_t* __restrict__ klen, int n, int tile, int d,
                                                                  int b1, uint32_t* __restrict__ counts) {
@@ -78,6 +128,115 @@ __global__ void k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles
     totals[b] = run;
 }
 
+// ------------------------------------------------------------------ staged partition
+struct StageSmem {
+    uint64_t rec[kStageChunk];     // records of the chunk, in arrival order
+    uint64_t sorted[kStageChunk];  // the same records grouped by bucket
+    uint16_t bkt[kStageChunk];     // bucket of rec[i]
+    uint16_t sbkt[kStageChunk];    // bucket of sorted[i]
+    uint32_t cnt[kMaxFan];
+    uint32_t lstart[kMaxFan];
+    uint32_t gcur[kMaxFan];        // next global position of each bucket for this CTA
+    uint32_t warp_sums[kStageThreads / 32 + 1];
+    uint32_t seq_end;
+};
+
+// Writes rec[0..m) (bucket bkt[]) to dst, each bucket's records appended at gcur[bucket],
+// as contiguous runs from consecutive threads.
+__device__ __forceinline__ void stage_partition(StageSmem& S, int nb, uint32_t m, uint64_t* __restrict__ dst) {
+    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[S.bkt[p]], 1u);
+    __syncthreads();
+    uint32_t tot;
+    const uint32_t v = threadIdx.x < (unsigned)nb ? S.cnt[threadIdx.x] : 0u;
+    const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(v, &tot, S.warp_sums);
+    if (threadIdx.x < (unsigned)nb) {
+        S.lstart[threadIdx.x] = ex;
+        S.cnt[threadIdx.x] = ex;
+    }
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
+        const uint16_t b = S.bkt[p];
+        const uint32_t q = atomicAdd(&S.cnt[b], 1u);
+        S.sorted[q] = S.rec[p];
+        S.sbkt[q] = b;
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < m; q += kStageThreads) {
+        const uint16_t b = S.sbkt[q];
+        dst[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
+    __syncthreads();
+}
+
+// First-level scatter for d <= 2 (flat variant index; a sequence has at most 172 variants).
+// runinfo[i] is key_run_info of sequence i.
+__global__ void __launch_bounds__(kStageThreads, 1) k_bucket_scatter_staged(
+    const u128* __restrict__ keys, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ voff, int n,
+    int tile, int b1, int idbits, const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart,
+    uint64_t* __restrict__ recs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    const int nb = 1 << b1;
+    const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
+    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] = (uint32_t)bstart[b] + off[b];
+    const int t0 = blockIdx.x * tile;
+    const int t1 = min(n, t0 + tile);
+    const int shift = 64 - b1;
+    const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
+    constexpr int kPer = kStageChunk / kStageThreads;  // 8 slots per thread in the slot scan
+    __syncthreads();
+    for (int s0 = t0; s0 < t1;) {
+        if (threadIdx.x == 0) {
+            // largest s1 <= t1 with voff[s1] - voff[s0] <= chunk (at least s0 + 1)
+            int lo = s0 + 1, hi = min(t1, s0 + kStageChunk);
+            const uint64_t lim = voff[s0] + kStageChunk;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (voff[mid] <= lim) lo = mid;
+                else hi = mid - 1;
+            }
+            S.seq_end = (uint32_t)lo;
+        }
+        for (int f = threadIdx.x; f < kStageChunk; f += kStageThreads) S.sbkt[f] = 0;
+        __syncthreads();
+        const int s1 = (int)S.seq_end;
+        const uint64_t base = voff[s0];
+        const uint32_t m = (uint32_t)(voff[s1] - base);
+        // slot -> owning sequence: mark each sequence's first slot, then an inclusive scan
+        for (int i = s0 + 1 + threadIdx.x; i < s1; i += kStageThreads) S.sbkt[voff[i] - base] = 1;
+        __syncthreads();
+        {
+            const int f0 = threadIdx.x * kPer;
+            uint32_t loc[kPer], sum = 0;
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                sum += S.sbkt[f0 + k];
+                loc[k] = sum;
+            }
+            uint32_t tot;
+            const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
+#pragma unroll
+            for (int k = 0; k < kPer; k++) S.sbkt[f0 + k] = (uint16_t)(ex + loc[k]);
+        }
+        __syncthreads();
+        for (uint32_t f = threadIdx.x; f < m; f += kStageThreads) {
+            const int i = s0 + S.sbkt[f];
+            const int v = (int)(base + f - voff[i]);
+            const uint64_t h = key_hash(variant_at(keys[i], runinfo[i], v));
+            S.bkt[f] = (uint16_t)(h >> shift);
+            S.rec[f] = ((h << b1) & hi_mask) | (uint64_t)i;
+        }
+        __syncthreads();
+        stage_partition(S, nb, m, recs);
+        s0 = s1;
+    }
+}
+
+// First-level scatter for any d: one thread per sequence, smem cursors, direct stores.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* __restrict__ keys,
                                                                    const uint8_t* __restrict__ klen, int n, int tile, int d,
                                                                    int b1, int idbits, const uint32_t* __restrict__ offsets,
@@ -115,97 +274,80 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
         unsigned k = atomicAdd(&counters[0], 1u);
         desc[k] = BucketDesc{s, size, 0};
     } else {
+        // sub-buckets aim at 7/8 of the shared-memory capacity (hash buckets are near-uniform)
+        const uint32_t target = group_cap * 7 / 8;
         uint32_t bits = 1;
-        while (bits < 10 && ((uint64_t)size >> bits) > (uint64_t)(group_cap / 2)) bits++;
+        while (bits < 10 && ((uint64_t)size >> bits) > (uint64_t)(target > 1 ? target : 1)) bits++;
         unsigned k = atomicAdd(&counters[1], 1u);
         jobs[k] = SplitJob{s, size, bits};
         atomicAdd(&counters[2], 1u << bits);
     }
 }
 
-// One CTA per split job: histogram of the next `bits` hash bits (the record's top bits),
-// prefix, then a scatter into buffer B at the same range. Sub-buckets that fit are listed
-// for grouping; larger ones go to the fallback list.
-__global__ void __launch_bounds__(1024) k_bucket_split(const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in,
-                                                       uint64_t* __restrict__ out, uint32_t group_cap,
-                                                       BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback,
-                                                       unsigned int* __restrict__ counters) {
-    __shared__ uint32_t s_cnt[1024];
-    __shared__ uint32_t s_cur[1024];
+// One CTA per split job: histogram of the record's top `bits` bits (the next hash bits),
+// sub-bucket descriptors, then the bucket's records, chunk by chunk, through the staged
+// partition into buffer B at the same range. Sub-buckets that fit are listed for grouping;
+// larger ones go to the fallback list.
+__global__ void __launch_bounds__(kStageThreads, 1) k_bucket_split_staged(
+    const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t group_cap,
+    BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
     const SplitJob job = jobs[blockIdx.x];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;
-    for (int i = threadIdx.x; i < nsub; i += blockDim.x) s_cnt[i] = 0;
+    for (int i = threadIdx.x; i < nsub; i += kStageThreads) S.cnt[i] = 0;
     __syncthreads();
     const uint64_t* src = in + job.start;
-    for (uint32_t i = threadIdx.x; i < job.size; i += blockDim.x) atomicAdd(&s_cnt[src[i] >> shift], 1u);
+    for (uint32_t i = threadIdx.x; i < job.size; i += kStageThreads) atomicAdd(&S.cnt[src[i] >> shift], 1u);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int i = 0; i < nsub; i++) {
-            uint32_t c = s_cnt[i];
-            s_cur[i] = run;
-            if (c >= 2) {
-                BucketDesc bd{job.start + run, c, 1};
-                if (c <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
-                else fallback[atomicAdd(&counters[3], 1u)] = bd;
-            }
-            run += c;
+    uint32_t tot;
+    const uint32_t v = threadIdx.x < (unsigned)nsub ? S.cnt[threadIdx.x] : 0u;
+    const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(v, &tot, S.warp_sums);
+    if (threadIdx.x < (unsigned)nsub) {
+        S.gcur[threadIdx.x] = (uint32_t)job.start + ex;
+        if (v >= 2) {
+            BucketDesc bd{job.start + ex, v, 1};
+            if (v <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
+            else fallback[atomicAdd(&counters[3], 1u)] = bd;
         }
     }
     __syncthreads();
-    uint64_t* dst = out + job.start;
-    for (uint32_t i = threadIdx.x; i < job.size; i += blockDim.x) {
-        uint64_t r = src[i];
-        dst[atomicAdd(&s_cur[r >> shift], 1u)] = r;
+    for (uint32_t c0 = 0; c0 < job.size; c0 += kStageChunk) {
+        const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
+        for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
+            const uint64_t r = src[c0 + p];
+            S.rec[p] = r;
+            S.bkt[p] = (uint16_t)(r >> shift);
+        }
+        __syncthreads();
+        stage_partition(S, nsub, m, out);
     }
 }
 
-// Shared-memory layout of k_bucket_group (about 99 KB: two CTAs per SM).
+// ------------------------------------------------------------------ group
+// Shared-memory layout of k_bucket_group (about 100 KB: two CTAs per SM). The two bitmaps
+// are only needed until the candidates are known; the grouping arrays reuse their space.
 struct GroupSmem {
     uint64_t rec[kGroupCap + 2];  // bucket records (+ alignment slack)
-    uint32_t cnt[kDigits];        // counting sort over kDigitBits hash bits
-    uint16_t perm[kGroupCap];     // record indexes grouped by digit
-    uint32_t big_start[kMaxBigGroups];
-    uint32_t big_size[kMaxBigGroups];
-    uint64_t big_poff[kMaxBigGroups + 1];
-    uint32_t warp_sums32[kGroupThreads / 32 + 1];
-    uint64_t warp_sums64[kGroupThreads / 32 + 1];
-    unsigned long long base;
-    uint32_t n_big;
+    union {
+        struct {
+            uint32_t seen[kBitmapWords];   // hash bit seen once
+            uint32_t twice[kBitmapWords];  // hash bit seen at least twice
+        } bm;
+        struct {
+            uint16_t perm[kGroupCap];  // candidate record indexes grouped by digit
+            uint32_t runs[kMaxRuns];   // contiguous << 31 | size << 16 | head slot, per run of >= 2
+            uint32_t poff[kMaxRuns];   // first pair index of each run
+        } gr;
+    } u;
+    uint16_t cand[kGroupCap];  // records whose bitmap bit was hit at least twice
+    uint32_t cnt[kDigits];     // digit counts -> digit ends
+    uint32_t warp_sums[kGroupThreads / 32 + 1];
     uint32_t wait_failed;
+    unsigned long long base;
     unsigned long long mbar;
 };
-
-// Exclusive block scan of one value per thread (kGroupThreads threads).
-template <typename T>
-__device__ __forceinline__ T group_block_scan(T v, T* total, T* warp_sums) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    T inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-    }
-    if (lane == 31) warp_sums[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        T w = lane < kGroupThreads / 32 ? warp_sums[lane] : T(0);
-        T winc = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T t = __shfl_up_sync(0xffffffffu, winc, o);
-            if (lane >= o) winc += t;
-        }
-        if (lane < kGroupThreads / 32) warp_sums[lane] = winc - w;
-        if (lane == kGroupThreads / 32 - 1) warp_sums[kGroupThreads / 32] = winc;
-    }
-    __syncthreads();
-    T r = inc - v + warp_sums[warp];
-    *total = warp_sums[kGroupThreads / 32];
-    __syncthreads();
-    return r;
-}
 
 __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
     uint32_t ok;
@@ -224,49 +366,70 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 }
 
 // Groups one bucket. Records of equal hash (record >> idbits) form a run; every pair of
-// positions in a run is written as (min id << idbits) | max id. The CTA reserves its output
-// range with one atomic on `cursor`; entries at or past `cap` are counted but not written,
-// so the caller can grow the buffer to the exact size and run again.
+// positions in a run is written as (min id << idbits) | max id.
+//   1. a two-bitmap filter over kBitmapBits hash bits keeps only records that can have a
+//      partner (every record of a run of >= 2 survives; ~1 in 40 singletons does too);
+//   2. the survivors are counting-sorted by kDigitBits further hash bits;
+//   3. each survivor checks its digit: it heads a run when no earlier survivor of the digit
+//      has its hash, and the run's size is the number with that hash (two passes: count,
+//      then write at block-scanned offsets);
+//   4. the CTA reserves its output range with one atomic on `cursor` and spreads the pairs
+//      over its threads. Entries at or past `cap` are counted but not written, so the caller
+//      can grow the buffer to the exact size and run again.
+// A bucket with more than kMaxRuns runs is appended to `overflow` (grouped later by sorting).
 __global__ void __launch_bounds__(kGroupThreads, 2) k_bucket_group(const BucketDesc* __restrict__ descs,
                                                                      const uint64_t* __restrict__ buf_a,
                                                                      const uint64_t* __restrict__ buf_b, int idbits,
                                                                      uint64_t* __restrict__ pairs, uint64_t cap,
                                                                      unsigned long long* __restrict__ cursor,
-                                                                     unsigned int* __restrict__ errors) {
+                                                                     unsigned int* __restrict__ errors, int use_tma,
+                                                                     BucketDesc* __restrict__ overflow,
+                                                                     unsigned int* __restrict__ n_overflow) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem& S = *reinterpret_cast<GroupSmem*>(smem_raw);
     const BucketDesc bd = descs[blockIdx.x];
     const uint32_t n = bd.size;
     const uint64_t* src = (bd.src ? buf_b : buf_a) + bd.start;
-    // TMA bulk copy of the bucket into shared memory. The source must start on 16 bytes and
-    // the size must be a multiple of 16: copy from the 16-byte boundary at or below the first
-    // record (one extra record at most on each side; the buffers carry 16 bytes of padding).
+    // The bucket goes to shared memory either by one TMA bulk copy (use_tma) or by plain
+    // 16-byte loads from all threads. A bulk copy must start on 16 bytes and move a multiple
+    // of 16 bytes: both paths copy from the 16-byte boundary at or below the first record (one
+    // extra record at most on each side; the record buffers carry 16 bytes of padding).
     const uint32_t lead = (uint32_t)(((uintptr_t)src & 15u) >> 3);
     const uint64_t* src16 = src - lead;
     const uint32_t bytes = ((lead + n) * 8u + 15u) & ~15u;
     const uint32_t mbar = smem_u32(&S.mbar);
-    if (threadIdx.x == 0) {
-        S.wait_failed = 0;
-        S.n_big = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                smem_u32(&S.rec[0])),
-            "l"(src16), "r"(bytes), "r"(mbar)
-            : "memory");
+    if (threadIdx.x == 0) S.wait_failed = 0;
+    if (use_tma) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(&S.rec[0])),
+                "l"(src16), "r"(bytes), "r"(mbar)
+                : "memory");
+        }
+    } else {
+        const uint4* g = reinterpret_cast<const uint4*>(src16);
+        uint4* dd = reinterpret_cast<uint4*>(&S.rec[0]);
+        for (uint32_t i = threadIdx.x; i < bytes / 16; i += kGroupThreads) dd[i] = __ldg(g + i);
+    }
+    for (int i = threadIdx.x; i < kBitmapWords; i += kGroupThreads) {
+        S.u.bm.seen[i] = 0;
+        S.u.bm.twice[i] = 0;
     }
     for (int i = threadIdx.x; i < kDigits; i += kGroupThreads) S.cnt[i] = 0;
-    __syncthreads();
-    {
+    if (use_tma && threadIdx.x == 0) {
+        // one thread polls the barrier (sleeping between polls); the others wait at __syncthreads
         uint32_t polls = 0;
         while (!mbar_try_wait(mbar, 0)) {
             if (++polls > kWaitLimit) {
-                atomicExch(&S.wait_failed, 1u);
+                S.wait_failed = 1;
                 break;
             }
+            __nanosleep(32);
         }
     }
     __syncthreads();
@@ -274,8 +437,7 @@ __global__ void __launch_bounds__(kGroupThreads, 2) k_bucket_group(const BucketD
         // one more bounded wait for the copy to land before the shared memory is released
         if (threadIdx.x == 0) {
             uint32_t polls = 0;
-            while (!mbar_try_wait(mbar, 0) && ++polls < kWaitLimit) {
-            }
+            while (!mbar_try_wait(mbar, 0) && ++polls < kWaitLimit) __nanosleep(64);
             atomicAdd(errors, 1u);
         }
         __syncthreads();
@@ -284,12 +446,33 @@ __global__ void __launch_bounds__(kGroupThreads, 2) k_bucket_group(const BucketD
     const uint64_t* rec = S.rec + lead;
     const uint64_t idmask = (1ull << idbits) - 1ull;
 
-    // counting sort by kDigitBits hash bits
-    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) atomicAdd(&S.cnt[(rec[i] >> idbits) & (kDigits - 1)], 1u);
+    // 1. bitmap filter
+    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
+        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+        const uint32_t bit = 1u << (b & 31);
+        if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
+    }
+    __syncthreads();
+    uint32_t my_c = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
+        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+        my_c += (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
+    }
+    uint32_t m;
+    uint32_t c_off = block_scan_ex<uint32_t, kGroupThreads>(my_c, &m, S.warp_sums);
+    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
+        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+        if ((S.u.bm.twice[b >> 5] >> (b & 31)) & 1u) S.cand[c_off++] = (uint16_t)i;
+    }
+    __syncthreads();  // the bitmaps are dead from here on
+
+    // 2. counting sort of the candidates by kDigitBits hash bits above the bitmap bits
+    for (uint32_t c = threadIdx.x; c < m; c += kGroupThreads)
+        atomicAdd(&S.cnt[(uint32_t)(rec[S.cand[c]] >> (idbits + kBitmapLog)) & (kDigits - 1)], 1u);
     __syncthreads();
     constexpr int kPer = kDigits / kGroupThreads;
-    const int d0 = threadIdx.x * kPer;
     {
+        const int d0 = threadIdx.x * kPer;
         uint32_t loc[kPer], sum = 0;
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
@@ -297,116 +480,99 @@ __global__ void __launch_bounds__(kGroupThreads, 2) k_bucket_group(const BucketD
             sum += S.cnt[d0 + k];
         }
         uint32_t tot;
-        uint32_t ex = group_block_scan<uint32_t>(sum, &tot, S.warp_sums32);
+        const uint32_t ex = block_scan_ex<uint32_t, kGroupThreads>(sum, &tot, S.warp_sums);
 #pragma unroll
         for (int k = 0; k < kPer; k++) S.cnt[d0 + k] = ex + loc[k];
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
-        uint32_t p = atomicAdd(&S.cnt[(rec[i] >> idbits) & (kDigits - 1)], 1u);
-        S.perm[p] = (uint16_t)i;
+    for (uint32_t c = threadIdx.x; c < m; c += kGroupThreads) {
+        const uint16_t i = S.cand[c];
+        const uint32_t p = atomicAdd(&S.cnt[(uint32_t)(rec[i] >> (idbits + kBitmapLog)) & (kDigits - 1)], 1u);
+        S.u.gr.perm[p] = i;
     }
     __syncthreads();
     // now digit dg occupies perm[cnt[dg-1] .. cnt[dg])
 
-    // runs of equal hash inside each of this thread's digits (a digit holds ~2 records)
-    uint64_t my_pairs = 0, listed = 0;
-    int seen_big = 0;
-    for (int k = 0; k < kPer; k++) {
-        const int dg = d0 + k;
+    // 3. runs
+    auto scan_pos = [&](uint32_t i, uint32_t& size, uint32_t& contiguous) -> bool {
+        const uint64_t kv = rec[S.u.gr.perm[i]] >> idbits;
+        const uint32_t dg = (uint32_t)(kv >> kBitmapLog) & (kDigits - 1);
         const uint32_t a = dg == 0 ? 0u : S.cnt[dg - 1], b = S.cnt[dg];
-        if (b - a < 2) continue;
-        for (uint32_t x = a + 1; x < b; x++) {
-            uint16_t v = S.perm[x];
-            uint64_t kv = rec[v] >> idbits;
-            uint32_t y = x;
-            while (y > a && (rec[S.perm[y - 1]] >> idbits) > kv) {
-                S.perm[y] = S.perm[y - 1];
-                y--;
-            }
-            S.perm[y] = v;
-        }
-        for (uint32_t x = a; x < b;) {
-            uint64_t kv = rec[S.perm[x]] >> idbits;
-            uint32_t y = x + 1;
-            while (y < b && (rec[S.perm[y]] >> idbits) == kv) y++;
-            const uint64_t s = y - x;
-            if (s >= (uint64_t)kBigGroup && seen_big < 64) {
-                uint32_t slot = atomicAdd(&S.n_big, 1u);
-                if (slot < (uint32_t)kMaxBigGroups) {
-                    S.big_start[slot] = x;
-                    S.big_size[slot] = (uint32_t)s;
-                    listed |= 1ull << seen_big;
-                } else {
-                    my_pairs += s * (s - 1) / 2;
-                }
-                seen_big++;
-            } else if (s >= 2) {
-                my_pairs += s * (s - 1) / 2;
-            }
-            x = y;
+        if (b - a < 2) return false;
+        for (uint32_t y = a; y < i; y++)
+            if ((rec[S.u.gr.perm[y]] >> idbits) == kv) return false;
+        uint32_t sz = 1;
+        for (uint32_t y = i + 1; y < b; y++) sz += (rec[S.u.gr.perm[y]] >> idbits) == kv;
+        size = sz;
+        contiguous = (sz == b - a) ? 1u : 0u;
+        return sz >= 2;
+    };
+    uint32_t my_runs = 0, my_pairs = 0;
+    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {
+        uint32_t sz, ct;
+        if (scan_pos(i, sz, ct)) {
+            my_runs++;
+            my_pairs += sz * (sz - 1) / 2;
         }
     }
-    __syncthreads();
-    const uint32_t n_big = min(S.n_big, (uint32_t)kMaxBigGroups);
-    if (threadIdx.x == 0) {
-        uint64_t run = 0;
-        for (uint32_t g = 0; g < n_big; g++) {
-            S.big_poff[g] = run;
-            uint64_t s = S.big_size[g];
-            run += s * (s - 1) / 2;
-        }
-        S.big_poff[n_big] = run;
+    uint32_t nr, total;
+    uint32_t run_off = block_scan_ex<uint32_t, kGroupThreads>(my_runs, &nr, S.warp_sums);
+    uint32_t pair_off = block_scan_ex<uint32_t, kGroupThreads>(my_pairs, &total, S.warp_sums);
+    if (nr > (uint32_t)kMaxRuns) {  // too many runs to list: the bucket is regrouped by sorting
+        if (threadIdx.x == 0) overflow[atomicAdd(n_overflow, 1u)] = bd;
+        return;
     }
-    uint64_t total;
-    const uint64_t my_off = group_block_scan<uint64_t>(my_pairs, &total, S.warp_sums64);
-    if (threadIdx.x == 0) S.base = atomicAdd(cursor, (unsigned long long)(total + S.big_poff[n_big]));
+    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {
+        uint32_t sz, ct;
+        if (scan_pos(i, sz, ct)) {
+            S.u.gr.runs[run_off] = (ct << 31) | (sz << 16) | i;  // head slot < 2^13, size < 2^15
+            S.u.gr.poff[run_off] = pair_off;
+            run_off++;
+            pair_off += sz * (sz - 1) / 2;
+        }
+    }
+    if (threadIdx.x == 0) S.base = atomicAdd(cursor, (unsigned long long)total);
     __syncthreads();
     const uint64_t base = S.base;
 
-    // runs emitted by their own thread
-    uint64_t o = base + my_off;
-    seen_big = 0;
-    for (int k = 0; k < kPer; k++) {
-        const int dg = d0 + k;
-        const uint32_t a = dg == 0 ? 0u : S.cnt[dg - 1], b = S.cnt[dg];
-        if (b - a < 2) continue;
-        for (uint32_t x = a; x < b;) {
-            uint64_t kv = rec[S.perm[x]] >> idbits;
-            uint32_t y = x + 1;
-            while (y < b && (rec[S.perm[y]] >> idbits) == kv) y++;
-            const uint32_t s = y - x;
-            bool mine = s >= 2;
-            if (s >= (uint32_t)kBigGroup && seen_big < 64) {
-                if ((listed >> seen_big) & 1ull) mine = false;
-                seen_big++;
-            }
-            if (mine)
-                for (uint32_t i = x; i < y; i++) {
-                    const uint64_t ai = rec[S.perm[i]] & idmask;
-                    for (uint32_t j = i + 1; j < y; j++) {
-                        if (o < cap) pairs[o] = pack_pair(ai, rec[S.perm[j]] & idmask, idbits);
-                        o++;
-                    }
+    // 4. pair t of the bucket -> run (binary search over the offsets) -> (i, j) inside the run
+    for (uint32_t t = threadIdx.x; t < total; t += kGroupThreads) {
+        uint32_t lo = 0, hi = nr - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (S.u.gr.poff[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const uint32_t run = S.u.gr.runs[lo];
+        const uint32_t s = (run >> 16) & 0x7fffu, x = run & 0xffffu;
+        const uint32_t l = t - S.u.gr.poff[lo];
+        uint32_t i = 0, j = 1;
+        if (s > 2) {
+            const float b2 = (float)(2 * s - 1);
+            int ii = (int)floorf((b2 - sqrtf(b2 * b2 - 8.0f * (float)l)) * 0.5f);
+            i = ii < 0 ? 0u : (uint32_t)ii;
+            while (i + 1 < s && (uint32_t)tri_row_start(i + 1, s) <= l) i++;
+            while (i > 0 && (uint32_t)tri_row_start(i, s) > l) i--;
+            j = i + 1 + (l - (uint32_t)tri_row_start(i, s));
+        }
+        uint32_t pi, pj;
+        if (run >> 31) {  // the run fills its digit: members are consecutive slots
+            pi = x + i;
+            pj = x + j;
+        } else {          // members are the slots of the digit with the head's hash
+            const uint64_t kv = rec[S.u.gr.perm[x]] >> idbits;
+            uint32_t mm = 0, y = x;
+            pi = pj = x;
+            for (; mm <= j; y++)
+                if ((rec[S.u.gr.perm[y]] >> idbits) == kv) {
+                    if (mm == i) pi = y;
+                    if (mm == j) pj = y;
+                    mm++;
                 }
-            x = y;
         }
-    }
-    // listed runs: the whole CTA, pair index t -> (i, j) inside the run
-    const uint64_t bo = base + total;
-    for (uint32_t g = 0; g < n_big; g++) {
-        const uint64_t s = S.big_size[g], x = S.big_start[g];
-        const uint64_t np = s * (s - 1) / 2;
-        for (uint64_t t = threadIdx.x; t < np; t += kGroupThreads) {
-            double b2 = (double)(2 * s - 1);
-            int64_t ii = (int64_t)floor((b2 - sqrt(b2 * b2 - 8.0 * (double)t)) * 0.5);
-            uint64_t i = ii < 0 ? 0 : (uint64_t)ii;
-            while (i + 1 < s && tri_row_start(i + 1, s) <= t) i++;
-            while (i > 0 && tri_row_start(i, s) > t) i--;
-            const uint64_t j = i + 1 + (t - tri_row_start(i, s));
-            const uint64_t q = bo + S.big_poff[g] + t;
-            if (q < cap) pairs[q] = pack_pair(rec[S.perm[x + i]] & idmask, rec[S.perm[x + j]] & idmask, idbits);
-        }
+        const uint64_t q = base + t;
+        if (q < cap)
+            pairs[q] = pack_pair(rec[S.u.gr.perm[pi]] & idmask, rec[S.u.gr.perm[pj]] & idmask, idbits);
     }
 }
 

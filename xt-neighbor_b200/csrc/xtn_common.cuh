@@ -149,6 +149,66 @@ XTN_HD int variant_count(u128 key, int L, int d) {
     return for_each_variant(key, L, d, CountOnly{});
 }
 
+// Position of the k-th (0-based) set bit of m (m has more than k set bits).
+XTN_HD int select_bit(uint32_t m, int k) {
+    int p = 0, c;
+    c = popc32(m & 0xffffu);
+    if (k >= c) { k -= c; m >>= 16; p += 16; }
+    c = popc32(m & 0xffu);
+    if (k >= c) { k -= c; m >>= 8; p += 8; }
+    c = popc32(m & 0xfu);
+    if (k >= c) { k -= c; m >>= 4; p += 4; }
+    c = popc32(m & 0x3u);
+    if (k >= c) { k -= c; m >>= 2; p += 2; }
+    c = (int)(m & 1u);
+    if (k >= c) p += 1;
+    return p;
+}
+
+// Run structure of a key: bits 0..31 = run starts (by position), bits 32..63 = which runs
+// (by run index) are at least two residues long.
+XTN_HD uint64_t key_run_info(u128 key, int L) {
+    const uint32_t rs = key_run_starts(key, L);
+    const uint32_t lmask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+    const uint32_t cont = ~rs & lmask;  // positions continuing a run
+    uint32_t longr = 0;
+    int j = 0;
+    for (uint32_t m = rs; m; m &= m - 1, j++) {
+        const int p = select_bit(m, 0);
+        if ((cont >> (p + 1)) & 1u) longr |= 1u << j;
+    }
+    return (uint64_t)rs | ((uint64_t)longr << 32);
+}
+
+// The v-th variant (0 <= v < variant_count) of a key for d <= 2, from its run structure: a
+// flat index over the run-prefix deletion sets, so variants can be produced in parallel. The
+// order differs from for_each_variant; the multiset is the same. v = 0 is the key; v = 1..R
+// delete the first residue of run v-1; then, for each run j in order, the pairs (first residue
+// of run j, q) with q the next residue of run j (when run j is long) or the first residue of
+// a later run, q ascending. Run j owns c_j = (R-1-j) + long_j pairs, so the pairs of runs
+// before j number j*(R-1) - j*(j-1)/2 + (long runs before j).
+XTN_HD u128 variant_at(u128 key, uint64_t info, int v) {
+    if (v == 0) return key;
+    const uint32_t rs = (uint32_t)info, longr = (uint32_t)(info >> 32);
+    const int R = popc32(rs);
+    if (v <= R) return key_del(key, select_bit(rs, v - 1));
+    const int w = v - R - 1;
+    // largest run j with pairs_before(j) <= w
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int before = mid * (R - 1) - mid * (mid - 1) / 2 + popc32(longr & ((1u << mid) - 1u));
+        if (before <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const int j = lo;
+    const int l = w - (j * (R - 1) - j * (j - 1) / 2 + popc32(longr & ((1u << j) - 1u)));
+    const int p = select_bit(rs, j);
+    const int lj = (int)((longr >> j) & 1u);
+    const int q = (lj && l == 0) ? p + 1 : select_bit(rs, j + 1 + l - lj);
+    return key_del(key_del(key, p), q - 1);
+}
+
 // Row i of a group of size s owns pairs (i, i+1..s-1); it starts at local index r(i).
 XTN_HD uint64_t tri_row_start(uint64_t i, uint64_t s) { return i * (2 * s - i - 1) / 2; }
 

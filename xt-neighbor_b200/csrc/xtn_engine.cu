@@ -55,7 +55,7 @@ constexpr int kThreads = 256;
 
 __global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
                        const int32_t* __restrict__ rows, int n, int d, u128* __restrict__ keys,
-                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt) {
+                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt, uint64_t* __restrict__ runinfo) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int r = rows ? rows[i] : i;
@@ -67,6 +67,7 @@ __global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __rest
     keys[i] = v;
     klen[i] = (uint8_t)Lk;
     vcnt[i] = (uint32_t)variant_count(v, Lk, d);
+    runinfo[i] = key_run_info(v, Lk);
 }
 
 __global__ void k_gen(const u128* __restrict__ keys, const uint8_t* __restrict__ klen,
@@ -283,11 +284,13 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
-    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB;
+    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
     bool attrs_set = false;
-    int bucket_bits_max = 15;
+    int bucket_bits_max = kMaxFirstLevelBits;
+    int scatter_ctas_per_sm = 2;
+    int group_tma = 1;
     uint32_t group_cap = kGroupCap;
     uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
     // results
@@ -439,9 +442,11 @@ static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t 
 static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_t V, uint64_t* Pc) {
     cudaStream_t s = c->stream;
     int b1 = 1;
-    while (b1 < c->bucket_bits_max && (V >> b1) > 3000) b1++;
+    while (b1 < c->bucket_bits_max && (V >> b1) > 7000) b1++;
     const int nb = 1 << b1;
-    const int ntiles = c->sms * (int)std::max<int64_t>(1, ((int64_t)n + (int64_t)c->sms * 8192 - 1) / ((int64_t)c->sms * 8192));
+    const int per_sm = c->scatter_ctas_per_sm;  // resident count/scatter CTAs per SM
+    const int64_t wave = (int64_t)c->sms * per_sm;
+    const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
     const int tile = (n + ntiles - 1) / ntiles;
     const size_t hist_smem = sizeof(uint32_t) * nb;
     XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)ntiles * nb));
@@ -451,8 +456,12 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
     XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
     if (!c->attrs_set) {
-        XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
         c->attrs_set = true;
     }
@@ -461,9 +470,14 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
-                                     P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
-                                     P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+    if (d <= 2 && b1 <= 10)
+        XTN_LAUNCH("bucket_scatter", k_bucket_scatter_staged<<<ntiles, kStageThreads, sizeof(StageSmem), s>>>(
+                                         P<u128>(c->keys), P<uint64_t>(c->runinfo), P<uint64_t>(c->voff), n, tile, b1,
+                                         idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+    else
+        XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
+                                         P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
+                                         P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
 
@@ -483,7 +497,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_CK(cudaStreamSynchronize(s));
     memcpy(cnt, c->h_scalar, 32);
     if (cnt[1] > 0) {
-        XTN_LAUNCH("bucket_split", k_bucket_split<<<cnt[1], 1024, 0, s>>>(
+        XTN_LAUNCH("bucket_split", k_bucket_split_staged<<<cnt[1], kStageThreads, sizeof(StageSmem), s>>>(
                                        P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
                                        P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
         XTN_CK(cudaGetLastError());
@@ -492,21 +506,27 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         memcpy(cnt, c->h_scalar, 32);
     }
     XTN_CK(cudaEventRecord(c->ev[3], s));
-    const uint32_t ndesc = cnt[0], nfall = cnt[3];
+    const uint32_t ndesc = cnt[0];
 
-    // group every listed bucket in shared memory
+    // group every listed bucket in shared memory; buckets with too many runs are appended
+    // to the fallback list (counter 3)
     uint64_t cap = std::max<uint64_t>({c->last_pc + c->last_pc / 4, V / 16, (uint64_t)1 << 20});
     uint64_t total = 0;
+    const uint32_t nfall_split = cnt[3];
     for (int attempt = 0; attempt < 2; attempt++) {
         XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * cap + 64));
         XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
+        XTN_CK(cudaMemsetAsync(P<unsigned int>(c->bcnt) + 3, 0, 4, s));
+        XTN_CK(cudaMemcpyAsync(P<unsigned int>(c->bcnt) + 3, &nfall_split, 4, cudaMemcpyHostToDevice, s));
         if (ndesc > 0)
             XTN_LAUNCH("bucket_group", k_bucket_group<<<ndesc, kGroupThreads, sizeof(GroupSmem), s>>>(
                                            P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
                                            P<uint64_t>(c->pairA), cap, P<unsigned long long>(c->counter),
-                                           P<unsigned int>(c->counter) + 2));
+                                           P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
+                                           P<unsigned int>(c->bcnt) + 3));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
         total = c->h_scalar[0];
         if ((c->h_scalar[1] & 0xffffffffu) != 0) {
@@ -516,6 +536,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         if (total <= cap) break;
         cap = total;
     }
+    const uint32_t nfall = (uint32_t)(c->h_scalar[3] >> 32);  // bcnt[3]: high half of the second word
     c->stats.n_groups = ndesc;
     XTN_CK(cudaEventRecord(c->ev[4], s));
 
@@ -526,8 +547,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         for (const BucketDesc& f : fl) {
             XTN_TRY(ensure(c->fbA, sizeof(uint64_t) * f.size + 64));
             XTN_TRY(ensure(c->fbB, sizeof(uint64_t) * f.size + 64));
-            XTN_CK(cudaMemcpyAsync(c->fbA.p, P<uint64_t>(c->recB) + f.start, sizeof(uint64_t) * f.size,
-                                   cudaMemcpyDeviceToDevice, s));
+            const uint64_t* srcbuf = f.src ? P<uint64_t>(c->recB) : P<uint64_t>(c->recA);
+            XTN_CK(cudaMemcpyAsync(c->fbA.p, srcbuf + f.start, sizeof(uint64_t) * f.size, cudaMemcpyDeviceToDevice, s));
             uint64_t* sorted = nullptr;
             XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, "fallback_sort_upsweep",
                              "fallback_sort_downsweep"));
@@ -559,8 +580,9 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->klen, (size_t)n));
     XTN_TRY(ensure(c->vcnt, sizeof(uint32_t) * n));
     XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (n + 1)));
+    XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * n));
     XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen),
-                                             P<uint32_t>(c->vcnt)));
+                                             P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo)));
     XTN_CK(cudaGetLastError());
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n));
     XTN_CK(cudaEventRecord(c->ev[1], s));
@@ -1040,7 +1062,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->pairA,   &c->pairB,    &c->dist,      &c->flag,      &c->fpos,     &c->scratch64,
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
-                      &c->bcnt,    &c->fbA,      &c->fbB};
+                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1117,8 +1139,10 @@ int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, 
 int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     if (!c || !name) return XTN_ERR_ARG;
     if (!strcmp(name, "engine") && (v == 0 || v == 1)) c->engine = (int)v;
-    else if (!strcmp(name, "bucket_bits_max") && v >= 1 && v <= 15) c->bucket_bits_max = (int)v;
+    else if (!strcmp(name, "bucket_bits_max") && v >= 1 && v <= 14) c->bucket_bits_max = (int)v;
     else if (!strcmp(name, "group_cap") && v >= 2 && v <= kGroupCap) c->group_cap = (uint32_t)v;
+    else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 1 && v <= 4) c->scatter_ctas_per_sm = (int)v;
+    else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
         return XTN_ERR_ARG;

@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libxtn_b200.so")
+LIB_PATH = os.environ.get("XTN_LIB") or os.path.join(HERE, "lib", "libxtn_b200.so")
 SYNTH_PATH = os.path.join(HERE, "lib", "libxtn_synth.so")
 CLI_PATH = os.path.join(HERE, "bin", "xt_neighbor")
 
