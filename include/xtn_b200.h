@@ -152,6 +152,33 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *                     (default), 0 = with plain 16-byte loads from every thread */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
+/* ------------------------------------------------------------------ search without allocation */
+
+/* Nearest-neighbour search that allocates nothing. It has no counterpart in the reference.
+ * Meant for callers that cannot allocate device memory while they run:
+ *   - a host whose framework caching allocator already holds the device memory;
+ *   - a latency-critical loop that cannot take the synchronisation of cudaMalloc/cudaFree;
+ *   - a plugin host that forbids allocation on the call path.
+ * The caller passes device pointers: the sequences (as in xtn_perform) and output buffers of
+ * out_cap pairs and distances. The result is the same as xtn_context_nn_device's, written to
+ * the caller's buffers, with its length in *n_out (a host pointer).
+ *
+ * Limits and behaviour:
+ *   - Scratch comes from one fixed 32 MiB device array inside the library, held by every GPU
+ *     that loads it until the process exits.
+ *   - At most 4096 sequences. Inputs whose variants, groups or candidate pairs do not fit the
+ *     array, or whose result exceeds out_cap, return XTN_ERR_LIMIT with a message. For an
+ *     oversized result, *n_out holds the needed size.
+ *   - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) on the current
+ *     device, and returns after the stream has drained.
+ *   - The first call on a device resolves the array's device address, so make that call before
+ *     any stream capture.
+ *   - Every call reuses the same array (the call resets what must start at zero), so calls that
+ *     overlap on the GPU, from any thread or stream, race. */
+int xtn_nn_search_static(const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets, int32_t n_seqs,
+                         xtn_int2* d_out_pairs, int8_t* d_out_distances, int64_t out_cap, int64_t* n_out,
+                         void* stream);
+
 /* Text of the last error on the calling thread ("" if none). */
 const char* xtn_last_error(void);
 

@@ -1199,3 +1199,175 @@ int xtn_perform(const xtn_args* args, const char* seqs, const uint32_t* offsets,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ search without allocation
+// Some callers cannot allocate device memory while they run: a host whose framework caching
+// allocator already owns the device's memory (so a raw cudaMalloc can fail or fragment it),
+// a latency-critical loop that must not pay the device-wide synchronisation cudaMalloc and
+// cudaFree can cause, or a plugin host whose policy forbids allocation on the call path. For
+// them, xtn_nn_search_static runs the nearest-neighbour search (the sort-engine kernels)
+// with all of its scratch carved out of one file-scope device array of fixed size. The caller
+// passes the inputs and the output buffers; the entry point calls no cudaMalloc, cudaFree or
+// allocating library routine.
+namespace xtn {
+
+constexpr size_t kStaticArenaBytes = size_t(32) << 20;  // 32 MiB, held by every GPU that loads the library
+constexpr int kStaticMaxSeqs = 4096;
+constexpr int kStaticMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_static_arena[kStaticArenaBytes];
+
+// Device address of g_static_arena per device (the host-side name is only a stand-in),
+// resolved once per device with that device current.
+static std::mutex g_static_mu;
+static void* g_static_addr[kStaticMaxDevices] = {};
+
+static int static_arena(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_arena);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            set_err(std::string("cudaGetSymbolAddress of the static scratch array failed: ") + cudaGetErrorString(e));
+            return XTN_ERR_CUDA;
+        }
+        g_static_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_static_addr[device]);
+    return XTN_SUCCESS;
+}
+
+// Bump allocator over the arena.
+struct Carver {
+    unsigned char* base;
+    size_t used, cap;
+    template <typename T>
+    bool take(T** p, size_t count) {
+        size_t bytes = (sizeof(T) * count + 64 + 255) & ~size_t(255);
+        if (used + bytes > cap) return false;
+        *p = reinterpret_cast<T*>(base + used);
+        used += bytes;
+        return true;
+    }
+};
+
+static int arena_full(const char* what) {
+    set_err(std::string("input exceeds the static scratch array (") + std::to_string(kStaticArenaBytes >> 20) +
+            " MiB) at: " + what);
+    return XTN_ERR_LIMIT;
+}
+
+static int read_u64(const void* d, size_t bytes, cudaStream_t s, uint64_t* out) {
+    uint64_t v = 0;
+    XTN_CK(cudaMemcpyAsync(&v, d, bytes, cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaStreamSynchronize(s));
+    *out = v;
+    return XTN_SUCCESS;
+}
+
+static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, int d, int measure, xtn_int2* out_pairs,
+                            int8_t* out_dist, int64_t out_cap, int64_t* n_out, cudaStream_t s, unsigned char* arena) {
+    Carver cv{arena, 0, kStaticArenaBytes};
+    const int idbits = id_bits_for(n);
+    u128* keys;
+    uint8_t* klen;
+    uint32_t* vcnt;
+    uint64_t *voff, *runinfo, *scan64;
+    unsigned long long* counter;
+    if (!cv.take(&keys, n) || !cv.take(&klen, n) || !cv.take(&vcnt, n) || !cv.take(&voff, n + 1) ||
+        !cv.take(&runinfo, n) || !cv.take(&scan64, scan_scratch_elems(n)) || !cv.take(&counter, 2))
+        return arena_full("sequence tables");
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo));
+    XTN_CK(cudaGetLastError());
+    scan_exclusive<uint32_t, uint64_t>(vcnt, voff, n, scan64, s);
+    uint64_t V = 0;
+    XTN_TRY(read_u64(voff + n, 8, s, &V));
+    uint64_t *recA, *recB;
+    uint32_t* rscratch;
+    if (!cv.take(&recA, V) || !cv.take(&recB, V) || !cv.take(&rscratch, radix_scratch_elems((int64_t)V)))
+        return arena_full("variant records");
+    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(keys, klen, voff, n, d, idbits, recA));
+    uint64_t* recs = radix_sort_u64(recA, recB, (int64_t)V, idbits, 64, rscratch, s, "key_sort_upsweep",
+                                    "key_sort_downsweep");
+    // groups: at most one per two records
+    const int64_t gcap = (int64_t)(V / 2 + 1);
+    uint64_t *gstart, *gcnt, *goff;
+    uint32_t* gsize;
+    if (!cv.take(&gstart, gcap) || !cv.take(&gsize, gcap) || !cv.take(&gcnt, gcap + 1) || !cv.take(&goff, gcap + 1))
+        return arena_full("groups");
+    XTN_CK(cudaMemsetAsync(counter, 0, 16, s));
+    XTN_LAUNCH("find_groups", k_find_groups<<<blocks_for((int64_t)V), kThreads, 0, s>>>(recs, (int64_t)V, idbits,
+                                                                                         gstart, gsize, counter, gcap));
+    XTN_CK(cudaGetLastError());
+    uint64_t G = 0, Pc = 0;
+    XTN_TRY(read_u64(counter, 8, s, &G));
+    uint64_t* scanG;
+    if (!cv.take(&scanG, scan_scratch_elems((int64_t)G + 1))) return arena_full("group scan");
+    if (G > 0) {
+        XTN_LAUNCH("pair_counts", k_pair_counts<<<blocks_for((int64_t)G), kThreads, 0, s>>>(gsize, (int64_t)G, gcnt));
+        scan_exclusive<uint64_t, uint64_t>(gcnt, goff, (int64_t)G, scanG, s);
+        XTN_TRY(read_u64(goff + G, 8, s, &Pc));
+    }
+    uint64_t *pairA, *pairB;
+    uint32_t *pscratch, *fpos;
+    int8_t* dist;
+    uint8_t* flag;
+    if (Pc >= (uint64_t)UINT32_MAX || !cv.take(&pairA, Pc) || !cv.take(&pairB, Pc) || !cv.take(&dist, Pc) ||
+        !cv.take(&flag, Pc) || !cv.take(&fpos, Pc + 1) ||
+        !cv.take(&pscratch, std::max<int64_t>(radix_scratch_elems((int64_t)Pc), scan_scratch_elems((int64_t)Pc))))
+        return arena_full("candidate pairs");
+    uint64_t nout = 0;
+    if (Pc > 0) {
+        uint64_t threads = (Pc + kEmitPer - 1) / kEmitPer;
+        XTN_LAUNCH("emit", k_emit<<<blocks_for((int64_t)threads), kThreads, 0, s>>>(recs, gstart, gsize, goff,
+                                                                                      (int64_t)G, Pc, idbits, pairA));
+        uint64_t* pairs = Pc > 1 ? radix_sort_u64(pairA, pairB, (int64_t)Pc, 0, 2 * idbits, pscratch, s,
+                                                  "pair_sort_upsweep", "pair_sort_downsweep")
+                                 : pairA;
+        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars,
+                                                                                    offs, nullptr, d, measure, dist, flag));
+        scan_exclusive<uint8_t, uint32_t>(flag, fpos, (int64_t)Pc, pscratch, s);
+        XTN_TRY(read_u64(fpos + Pc, 4, s, &nout));
+        if ((int64_t)nout > out_cap) {
+            *n_out = (int64_t)nout;
+            set_err("output buffer too small: " + std::to_string(nout) + " pairs");
+            return XTN_ERR_LIMIT;
+        }
+        if (nout > 0)
+            XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits,
+                                                                                          dist, flag, fpos, out_pairs,
+                                                                                          out_dist));
+    }
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaStreamSynchronize(s));
+    *n_out = (int64_t)nout;
+    return XTN_SUCCESS;
+}
+
+}  // namespace xtn
+
+extern "C" int xtn_nn_search_static(const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets, int32_t n_seqs,
+                                    xtn_int2* d_out_pairs, int8_t* d_out_distances, int64_t out_cap, int64_t* n_out,
+                                    void* stream) {
+    if (!d_seqs || !d_offsets || !n_out || n_seqs < 1 || out_cap < 0 || (out_cap > 0 && (!d_out_pairs || !d_out_distances))) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    if (n_seqs > kStaticMaxSeqs) {
+        set_err("xtn_nn_search_static accepts at most " + std::to_string(kStaticMaxSeqs) + " sequences (got " +
+                std::to_string(n_seqs) + ")");
+        return XTN_ERR_LIMIT;
+    }
+    int device = 0;
+    XTN_CK(cudaGetDevice(&device));
+    if (device < 0 || device >= kStaticMaxDevices) {
+        set_err("device index beyond the static scratch table");
+        return XTN_ERR_LIMIT;
+    }
+    unsigned char* arena = nullptr;
+    XTN_TRY(static_arena(device, &arena));
+    return nn_search_static(reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n_seqs, args->distance, args->measure,
+                            d_out_pairs, d_out_distances, out_cap, n_out, static_cast<cudaStream_t>(stream), arena);
+}
