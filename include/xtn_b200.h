@@ -144,9 +144,9 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *                     1 = full radix sort of the variant records (the plain comparison form)
  *   "bucket_bits_max" 1..14: upper bound on log2(number of first-level buckets) (default 9;
  *                     above 10 the first-level scatter stores records one by one)
- *   "group_cap"       2..6144: largest bucket grouped in shared memory; larger ones are split
+ *   "group_cap"       2..4096: largest bucket grouped in shared memory; larger ones are split
  *                     by further hash bits, and what still does not fit is grouped by sorting
- *                     (default 6144)
+ *                     (default 4096)
  *   "scatter_ctas_per_sm" 1..4: first-level tiles per SM (default 2)
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
  *                     (default), 0 = with plain 16-byte loads from every thread */

@@ -53,6 +53,25 @@ int hc_variants_flat(const char* s, int L, int d, char* out, int cap) {
     return n;
 }
 
+// 1 when the staged scatter's tasks (for_each_task_variant, t < 2*ceil(R/2)) produce every
+// flat variant index exactly once, each with variant_at's value.
+int hc_task_variants_ok(const char* s, int L, int d) {
+    u128 key = pack(s, L);
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    const int n = variant_count(key, Lk, d);
+    const uint64_t info = key_run_info(key, Lk);
+    const int R = popc32((uint32_t)info), T = 2 * ((R + 1) / 2);
+    int seen[1024] = {0};
+    bool ok = n <= 1024;
+    for (int t = 0; t < T && ok; t++)
+        for_each_task_variant(key, Lk, info, d, t, [&](int v, u128 k) {
+            if (v < 0 || v >= n || k != variant_at(key, info, v)) ok = false;
+            else seen[v]++;
+        });
+    for (int v = 0; v < n && ok; v++) ok = seen[v] == 1;
+    return ok ? 1 : 0;
+}
+
 int hc_variant_count(const char* s, int L, int d) {
     int Lk = L < kKeyLen ? L : kKeyLen;
     return variant_count(pack(s, L), Lk, d);

@@ -75,6 +75,14 @@ def test_flat_variant_index_matches_enumeration(hc):
             assert sorted(flat) == sorted(ref), (s, d)
 
 
+def test_task_partition_of_variants(hc):
+    """The staged scatter's balanced tasks cover every flat variant index exactly once."""
+    rng = np.random.default_rng(23)
+    for s in rand_seqs(rng, 2000, 1, 26):
+        for d in (1, 2):
+            assert hc.hc_task_variants_ok(s.encode(), len(s), d) == 1, (s, d)
+
+
 def test_key_delete(hc):
     rng = np.random.default_rng(5)
     for s in rand_seqs(rng, 200, 1, 19):

@@ -8,8 +8,8 @@
 //                              (variants generated and hashed, not stored)
 //   offsets  k_bucket_colscan  per bucket: exclusive prefix over tiles, bucket totals
 //   scatter  k_bucket_scatter_staged
-//                              the variants again, 8192 at a time in shared memory (one
-//                              variant per thread from a flat index), counting-sorted by
+//                              the variants again, 8192 at a time in shared memory (made by
+//                              balanced tasks, for_each_task_variant), counting-sorted by
 //                              bucket there and written out as contiguous runs: every
 //                              global store is part of a coalesced run, so L2 receives
 //                              whole sectors instead of read-modify-writing partial ones
@@ -32,22 +32,25 @@
 namespace xtn {
 
 constexpr int kBucketThreads = 512;    // k_bucket_count and the direct scatter (d > 2)
-constexpr int kStageThreads = 1024;    // staged scatter / split
-constexpr int kStageChunk = 8192;      // records per staged chunk
+constexpr int kStageThreads = 512;     // staged scatter / split (two CTAs per SM)
+constexpr int kStageChunk = 4096;      // records per staged chunk
 constexpr int kMaxFan = 1024;          // fan-out of one staged partition
-// First-level fan-out: each staged chunk of 8192 records then leaves runs of ~16 records per
-// bucket (128 bytes), enough for whole-sector writes.
+constexpr int kFanPer = kMaxFan / kStageThreads;
+constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp histograms
+// First-level fan-out: each staged chunk of 4096 records leaves runs of ~8 records (64 bytes)
+// per bucket; consecutive chunks of one CTA extend the same runs, so their boundary sectors
+// complete in L2.
 constexpr int kMaxFirstLevelBits = 9;
 constexpr int kGroupThreads = 512;
-constexpr int kGroupCap = 6144;        // records a grouping CTA holds in shared memory
-constexpr int kBitmapLog = 17;         // hash bits of the "seen" / "seen twice" bitmaps
+constexpr int kGroupCap = 4096;        // records a grouping CTA holds in shared memory
+constexpr int kBitmapLog = 16;         // hash bits of the "seen" / "seen twice" bitmaps
 constexpr int kBitmapBits = 1 << kBitmapLog;
 constexpr int kBitmapWords = kBitmapBits / 32;
 constexpr int kDigitBits = 11;         // hash bits of the candidates' counting sort
 constexpr int kDigits = 1 << kDigitBits;
-// Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to 3072;
+// Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to 2048;
 // buckets with more than this go to the sort-based fallback).
-constexpr int kMaxRuns = 2048;
+constexpr int kMaxRuns = 1024;
 constexpr uint32_t kWaitLimit = 1u << 26;  // bound on mbarrier polls
 
 // Descriptor of one bucket (or sub-bucket) handed to the grouping kernel.
@@ -137,6 +140,8 @@ struct StageSmem {
     uint32_t cnt[kMaxFan];
     uint32_t lstart[kMaxFan];
     uint32_t gcur[kMaxFan];        // next global position of each bucket for this CTA
+    uint16_t rel_v[kStageChunk];   // voff of the chunk's sequences, relative to the chunk
+    uint16_t rel_t[kStageChunk];   // toff of the chunk's sequences, relative to the chunk
     uint32_t warp_sums[kStageThreads / 32 + 1];
     uint32_t seq_end;
 };
@@ -148,12 +153,21 @@ __device__ __forceinline__ void stage_partition(StageSmem& S, int nb, uint32_t m
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[S.bkt[p]], 1u);
     __syncthreads();
-    uint32_t tot;
-    const uint32_t v = threadIdx.x < (unsigned)nb ? S.cnt[threadIdx.x] : 0u;
-    const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(v, &tot, S.warp_sums);
-    if (threadIdx.x < (unsigned)nb) {
-        S.lstart[threadIdx.x] = ex;
-        S.cnt[threadIdx.x] = ex;
+    {
+        uint32_t tot, loc[kFanPer], sum = 0;
+        const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++) {
+            loc[k] = sum;
+            sum += (b0 + k < nb) ? S.cnt[b0 + k] : 0u;
+        }
+        const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++)
+            if (b0 + k < nb) {
+                S.lstart[b0 + k] = ex + loc[k];
+                S.cnt[b0 + k] = ex + loc[k];
+            }
     }
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
@@ -172,12 +186,23 @@ __device__ __forceinline__ void stage_partition(StageSmem& S, int nb, uint32_t m
     __syncthreads();
 }
 
-// First-level scatter for d <= 2 (flat variant index; a sequence has at most 172 variants).
-// runinfo[i] is key_run_info of sequence i.
-__global__ void __launch_bounds__(kStageThreads, 1) k_bucket_scatter_staged(
-    const u128* __restrict__ keys, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ voff, int n,
-    int tile, int b1, int idbits, const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart,
-    uint64_t* __restrict__ recs) {
+// Tasks per sequence for the staged scatter (for_each_task_variant): 2 * ceil(runs / 2).
+__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint32_t* __restrict__ tcnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t R = (uint32_t)popc32((uint32_t)runinfo[i]);
+    tcnt[i] = 2u * ((R + 1u) >> 1);
+}
+
+// First-level scatter for d <= 2. The tile's sequences go through shared memory 4096
+// variants at a time; each chunk's variants are produced by balanced tasks (about R/2 + 1
+// variants each, one key deletion and one hash per variant) written at their flat index, then
+// the staged partition writes them out by bucket. runinfo[i] is key_run_info of sequence i;
+// toff is the exclusive scan of k_task_counts.
+__global__ void __launch_bounds__(kStageThreads, 2) k_bucket_scatter_staged(
+    const u128* __restrict__ keys, const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo,
+    const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, int n, int tile, int d, int b1, int idbits,
+    const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
     const int nb = 1 << b1;
@@ -187,27 +212,33 @@ __global__ void __launch_bounds__(kStageThreads, 1) k_bucket_scatter_staged(
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
-    constexpr int kPer = kStageChunk / kStageThreads;  // 8 slots per thread in the slot scan
+    constexpr int kPer = kStageChunk / kStageThreads;  // task slots per thread in the scan
     __syncthreads();
     for (int s0 = t0; s0 < t1;) {
-        if (threadIdx.x == 0) {
-            // largest s1 <= t1 with voff[s1] - voff[s0] <= chunk (at least s0 + 1)
-            int lo = s0 + 1, hi = min(t1, s0 + kStageChunk);
-            const uint64_t lim = voff[s0] + kStageChunk;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (voff[mid] <= lim) lo = mid;
-                else hi = mid - 1;
-            }
-            S.seq_end = (uint32_t)lo;
-        }
+        // chunk end: the largest s1 <= t1 with voff[s1] - voff[s0] <= chunk, found by all threads
+        // reading consecutive voff entries (coalesced) instead of one thread's binary search
+        const uint64_t base = voff[s0], tbase = toff[s0];
+        if (threadIdx.x == 0) S.seq_end = (uint32_t)(s0 + 1);
         for (int f = threadIdx.x; f < kStageChunk; f += kStageThreads) S.sbkt[f] = 0;
         __syncthreads();
+        for (int r0 = s0 + 1; r0 <= t1; r0 += kStageThreads) {
+            const int idx = r0 + threadIdx.x;
+            if (idx <= t1 && voff[idx] - base <= (uint64_t)kStageChunk) atomicMax(&S.seq_end, (uint32_t)idx);
+            __syncthreads();
+            if ((int)S.seq_end < r0 + kStageThreads - 1 || r0 + kStageThreads > t1) break;
+            __syncthreads();
+        }
         const int s1 = (int)S.seq_end;
-        const uint64_t base = voff[s0];
         const uint32_t m = (uint32_t)(voff[s1] - base);
-        // slot -> owning sequence: mark each sequence's first slot, then an inclusive scan
-        for (int i = s0 + 1 + threadIdx.x; i < s1; i += kStageThreads) S.sbkt[voff[i] - base] = 1;
+        const uint32_t nt = (uint32_t)(toff[s1] - tbase);  // <= m (a sequence has >= its task count of variants)
+        // per-sequence offsets into smem; task -> owning sequence: mark each sequence's first
+        // task, then an inclusive scan
+        for (int i = s0 + threadIdx.x; i < s1; i += kStageThreads) {
+            const uint32_t rv = (uint32_t)(voff[i] - base), rt = (uint32_t)(toff[i] - tbase);
+            S.rel_v[i - s0] = (uint16_t)rv;
+            S.rel_t[i - s0] = (uint16_t)rt;
+            if (i > s0) S.sbkt[rt] = 1;
+        }
         __syncthreads();
         {
             const int f0 = threadIdx.x * kPer;
@@ -223,12 +254,17 @@ __global__ void __launch_bounds__(kStageThreads, 1) k_bucket_scatter_staged(
             for (int k = 0; k < kPer; k++) S.sbkt[f0 + k] = (uint16_t)(ex + loc[k]);
         }
         __syncthreads();
-        for (uint32_t f = threadIdx.x; f < m; f += kStageThreads) {
-            const int i = s0 + S.sbkt[f];
-            const int v = (int)(base + f - voff[i]);
-            const uint64_t h = key_hash(variant_at(keys[i], runinfo[i], v));
-            S.bkt[f] = (uint16_t)(h >> shift);
-            S.rec[f] = ((h << b1) & hi_mask) | (uint64_t)i;
+        for (uint32_t tau = threadIdx.x; tau < nt; tau += kStageThreads) {
+            const int li = S.sbkt[tau];
+            const int i = s0 + li;
+            const int t = (int)(tau - S.rel_t[li]);
+            const uint32_t vb = S.rel_v[li];
+            const uint64_t id = (uint64_t)i;
+            for_each_task_variant(keys[i], klen[i], runinfo[i], d, t, [&](int v, u128 k) {
+                const uint64_t h = key_hash(k);
+                S.bkt[vb + v] = (uint16_t)(h >> shift);
+                S.rec[vb + v] = ((h << b1) & hi_mask) | id;
+            });
         }
         __syncthreads();
         stage_partition(S, nb, m, recs);
@@ -288,7 +324,7 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
 // sub-bucket descriptors, then the bucket's records, chunk by chunk, through the staged
 // partition into buffer B at the same range. Sub-buckets that fit are listed for grouping;
 // larger ones go to the fallback list.
-__global__ void __launch_bounds__(kStageThreads, 1) k_bucket_split_staged(
+__global__ void __launch_bounds__(kStageThreads, 2) k_bucket_split_staged(
     const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t group_cap,
     BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -296,27 +332,73 @@ __global__ void __launch_bounds__(kStageThreads, 1) k_bucket_split_staged(
     const SplitJob job = jobs[blockIdx.x];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;
-    for (int i = threadIdx.x; i < nsub; i += kStageThreads) S.cnt[i] = 0;
+    const bool priv = nsub <= kPrivFan;
+    // histogram: per-warp copies (in `sorted`, unused until the first chunk) for small fan-outs
+    uint32_t* hist = priv ? reinterpret_cast<uint32_t*>(S.sorted) + (threadIdx.x >> 5) * kPrivFan : S.cnt;
+    for (int i = threadIdx.x; i < (priv ? kPrivFan * (kStageThreads / 32) : nsub); i += kStageThreads)
+        (priv ? reinterpret_cast<uint32_t*>(S.sorted) : S.cnt)[i] = 0;
     __syncthreads();
     const uint64_t* src = in + job.start;
-    for (uint32_t i = threadIdx.x; i < job.size; i += kStageThreads) atomicAdd(&S.cnt[src[i] >> shift], 1u);
+    {
+        // 16-byte loads, four in flight per thread (job.start is 8-byte aligned: peel one)
+        const uint32_t lead = (uint32_t)(((uintptr_t)src & 15u) >> 3);
+        if (lead && threadIdx.x == 0 && job.size > 0) atomicAdd(&hist[src[0] >> shift], 1u);
+        const uint32_t nv = (job.size - lead) >> 1;
+        const uint4* v = reinterpret_cast<const uint4*>(src + lead);
+        uint32_t i = threadIdx.x;
+        for (; i + 3 * kStageThreads < nv; i += 4 * kStageThreads) {
+            const uint4 w[4] = {__ldg(v + i), __ldg(v + i + kStageThreads), __ldg(v + i + 2 * kStageThreads),
+                                __ldg(v + i + 3 * kStageThreads)};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                atomicAdd(&hist[(((uint64_t)w[k].y << 32) | w[k].x) >> shift], 1u);
+                atomicAdd(&hist[(((uint64_t)w[k].w << 32) | w[k].z) >> shift], 1u);
+            }
+        }
+        for (; i < nv; i += kStageThreads) {
+            const uint4 a = __ldg(v + i);
+            atomicAdd(&hist[(((uint64_t)a.y << 32) | a.x) >> shift], 1u);
+            atomicAdd(&hist[(((uint64_t)a.w << 32) | a.z) >> shift], 1u);
+        }
+        if (threadIdx.x == 0 && ((job.size - lead) & 1u)) atomicAdd(&hist[src[job.size - 1] >> shift], 1u);
+    }
     __syncthreads();
-    uint32_t tot;
-    const uint32_t v = threadIdx.x < (unsigned)nsub ? S.cnt[threadIdx.x] : 0u;
-    const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(v, &tot, S.warp_sums);
-    if (threadIdx.x < (unsigned)nsub) {
-        S.gcur[threadIdx.x] = (uint32_t)job.start + ex;
-        if (v >= 2) {
-            BucketDesc bd{job.start + ex, v, 1};
-            if (v <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
-            else fallback[atomicAdd(&counters[3], 1u)] = bd;
+    if (priv) {
+        for (int b = threadIdx.x; b < nsub; b += kStageThreads) {
+            uint32_t t = 0;
+            for (int w = 0; w < kStageThreads / 32; w++) t += reinterpret_cast<uint32_t*>(S.sorted)[w * kPrivFan + b];
+            S.cnt[b] = t;
+        }
+        __syncthreads();
+    }
+    {
+        uint32_t tot, loc[kFanPer], sum = 0;
+        const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++) {
+            loc[k] = sum;
+            sum += (b0 + k < nsub) ? S.cnt[b0 + k] : 0u;
+        }
+        const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++) {
+            const int b = b0 + k;
+            if (b >= nsub) continue;
+            const uint32_t c = S.cnt[b], st = ex + loc[k];
+            S.gcur[b] = (uint32_t)job.start + st;
+            if (c >= 2) {
+                BucketDesc bd{job.start + st, c, 1};
+                if (c <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
+                else fallback[atomicAdd(&counters[3], 1u)] = bd;
+            }
         }
     }
     __syncthreads();
     for (uint32_t c0 = 0; c0 < job.size; c0 += kStageChunk) {
         const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
+#pragma unroll 4
         for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
-            const uint64_t r = src[c0 + p];
+            const uint64_t r = __ldg(src + c0 + p);
             S.rec[p] = r;
             S.bkt[p] = (uint16_t)(r >> shift);
         }
@@ -326,7 +408,7 @@ __global__ void __launch_bounds__(kStageThreads, 1) k_bucket_split_staged(
 }
 
 // ------------------------------------------------------------------ group
-// Shared-memory layout of k_bucket_group (about 100 KB: two CTAs per SM). The two bitmaps
+// Shared-memory layout of k_bucket_group (about 65 KB: three CTAs per SM). The two bitmaps
 // are only needed until the candidates are known; the grouping arrays reuse their space.
 struct GroupSmem {
     uint64_t rec[kGroupCap + 2];  // bucket records (+ alignment slack)
@@ -368,7 +450,7 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 // Groups one bucket. Records of equal hash (record >> idbits) form a run; every pair of
 // positions in a run is written as (min id << idbits) | max id.
 //   1. a two-bitmap filter over kBitmapBits hash bits keeps only records that can have a
-//      partner (every record of a run of >= 2 survives; ~1 in 40 singletons does too);
+//      partner (every record of a run of >= 2 survives; ~1 in 20 singletons does too);
 //   2. the survivors are counting-sorted by kDigitBits further hash bits;
 //   3. each survivor checks its digit: it heads a run when no earlier survivor of the digit
 //      has its hash, and the run's size is the number with that hash (two passes: count,
@@ -377,7 +459,7 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 //      over its threads. Entries at or past `cap` are counted but not written, so the caller
 //      can grow the buffer to the exact size and run again.
 // A bucket with more than kMaxRuns runs is appended to `overflow` (grouped later by sorting).
-__global__ void __launch_bounds__(kGroupThreads, 2) k_bucket_group(const BucketDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketDesc* __restrict__ descs,
                                                                      const uint64_t* __restrict__ buf_a,
                                                                      const uint64_t* __restrict__ buf_b, int idbits,
                                                                      uint64_t* __restrict__ pairs, uint64_t cap,

@@ -209,6 +209,60 @@ XTN_HD u128 variant_at(u128 key, uint64_t info, int v) {
     return key_del(key_del(key, p), q - 1);
 }
 
+// Pairs (two-deletion variants) owned by runs 0..j-1 in variant_at's order.
+XTN_HD int pairs_before_run(int j, int R, uint32_t longr) {
+    return j * (R - 1) - j * (j - 1) / 2 + popc32(longr & ((1u << j) - 1u));
+}
+
+// Task t (0 <= t < 2*ceil(R/2)) of a key's d <= 2 variants, for parallel generation with even work:
+// tasks 2j and 2j+1 share the variants of runs j and R-1-j (the single deletion of each run and
+// its pairs; about R+1 variants together), split into two halves; task 0 also emits the key
+// itself. f(v, key) is called with each variant's flat index (variant_at's order) and value.
+template <class F>
+XTN_HD void for_each_task_variant(u128 key, int L, uint64_t info, int d, int t, F&& f) {
+    const uint32_t rs = (uint32_t)info, longr = (uint32_t)(info >> 32);
+    const uint32_t lmask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+    const int R = popc32(rs);
+    const bool two = d >= 2 && L >= 2;
+    if (t == 0) f(0, key);
+    const int jA = t >> 1, jB = R - 1 - jA;
+    // items of one run: the single deletion, then its pairs in ascending q
+    int wA, wB = 0;
+    uint32_t allowA = 0, allowB = 0;
+    auto allowed = [&](int j, int p) -> uint32_t {
+        uint32_t a = rs & lmask & ~((2u << p) - 1u);
+        if (p + 1 < L && ((longr >> j) & 1u)) a |= 1u << (p + 1);
+        return a;
+    };
+    const int pA = select_bit(rs, jA), pB = select_bit(rs, jB);
+    if (two) allowA = allowed(jA, pA);
+    wA = 1 + popc32(allowA);
+    if (jB != jA) {
+        if (two) allowB = allowed(jB, pB);
+        wB = 1 + popc32(allowB);
+    }
+    const int total = wA + wB, half = total >> 1;
+    const int i0 = (t & 1) ? half : 0, i1 = (t & 1) ? total : half;
+    auto run_items = [&](int j, int p, uint32_t allow, int a, int b) {  // local items [a, b)
+        if (a >= b) return;
+        const u128 v1 = key_del(key, p);
+        if (a == 0) {
+            f(1 + j, v1);
+            a = 1;
+        }
+        uint32_t m = allow;
+        for (int k = 1; k < a; k++) m &= m - 1;  // skip the pairs before item a
+        const int base = 1 + R + pairs_before_run(j, R, longr) - 1;
+        for (int it = a; it < b; it++) {
+            const int q = select_bit(m, 0);
+            m &= m - 1;
+            f(base + it, key_del(v1, q - 1));
+        }
+    };
+    run_items(jA, pA, allowA, i0 < wA ? i0 : wA, i1 < wA ? i1 : wA);
+    if (wB) run_items(jB, pB, allowB, (i0 > wA ? i0 : wA) - wA, (i1 > wA ? i1 : wA) - wA);
+}
+
 // Row i of a group of size s owns pairs (i, i+1..s-1); it starts at local index r(i).
 XTN_HD uint64_t tri_row_start(uint64_t i, uint64_t s) { return i * (2 * s - i - 1) / 2; }
 

@@ -284,7 +284,7 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
-    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo;
+    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
     bool attrs_set = false;
@@ -470,11 +470,17 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    if (d <= 2 && b1 <= 10)
+    if (d <= 2 && b1 <= 10) {
+        XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
+        XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
+        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
+                                                                                   P<uint32_t>(c->tcnt)));
+        XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter_staged<<<ntiles, kStageThreads, sizeof(StageSmem), s>>>(
-                                         P<u128>(c->keys), P<uint64_t>(c->runinfo), P<uint64_t>(c->voff), n, tile, b1,
-                                         idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
-    else
+                                         P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
+                                         P<uint64_t>(c->voff), P<uint64_t>(c->toff), n, tile, d, b1, idbits,
+                                         P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+    } else
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
                                          P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
@@ -1062,7 +1068,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->pairA,   &c->pairB,    &c->dist,      &c->flag,      &c->fpos,     &c->scratch64,
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
-                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo};
+                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
