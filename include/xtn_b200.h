@@ -149,7 +149,9 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *                     (default 4096)
  *   "scatter_ctas_per_sm" 1..4: first-level tiles per SM (default 2)
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
- *                     (default), 0 = with plain 16-byte loads from every thread */
+ *                     (default), 0 = with plain 16-byte loads from every thread
+ *   "key_tables"      1 = for d <= 2, hash variants from per-sequence tables (default),
+ *                     0 = hash each variant key directly (same hash values, slower) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* ------------------------------------------------------------------ search without allocation */

@@ -2,6 +2,7 @@
 // enumeration, Myers/Hamming distances, prefix-variant test) compiled for the CPU, so the
 // test suite can compare them with the oracle without a GPU. Not part of the product.
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 
 #include "../../xt-neighbor_b200/csrc/xtn_common.cuh"
@@ -71,6 +72,37 @@ int hc_task_variants_ok(const char* s, int L, int d) {
     for (int v = 0; v < n && ok; v++) ok = seen[v] == 1;
     return ok ? 1 : 0;
 }
+
+// 1 when the key-table hashes equal key_hash of the variant keys: per task with the flat
+// index (for_each_task_hash), and as a whole multiset (for_each_hash); d <= 2.
+int hc_table_hash_ok(const char* s, int L, int d) {
+    u128 key = pack(s, L);
+    int Lk = L < kKeyLen ? L : kKeyLen;
+    const int n = variant_count(key, Lk, d);
+    const uint64_t info = key_run_info(key, Lk);
+    uint64_t tab[kTabLen];
+    key_table(key, [&](int slot, uint64_t x) { tab[slot] = x; });
+    const int R = popc32((uint32_t)info), T = 2 * ((R + 1) / 2);
+    int seen[1024] = {0};
+    bool ok = n <= 1024;
+    for (int t = 0; t < T && ok; t++)
+        for_each_task_hash(tab, Lk, info, d, t, [&](int v, uint64_t h) {
+            if (v < 0 || v >= n || h != key_hash(variant_at(key, info, v))) ok = false;
+            else seen[v]++;
+        });
+    for (int v = 0; v < n && ok; v++) ok = seen[v] == 1;
+    uint64_t a[1024], b[1024];
+    int na = 0, nb = 0;
+    for_each_hash(tab, Lk, info, d, [&](uint64_t h) { if (na < 1024) a[na++] = h; });
+    for_each_variant(key, Lk, d, [&](u128 k) { if (nb < 1024) b[nb++] = key_hash(k); });
+    if (na != n || nb != n) return 0;
+    std::sort(a, a + na);
+    std::sort(b, b + nb);
+    for (int i = 0; i < n && ok; i++) ok = a[i] == b[i];
+    return ok ? 1 : 0;
+}
+
+uint64_t hc_key_hash(const char* s, int L) { return key_hash(pack(s, L)); }
 
 int hc_variant_count(const char* s, int L, int d) {
     int Lk = L < kKeyLen ? L : kKeyLen;

@@ -25,6 +25,7 @@ def hc():
     lib.hc_variants.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
     lib.hc_tri_row_start.restype = ctypes.c_uint64
     lib.hc_tri_row_start.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+    lib.hc_key_hash.restype = ctypes.c_uint64
     return lib
 
 
@@ -81,6 +82,30 @@ def test_task_partition_of_variants(hc):
     for s in rand_seqs(rng, 2000, 1, 26):
         for d in (1, 2):
             assert hc.hc_task_variants_ok(s.encode(), len(s), d) == 1, (s, d)
+
+
+def test_table_hashes_equal_variant_hashes(hc):
+    """The key-table hashes of the d <= 2 kernels equal key_hash of each variant key."""
+    rng = np.random.default_rng(29)
+    for s in rand_seqs(rng, 1500, 1, 26) + ["A" * 30, "AAC" * 8, "ACACAC", "A", "AC"]:
+        for d in (1, 2):
+            assert hc.hc_table_hash_ok(s.encode(), len(s), d) == 1, (s, d)
+
+
+def test_key_hash_definition(hc):
+    """key_hash = finaliser(sum_k c_k r^k mod 2^64) over the first 18 residue codes."""
+    M = (1 << 64) - 1
+    r = 0x2545F4914F6CDD1D
+
+    def fin(x):
+        x ^= x >> 31
+        x = (x * 0x9E3779B97F4A7C15) & M
+        return x ^ (x >> 29)
+
+    rng = np.random.default_rng(31)
+    for s in rand_seqs(rng, 300, 1, 30):
+        p = sum((ord(ch) - 64) * pow(r, k, 1 << 64) for k, ch in enumerate(s[:18])) & M
+        assert hc.hc_key_hash(s.encode(), len(s)) == fin(p), s
 
 
 def test_key_delete(hc):

@@ -21,6 +21,9 @@ ENGINES = {
     "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64},
     # buckets loaded into shared memory by plain loads instead of a TMA bulk copy
     "bucket_plain_loads": {"group_tma": 0, "scatter_ctas_per_sm": 1},
+    # every variant key hashed directly (the d > 2 and no-allocation form) instead of from
+    # per-sequence tables; direct first-level scatter
+    "bucket_key_hash": {"key_tables": 0},
 }
 
 

@@ -100,8 +100,12 @@ __device__ __forceinline__ T block_scan_ex(T v, T* total, T* warp_sums) {
 }
 
 // ------------------------------------------------------------------ count
+// Per-tile histogram of the variants' first-level buckets; d <= 2 hashes come from the key
+// tables when given.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const u128* __restrict__ keys,
-                                                                 const uint8_t* __restrict__ klen, int n, int tile, int d,
+                                                                 const uint8_t* __restrict__ klen,
+                                                                 const uint64_t* __restrict__ runinfo,
+                                                                 const uint64_t* __restrict__ tab, int n, int tile, int d,
                                                                  int b1, uint32_t* __restrict__ counts) {
     extern __shared__ uint32_t s_hist[];
     const int nb = 1 << b1;
@@ -110,8 +114,13 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const u128* __r
     const int base = blockIdx.x * tile;
     const int end = min(n, base + tile);
     const int shift = 64 - b1;
-    for (int i = base + threadIdx.x; i < end; i += blockDim.x)
-        for_each_variant(keys[i], klen[i], d, [&](u128 k) { atomicAdd(&s_hist[key_hash(k) >> shift], 1u); });
+    if (tab && d <= 2)
+        for (int i = base + threadIdx.x; i < end; i += blockDim.x)
+            for_each_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d,
+                          [&](uint64_t h) { atomicAdd(&s_hist[h >> shift], 1u); });
+    else
+        for (int i = base + threadIdx.x; i < end; i += blockDim.x)
+            for_each_variant(keys[i], klen[i], d, [&](u128 k) { atomicAdd(&s_hist[key_hash(k) >> shift], 1u); });
     __syncthreads();
     uint32_t* out = counts + (size_t)blockIdx.x * nb;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) out[i] = s_hist[i];
@@ -196,11 +205,11 @@ __global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint3
 
 // First-level scatter for d <= 2. The tile's sequences go through shared memory 4096
 // variants at a time; each chunk's variants are produced by balanced tasks (about R/2 + 1
-// variants each, one key deletion and one hash per variant) written at their flat index, then
-// the staged partition writes them out by bucket. runinfo[i] is key_run_info of sequence i;
-// toff is the exclusive scan of k_task_counts.
+// variants each, one table load and one add per variant hash) written at their flat index,
+// then the staged partition writes them out by bucket. runinfo[i] is key_run_info of
+// sequence i, tab its key_table; toff is the exclusive scan of k_task_counts.
 __global__ void __launch_bounds__(kStageThreads, 2) k_bucket_scatter_staged(
-    const u128* __restrict__ keys, const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo,
+    const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, int n, int tile, int d, int b1, int idbits,
     const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -260,8 +269,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_bucket_scatter_staged(
             const int t = (int)(tau - S.rel_t[li]);
             const uint32_t vb = S.rel_v[li];
             const uint64_t id = (uint64_t)i;
-            for_each_task_variant(keys[i], klen[i], runinfo[i], d, t, [&](int v, u128 k) {
-                const uint64_t h = key_hash(k);
+            for_each_task_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d, t, [&](int v, uint64_t h) {
                 S.bkt[vb + v] = (uint16_t)(h >> shift);
                 S.rec[vb + v] = ((h << b1) & hi_mask) | id;
             });

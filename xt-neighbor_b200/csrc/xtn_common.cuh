@@ -53,22 +53,81 @@ XTN_HD uint32_t key_run_starts(u128 v, int L) {
     return m;
 }
 
-// MurmurHash3's 64-bit finaliser (Appleby, public domain).
-XTN_HD uint64_t fmix64(uint64_t k) {
-    k ^= k >> 33;
-    k *= 0xff51afd7ed558ccdULL;
-    k ^= k >> 33;
-    k *= 0xc4ceb9fe1a85ec53ULL;
-    k ^= k >> 33;
-    return k;
+// Variant hash. A variant string v_0..v_{m-1} (residue codes) hashes to
+// hash_fin(P(v)), P(v) = sum_k v_k r^k (mod 2^64) for a fixed odd r. Only equality of
+// variants matters for correctness: equal strings always get equal hashes, and pairs that
+// share only a hash are removed by exact verification. The polynomial form makes every
+// one- and two-deletion variant of a key a sum of two entries of a per-key table
+// (key_table), so the d <= 2 paths hash a variant with one load and one add.
+constexpr uint64_t kPolyR = 0x2545F4914F6CDD1DULL;
+
+// Inverse of an odd number modulo 2^64 (Newton's iteration; each step doubles the
+// correct low bits, starting from 3).
+XTN_HD constexpr uint64_t inverse_odd(uint64_t a) {
+    uint64_t x = a;
+    for (int i = 0; i < 6; i++) x *= 2 - a * x;
+    return x;
+}
+constexpr uint64_t kPolyRI = inverse_odd(kPolyR);
+constexpr uint64_t kPolyRI2 = kPolyRI * kPolyRI;
+
+// Xorshift-multiply finaliser: a bijection that spreads all input bits into the top bits
+// (the bucket index) and the middle bits (the stored record hash).
+XTN_HD uint64_t hash_fin(uint64_t x) {
+    x ^= x >> 31;
+    x *= 0x9E3779B97F4A7C15ULL;
+    x ^= x >> 29;
+    return x;
 }
 
-// Hash of a packed key. Only equality of keys matters for correctness: two sequences
-// that share a key always share its hash, and pairs that share only a hash are removed
-// by exact verification.
-XTN_HD uint64_t key_hash(u128 v) {
-    uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;
-    return fmix64(hi ^ fmix64(lo + 0x9e3779b97f4a7c15ULL));
+// The 90 key bits as two 64-bit words: residues 0..11 in a (residue i at bits [55-5i, 60-5i)),
+// residues 12..17 in b (residue 12+j at bits [25-5j, 30-5j)). The hash code reads codes from
+// these words with 64-bit shifts only: a Horner loop over 128-bit shifts of the key gave
+// wrong values in one device kernel build (the same source, with 64-bit words, is correct).
+struct KeyWords {
+    uint64_t a, b;
+};
+XTN_HD KeyWords key_words(u128 v) { return KeyWords{(uint64_t)(v >> 68), (uint64_t)(v >> 38) & ((1ull << 30) - 1ull)}; }
+XTN_HD uint64_t word_code(KeyWords w, int i) {
+    return i < 12 ? (w.a >> (55 - 5 * i)) & 31u : (w.b >> (25 - 5 * (i - 12))) & 31u;
+}
+
+// P of a packed key, by Horner's rule from the last position (zero padding adds nothing).
+XTN_HD uint64_t key_poly(u128 v) {
+    const KeyWords w = key_words(v);
+    uint64_t acc = 0;
+    for (int i = kKeyLen - 1; i >= 0; i--) acc = acc * kPolyR + word_code(w, i);
+    return acc;
+}
+
+XTN_HD uint64_t key_hash(u128 v) { return hash_fin(key_poly(v)); }
+
+// Per-key hash table. With prefix sums P_i = sum_{j<i} c_j r^j of the key's codes and
+// P_L its full polynomial, deleting p < q gives
+//   P(del p,q) = P_p + r^-1 (P_q - P_{p+1}) + r^-2 (P_L - P_{q+1}) = K[p] + G[q]
+//   K[p] = P_p - r^-1 P_{p+1} + r^-2 P_L,   G[q] = r^-1 P_q - r^-2 P_{q+1},
+// and deleting p alone gives P_p + r^-1 (P_L - P_{p+1}) = K[p] + S, S = (r^-1 - r^-2) P_L.
+constexpr int kTabK = 0;                  // K[0..17]
+constexpr int kTabG = kKeyLen;            // G[0..17]
+constexpr int kTabKey = 2 * kKeyLen;      // P_L, the key's own polynomial
+constexpr int kTabSingle = 2 * kKeyLen + 1;  // S
+constexpr int kTabLen = 2 * kKeyLen + 2;  // 38 words per key
+
+// st(slot, value) for every slot 0..kTabLen-1 (entries past the key's length are unused).
+template <class Store>
+XTN_HD void key_table(u128 key, Store&& st) {
+    const uint64_t PL = key_poly(key);
+    const KeyWords w = key_words(key);
+    uint64_t P = 0, pw = 1;
+    for (int i = 0; i < kKeyLen; i++) {
+        const uint64_t Pn = P + word_code(w, i) * pw;
+        st(kTabK + i, P - kPolyRI * Pn + kPolyRI2 * PL);
+        st(kTabG + i, kPolyRI * P - kPolyRI2 * Pn);
+        P = Pn;
+        pw *= kPolyR;
+    }
+    st(kTabKey, PL);
+    st(kTabSingle, (kPolyRI - kPolyRI2) * PL);
 }
 
 // Calls f(key) once per run-prefix deletion set of at most min(d, L) positions
@@ -131,6 +190,15 @@ XTN_HD int popc32(uint32_t x) {
     return __popc(x);
 #else
     return __builtin_popcount(x);
+#endif
+}
+
+// Position of the lowest set bit (x != 0).
+XTN_HD int ctz32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __ffs(x) - 1;
+#else
+    return __builtin_ctz(x);
 #endif
 }
 
@@ -214,53 +282,126 @@ XTN_HD int pairs_before_run(int j, int R, uint32_t longr) {
     return j * (R - 1) - j * (j - 1) / 2 + popc32(longr & ((1u << j) - 1u));
 }
 
-// Task t (0 <= t < 2*ceil(R/2)) of a key's d <= 2 variants, for parallel generation with even work:
-// tasks 2j and 2j+1 share the variants of runs j and R-1-j (the single deletion of each run and
-// its pairs; about R+1 variants together), split into two halves; task 0 also emits the key
-// itself. f(v, key) is called with each variant's flat index (variant_at's order) and value.
-template <class F>
-XTN_HD void for_each_task_variant(u128 key, int L, uint64_t info, int d, int t, F&& f) {
+// Enumerations of a key's d <= 2 variants, by deletion positions. An emitter E provides
+//   e.key(v)      item v is the key itself
+//   e.run(p)      the items that follow delete residue p, the first residue of a run
+//   e.single(v)   item v deletes p only
+//   e.pair(v, q)  item v deletes p and q (q > p: the next residue of p's run, or the first
+//                 residue of a later run)
+
+// Positions q that pair with run j starting at p.
+XTN_HD uint32_t pair_positions(uint32_t rs, uint32_t longr, uint32_t lmask, int L, int j, int p) {
+    uint32_t a = rs & lmask & ~((2u << p) - 1u);
+    if (p + 1 < L && ((longr >> j) & 1u)) a |= 1u << (p + 1);
+    return a;
+}
+
+// Task t (0 <= t < 2*ceil(R/2)) of a key's d <= 2 variants, for parallel generation with even
+// work: tasks 2j and 2j+1 share the items of runs j and R-1-j (the single deletion of each run
+// and its pairs; about R+1 items together), split into two halves; task 0 also emits the key.
+// Item indices v are variant_at's flat order.
+template <class E>
+XTN_HD void task_items(int L, uint64_t info, int d, int t, E& e) {
     const uint32_t rs = (uint32_t)info, longr = (uint32_t)(info >> 32);
     const uint32_t lmask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
     const int R = popc32(rs);
     const bool two = d >= 2 && L >= 2;
-    if (t == 0) f(0, key);
+    if (t == 0) e.key(0);
     const int jA = t >> 1, jB = R - 1 - jA;
     // items of one run: the single deletion, then its pairs in ascending q
     int wA, wB = 0;
     uint32_t allowA = 0, allowB = 0;
-    auto allowed = [&](int j, int p) -> uint32_t {
-        uint32_t a = rs & lmask & ~((2u << p) - 1u);
-        if (p + 1 < L && ((longr >> j) & 1u)) a |= 1u << (p + 1);
-        return a;
-    };
     const int pA = select_bit(rs, jA), pB = select_bit(rs, jB);
-    if (two) allowA = allowed(jA, pA);
+    if (two) allowA = pair_positions(rs, longr, lmask, L, jA, pA);
     wA = 1 + popc32(allowA);
     if (jB != jA) {
-        if (two) allowB = allowed(jB, pB);
+        if (two) allowB = pair_positions(rs, longr, lmask, L, jB, pB);
         wB = 1 + popc32(allowB);
     }
     const int total = wA + wB, half = total >> 1;
     const int i0 = (t & 1) ? half : 0, i1 = (t & 1) ? total : half;
     auto run_items = [&](int j, int p, uint32_t allow, int a, int b) {  // local items [a, b)
         if (a >= b) return;
-        const u128 v1 = key_del(key, p);
+        e.run(p);
         if (a == 0) {
-            f(1 + j, v1);
+            e.single(1 + j);
             a = 1;
         }
         uint32_t m = allow;
         for (int k = 1; k < a; k++) m &= m - 1;  // skip the pairs before item a
         const int base = 1 + R + pairs_before_run(j, R, longr) - 1;
         for (int it = a; it < b; it++) {
-            const int q = select_bit(m, 0);
+            e.pair(base + it, ctz32(m));
             m &= m - 1;
-            f(base + it, key_del(v1, q - 1));
         }
     };
     run_items(jA, pA, allowA, i0 < wA ? i0 : wA, i1 < wA ? i1 : wA);
     if (wB) run_items(jB, pB, allowB, (i0 > wA ? i0 : wA) - wA, (i1 > wA ? i1 : wA) - wA);
+}
+
+// All d <= 2 items of a key in one pass (v counts the calls; the order is by run, not
+// variant_at's).
+template <class E>
+XTN_HD void seq_items(int L, uint64_t info, int d, E& e) {
+    e.key(0);
+    if (L <= 0) return;
+    const uint32_t rs = (uint32_t)info, longr = (uint32_t)(info >> 32);
+    const uint32_t lmask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+    const bool two = d >= 2 && L >= 2;
+    int v = 1, j = 0;
+    for (uint32_t m = rs; m; m &= m - 1, j++) {
+        const int p = ctz32(m);
+        e.run(p);
+        e.single(v++);
+        if (two)
+            for (uint32_t a = pair_positions(rs, longr, lmask, L, j, p); a; a &= a - 1) e.pair(v++, ctz32(a));
+    }
+}
+
+// Emitter producing variant keys: f(v, key).
+template <class F>
+struct KeyEmitter {
+    u128 k0, v1;
+    F& f;
+    XTN_HD void key(int v) { f(v, k0); }
+    XTN_HD void run(int p) { v1 = key_del(k0, p); }
+    XTN_HD void single(int v) { f(v, v1); }
+    XTN_HD void pair(int v, int q) { f(v, key_del(v1, q - 1)); }
+};
+
+// Emitter producing variant hashes from a key_table: f(v, hash), equal to
+// key_hash of the variant key.
+template <class F>
+struct TableHashEmitter {
+    const uint64_t* tab;
+    uint64_t kp;
+    F& f;
+    XTN_HD void key(int v) { f(v, hash_fin(tab[kTabKey])); }
+    XTN_HD void run(int p) { kp = tab[kTabK + p]; }
+    XTN_HD void single(int v) { f(v, hash_fin(kp + tab[kTabSingle])); }
+    XTN_HD void pair(int v, int q) { f(v, hash_fin(kp + tab[kTabG + q])); }
+};
+
+// Task t's variants as keys: f(v, key) with v the flat index (variant_at's order).
+template <class F>
+XTN_HD void for_each_task_variant(u128 key, int L, uint64_t info, int d, int t, F&& f) {
+    KeyEmitter<F> e{key, key, f};
+    task_items(L, info, d, t, e);
+}
+
+// Task t's variants as hashes: f(v, hash).
+template <class F>
+XTN_HD void for_each_task_hash(const uint64_t* tab, int L, uint64_t info, int d, int t, F&& f) {
+    TableHashEmitter<F> e{tab, 0, f};
+    task_items(L, info, d, t, e);
+}
+
+// All of a key's d <= 2 variants as hashes: f(hash).
+template <class F>
+XTN_HD void for_each_hash(const uint64_t* tab, int L, uint64_t info, int d, F&& f) {
+    auto g = [&](int, uint64_t h) { f(h); };
+    TableHashEmitter<decltype(g)> e{tab, 0, g};
+    seq_items(L, info, d, e);
 }
 
 // Row i of a group of size s owns pairs (i, i+1..s-1); it starts at local index r(i).

@@ -53,9 +53,11 @@ static void set_err(const std::string& s) { t_err = s; }
 // ------------------------------------------------------------------ kernels
 constexpr int kThreads = 256;
 
+// Packs each sequence's key; with tab != nullptr also writes its key_table (kTabLen words).
 __global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
                        const int32_t* __restrict__ rows, int n, int d, u128* __restrict__ keys,
-                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt, uint64_t* __restrict__ runinfo) {
+                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt, uint64_t* __restrict__ runinfo,
+                       uint64_t* __restrict__ tab) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int r = rows ? rows[i] : i;
@@ -68,16 +70,27 @@ __global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __rest
     klen[i] = (uint8_t)Lk;
     vcnt[i] = (uint32_t)variant_count(v, Lk, d);
     runinfo[i] = key_run_info(v, Lk);
+    if (tab) {
+        uint64_t* t = tab + (size_t)i * kTabLen;
+        key_table(v, [&](int slot, uint64_t x) { t[slot] = x; });
+    }
 }
 
+// One thread per sequence writes its variant records at voff[i]; d <= 2 hashes come from
+// the key tables when given.
 __global__ void k_gen(const u128* __restrict__ keys, const uint8_t* __restrict__ klen,
+                      const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
                       const uint64_t* __restrict__ voff, int n, int d, int idbits, uint64_t* __restrict__ recs) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
     uint64_t o = voff[i];
     const uint64_t id = (uint64_t)i;
-    for_each_variant(keys[i], klen[i], d, [&](u128 k) { recs[o++] = (key_hash(k) & hi_mask) | id; });
+    if (tab && d <= 2)
+        for_each_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d,
+                      [&](uint64_t h) { recs[o++] = (h & hi_mask) | id; });
+    else
+        for_each_variant(keys[i], klen[i], d, [&](u128 k) { recs[o++] = (key_hash(k) & hi_mask) | id; });
 }
 
 // Heads of runs of >= 2 equal hashes; appended in any order through a warp-aggregated cursor.
@@ -284,13 +297,14 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
-    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff;
+    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
     bool attrs_set = false;
     int bucket_bits_max = kMaxFirstLevelBits;
     int scatter_ctas_per_sm = 2;
     int group_tma = 1;
+    int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
     uint32_t group_cap = kGroupCap;
     uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
     // results
@@ -426,8 +440,10 @@ static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t 
     cudaStream_t s = c->stream;
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
     XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
-    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(P<u128>(c->keys), P<uint8_t>(c->klen),
-                                                              P<uint64_t>(c->voff), n, d, idbits, P<uint64_t>(c->recA)));
+    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(
+                          P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
+                          d <= 2 && c->key_tables ? P<uint64_t>(c->ktab) : nullptr, P<uint64_t>(c->voff), n, d, idbits,
+                          P<uint64_t>(c->recA)));
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
     uint64_t* recs = nullptr;
@@ -466,18 +482,20 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         c->attrs_set = true;
     }
     XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
-                                   P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, P<uint32_t>(c->bcounts)));
+                                   P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
+                                   d <= 2 && c->key_tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1,
+                                   P<uint32_t>(c->bcounts)));
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    if (d <= 2 && b1 <= 10) {
+    if (d <= 2 && b1 <= 10 && c->key_tables) {
         XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
         XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
                                                                                    P<uint32_t>(c->tcnt)));
         XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter_staged<<<ntiles, kStageThreads, sizeof(StageSmem), s>>>(
-                                         P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
+                                         P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
                                          P<uint64_t>(c->voff), P<uint64_t>(c->toff), n, tile, d, b1, idbits,
                                          P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
     } else
@@ -587,8 +605,11 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->vcnt, sizeof(uint32_t) * n));
     XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (n + 1)));
     XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * n));
+    const bool tables = d <= 2 && c->key_tables;
+    if (tables) XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)n));
     XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen),
-                                             P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo)));
+                                             P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo),
+                                             tables ? P<uint64_t>(c->ktab) : nullptr));
     XTN_CK(cudaGetLastError());
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n));
     XTN_CK(cudaEventRecord(c->ev[1], s));
@@ -758,7 +779,7 @@ __global__ void k_row_hash(const uint8_t* __restrict__ chars, const uint32_t* __
     int L = (int)(offs[i + 1] - s);
     uint64_t h = 0x84222325cbf29ce4ULL ^ (uint64_t)L;
     for (int j = 0; j < L; j++) h = (h ^ chars[s + j]) * 0x100000001b3ULL;
-    h = fmix64(h);
+    h = hash_fin(h);
     recs[i] = (h & ~((1ull << idbits) - 1ull)) | (uint64_t)i;
 }
 
@@ -1068,7 +1089,8 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->pairA,   &c->pairB,    &c->dist,      &c->flag,      &c->fpos,     &c->scratch64,
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
-                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff};
+                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
+                      &c->ktab};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1149,6 +1171,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "group_cap") && v >= 2 && v <= kGroupCap) c->group_cap = (uint32_t)v;
     else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 1 && v <= 4) c->scatter_ctas_per_sm = (int)v;
     else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
+    else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
         return XTN_ERR_ARG;
@@ -1284,7 +1307,8 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
     if (!cv.take(&keys, n) || !cv.take(&klen, n) || !cv.take(&vcnt, n) || !cv.take(&voff, n + 1) ||
         !cv.take(&runinfo, n) || !cv.take(&scan64, scan_scratch_elems(n)) || !cv.take(&counter, 2))
         return arena_full("sequence tables");
-    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo));
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo,
+                                                                 nullptr));
     XTN_CK(cudaGetLastError());
     scan_exclusive<uint32_t, uint64_t>(vcnt, voff, n, scan64, s);
     uint64_t V = 0;
@@ -1293,7 +1317,7 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
     uint32_t* rscratch;
     if (!cv.take(&recA, V) || !cv.take(&recB, V) || !cv.take(&rscratch, radix_scratch_elems((int64_t)V)))
         return arena_full("variant records");
-    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(keys, klen, voff, n, d, idbits, recA));
+    XTN_LAUNCH("gen", k_gen<<<blocks_for(n), kThreads, 0, s>>>(keys, klen, runinfo, nullptr, voff, n, d, idbits, recA));
     uint64_t* recs = radix_sort_u64(recA, recB, (int64_t)V, idbits, 64, rscratch, s, "key_sort_upsweep",
                                     "key_sort_downsweep");
     // groups: at most one per two records
