@@ -143,11 +143,14 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *   "engine"          0 = hash-bucket grouping in shared memory (default),
  *                     1 = full radix sort of the variant records (the plain comparison form)
  *   "bucket_bits_max" 1..14: upper bound on log2(number of first-level buckets) (default 9;
- *                     above 10 the first-level scatter stores records one by one)
+ *                     above 9 the first-level scatter stores records one by one)
  *   "group_cap"       2..4096: largest bucket grouped in shared memory; larger ones are split
  *                     by further hash bits, and what still does not fit is grouped by sorting
  *                     (default 4096)
- *   "scatter_ctas_per_sm" 1..4: first-level tiles per SM (default 2)
+ *   "scatter_ctas_per_sm" 0..4: first-level tiles per SM (default 0: as many CTAs as fit)
+ *   "stage_chunk"     2048 | 4096: records per shared-memory chunk of the first-level scatter
+ *                     (default 4096: two CTAs per SM; 2048: four)
+ *   "split_chunk"     2048 | 4096: the same for the split of large buckets (default 4096)
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
  *                     (default), 0 = with plain 16-byte loads from every thread
  *   "key_tables"      1 = for d <= 2, hash variants from per-sequence tables (default),

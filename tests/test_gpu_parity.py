@@ -18,9 +18,10 @@ ENGINES = {
     "sort": {"engine": 1},
     # tiny first-level table and shared-memory cap: exercises the bucket split and the
     # sort-based fallback for oversized buckets on small inputs
-    "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64},
-    # buckets loaded into shared memory by plain loads instead of a TMA bulk copy
-    "bucket_plain_loads": {"group_tma": 0, "scatter_ctas_per_sm": 1},
+    "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64, "split_chunk": 2048},
+    # buckets loaded into shared memory by plain loads instead of a TMA bulk copy; the larger
+    # first-level stage shape
+    "bucket_plain_loads": {"group_tma": 0, "scatter_ctas_per_sm": 1, "stage_chunk": 4096},
     # every variant key hashed directly (the d > 2 and no-allocation form) instead of from
     # per-sequence tables; direct first-level scatter
     "bucket_key_hash": {"key_tables": 0},

@@ -32,15 +32,26 @@
 namespace xtn {
 
 constexpr int kBucketThreads = 512;    // k_bucket_count and the direct scatter (d > 2)
-constexpr int kStageThreads = 512;     // staged scatter / split (two CTAs per SM)
-constexpr int kStageChunk = 4096;      // records per staged chunk
-constexpr int kMaxFan = 1024;          // fan-out of one staged partition
-constexpr int kFanPer = kMaxFan / kStageThreads;
 constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp histograms
-// First-level fan-out: each staged chunk of 4096 records leaves runs of ~8 records (64 bytes)
-// per bucket; consecutive chunks of one CTA extend the same runs, so their boundary sectors
-// complete in L2.
+// First-level fan-out: a staged chunk of 2048..4096 records leaves runs of 4..8 records
+// (32..64 bytes) per bucket; consecutive chunks of one CTA extend the same runs, so their
+// boundary sectors complete in L2.
 constexpr int kMaxFirstLevelBits = 9;
+constexpr int kMaxSplitBits = 10;
+
+// Shape of a staged partition: threads per CTA, records per chunk, largest fan-out.
+template <int THREADS, int CHUNK, int FAN>
+struct StageCfg {
+    static constexpr int kThreads = THREADS;
+    static constexpr int kChunk = CHUNK;
+    static constexpr int kFan = FAN;
+    static constexpr int kFanPer = FAN / THREADS;
+    static constexpr int kPer = CHUNK / THREADS;
+    static_assert(FAN % THREADS == 0 && CHUNK % THREADS == 0 && CHUNK <= 65536, "stage shape");
+};
+using StageLarge = StageCfg<512, 4096, 1024>;  // ~110 KB of shared memory: two CTAs per SM
+using StageSmall = StageCfg<256, 2048, 512>;   // ~55 KB: four CTAs per SM (first level, b1 <= 9)
+using SplitSmall = StageCfg<256, 2048, 1024>;  // ~60 KB: three CTAs per SM
 constexpr int kGroupThreads = 512;
 constexpr int kGroupCap = 4096;        // records a grouping CTA holds in shared memory
 constexpr int kBitmapLog = 16;         // hash bits of the "seen" / "seen twice" bitmaps
@@ -141,23 +152,33 @@ __global__ void k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles
 }
 
 // ------------------------------------------------------------------ staged partition
+template <class C>
 struct StageSmem {
-    uint64_t rec[kStageChunk];     // records of the chunk, in arrival order
-    uint64_t sorted[kStageChunk];  // the same records grouped by bucket
-    uint16_t bkt[kStageChunk];     // bucket of rec[i]
-    uint16_t sbkt[kStageChunk];    // bucket of sorted[i]
-    uint32_t cnt[kMaxFan];
-    uint32_t lstart[kMaxFan];
-    uint32_t gcur[kMaxFan];        // next global position of each bucket for this CTA
-    uint16_t rel_v[kStageChunk];   // voff of the chunk's sequences, relative to the chunk
-    uint16_t rel_t[kStageChunk];   // toff of the chunk's sequences, relative to the chunk
-    uint32_t warp_sums[kStageThreads / 32 + 1];
+    uint64_t rec[C::kChunk];     // records of the chunk, in arrival order
+    uint64_t sorted[C::kChunk];  // the same records grouped by bucket
+    uint16_t bkt[C::kChunk];     // bucket of rec[i]
+    uint16_t sbkt[C::kChunk];    // bucket of sorted[i]
+    uint32_t cnt[C::kFan];
+    uint32_t lstart[C::kFan];
+    uint32_t gcur[C::kFan];      // next global position of each bucket for this CTA
+    uint16_t rel_v[C::kChunk];   // voff of the chunk's sequences, relative to the chunk
+    uint16_t rel_t[C::kChunk];   // toff of the chunk's sequences, relative to the chunk
+    uint32_t warp_sums[C::kThreads / 32 + 1];
     uint32_t seq_end;
 };
 
+// Resident CTAs per SM that a stage shape's shared memory allows (228 KB per SM, 1 KB
+// reserved per CTA).
+template <class C>
+constexpr int stage_ctas_per_sm() {
+    return (int)((228u * 1024u) / (sizeof(StageSmem<C>) + 1024u));
+}
+
 // Writes rec[0..m) (bucket bkt[]) to dst, each bucket's records appended at gcur[bucket],
 // as contiguous runs from consecutive threads.
-__device__ __forceinline__ void stage_partition(StageSmem& S, int nb, uint32_t m, uint64_t* __restrict__ dst) {
+template <class C>
+__device__ __forceinline__ void stage_partition(StageSmem<C>& S, int nb, uint32_t m, uint64_t* __restrict__ dst) {
+    constexpr int kStageThreads = C::kThreads, kFanPer = C::kFanPer;
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[S.bkt[p]], 1u);
@@ -208,12 +229,14 @@ __global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint3
 // variants each, one table load and one add per variant hash) written at their flat index,
 // then the staged partition writes them out by bucket. runinfo[i] is key_run_info of
 // sequence i, tab its key_table; toff is the exclusive scan of k_task_counts.
-__global__ void __launch_bounds__(kStageThreads, 2) k_bucket_scatter_staged(
+template <class C>
+__global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_scatter_staged(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, int n, int tile, int d, int b1, int idbits,
     const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs) {
+    constexpr int kStageThreads = C::kThreads, kStageChunk = C::kChunk;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
     const int nb = 1 << b1;
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] = (uint32_t)bstart[b] + off[b];
@@ -221,7 +244,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) k_bucket_scatter_staged(
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
-    constexpr int kPer = kStageChunk / kStageThreads;  // task slots per thread in the scan
+    constexpr int kPer = C::kPer;  // task slots per thread in the scan
     __syncthreads();
     for (int s0 = t0; s0 < t1;) {
         // chunk end: the largest s1 <= t1 with voff[s1] - voff[s0] <= chunk, found by all threads
@@ -321,7 +344,7 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
         // sub-buckets aim at 7/8 of the shared-memory capacity (hash buckets are near-uniform)
         const uint32_t target = group_cap * 7 / 8;
         uint32_t bits = 1;
-        while (bits < 10 && ((uint64_t)size >> bits) > (uint64_t)(target > 1 ? target : 1)) bits++;
+        while (bits < kMaxSplitBits && ((uint64_t)size >> bits) > (uint64_t)(target > 1 ? target : 1)) bits++;
         unsigned k = atomicAdd(&counters[1], 1u);
         jobs[k] = SplitJob{s, size, bits};
         atomicAdd(&counters[2], 1u << bits);
@@ -332,11 +355,13 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
 // sub-bucket descriptors, then the bucket's records, chunk by chunk, through the staged
 // partition into buffer B at the same range. Sub-buckets that fit are listed for grouping;
 // larger ones go to the fallback list.
-__global__ void __launch_bounds__(kStageThreads, 2) k_bucket_split_staged(
+template <class C>
+__global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_split_staged(
     const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t group_cap,
     BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
+    constexpr int kStageThreads = C::kThreads, kStageChunk = C::kChunk, kFanPer = C::kFanPer;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
     const SplitJob job = jobs[blockIdx.x];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;

@@ -105,29 +105,25 @@ XTN_HD uint64_t key_hash(u128 v) { return hash_fin(key_poly(v)); }
 // Per-key hash table. With prefix sums P_i = sum_{j<i} c_j r^j of the key's codes and
 // P_L its full polynomial, deleting p < q gives
 //   P(del p,q) = P_p + r^-1 (P_q - P_{p+1}) + r^-2 (P_L - P_{q+1}) = K[p] + G[q]
-//   K[p] = P_p - r^-1 P_{p+1} + r^-2 P_L,   G[q] = r^-1 P_q - r^-2 P_{q+1},
-// and deleting p alone gives P_p + r^-1 (P_L - P_{p+1}) = K[p] + S, S = (r^-1 - r^-2) P_L.
-constexpr int kTabK = 0;                  // K[0..17]
-constexpr int kTabG = kKeyLen;            // G[0..17]
-constexpr int kTabKey = 2 * kKeyLen;      // P_L, the key's own polynomial
-constexpr int kTabSingle = 2 * kKeyLen + 1;  // S
-constexpr int kTabLen = 2 * kKeyLen + 2;  // 38 words per key
+//   G[q] = r^-1 P_q - r^-2 P_{q+1},   K[p] = P_p - r^-1 P_{p+1} + r^-2 P_L = r G[p] + r^-2 P_L,
+// and deleting p alone gives P_p + r^-1 (P_L - P_{p+1}) = r G[p] + r^-1 P_L. The table holds
+// G[0..17] and P_L; K[p] costs one multiply-add.
+constexpr int kTabG = 0;                  // G[0..17]
+constexpr int kTabKey = kKeyLen;          // P_L, the key's own polynomial
+constexpr int kTabLen = kKeyLen + 1;      // 19 words per key
 
 // st(slot, value) for every slot 0..kTabLen-1 (entries past the key's length are unused).
 template <class Store>
 XTN_HD void key_table(u128 key, Store&& st) {
-    const uint64_t PL = key_poly(key);
     const KeyWords w = key_words(key);
     uint64_t P = 0, pw = 1;
     for (int i = 0; i < kKeyLen; i++) {
         const uint64_t Pn = P + word_code(w, i) * pw;
-        st(kTabK + i, P - kPolyRI * Pn + kPolyRI2 * PL);
         st(kTabG + i, kPolyRI * P - kPolyRI2 * Pn);
         P = Pn;
         pw *= kPolyR;
     }
-    st(kTabKey, PL);
-    st(kTabSingle, (kPolyRI - kPolyRI2) * PL);
+    st(kTabKey, P);
 }
 
 // Calls f(key) once per run-prefix deletion set of at most min(d, L) positions
@@ -369,16 +365,21 @@ struct KeyEmitter {
     XTN_HD void pair(int v, int q) { f(v, key_del(v1, q - 1)); }
 };
 
-// Emitter producing variant hashes from a key_table: f(v, hash), equal to
-// key_hash of the variant key.
+// Emitter producing variant hashes from a key_table: f(v, hash), equal to key_hash of the
+// variant key.
 template <class F>
 struct TableHashEmitter {
     const uint64_t* tab;
-    uint64_t kp;
+    uint64_t c1, s1, kp;
     F& f;
+    XTN_HD TableHashEmitter(const uint64_t* t, F& fn) : tab(t), kp(0), f(fn) {
+        const uint64_t PL = t[kTabKey];
+        c1 = kPolyRI2 * PL;             // K[p] = r G[p] + c1
+        s1 = (kPolyRI - kPolyRI2) * PL;  // single deletion = K[p] + s1
+    }
     XTN_HD void key(int v) { f(v, hash_fin(tab[kTabKey])); }
-    XTN_HD void run(int p) { kp = tab[kTabK + p]; }
-    XTN_HD void single(int v) { f(v, hash_fin(kp + tab[kTabSingle])); }
+    XTN_HD void run(int p) { kp = kPolyR * tab[kTabG + p] + c1; }
+    XTN_HD void single(int v) { f(v, hash_fin(kp + s1)); }
     XTN_HD void pair(int v, int q) { f(v, hash_fin(kp + tab[kTabG + q])); }
 };
 
@@ -392,7 +393,7 @@ XTN_HD void for_each_task_variant(u128 key, int L, uint64_t info, int d, int t, 
 // Task t's variants as hashes: f(v, hash).
 template <class F>
 XTN_HD void for_each_task_hash(const uint64_t* tab, int L, uint64_t info, int d, int t, F&& f) {
-    TableHashEmitter<F> e{tab, 0, f};
+    TableHashEmitter<F> e(tab, f);
     task_items(L, info, d, t, e);
 }
 
@@ -400,7 +401,7 @@ XTN_HD void for_each_task_hash(const uint64_t* tab, int L, uint64_t info, int d,
 template <class F>
 XTN_HD void for_each_hash(const uint64_t* tab, int L, uint64_t info, int d, F&& f) {
     auto g = [&](int, uint64_t h) { f(h); };
-    TableHashEmitter<decltype(g)> e{tab, 0, g};
+    TableHashEmitter<decltype(g)> e(tab, g);
     seq_items(L, info, d, e);
 }
 

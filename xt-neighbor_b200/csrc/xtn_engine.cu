@@ -54,26 +54,42 @@ static void set_err(const std::string& s) { t_err = s; }
 constexpr int kThreads = 256;
 
 // Packs each sequence's key; with tab != nullptr also writes its key_table (kTabLen words).
-__global__ void k_pack(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
-                       const int32_t* __restrict__ rows, int n, int d, u128* __restrict__ keys,
-                       uint8_t* __restrict__ klen, uint32_t* __restrict__ vcnt, uint64_t* __restrict__ runinfo,
-                       uint64_t* __restrict__ tab) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int r = rows ? rows[i] : i;
-    uint32_t s = offs[r];
-    int L = (int)(offs[r + 1] - s);
-    int Lk = L < kKeyLen ? L : kKeyLen;
+// Each warp builds its 32 tables in shared memory (rows of an odd number of words, so the
+// lanes' 8-byte stores fall in distinct banks) and stores them with consecutive lanes on
+// consecutive words.
+constexpr int kPackThreads = 128;
+constexpr int kPackRow = kTabLen | 1;
+
+__global__ void __launch_bounds__(kPackThreads) k_pack(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
+                                                       const int32_t* __restrict__ rows, int n, int d,
+                                                       u128* __restrict__ keys, uint8_t* __restrict__ klen,
+                                                       uint32_t* __restrict__ vcnt, uint64_t* __restrict__ runinfo,
+                                                       uint64_t* __restrict__ tab) {
+    __shared__ uint64_t s_tab[kPackThreads / 32][32 * kPackRow];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool live = i < n;
     u128 v = 0;
-    for (int j = 0; j < Lk; j++) v = key_put(v, j, (unsigned)code_of(chars[s + j]));
-    keys[i] = v;
-    klen[i] = (uint8_t)Lk;
-    vcnt[i] = (uint32_t)variant_count(v, Lk, d);
-    runinfo[i] = key_run_info(v, Lk);
-    if (tab) {
-        uint64_t* t = tab + (size_t)i * kTabLen;
-        key_table(v, [&](int slot, uint64_t x) { t[slot] = x; });
+    if (live) {
+        int r = rows ? rows[i] : i;
+        uint32_t s = offs[r];
+        int L = (int)(offs[r + 1] - s);
+        int Lk = L < kKeyLen ? L : kKeyLen;
+        for (int j = 0; j < Lk; j++) v = key_put(v, j, (unsigned)code_of(chars[s + j]));
+        keys[i] = v;
+        klen[i] = (uint8_t)Lk;
+        vcnt[i] = (uint32_t)variant_count(v, Lk, d);
+        runinfo[i] = key_run_info(v, Lk);
     }
+    if (!tab) return;
+    uint64_t* row = s_tab[w] + lane * kPackRow;
+    if (live) key_table(v, [&](int slot, uint64_t x) { row[slot] = x; });
+    __syncwarp();
+    const int i0 = i - lane;
+    const int cnt = min(32, n - i0);
+    if (cnt <= 0) return;
+    uint64_t* dst = tab + (size_t)i0 * kTabLen;
+    for (int k = lane; k < cnt * kTabLen; k += 32) dst[k] = s_tab[w][(k / kTabLen) * kPackRow + k % kTabLen];
 }
 
 // One thread per sequence writes its variant records at voff[i]; d <= 2 hashes come from
@@ -302,9 +318,11 @@ struct xtn_context {
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
     bool attrs_set = false;
     int bucket_bits_max = kMaxFirstLevelBits;
-    int scatter_ctas_per_sm = 2;
+    int scatter_ctas_per_sm = 0;  // 0: as many as the stage shape's shared memory allows
     int group_tma = 1;
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
+    int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
+    int split_chunk = 4096;  // the same for the split (2048 | 4096)
     uint32_t group_cap = kGroupCap;
     uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
     // results
@@ -460,7 +478,9 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     int b1 = 1;
     while (b1 < c->bucket_bits_max && (V >> b1) > 7000) b1++;
     const int nb = 1 << b1;
-    const int per_sm = c->scatter_ctas_per_sm;  // resident count/scatter CTAs per SM
+    const bool small = c->stage_chunk == 2048;
+    const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
+                                              : (small ? stage_ctas_per_sm<StageSmall>() : stage_ctas_per_sm<StageLarge>());
     const int64_t wave = (int64_t)c->sms * per_sm;
     const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
     const int tile = (n + ntiles - 1) / ntiles;
@@ -474,10 +494,14 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     if (!c->attrs_set) {
         XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem<StageLarge>)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem<StageSmall>)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem<StageLarge>)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StageSmem<SplitSmall>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
         c->attrs_set = true;
     }
@@ -488,16 +512,24 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    if (d <= 2 && b1 <= 10 && c->key_tables) {
+    if (d <= 2 && b1 <= kMaxFirstLevelBits && c->key_tables) {
         XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
         XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
                                                                                    P<uint32_t>(c->tcnt)));
         XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
-        XTN_LAUNCH("bucket_scatter", k_bucket_scatter_staged<<<ntiles, kStageThreads, sizeof(StageSmem), s>>>(
-                                         P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
-                                         P<uint64_t>(c->voff), P<uint64_t>(c->toff), n, tile, d, b1, idbits,
-                                         P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+        if (small)
+            XTN_LAUNCH("bucket_scatter",
+                       k_bucket_scatter_staged<StageSmall><<<ntiles, StageSmall::kThreads, sizeof(StageSmem<StageSmall>), s>>>(
+                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
+                           P<uint64_t>(c->toff), n, tile, d, b1, idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart),
+                           P<uint64_t>(c->recA)));
+        else
+            XTN_LAUNCH("bucket_scatter",
+                       k_bucket_scatter_staged<StageLarge><<<ntiles, StageLarge::kThreads, sizeof(StageSmem<StageLarge>), s>>>(
+                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
+                           P<uint64_t>(c->toff), n, tile, d, b1, idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart),
+                           P<uint64_t>(c->recA)));
     } else
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
@@ -521,9 +553,16 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_CK(cudaStreamSynchronize(s));
     memcpy(cnt, c->h_scalar, 32);
     if (cnt[1] > 0) {
-        XTN_LAUNCH("bucket_split", k_bucket_split_staged<<<cnt[1], kStageThreads, sizeof(StageSmem), s>>>(
-                                       P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
-                                       P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
+        if (c->split_chunk == 2048)
+            XTN_LAUNCH("bucket_split",
+                       k_bucket_split_staged<SplitSmall><<<cnt[1], SplitSmall::kThreads, sizeof(StageSmem<SplitSmall>), s>>>(
+                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                           P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
+        else
+            XTN_LAUNCH("bucket_split",
+                       k_bucket_split_staged<StageLarge><<<cnt[1], StageLarge::kThreads, sizeof(StageSmem<StageLarge>), s>>>(
+                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                           P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -607,7 +646,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * n));
     const bool tables = d <= 2 && c->key_tables;
     if (tables) XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)n));
-    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen),
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(chars, offs, rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen),
                                              P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo),
                                              tables ? P<uint64_t>(c->ktab) : nullptr));
     XTN_CK(cudaGetLastError());
@@ -1169,9 +1208,11 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     if (!strcmp(name, "engine") && (v == 0 || v == 1)) c->engine = (int)v;
     else if (!strcmp(name, "bucket_bits_max") && v >= 1 && v <= 14) c->bucket_bits_max = (int)v;
     else if (!strcmp(name, "group_cap") && v >= 2 && v <= kGroupCap) c->group_cap = (uint32_t)v;
-    else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 1 && v <= 4) c->scatter_ctas_per_sm = (int)v;
+    else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 0 && v <= 4) c->scatter_ctas_per_sm = (int)v;
     else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
+    else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
+    else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
         return XTN_ERR_ARG;
@@ -1307,7 +1348,7 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
     if (!cv.take(&keys, n) || !cv.take(&klen, n) || !cv.take(&vcnt, n) || !cv.take(&voff, n + 1) ||
         !cv.take(&runinfo, n) || !cv.take(&scan64, scan_scratch_elems(n)) || !cv.take(&counter, 2))
         return arena_full("sequence tables");
-    XTN_LAUNCH("pack", k_pack<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo,
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo,
                                                                  nullptr));
     XTN_CK(cudaGetLastError());
     scan_exclusive<uint32_t, uint64_t>(vcnt, voff, n, scan64, s);
