@@ -61,30 +61,69 @@ def measured_peak_hbm():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clock and clock-event reasons of one GPU while the timed steps run: NVML read-only
+    queries every 10 ms from a thread (nvidia-smi every 200 ms when NVML is unavailable)."""
 
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+               0x80: "hw_power_brake_slowdown"}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    def __init__(self, device: int, period: float = 0.01):
+        self.device = device
+        self.period = period
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self.thread = self.proc = self.path = None
+        self.stop_flag = False
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        import threading
+
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def loop():
+                while not self.stop_flag:
+                    self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.reasons.update(name for bit, name in self.REASONS.items() if r & bit)
+                    time.sleep(self.period)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.thread:
+            self.stop_flag = True
+            self.thread.join(timeout=5)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 10 ms"}
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -106,12 +145,8 @@ class ClockSampler:
                     if v.lower() == "active":
                         reasons.add(nm)
         os.unlink(self.path)
-        return {
-            "sm_mhz": statistics.median(sm) if sm else None,
-            "sm_max_mhz": max(mx) if mx else None,
-            "reasons": sorted(reasons),
-            "samples": len(sm),
-        }
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | None:
@@ -136,6 +171,21 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
         return 8.0 * V
     if kernel == "verify":
         return 10.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
+    return None
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` on
+    `workload`, from the committed ncu summary profiles/<kernel>_<workload>.md (its line
+    `traffic_bytes_per_launch: N`), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
     return None
 
 
@@ -285,7 +335,7 @@ def run_ours(args, w):
             "peak_kind": peak_kind,
             "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None,
-            "traffic": None,
+            "traffic": ncu_traffic(dom_name, args.workload),
             "algorithmic_bytes_per_launch": (ab / launches_per_step) if ab else None,
             "launch_ms": per_launch_ms,
             "share_of_kernel_time": dom_ms / total_kernel_ms,

@@ -143,7 +143,8 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *   "engine"          0 = hash-bucket grouping in shared memory (default),
  *                     1 = full radix sort of the variant records (the plain comparison form)
  *   "bucket_bits_max" 1..14: upper bound on log2(number of first-level buckets) (default 9;
- *                     above 9 the first-level scatter stores records one by one)
+ *                     above the stage shape's fan-out, 10 for stage_chunk 4096 and 9 for
+ *                     2048, the first-level scatter stores records one by one)
  *   "group_cap"       2..4096: largest bucket grouped in shared memory; larger ones are split
  *                     by further hash bits, and what still does not fit is grouped by sorting
  *                     (default 4096)

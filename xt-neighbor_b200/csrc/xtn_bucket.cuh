@@ -36,7 +36,7 @@ constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp
 // First-level fan-out: a staged chunk of 2048..4096 records leaves runs of 4..8 records
 // (32..64 bytes) per bucket; consecutive chunks of one CTA extend the same runs, so their
 // boundary sectors complete in L2.
-constexpr int kMaxFirstLevelBits = 9;
+constexpr int kMaxFirstLevelBits = 9;  // default bound; the large stage shape takes up to 10
 constexpr int kMaxSplitBits = 10;
 
 // Shape of a staged partition: threads per CTA, records per chunk, largest fan-out.
@@ -62,7 +62,6 @@ constexpr int kDigits = 1 << kDigitBits;
 // Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to 2048;
 // buckets with more than this go to the sort-based fallback).
 constexpr int kMaxRuns = 1024;
-constexpr uint32_t kWaitLimit = 1u << 26;  // bound on mbarrier polls
 
 // Descriptor of one bucket (or sub-bucket) handed to the grouping kernel.
 struct BucketDesc {
@@ -154,7 +153,7 @@ __global__ void k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles
 // ------------------------------------------------------------------ staged partition
 template <class C>
 struct StageSmem {
-    uint64_t rec[C::kChunk];     // records of the chunk, in arrival order
+    uint64_t rec[C::kChunk + 2]; // records of the chunk, in arrival order (+ bulk-copy alignment)
     uint64_t sorted[C::kChunk];  // the same records grouped by bucket
     uint16_t bkt[C::kChunk];     // bucket of rec[i]
     uint16_t sbkt[C::kChunk];    // bucket of sorted[i]
@@ -165,6 +164,8 @@ struct StageSmem {
     uint16_t rel_t[C::kChunk];   // toff of the chunk's sequences, relative to the chunk
     uint32_t warp_sums[C::kThreads / 32 + 1];
     uint32_t seq_end;
+    uint32_t wait_failed;
+    unsigned long long mbar;     // completion barrier of the chunk bulk copies (split)
 };
 
 // Resident CTAs per SM that a stage shape's shared memory allows (228 KB per SM, 1 KB
@@ -214,6 +215,76 @@ __device__ __forceinline__ void stage_partition(StageSmem<C>& S, int nb, uint32_
     __syncthreads();
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
     __syncthreads();
+}
+
+// Split form of stage_partition: the chunk's records are r[0..m) and their bucket is
+// r[p] >> shift; after_rank() runs once every thread is done reading r.
+template <class C, class Hook>
+__device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r, int shift,
+                                                uint64_t* __restrict__ dst, Hook&& after_rank) {
+    constexpr int kStageThreads = C::kThreads, kFanPer = C::kFanPer;
+    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[(uint32_t)(r[p] >> shift)], 1u);
+    __syncthreads();
+    {
+        uint32_t tot, loc[kFanPer], sum = 0;
+        const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++) {
+            loc[k] = sum;
+            sum += (b0 + k < nb) ? S.cnt[b0 + k] : 0u;
+        }
+        const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++)
+            if (b0 + k < nb) {
+                S.lstart[b0 + k] = ex + loc[k];
+                S.cnt[b0 + k] = ex + loc[k];
+            }
+    }
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
+        const uint64_t x = r[p];
+        const uint32_t b = (uint32_t)(x >> shift);
+        const uint32_t q = atomicAdd(&S.cnt[b], 1u);
+        S.sorted[q] = x;
+        S.sbkt[q] = (uint16_t)b;
+    }
+    __syncthreads();
+    after_rank();
+    for (uint32_t q = threadIdx.x; q < m; q += kStageThreads) {
+        const uint16_t b = S.sbkt[q];
+        dst[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
+    __syncthreads();
+}
+
+constexpr uint32_t kWaitLimit = 1u << 26;  // bound on mbarrier polls
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// One bulk copy of `bytes` (a multiple of 16) from 16-byte aligned global memory into shared
+// memory, completing on `mbar` (issued by one thread).
+__device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst_smem),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
 }
 
 // Tasks per sequence for the staged scatter (for_each_task_variant): 2 * ceil(runs / 2).
@@ -354,7 +425,8 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
 // One CTA per split job: histogram of the record's top `bits` bits (the next hash bits),
 // sub-bucket descriptors, then the bucket's records, chunk by chunk, through the staged
 // partition into buffer B at the same range. Sub-buckets that fit are listed for grouping;
-// larger ones go to the fallback list.
+// larger ones go to the fallback list. counters[5] counts CTAs whose chunk copy did not
+// complete within the wait bound (their output is incomplete; the host reports an error).
 template <class C>
 __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_split_staged(
     const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t group_cap,
@@ -366,12 +438,29 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;
     const bool priv = nsub <= kPrivFan;
+    const uint64_t* src = in + job.start;
+    // Chunk c of the job reaches S.rec by one bulk copy from the 16-byte boundary at or below
+    // its first record (the record buffers carry 16 bytes of padding), completing on S.mbar
+    // with parity c & 1. The copy of chunk c + 1 is issued as soon as chunk c's records are
+    // ranked, so it overlaps chunk c's write-out.
+    const uint32_t mbar = smem_u32(&S.mbar);
+    auto issue = [&](uint32_t c0) {
+        const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
+        const uint64_t* a = src + c0;
+        const uint32_t lead = (uint32_t)(((uintptr_t)a & 15u) >> 3);
+        bulk_load(smem_u32(&S.rec[0]), a - lead, ((lead + m) * 8u + 15u) & ~15u, mbar);
+    };
+    if (threadIdx.x == 0) {
+        S.wait_failed = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (job.size > 0) issue(0);
+    }
     // histogram: per-warp copies (in `sorted`, unused until the first chunk) for small fan-outs
     uint32_t* hist = priv ? reinterpret_cast<uint32_t*>(S.sorted) + (threadIdx.x >> 5) * kPrivFan : S.cnt;
     for (int i = threadIdx.x; i < (priv ? kPrivFan * (kStageThreads / 32) : nsub); i += kStageThreads)
         (priv ? reinterpret_cast<uint32_t*>(S.sorted) : S.cnt)[i] = 0;
     __syncthreads();
-    const uint64_t* src = in + job.start;
     {
         // 16-byte loads, four in flight per thread (job.start is 8-byte aligned: peel one)
         const uint32_t lead = (uint32_t)(((uintptr_t)src & 15u) >> 3);
@@ -427,16 +516,34 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
         }
     }
     __syncthreads();
-    for (uint32_t c0 = 0; c0 < job.size; c0 += kStageChunk) {
+    uint32_t parity = 0;
+    for (uint32_t c0 = 0; c0 < job.size; c0 += kStageChunk, parity ^= 1u) {
         const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
-#pragma unroll 4
-        for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
-            const uint64_t r = __ldg(src + c0 + p);
-            S.rec[p] = r;
-            S.bkt[p] = (uint16_t)(r >> shift);
+        const uint32_t lead = (uint32_t)(((uintptr_t)(src + c0) & 15u) >> 3);
+        if (threadIdx.x == 0) {
+            uint32_t polls = 0;
+            while (!mbar_try_wait(mbar, parity)) {
+                if (++polls > kWaitLimit) {
+                    S.wait_failed = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
         }
         __syncthreads();
-        stage_partition(S, nsub, m, out);
+        if (S.wait_failed) {
+            // one more bounded wait for the copy to land before the shared memory is released
+            if (threadIdx.x == 0) {
+                uint32_t polls = 0;
+                while (!mbar_try_wait(mbar, parity) && ++polls < kWaitLimit) __nanosleep(64);
+                atomicAdd(&counters[5], 1u);
+            }
+            __syncthreads();
+            return;
+        }
+        split_partition(S, nsub, m, S.rec + lead, shift, out, [&] {
+            if (threadIdx.x == 0 && c0 + kStageChunk < job.size) issue(c0 + kStageChunk);
+        });
     }
 }
 
@@ -463,18 +570,6 @@ struct GroupSmem {
     unsigned long long base;
     unsigned long long mbar;
 };
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(mbar), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
 
 __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits) {
     return a < b ? ((a << idbits) | b) : ((b << idbits) | a);

@@ -512,7 +512,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    if (d <= 2 && b1 <= kMaxFirstLevelBits && c->key_tables) {
+    const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
+    if (d <= 2 && (1 << b1) <= stage_fan && c->key_tables) {
         XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
         XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
@@ -567,6 +568,10 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
         memcpy(cnt, c->h_scalar, 32);
+        if (cnt[5] != 0) {
+            set_err("bucket split: " + std::to_string(cnt[5]) + " chunk copies did not complete in time");
+            return XTN_ERR_CUDA;
+        }
     }
     XTN_CK(cudaEventRecord(c->ev[3], s));
     const uint32_t ndesc = cnt[0];
