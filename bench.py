@@ -36,6 +36,10 @@ WORKLOADS = {
     "nn_10k_leven_d1": dict(kind="mutants", n=10_000, d=1, measure=0, seed=20240),
     "nn_10m_leven_d2": dict(kind="clusters", n=10_000_000, d=2, measure=0, seed=20242),
     "nn_10m_hamming_d2": dict(kind="clusters", n=10_000_000, d=2, measure=1, seed=20242),
+    # repertoire overlap: 64 repertoires, sizes log-uniform in [1e4, 2e6] (23.9M rows with this
+    # seed), 5% of each drawn from a shared pool, power-law duplicate counts; Levenshtein d = 1
+    "overlap_64rep_leven_d1": dict(kind="repertoires", n_reps=64, min=1e4, max=2e6, shared=0.05, d=1, measure=0,
+                                   seed=20244),
 }
 DEFAULT_WORKLOAD = "nn_1m_leven_d2"
 METRIC = "seqs/s (symmetric-deletion NN search, whole job)"
@@ -43,11 +47,14 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def gen_workload(w):
+    """(chars, offsets, info or None, repertoire sizes or None)."""
     import xtn
 
+    if w["kind"] == "repertoires":
+        return xtn.synth_repertoires(w["seed"], w["n_reps"], w["min"], w["max"], w["shared"])
     if w["kind"] == "clusters":
-        return xtn.synth_clusters(w["seed"], w["n"], 0.20, 0.02)
-    return xtn.synth_mutants(w["seed"], w["n"], 0.10)
+        return (*xtn.synth_clusters(w["seed"], w["n"], 0.20, 0.02), None, None)
+    return (*xtn.synth_mutants(w["seed"], w["n"], 0.10), None, None)
 
 
 def measured_peak_hbm():
@@ -212,7 +219,8 @@ def run_ours(args, w):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
         pg = dist
-    chars, offs = gen_workload(w)
+    chars, offs, info, reps = gen_workload(w)
+    overlap = info is not None
     n = len(offs) - 1
     opts = {k: int(v) for k, v in (o.split("=", 1) for o in args.opt)}
     opts.setdefault("engine", 1 if args.engine == "sort" else 0)
@@ -220,11 +228,15 @@ def run_ours(args, w):
     ctx.set_profiling(True)
     d_chars = torch.from_numpy(chars).cuda()
     d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
+    d_info = torch.from_numpy(np.ascontiguousarray(info)).cuda() if overlap else None
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     ext = torch.cuda.ExternalStream(ctx.stream())
     torch.cuda.synchronize()
 
     def step():
+        if overlap:
+            return ctx.overlap_device(d_chars.data_ptr(), d_offs.data_ptr(), n, d_info.data_ptr(), len(reps), w["d"],
+                                      w["measure"])
         return ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
 
     for _ in range(args.warmup):
@@ -267,7 +279,10 @@ def run_ours(args, w):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(ext)
-        res = ctx.perform(hc, ho, distance=w["d"], measure=w["measure"])
+        if overlap:
+            res = ctx.perform(hc, ho, distance=w["d"], measure=w["measure"], info=info, n_reps=len(reps))
+        else:
+            res = ctx.perform(hc, ho, distance=w["d"], measure=w["measure"])
         e1.record(ext)
         e1.synchronize()
         if i >= args.warmup:
@@ -311,20 +326,23 @@ def run_ours(args, w):
             "n_seqs": n,
             "distance": w["d"],
             "measure": "hamming" if w["measure"] else "leven",
+            "mode": "overlap" if overlap else "nn",
+            "repertoires": len(reps) if overlap else None,
             "parallelism": f"replicas x{world}",
             "engine": args.engine,
             "options": {o.split("=", 1)[0]: int(o.split("=", 1)[1]) for o in args.opt},
             "l2": "flushed between steps (256 MiB write)",
         },
-        "pairs_per_s": world * n_out / (ms_step / 1e3),
-        "verified_pairs": n_out,
+        "pairs_per_s": None if overlap else world * n_out / (ms_step / 1e3),
+        "verified_pairs": stats["n_verified_pairs"] if overlap else n_out,
+        "output_entries": n_out,
         "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_out")},
         "e2e": {
             "value": world * n / (e2e_ms / 1e3),
             "unit": "seqs/s",
             "ms_per_step": e2e_ms,
-            "h2d_bytes_per_step": int(len(chars) + 4 * len(offs)),
-            "d2h_bytes_per_step": int(n_out * 9),
+            "h2d_bytes_per_step": int(len(chars) + 4 * len(offs) + (12 * n if overlap else 0)),
+            "d2h_bytes_per_step": int(n_out * (16 if overlap else 9)),
         },
         "gpu_launches": int(launches),
         "roofline": {
@@ -344,49 +362,58 @@ def run_ours(args, w):
         "clocks": clocks,
     }
     if world == 1 and not args.no_cli:
-        line["cli_process"] = cli_process(args, w, chars, offs)
+        line["cli_process"] = cli_process(args, w, chars, offs, info, reps)
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(chars, offs, w)
+        line["cpu_baseline"] = cpu_baseline(chars, offs, w, info, reps)
     ctx.close()
     if pg:
         pg.destroy_process_group()
     return line
 
 
-def cpu_baseline(chars, offs, w, max_seconds=30.0):
-    """The CPU oracle (multithreaded restatement of the reference algorithm) on the workload."""
+def cpu_baseline(chars, offs, w, info=None, reps=None, max_seqs=2_000_000):
+    """The CPU oracle (multithreaded restatement of the reference algorithm) on the workload:
+    the whole input in nearest-neighbour mode; in overlap mode the leading repertoires up to
+    about max_seqs rows (a bounded sample of the same workload)."""
+    import numpy as np
+
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
     n = len(offs) - 1
-    sample = n
     t0 = time.perf_counter()
-    orc.nn_search(chars, offs, w["d"], w["measure"])
+    if info is None:
+        orc.nn_search(chars, offs, w["d"], w["measure"])
+        sample, what = n, f"whole workload ({n} seqs), one search"
+    else:
+        k = max(1, int(np.searchsorted(np.cumsum(reps), max_seqs, side="right")))
+        rows = int(np.sum(reps[:k]))
+        sub_info = np.ascontiguousarray(info[:rows])
+        orc.overlap_search(chars[: offs[rows]], offs[: rows + 1], sub_info, w["d"], w["measure"])
+        sample, what = rows, f"first {k} repertoires ({rows} rows), one overlap search"
     dt = time.perf_counter() - t0
     return {
         "value": sample / dt,
         "unit": "seqs/s",
         "cores": orc.threads(),
         "kind": "port",
-        "sample": f"whole workload ({sample} seqs), one search",
+        "sample": what,
         "seconds": dt,
     }
 
 
-def cli_process(args, w, chars, offs):
-    """The xt_neighbor CLI as a whole process on the workload file (parse + search, no -o),
+def cli_process(args, w, chars, offs, info=None, reps=None):
+    """The xt_neighbor CLI as a whole process on the workload files (parse + search, no -o),
     timed like the reference's published harness: wall clock around the process."""
     import xtn
 
     n = len(offs) - 1
     with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "seqs.csv")
-        write_csv(chars, offs, path)
-        cmd = [xtn.CLI_PATH, "-i", path, "-n", str(n), "-d", str(w["d"])] + (["-m", "hamming"] if w["measure"] else [])
+        cmd = [xtn.CLI_PATH] + workload_files(td, w, chars, offs, info, reps)
         times = []
         for i in range(2 + 3):
             t0 = time.perf_counter()
-            p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
             dt = time.perf_counter() - t0
             if p.returncode != 0:
                 return {"error": p.stderr[-200:]}
@@ -397,16 +424,33 @@ def cli_process(args, w, chars, offs):
             "what": "xt_neighbor CLI process: CSV parse + search, no -o, wall clock"}
 
 
-def write_csv(chars, offs, path):
-    import numpy as np
+def workload_files(td, w, chars, offs, info=None, reps=None):
+    """Writes the workload in the CLI's input format under td; returns the CLI arguments."""
+    n = len(offs) - 1
+    path = os.path.join(td, "seqs.csv")
+    write_csv(chars, offs, path, None if info is None else info[:, 0])
+    cmd = ["-i", path, "-n", str(n), "-d", str(w["d"])] + (["-m", "hamming"] if w["measure"] else [])
+    if info is not None:
+        ipath = os.path.join(td, "info.csv")
+        with open(ipath, "w") as f:
+            f.write("size\n" + "".join(f"{int(r)}\n" for r in reps))
+        cmd += ["-I", ipath, "-N", str(len(reps))]
+    return cmd
 
+
+def write_csv(chars, offs, path, counts=None):
     b = chars.tobytes()
     with open(path, "wb") as f:
-        f.write(b"cdr3\n")
+        f.write(b"cdr3\n" if counts is None else b"cdr3,count\n")
         out = bytearray()
         for i in range(len(offs) - 1):
             out += b[offs[i] : offs[i + 1]]
+            if counts is not None:
+                out += b",%d" % int(counts[i])
             out += b"\n"
+            if len(out) > (64 << 20):
+                f.write(out)
+                out = bytearray()
         f.write(out)
 
 
@@ -418,16 +462,12 @@ def run_reference(args, w):
     if rank != 0:
         return None
     ref = os.path.join(ROOT, "oracle", "_ref", "xt_neighbor_ref")
-    chars, offs = gen_workload(w)
+    chars, offs, info, reps = gen_workload(w)
     n = len(offs) - 1
     if not os.path.exists(ref):
         return {"impl": "reference", "unavailable": "reference build oracle/_ref/xt_neighbor_ref missing"}
     with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "seqs.csv")
-        write_csv(chars, offs, path)
-        cmd = [ref, "-i", path, "-n", str(n), "-d", str(w["d"])]
-        if w["measure"]:
-            cmd += ["-m", "hamming"]
+        cmd = [ref] + workload_files(td, w, chars, offs, info, reps)
         env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
         times = []
         for i in range(args.warmup + args.steps):
@@ -455,7 +495,8 @@ def run_reference(args, w):
         "dtype": "u32",
         "data": "synthetic (seeded CDR3 generator)",
         "config": {"workload": args.workload, "n_seqs": n, "distance": w["d"],
-                   "measure": "hamming" if w["measure"] else "leven", "parallelism": "single process"},
+                   "measure": "hamming" if w["measure"] else "leven", "mode": "nn" if info is None else "overlap",
+                   "parallelism": "single process"},
         "cpu_baseline": {"value": v, "unit": "seqs/s", "cores": 1, "kind": "reference",
                          "sample": "reference xt_neighbor (CUDA build, sm_100a) on this GPU; whole process: "
                                    "parse + search, no -o, wall clock"},

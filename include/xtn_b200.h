@@ -120,6 +120,14 @@ int xtn_context_perform(xtn_context* ctx, const xtn_args* args, const char* seqs
 int xtn_context_nn_device(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
                           int32_t n_seqs, int64_t* n_out);
 
+/* Overlap mode on inputs already in device memory: d_info holds one xtn_seq_info per row
+ * (row order) and args->info_len is the number of repertoires. The result (repertoire pairs
+ * with their sums) stays on the device; *n_out receives its length. Read it with
+ * xtn_context_fetch. Replaces the device-side part of xtn_perform's overlap mode
+ * (xtneighbor_streaming/src/xtn.cu:267-509 with a non-null SeqInfo). */
+int xtn_context_overlap_device(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                               int32_t n_seqs, const xtn_seq_info* d_info, int64_t* n_out);
+
 /* Copies up to `cap` entries of the last result to host memory (either pointer may be NULL). */
 int xtn_context_fetch(xtn_context* ctx, xtn_int2* pairs, int8_t* distances, uint64_t* frequencies, int64_t cap);
 

@@ -19,6 +19,7 @@
  * Parallelism: OpenMP across host cores (the CPU baseline reports the thread count).
  */
 #include <algorithm>
+#include <array>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -728,6 +729,37 @@ int orc_overlap_search(const char* chars, const uint32_t* offs, int n, const int
         R->freq.push_back(kv.second);
     }
     return 0;
+}
+
+// Exhaustive neighbours of a few query sequences: every (min, max, dist) with the query on
+// one side and dist(query, j) <= d under the verification semantics above (x != y). This is
+// the reference's output restricted to those queries when every sequence is shorter than 128
+// residues: there a distance <= d implies a shared deletion variant of the 18-residue keys,
+// so the candidate stage of S/src/xtn.cu misses nothing. Used to check completeness on
+// inputs too large for a full oracle run. Returns the number of triples (written up to cap).
+int64_t orc_brute_neighbors(const char* chars, const uint32_t* offs, int n, const int32_t* queries, int nq, int d,
+                            int measure, int32_t* out, int64_t cap) {
+    std::vector<std::array<int32_t, 3>> all;
+    const int nt = nthreads_or_default();
+    for (int qi = 0; qi < nq; qi++) {
+        const int q = queries[qi];
+        const int lq = (int)(offs[q + 1] - offs[q]);
+        std::vector<std::vector<std::array<int32_t, 3>>> part(nt);
+#pragma omp parallel for schedule(static) num_threads(nt)
+        for (int j = 0; j < n; j++) {
+            if (j == q) continue;
+            const int lj = (int)(offs[j + 1] - offs[j]);
+            if (measure == LEVENSHTEIN ? std::abs(lq - lj) > d : (lq != lj && 77 > d)) continue;
+            const int dist = pair_distance(chars, offs, q, j, measure);
+            if (dist <= d) part[omp_get_thread_num()].push_back({std::min(q, j), std::max(q, j), dist});
+        }
+        for (auto& v : part) all.insert(all.end(), v.begin(), v.end());
+    }
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    for (int64_t i = 0; i < (int64_t)all.size() && i < cap; i++)
+        for (int k = 0; k < 3; k++) out[3 * i + k] = all[i][k];
+    return (int64_t)all.size();
 }
 
 }  // extern "C"

@@ -43,6 +43,9 @@ def load():
         lib.orc_result_copy.argtypes = [P, P, P, P]
         lib.orc_nn_search.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
         lib.orc_overlap_search.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P]
+        lib.orc_brute_neighbors.restype = ctypes.c_int64
+        lib.orc_brute_neighbors.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P,
+                                            ctypes.c_int64]
         _lib = lib
     return _lib
 
@@ -231,6 +234,22 @@ def overlap_search(chars, offs, info, d: int, measure: int = 0):
         return pairs, sums
     finally:
         lib.orc_result_free(r)
+
+
+def brute_neighbors(chars, offs, queries, d: int, measure: int = 0):
+    """Exhaustive (min, max, dist) neighbours of the query sequences, sorted; equal to the
+    reference output restricted to those queries for sequences shorter than 128 residues."""
+    lib = load()
+    chars = np.ascontiguousarray(chars, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint32)
+    q = np.ascontiguousarray(queries, dtype=np.int32)
+    cap = 1 << 16
+    while True:
+        out = np.zeros(3 * cap, np.int32)
+        m = lib.orc_brute_neighbors(ptr(chars), ptr(offs), len(offs) - 1, ptr(q), len(q), d, measure, ptr(out), cap)
+        if m <= cap:
+            return out[: 3 * m].reshape(-1, 3)
+        cap = int(m)
 
 
 def levenshtein(a: str, b: str) -> int:

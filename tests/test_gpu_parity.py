@@ -165,3 +165,25 @@ def test_context_reuse_and_device_entry(ctx):
     assert_same_pairs(b.pairs, b.distances, a.pairs, a.distances, "device entry")
     st = ctx.stats()
     assert st["n_out"] == len(a.pairs) and st["n_variants"] > 0
+
+
+def test_overlap_device_entry(ctx):
+    """xtn_context_overlap_device (inputs in device memory) equals the host-buffer entry; a
+    repertoire id outside [0, R) is reported with the first offending row."""
+    import torch
+
+    chars, offs, info, reps = xtn.synth_repertoires(seed=11, n_reps=6, min_size=300, max_size=3000, shared=0.2)
+    a = ctx.perform(chars, offs, distance=1, info=info, n_reps=len(reps))
+    dch = torch.from_numpy(chars).cuda()
+    dof = torch.from_numpy(offs.view(np.int32)).cuda()
+    dinf = torch.from_numpy(np.ascontiguousarray(info)).cuda()
+    torch.cuda.synchronize()
+    m = ctx.overlap_device(dch.data_ptr(), dof.data_ptr(), len(offs) - 1, dinf.data_ptr(), len(reps), distance=1)
+    b = ctx.fetch_overlap(m)
+    assert a.pairs.tolist() == b.pairs.tolist()
+    assert np.array_equal(a.frequencies, b.frequencies)
+    bad = info.copy()
+    bad[9, 1] = -1
+    bad[7, 1] = len(reps)
+    with pytest.raises(xtn.XtnError, match="out of range at row 7$"):
+        ctx.perform(chars, offs, distance=1, info=bad, n_reps=len(reps))

@@ -309,7 +309,7 @@ struct xtn_context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[S_COUNT + 1] = {};
     // inputs (host-buffer API)
-    DevBuf chars, offs;
+    DevBuf chars, offs, info;
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
@@ -985,30 +985,42 @@ namespace xtn {
 
 constexpr int kMaxRepertoires = 8192;
 
-int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* h_info, int n, int d,
+// De-interleaves the per-row info into frequency and repertoire arrays; *bad_row receives the
+// smallest row whose repertoire id is outside [0, R) (it starts at INT_MAX).
+__global__ void k_split_info(const xtn_seq_info* __restrict__ info, int n, int R, int32_t* __restrict__ freq,
+                             int32_t* __restrict__ rep, int* __restrict__ bad_row) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const xtn_seq_info v = info[i];
+    freq[i] = v.frequency;
+    rep[i] = v.repertoire;
+    if (v.repertoire < 0 || v.repertoire >= R) atomicMin(bad_row, i);
+}
+
+// Overlap mode on device-resident inputs (d_info: one xtn_seq_info per row, row order).
+int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* d_info, int n, int d,
                 int measure, int R) {
     if (R > kMaxRepertoires) {
         set_err("overlap mode supports at most " + std::to_string(kMaxRepertoires) + " repertoires");
         return XTN_ERR_LIMIT;
     }
-    for (int i = 0; i < n; i++)
-        if (h_info[i].repertoire < 0 || h_info[i].repertoire >= R) {
-            set_err("repertoire id out of range at row " + std::to_string(i));
-            return XTN_ERR_ARG;
-        }
     cudaStream_t s = c->stream;
     xtn_overlap_bufs& b = *reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
     const int idbits = id_bits_for(n);
-    // frequencies and repertoires, de-interleaved on the host
-    std::vector<int32_t> hf(n), hr(n);
-    for (int i = 0; i < n; i++) {
-        hf[i] = h_info[i].frequency;
-        hr[i] = h_info[i].repertoire;
-    }
     XTN_TRY(ensure(b.freq, sizeof(int32_t) * n));
     XTN_TRY(ensure(b.rep, sizeof(int32_t) * n));
-    XTN_CK(cudaMemcpyAsync(b.freq.p, hf.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-    XTN_CK(cudaMemcpyAsync(b.rep.p, hr.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    XTN_TRY(ensure(c->counter, 64));
+    const int int_max = 0x7fffffff;
+    XTN_CK(cudaMemcpyAsync(c->counter.p, &int_max, sizeof(int), cudaMemcpyHostToDevice, s));
+    XTN_LAUNCH("split_info", k_split_info<<<blocks_for(n), kThreads, 0, s>>>(d_info, n, R, P<int32_t>(b.freq),
+                                                                              P<int32_t>(b.rep), P<int>(c->counter)));
+    XTN_CK(cudaGetLastError());
+    uint64_t bad = 0;
+    XTN_TRY(read_scalar(c, c->counter.p, 4, &bad));
+    if ((int)bad != int_max) {
+        set_err("repertoire id out of range at row " + std::to_string((int)bad));
+        return XTN_ERR_ARG;
+    }
 
     // 1. merge identical strings
     XTN_TRY(ensure(b.recA, sizeof(uint64_t) * n));
@@ -1134,7 +1146,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab};
+                      &c->ktab,    &c->info};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1174,6 +1186,26 @@ int xtn_context_nn_device(xtn_context* c, const xtn_args* args, const char* d_se
     return r;
 }
 
+int xtn_context_overlap_device(xtn_context* c, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                               int32_t n, const xtn_seq_info* d_info, int64_t* n_out) {
+    if (!c || !d_seqs || !d_offsets || !d_info || n < 1) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    if (args->info_len < 1) {
+        set_err("invalid info length");
+        return XTN_ERR_ARG;
+    }
+    XTN_CK(cudaSetDevice(c->device));
+    begin_run(c);
+    int r = run_overlap(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, d_info, n, args->distance, args->measure,
+                        args->info_len);
+    end_run(c);
+    if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
+    return r;
+}
+
 int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, const uint32_t* offsets, int32_t n,
                         const xtn_seq_info* info, xtn_callback cb, void* user) {
     if (!c || !seqs || !offsets || n < 1) {
@@ -1193,7 +1225,9 @@ int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, 
             set_err("invalid info length");
             return XTN_ERR_ARG;
         }
-        r = run_overlap(c, dch, dof, info, n, args->distance, args->measure, args->info_len);
+        XTN_TRY(ensure(c->info, sizeof(xtn_seq_info) * (size_t)n));
+        XTN_CK(cudaMemcpyAsync(c->info.p, info, sizeof(xtn_seq_info) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        r = run_overlap(c, dch, dof, P<xtn_seq_info>(c->info), n, args->distance, args->measure, args->info_len);
     } else {
         r = run_nn(c, dch, dof, nullptr, n, args->distance, args->measure);
     }

@@ -32,6 +32,7 @@ SYMBOLS = (
     "xtn_context_destroy",
     "xtn_context_perform",
     "xtn_context_nn_device",
+    "xtn_context_overlap_device",
     "xtn_context_fetch",
     "xtn_context_result_device",
     "xtn_context_stream",
@@ -120,6 +121,8 @@ def load():
     lib.xtn_context_perform.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P, CALLBACK, P]
     lib.xtn_perform.argtypes = [ctypes.POINTER(Args), P, P, ctypes.c_int32, P, CALLBACK, P]
     lib.xtn_context_nn_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_context_overlap_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P,
+                                               ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_fetch.argtypes = [P, P, P, P, ctypes.c_int64]
     lib.xtn_context_result_device.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_stream.argtypes = [P]
@@ -243,6 +246,30 @@ class Context:
             )
         )
         return nout.value
+
+    def overlap_device(self, d_chars: int, d_offsets: int, n: int, d_info: int, n_reps: int, distance=1,
+                       measure=LEVENSHTEIN) -> int:
+        """Overlap mode on device pointers (d_info: n x 3 int32 rows of frequency, repertoire,
+        original index); returns the number of (rep_x, rep_y) entries (kept on device)."""
+        args = Args(distance, measure, 0, n_reps)
+        nout = ctypes.c_int64()
+        _check(
+            self.lib.xtn_context_overlap_device(
+                self.h, ctypes.byref(args), ctypes.c_void_p(d_chars), ctypes.c_void_p(d_offsets), n,
+                ctypes.c_void_p(d_info), ctypes.byref(nout)
+            )
+        )
+        return nout.value
+
+    def fetch_overlap(self, n: int) -> Result:
+        pairs = np.zeros((n, 2), np.int32)
+        sums = np.zeros(n, np.uint64)
+        _check(
+            self.lib.xtn_context_fetch(
+                self.h, pairs.ctypes.data_as(ctypes.c_void_p), None, sums.ctypes.data_as(ctypes.c_void_p), n
+            )
+        )
+        return Result(pairs, None, sums)
 
     def fetch(self, n: int) -> Result:
         pairs = np.zeros((n, 2), np.int32)
