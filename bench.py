@@ -161,13 +161,15 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
     by the caller). V = deletion variants, P = candidate pairs, n = sequences."""
     V, Pc = st["n_variants"], st["n_candidates"]
     if kernel == "bucket_scatter":
-        return 8.0 * V + 48.0 * n  # each 8-byte record written once; key, run info, offsets read
+        # each 8-byte record written once; per sequence its 19-word key table (152 B), run info,
+        # variant and task offsets (8 B each) and key length (1 B) read once
+        return 8.0 * V + 177.0 * n
     if kernel == "bucket_group":
         return 8.0 * V + 8.0 * Pc  # each record read once; candidate pairs written
     if kernel == "bucket_split":
         return 16.0 * V  # records of split buckets read once and written once
     if kernel == "bucket_count":
-        return 17.0 * n  # key and length of each sequence
+        return 161.0 * n  # key table (152 B), run info (8 B) and key length (1 B) of each sequence
     if kernel == "key_sort_downsweep":
         return 16.0 * V  # sort engine: read + write each 8-byte record once
     if kernel == "key_sort_upsweep":

@@ -287,19 +287,22 @@ __device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void* src, ui
                  : "memory");
 }
 
-// Tasks per sequence for the staged scatter (for_each_task_variant): 2 * ceil(runs / 2).
-__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint32_t* __restrict__ tcnt) {
+// Tasks per sequence for the staged scatter: for d = 2, 2 * ceil(runs / 2) balanced tasks
+// (task_items); for d = 1 one task per variant (the key, then the single deletion of each
+// run), so a chunk's table loads are spread over all threads.
+__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, int d, uint32_t* __restrict__ tcnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t R = (uint32_t)popc32((uint32_t)runinfo[i]);
-    tcnt[i] = 2u * ((R + 1u) >> 1);
+    tcnt[i] = d >= 2 ? 2u * ((R + 1u) >> 1) : 1u + R;
 }
 
 // First-level scatter for d <= 2. The tile's sequences go through shared memory 4096
-// variants at a time; each chunk's variants are produced by balanced tasks (about R/2 + 1
-// variants each, one table load and one add per variant hash) written at their flat index,
-// then the staged partition writes them out by bucket. runinfo[i] is key_run_info of
-// sequence i, tab its key_table; toff is the exclusive scan of k_task_counts.
+// variants at a time; each chunk's variants are produced by tasks (at d = 2 balanced tasks of
+// about R/2 + 1 variants, at d = 1 single variants; one table load and one add per variant
+// hash), written at their index within the sequence; then the staged partition writes them out
+// by bucket. runinfo[i] is key_run_info of sequence i, tab its key_table; toff is the
+// exclusive scan of k_task_counts.
 template <class C>
 __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_scatter_staged(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
@@ -363,10 +366,19 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
             const int t = (int)(tau - S.rel_t[li]);
             const uint32_t vb = S.rel_v[li];
             const uint64_t id = (uint64_t)i;
-            for_each_task_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d, t, [&](int v, uint64_t h) {
+            auto put = [&](int v, uint64_t h) {
                 S.bkt[vb + v] = (uint16_t)(h >> shift);
                 S.rec[vb + v] = ((h << b1) & hi_mask) | id;
-            });
+            };
+            const uint64_t* row = tab + (size_t)i * kTabLen;
+            if (d >= 2) {
+                for_each_task_hash(row, klen[i], runinfo[i], d, t, put);
+            } else if (t == 0) {
+                put(0, hash_fin(row[kTabKey]));
+            } else {  // single deletion of run t - 1: r G[p] + r^-1 P_L
+                const int p = select_bit((uint32_t)runinfo[i], t - 1);
+                put(t, hash_fin(kPolyR * row[kTabG + p] + kPolyRI * row[kTabKey]));
+            }
         }
         __syncthreads();
         stage_partition(S, nb, m, recs);

@@ -88,8 +88,8 @@ struct KeyWords {
     uint64_t a, b;
 };
 XTN_HD KeyWords key_words(u128 v) { return KeyWords{(uint64_t)(v >> 68), (uint64_t)(v >> 38) & ((1ull << 30) - 1ull)}; }
-XTN_HD uint64_t word_code(KeyWords w, int i) {
-    return i < 12 ? (w.a >> (55 - 5 * i)) & 31u : (w.b >> (25 - 5 * (i - 12))) & 31u;
+XTN_HD uint32_t word_code(KeyWords w, int i) {
+    return (uint32_t)(i < 12 ? (w.a >> (55 - 5 * i)) & 31u : (w.b >> (25 - 5 * (i - 12))) & 31u);
 }
 
 // P of a packed key, by Horner's rule from the last position (zero padding adds nothing).
@@ -238,7 +238,7 @@ XTN_HD uint64_t key_run_info(u128 key, int L) {
     uint32_t longr = 0;
     int j = 0;
     for (uint32_t m = rs; m; m &= m - 1, j++) {
-        const int p = select_bit(m, 0);
+        const int p = ctz32(m);
         if ((cont >> (p + 1)) & 1u) longr |= 1u << j;
     }
     return (uint64_t)rs | ((uint64_t)longr << 32);
@@ -395,6 +395,13 @@ template <class F>
 XTN_HD void for_each_task_hash(const uint64_t* tab, int L, uint64_t info, int d, int t, F&& f) {
     TableHashEmitter<F> e(tab, f);
     task_items(L, info, d, t, e);
+}
+
+// All of a key's d <= 2 variants as hashes with the call count v = 0, 1, ...: f(v, hash).
+template <class F>
+XTN_HD void for_each_seq_hash(const uint64_t* tab, int L, uint64_t info, int d, F&& f) {
+    TableHashEmitter<F> e(tab, f);
+    seq_items(L, info, d, e);
 }
 
 // All of a key's d <= 2 variants as hashes: f(hash).

@@ -75,7 +75,14 @@ __global__ void __launch_bounds__(kPackThreads) k_pack(const uint8_t* __restrict
         uint32_t s = offs[r];
         int L = (int)(offs[r + 1] - s);
         int Lk = L < kKeyLen ? L : kKeyLen;
-        for (int j = 0; j < Lk; j++) v = key_put(v, j, (unsigned)code_of(chars[s + j]));
+        // the key's two 64-bit words (key_words), built with 64-bit shifts
+        uint64_t wa = 0, wb = 0;
+        for (int j = 0; j < Lk; j++) {
+            const uint64_t code = (uint64_t)code_of(chars[s + j]);
+            if (j < 12) wa |= code << (55 - 5 * j);
+            else wb |= code << (25 - 5 * (j - 12));
+        }
+        v = ((u128)wa << 68) | ((u128)wb << 38);
         keys[i] = v;
         klen[i] = (uint8_t)Lk;
         vcnt[i] = (uint32_t)variant_count(v, Lk, d);
@@ -516,7 +523,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     if (d <= 2 && (1 << b1) <= stage_fan && c->key_tables) {
         XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
         XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
-        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
+        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n, d,
                                                                                    P<uint32_t>(c->tcnt)));
         XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
         if (small)
@@ -896,25 +903,53 @@ __device__ __forceinline__ uint64_t freq_product(int32_t a, int32_t b) {
     return (uint64_t)(int64_t)a * (uint64_t)(int64_t)b;
 }
 
+// Diagonal term; with R <= kSmemReps the block accumulates into shared memory first.
+constexpr int kSmemReps = 96;
+
 __global__ void k_diag(const uint32_t* __restrict__ occ_start, const uint32_t* __restrict__ srow, int U,
                        const int32_t* __restrict__ freq, const int32_t* __restrict__ rep, int R,
                        unsigned long long* __restrict__ M, uint8_t* __restrict__ present) {
-    int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= U) return;
-    uint32_t s = occ_start[u], e = occ_start[u + 1];
-    for (uint32_t a = s; a < e; a++) {
-        uint32_t ra = srow[a];
-        for (uint32_t b = a; b < e; b++) {
-            uint32_t rb = srow[b];
-            size_t cell = (size_t)rep[ra] * R + rep[rb];
-            atomicAdd(&M[cell], (unsigned long long)freq_product(freq[ra], freq[rb]));
-            present[cell] = 1;
+    extern __shared__ unsigned long long s_m[];
+    const bool local = R <= kSmemReps;
+    uint8_t* s_p = reinterpret_cast<uint8_t*>(s_m + (local ? R * R : 0));
+    if (local) {
+        for (int k = threadIdx.x; k < R * R; k += blockDim.x) {
+            s_m[k] = 0;
+            s_p[k] = 0;
         }
+        __syncthreads();
+    }
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < U; u += gridDim.x * blockDim.x) {
+        const uint32_t s = occ_start[u], e = occ_start[u + 1];
+        for (uint32_t a = s; a < e; a++) {
+            const uint32_t ra = srow[a];
+            const int qa = rep[ra];
+            const int32_t fa = freq[ra];
+            for (uint32_t b = a; b < e; b++) {
+                const uint32_t rb = srow[b];
+                const size_t cell = (size_t)qa * R + rep[rb];
+                const unsigned long long f = (unsigned long long)freq_product(fa, freq[rb]);
+                if (local) {
+                    atomicAdd(&s_m[cell], f);
+                    s_p[cell] = 1;
+                } else {
+                    atomicAdd(&M[cell], f);
+                    present[cell] = 1;
+                }
+            }
+        }
+    }
+    if (local) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < R * R; k += blockDim.x)
+            if (s_p[k]) {
+                atomicAdd(&M[k], s_m[k]);
+                present[k] = 1;
+            }
     }
 }
 
 // Cross term; with R <= kSmemReps the block accumulates into shared memory first.
-constexpr int kSmemReps = 96;
 
 __global__ void k_cross(const xtn_int2* __restrict__ pairs, int64_t np, const uint32_t* __restrict__ occ_start,
                         const uint32_t* __restrict__ srow, const int32_t* __restrict__ freq,
@@ -1052,7 +1087,13 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     XTN_TRY(ensure(b.present, RR));
     XTN_CK(cudaMemsetAsync(b.M.p, 0, sizeof(unsigned long long) * RR, s));
     XTN_CK(cudaMemsetAsync(b.present.p, 0, RR, s));
-    XTN_LAUNCH("diag", k_diag<<<blocks_for((int64_t)U), kThreads, 0, s>>>(P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), (int)U,
+    const size_t msmem = R <= kSmemReps ? RR * (sizeof(unsigned long long) + 1) : 0;
+    if (msmem > 48 * 1024) {
+        XTN_CK(cudaFuncSetAttribute(k_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+        XTN_CK(cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+    }
+    const unsigned dblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(blocks_for((int64_t)U), c->sms * 4));
+    XTN_LAUNCH("diag", k_diag<<<dblocks, kThreads, msmem, s>>>(P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), (int)U,
                                                        P<int32_t>(b.freq), P<int32_t>(b.rep), R,
                                                        P<unsigned long long>(b.M), P<uint8_t>(b.present)));
     XTN_CK(cudaGetLastError());
@@ -1063,9 +1104,8 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
 
     // 4. cross term
     if (nverified > 0) {
-        size_t smem = R <= kSmemReps ? RR * (sizeof(unsigned long long) + 1) : 0;
-        if (smem > 48 * 1024) XTN_CK(cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int64_t blocks = std::min<int64_t>((nverified + kThreads - 1) / kThreads, 148 * 4);
+        const size_t smem = msmem;
+        int64_t blocks = std::min<int64_t>((nverified + kThreads - 1) / kThreads, (int64_t)c->sms * 4);
         XTN_LAUNCH("cross", k_cross<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, smem, s>>>(
             P<xtn_int2>(c->out_pairs), nverified, P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), P<int32_t>(b.freq),
             P<int32_t>(b.rep), R, P<unsigned long long>(b.M), P<uint8_t>(b.present)));
