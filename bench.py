@@ -41,6 +41,12 @@ WORKLOADS = {
     "overlap_64rep_leven_d1": dict(kind="repertoires", n_reps=64, min=1e4, max=2e6, shared=0.05, d=1, measure=0,
                                    seed=20244),
 }
+# serving: resident d = 2 index over 5M generator sequences; query requests drawn from a further
+# 1M rows of the same generator run (rows are shuffled, so clusters span index and pool)
+SERVE_WORKLOADS = {
+    "serve_5m_d2": dict(n_index=5_000_000, n_pool=1_000_000, seed=20245, rates=(10, 100, 1000), seconds=3.0,
+                        max_size=100_000, p_d1=0.7),
+}
 DEFAULT_WORKLOAD = "nn_1m_leven_d2"
 METRIC = "seqs/s (symmetric-deletion NN search, whole job)"
 L2_FLUSH_BYTES = 256 << 20
@@ -181,6 +187,92 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
     if kernel == "verify":
         return 10.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
     return None
+
+
+def run_serve(args, w):
+    """Serving loop on a resident deletion index (xtn_index_serve): Poisson request arrivals at
+    each rate, request sizes log-uniform in [1, max_size] sequences, d = 1 with probability p_d1
+    else 2, Levenshtein. Latency = completion - arrival of each request (host clock, the
+    request's pairs delivered to the host)."""
+    import numpy as np
+    import torch
+
+    import xtn
+
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local)
+    chars, offs = xtn.synth_clusters(w["seed"], w["n_index"] + w["n_pool"], 0.20, 0.02)
+    ni = w["n_index"]
+    t0 = time.perf_counter()
+    ix = xtn.Index(chars[: offs[ni]], offs[: ni + 1], max_distance=2, device=local)
+    build_wall = time.perf_counter() - t0
+    info = ix.info()
+    pool_c, pool_o = chars[offs[ni] :], (offs[ni:] - offs[ni]).astype(np.uint32)
+    n_pool = len(pool_o) - 1
+    rng = np.random.default_rng(w["seed"] + 1)
+    sampler = ClockSampler(local)
+    sampler.start()
+    per_rate = {}
+    total_seqs, total_busy = 0, 0.0
+    for rate in w["rates"]:
+        n_req = max(5, int(rate * w["seconds"]))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        sizes = np.minimum(np.exp(rng.uniform(0, np.log(w["max_size"]), n_req)).astype(np.int64), w["max_size"])
+        sizes = np.maximum(sizes, 1)
+        dists = np.where(rng.random(n_req) < w["p_d1"], 1, 2)
+        reqs = []
+        for k in range(n_req):
+            a = int(rng.integers(0, n_pool - sizes[k] + 1))
+            o = (pool_o[a : a + sizes[k] + 1] - pool_o[a]).astype(np.uint32)
+            reqs.append((pool_c[pool_o[a] : pool_o[a + sizes[k]]], o, int(dists[k]), 0, float(arrivals[k])))
+        # warm-up: the first requests once, untimed
+        ix.serve(reqs[:3], realtime=False, keep_results=False)
+        stats, _ = ix.serve(reqs, realtime=True, keep_results=False)
+        lat = np.array([(st["done_s"] - t) * 1e3 for st, (_, _, _, _, t) in zip(stats, reqs)])
+        span = max(st["done_s"] for st in stats) - float(arrivals[0])
+        small_d1 = np.array([l for l, (_, o, d, _, _) in zip(lat, reqs) if d == 1 and len(o) - 1 <= 1000])
+        per_rate[str(rate)] = {
+            "requests": n_req,
+            "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)),
+            "p50_ms_d1": float(np.percentile(lat[dists == 1], 50)),
+            "p99_ms_d1": float(np.percentile(lat[dists == 1], 99)),
+            "p99_ms_d2": float(np.percentile(lat[dists == 2], 99)) if (dists == 2).any() else None,
+            "p99_ms_d1_le_1k_seqs": float(np.percentile(small_d1, 99)) if len(small_d1) else None,
+            "seqs_per_s": float(sizes.sum() / span),
+            "batches": len({st["batch"] for st in stats}),
+            "pairs": int(sum(st["n_out"] for st in stats)),
+        }
+        total_seqs += int(sizes.sum())
+        total_busy += span
+    clocks = sampler.stop()
+    ix.close()
+    top = per_rate[str(max(w["rates"]))]
+    return {
+        "metric": "served query latency p99 (resident 5M-sequence d=2 index), ms",
+        "value": per_rate[str(w["rates"][len(w["rates"]) // 2])]["p99_ms"],
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": len(w["rates"]),
+        "warmup": 1,
+        "ms_per_step": None,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded CDR3 generator)",
+        "config": {"workload": args.workload, "index_seqs": ni, "index_max_distance": 2,
+                   "request_sizes": f"log-uniform 1..{w['max_size']}", "p_d1": w["p_d1"],
+                   "rates_req_per_s": list(w["rates"]), "seconds_per_rate": w["seconds"],
+                   "value_is": f"p99 at {w['rates'][len(w['rates']) // 2]} req/s"},
+        "per_rate": per_rate,
+        "seqs_per_s_at_top_rate": top["seqs_per_s"],
+        "index": {"records": info["n_records"], "bytes": info["bytes"], "directory_bits": info["directory_bits"],
+                  "build_ms_device": info["ms_build"], "build_s_wall": build_wall},
+        "clocks": clocks,
+    }
 
 
 def ncu_traffic(kernel: str, workload: str):
@@ -512,7 +604,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(SERVE_WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", choices=["bucket", "sort"], default="bucket",
                     help="key grouping: shared-memory hash buckets (default) or full radix sort")
@@ -520,8 +612,14 @@ def main():
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
                     help="context option (xtn_context_set_option), repeatable")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
-    line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
+    if args.workload in SERVE_WORKLOADS:
+        if args.impl == "reference":
+            line = {"impl": "reference", "unavailable": "the reference has no query-serving mode (offline searches only)"}
+        else:
+            line = run_serve(args, SERVE_WORKLOADS[args.workload])
+    else:
+        w = WORKLOADS[args.workload]
+        line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
     if line is not None:
         print(json.dumps(line), flush=True)
 

@@ -166,6 +166,83 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *                     0 = hash each variant key directly (same hash values, slower) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
+/* ------------------------------------------------------------------ resident index and serving */
+
+/* A resident deletion index: every deletion variant (at most max_distance <= 2 deletions) of
+ * the first 18 residues of n_seqs reference sequences, hashed, tagged with its deletion count
+ * and sorted in device memory, with a directory on the top hash bits. It has no counterpart
+ * in the reference, which only runs whole offline searches (xtneighbor_streaming/src/xtn.cu:
+ * 267-509); a query batch is answered exactly as that offline search would answer the
+ * sequences (index rows 0..n_seqs-1 followed by the batch), restricted to the pairs with one
+ * index row x and one batch row q: pairs (x, n_seqs + q) in (x, y) order with the reference
+ * distance. Inputs as in xtn_perform. Owns a context (stream and scratch) on `device`. */
+typedef struct xtn_index xtn_index;
+
+typedef struct {
+    int64_t n_seqs;
+    int64_t n_records;      /* deletion variants held */
+    int64_t bytes;          /* device memory held by the index */
+    int32_t max_distance;
+    int32_t directory_bits; /* log2 of the directory size */
+    double ms_build;        /* device time of the build */
+} xtn_index_info;
+
+int xtn_index_create(int device, const char* seqs, const uint32_t* offsets, int32_t n_seqs, int32_t max_distance,
+                     xtn_index** out);
+/* The same from device-resident inputs (copied: the caller may free them afterwards). */
+int xtn_index_create_device(int device, const char* d_seqs, const uint32_t* d_offsets, int32_t n_seqs,
+                            int32_t max_distance, xtn_index** out);
+void xtn_index_destroy(xtn_index* index);
+int xtn_index_stats(const xtn_index* index, xtn_index_info* out);
+/* The index's context: its stream, stats, kernel times and last query result
+ * (xtn_context_fetch / xtn_context_result_device). */
+xtn_context* xtn_index_context(xtn_index* index);
+
+/* One query batch from host buffers; args->distance <= max_distance. The result reaches the
+ * callback in chunks, as in xtn_perform. */
+int xtn_index_query(xtn_index* index, const xtn_args* args, const char* seqs, const uint32_t* offsets,
+                    int32_t n_queries, xtn_callback callback, void* user);
+/* One query batch from device buffers; the result stays on the index's context. */
+int xtn_index_query_device(xtn_index* index, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                           int32_t n_queries, int64_t* n_out);
+
+/* Serving loop. Requests (host buffers) arrive at arrival_s seconds after the call starts
+ * (realtime) or all at once. Whenever the device is free, the loop admits the ready requests
+ * of the oldest one's (distance, measure) in arrival order while the batch fits the memory
+ * budget (hbm_fraction of the free device memory, at most max_batch_seqs sequences), runs them
+ * as one query batch, splits the answer by request and hands each request its pairs
+ * (y = n_seqs + the request's own row) through the callback. A request larger than the budget
+ * runs in pieces. results[i] receives the admission and completion times (seconds since the
+ * call started), the pair count and the status of request i. */
+typedef struct {
+    const char* seqs;
+    const uint32_t* offsets;
+    int32_t n_seqs;
+    int32_t distance;
+    int32_t measure;
+    double arrival_s;
+} xtn_request;
+
+typedef struct {
+    double admitted_s;
+    double done_s;
+    int64_t n_out;
+    int32_t batch;
+    int32_t status;
+} xtn_request_result;
+
+typedef struct {
+    int64_t max_batch_seqs; /* <= 0: 2^20 */
+    double hbm_fraction;    /* of free device memory a batch may use; <= 0: 0.5 */
+    int32_t realtime;       /* 1: honour arrival_s; 0: every request is ready at once */
+} xtn_serve_options;
+
+typedef void (*xtn_request_callback)(int32_t request, const xtn_output* out, void* user);
+
+int xtn_index_serve(xtn_index* index, const xtn_request* requests, int32_t n_requests,
+                    const xtn_serve_options* options, xtn_request_result* results, xtn_request_callback callback,
+                    void* user);
+
 /* ------------------------------------------------------------------ search without allocation */
 
 /* Nearest-neighbour search that allocates nothing. It has no counterpart in the reference.

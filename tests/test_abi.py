@@ -47,3 +47,16 @@ def test_argument_errors_need_no_device():
     # a null context / null inputs are rejected before any CUDA call
     assert lib.xtn_context_perform(None, ctypes.byref(args), None, None, 0, None, cb, None) == xtn.ERR_ARG
     assert lib.xtn_context_nn_device(None, ctypes.byref(args), None, None, 0, None) == xtn.ERR_ARG
+
+
+def test_index_argument_errors_need_no_device():
+    """Invalid index arguments are rejected before any device work."""
+    import ctypes
+
+    lib = xtn.load()
+    h = ctypes.c_void_p()
+    assert lib.xtn_index_create(0, None, None, 0, 2, ctypes.byref(h)) == xtn.ERR_ARG
+    chars, offs = xtn.pack_sequences(["CASSF", "CASSG"])
+    assert lib.xtn_index_create(0, chars.ctypes.data, offs.ctypes.data, 2, 3, ctypes.byref(h)) == xtn.ERR_ARG
+    assert b"maximum distance" in lib.xtn_last_error()
+    assert lib.xtn_index_serve(None, None, 0, None, None, xtn.REQUEST_CALLBACK(0), None) == xtn.ERR_ARG

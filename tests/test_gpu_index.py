@@ -1,0 +1,143 @@
+"""Resident deletion index (xtn_index_*): query batches against an index must return exactly the
+pairs that the offline search reports on (index sequences followed by the batch) with one
+side in the index and the other in the batch. The same holds for every request of the serving
+loop, including requests split into pieces by the batch budget.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import xtn
+from conftest import csr
+
+pytestmark = pytest.mark.gpu
+
+ALPHA = "ACDEFGHIKLMNPQRSTVWY"
+
+
+def seqs_of(chars, offs):
+    b = chars.tobytes()
+    return [b[offs[i] : offs[i + 1]].decode() for i in range(len(offs) - 1)]
+
+
+def mutate(s, rng, k):
+    s = list(s)
+    for _ in range(k):
+        op = rng.integers(3)
+        p = int(rng.integers(len(s)))
+        if op == 0:
+            s[p] = ALPHA[int(rng.integers(20))]
+        elif op == 1:
+            s.insert(p, ALPHA[int(rng.integers(20))])
+        elif len(s) > 1:
+            del s[p]
+    return "".join(s)
+
+
+def make_queries(index_seqs, n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        base = index_seqs[int(rng.integers(len(index_seqs)))]
+        kind = i % 4
+        if kind == 0:
+            out.append(base)  # exact copy: distance 0
+        elif kind == 3:
+            out.append("".join(rng.choice(list(ALPHA), int(rng.integers(8, 23)))))
+        else:
+            out.append(mutate(base, rng, kind))
+    return out
+
+
+def offline_cross(index_seqs, query_seqs, d, measure):
+    """The offline GPU search on the union, restricted to (index row, batch row) pairs."""
+    chars, offs = csr(index_seqs + query_seqs)
+    ctx = xtn.Context(0)
+    r = ctx.perform(chars, offs, distance=d, measure=measure)
+    ctx.close()
+    n = len(index_seqs)
+    sel = (r.pairs[:, 0] < n) & (r.pairs[:, 1] >= n)
+    return r.pairs[sel], r.distances[sel]
+
+
+@pytest.fixture(scope="module")
+def index_setup():
+    chars, offs = xtn.synth_clusters(321, 100_000, 0.20, 0.02)
+    index_seqs = seqs_of(chars, offs)
+    ix = xtn.Index(chars, offs, max_distance=2)
+    yield ix, index_seqs
+    ix.close()
+
+
+@pytest.mark.parametrize("d,measure", [(1, 0), (2, 0), (1, 1), (2, 1)])
+def test_query_equals_offline_union(index_setup, d, measure):
+    ix, index_seqs = index_setup
+    q = make_queries(index_seqs, 3000, seed=d * 10 + measure)
+    qc, qo = csr(q)
+    got = ix.query(qc, qo, distance=d, measure=measure)
+    exp_p, exp_d = offline_cross(index_seqs, q, d, measure)
+    assert len(exp_p) > 500
+    assert np.array_equal(got.pairs, exp_p)
+    assert np.array_equal(got.distances, exp_d)
+
+
+def test_query_equals_oracle_small():
+    """Against the CPU oracle itself on a union small enough for it."""
+    chars, offs = xtn.synth_clusters(77, 20_000, 0.30, 0.02)
+    index_seqs = seqs_of(chars, offs)
+    q = make_queries(index_seqs, 800, seed=5)
+    with xtn.Index(chars, offs, max_distance=2) as ix:
+        for d in (1, 2):
+            got = ix.query(*csr(q), distance=d)
+            uc, uo = csr(index_seqs + q)
+            p, dist, _ = orc.nn_search(uc, uo, d, 0)
+            sel = (p[:, 0] < len(index_seqs)) & (p[:, 1] >= len(index_seqs))
+            assert np.array_equal(got.pairs, p[sel])
+            assert np.array_equal(got.distances, dist[sel])
+
+
+def test_device_query_and_limits(index_setup):
+    import torch
+
+    ix, index_seqs = index_setup
+    q = make_queries(index_seqs, 500, seed=9)
+    qc, qo = csr(q)
+    host = ix.query(qc, qo, distance=2)
+    dch = torch.from_numpy(qc).cuda()
+    dof = torch.from_numpy(qo.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    n = ix.query_device(dch.data_ptr(), dof.data_ptr(), len(qo) - 1, distance=2)
+    dev = ix.ctx.fetch(n)
+    assert np.array_equal(dev.pairs, host.pairs) and np.array_equal(dev.distances, host.distances)
+    info = ix.info()
+    assert info["n_seqs"] == 100_000 and info["n_records"] > 100_000 and info["max_distance"] == 2
+    with xtn.Index(qc, qo, max_distance=1) as small:
+        with pytest.raises(xtn.XtnError, match="exceeds the index's maximum distance"):
+            small.query(qc, qo, distance=2)
+
+
+def test_serving_loop_matches_direct_queries(index_setup):
+    """Requests arriving over 50 ms, mixed d = 1 / 2 and measures, one larger than the batch
+    budget: each request's answer equals a direct query of the same sequences."""
+    ix, index_seqs = index_setup
+    rng = np.random.default_rng(12)
+    reqs = []
+    for i in range(24):
+        size = int(rng.integers(1, 400)) if i != 7 else 1300
+        q = make_queries(index_seqs, size, seed=100 + i)
+        c, o = csr(q)
+        d = 1 if rng.random() < 0.7 else 2
+        m = 1 if i % 5 == 4 else 0
+        reqs.append((c, o, d, m, float(rng.uniform(0, 0.05))))
+    stats, outs = ix.serve(reqs, max_batch_seqs=1000, realtime=True)
+    batches = set()
+    for (c, o, d, m, t), st, out in zip(reqs, stats, outs):
+        assert st["status"] == 0
+        assert st["admitted_s"] >= t - 1e-6 and st["done_s"] >= st["admitted_s"]
+        exp = ix.query(c, o, distance=d, measure=m)
+        assert np.array_equal(out.pairs, exp.pairs)
+        assert np.array_equal(out.distances, exp.distances)
+        assert st["n_out"] == len(exp.pairs)
+        batches.add(st["batch"])
+    assert len(batches) < len(reqs)  # requests were batched together
+    assert sum(len(out.pairs) for out in outs) > 0

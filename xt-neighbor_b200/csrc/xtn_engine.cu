@@ -16,12 +16,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/xtn_b200.h"
@@ -1348,6 +1350,8 @@ int xtn_perform(const xtn_args* args, const char* seqs, const uint32_t* offsets,
 }
 
 }  // extern "C"
+
+#include "xtn_index.cuh"
 
 // ------------------------------------------------------------------ search without allocation
 // Some callers cannot allocate device memory while they run: a host whose framework caching

@@ -33,6 +33,14 @@ SYMBOLS = (
     "xtn_context_perform",
     "xtn_context_nn_device",
     "xtn_context_overlap_device",
+    "xtn_index_create",
+    "xtn_index_create_device",
+    "xtn_index_destroy",
+    "xtn_index_stats",
+    "xtn_index_context",
+    "xtn_index_query",
+    "xtn_index_query_device",
+    "xtn_index_serve",
     "xtn_context_fetch",
     "xtn_context_result_device",
     "xtn_context_stream",
@@ -95,6 +103,45 @@ class Stats(ctypes.Structure):
 
 CALLBACK = ctypes.CFUNCTYPE(None, ctypes.POINTER(Output), ctypes.c_void_p)
 
+
+class IndexInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_seqs", ctypes.c_int64),
+        ("n_records", ctypes.c_int64),
+        ("bytes", ctypes.c_int64),
+        ("max_distance", ctypes.c_int32),
+        ("directory_bits", ctypes.c_int32),
+        ("ms_build", ctypes.c_double),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("seqs", ctypes.c_void_p),
+        ("offsets", ctypes.c_void_p),
+        ("n_seqs", ctypes.c_int32),
+        ("distance", ctypes.c_int32),
+        ("measure", ctypes.c_int32),
+        ("arrival_s", ctypes.c_double),
+    ]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("admitted_s", ctypes.c_double),
+        ("done_s", ctypes.c_double),
+        ("n_out", ctypes.c_int64),
+        ("batch", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+    ]
+
+
+class ServeOptions(ctypes.Structure):
+    _fields_ = [("max_batch_seqs", ctypes.c_int64), ("hbm_fraction", ctypes.c_double), ("realtime", ctypes.c_int32)]
+
+
+REQUEST_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_int32, ctypes.POINTER(Output), ctypes.c_void_p)
+
 _lib = None
 
 
@@ -124,6 +171,17 @@ def load():
     lib.xtn_context_overlap_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P,
                                                ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_fetch.argtypes = [P, P, P, P, ctypes.c_int64]
+    lib.xtn_index_create.argtypes = [ctypes.c_int, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(P)]
+    lib.xtn_index_create_device.argtypes = [ctypes.c_int, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(P)]
+    lib.xtn_index_destroy.argtypes = [P]
+    lib.xtn_index_destroy.restype = None
+    lib.xtn_index_stats.argtypes = [P, ctypes.POINTER(IndexInfo)]
+    lib.xtn_index_context.argtypes = [P]
+    lib.xtn_index_context.restype = P
+    lib.xtn_index_query.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, CALLBACK, P]
+    lib.xtn_index_query_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_index_serve.argtypes = [P, ctypes.POINTER(Request), ctypes.c_int32, ctypes.POINTER(ServeOptions),
+                                    ctypes.POINTER(RequestResult), REQUEST_CALLBACK, P]
     lib.xtn_context_result_device.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_stream.argtypes = [P]
     lib.xtn_context_stream.restype = P
@@ -359,3 +417,94 @@ def synth_repertoires(seed: int, n_reps: int, min_size: float, max_size: float, 
     rep_of = np.repeat(np.arange(len(reps), dtype=np.int32), reps)
     info = np.stack([freq, rep_of, np.arange(n, dtype=np.int32)], axis=1).astype(np.int32)
     return chars, offs, info, reps
+
+
+class Index:
+    """Resident deletion index over reference sequences (xtn_index_*): query batches return the
+    (index row, n_index + batch row) pairs the offline search would report on the union."""
+
+    def __init__(self, chars, offsets, max_distance: int = 2, device: int = 0):
+        self.lib = load()
+        self.h = ctypes.c_void_p()
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.n = len(offsets) - 1
+        _check(self.lib.xtn_index_create(device, chars.ctypes.data_as(ctypes.c_void_p),
+                                         offsets.ctypes.data_as(ctypes.c_void_p), self.n, max_distance,
+                                         ctypes.byref(self.h)))
+        self.ctx = Context.__new__(Context)
+        self.ctx.lib = self.lib
+        self.ctx.h = ctypes.c_void_p(self.lib.xtn_index_context(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.xtn_index_destroy(self.h)
+            self.h = ctypes.c_void_p()
+            self.ctx.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def info(self) -> dict:
+        st = IndexInfo()
+        _check(self.lib.xtn_index_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def query(self, chars, offsets, distance=1, measure=LEVENSHTEIN) -> Result:
+        chars = np.ascontiguousarray(chars, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        args = Args(distance, measure, 0, 0)
+        chunks_p, chunks_d = [], []
+
+        def cb(out_ptr, _user):
+            o = out_ptr.contents
+            if o.len <= 0:
+                return
+            pp = ctypes.cast(o.index_pairs, ctypes.POINTER(ctypes.c_int32))
+            chunks_p.append(np.ctypeslib.as_array(pp, shape=(o.len, 2)).copy())
+            chunks_d.append(np.ctypeslib.as_array(o.pairwise_distances, shape=(o.len,)).copy())
+
+        ccb = CALLBACK(cb)
+        _check(self.lib.xtn_index_query(self.h, ctypes.byref(args), chars.ctypes.data_as(ctypes.c_void_p),
+                                        offsets.ctypes.data_as(ctypes.c_void_p), len(offsets) - 1, ccb, None))
+        pairs = np.concatenate(chunks_p) if chunks_p else np.zeros((0, 2), np.int32)
+        dist = np.concatenate(chunks_d) if chunks_d else np.zeros(0, np.int8)
+        return Result(pairs, dist, None)
+
+    def query_device(self, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN) -> int:
+        args = Args(distance, measure, 0, 0)
+        nout = ctypes.c_int64()
+        _check(self.lib.xtn_index_query_device(self.h, ctypes.byref(args), ctypes.c_void_p(d_chars),
+                                               ctypes.c_void_p(d_offsets), n, ctypes.byref(nout)))
+        return nout.value
+
+    def serve(self, requests, max_batch_seqs=0, hbm_fraction=0.5, realtime=True, keep_results=True):
+        """requests: list of (chars, offsets, distance, measure, arrival_s). Returns (per-request
+        dicts with admitted_s, done_s, n_out, batch, status; per-request Result or None)."""
+        keep = [(np.ascontiguousarray(c, dtype=np.uint8), np.ascontiguousarray(o, dtype=np.uint32))
+                for c, o, *_ in requests]
+        arr = (Request * max(1, len(requests)))()
+        for i, ((c, o), (_, _, d, m, t)) in enumerate(zip(keep, requests)):
+            arr[i] = Request(c.ctypes.data, o.ctypes.data, len(o) - 1, d, m, float(t))
+        res = (RequestResult * max(1, len(requests)))()
+        outs = [None] * len(requests)
+
+        def cb(r, out_ptr, _user):
+            if not keep_results:
+                return
+            o = out_ptr.contents
+            if o.len <= 0:
+                outs[r] = Result(np.zeros((0, 2), np.int32), np.zeros(0, np.int8), None)
+                return
+            pp = ctypes.cast(o.index_pairs, ctypes.POINTER(ctypes.c_int32))
+            outs[r] = Result(np.ctypeslib.as_array(pp, shape=(o.len, 2)).copy(),
+                             np.ctypeslib.as_array(o.pairwise_distances, shape=(o.len,)).copy(), None)
+
+        ccb = REQUEST_CALLBACK(cb)
+        opt = ServeOptions(max_batch_seqs, hbm_fraction, 1 if realtime else 0)
+        _check(self.lib.xtn_index_serve(self.h, arr, len(requests), ctypes.byref(opt), res, ccb, None))
+        stats = [{k: getattr(res[i], k) for k, _ in RequestResult._fields_} for i in range(len(requests))]
+        return stats, outs
