@@ -209,7 +209,8 @@ int xtn_index_query_device(xtn_index* index, const xtn_args* args, const char* d
 /* Serving loop. Requests (host buffers) arrive at arrival_s seconds after the call starts
  * (realtime) or all at once. Whenever the device is free, the loop admits the ready requests
  * of the oldest one's (distance, measure) in arrival order while the batch fits the memory
- * budget (hbm_fraction of the free device memory, at most max_batch_seqs sequences), runs them
+ * budget (hbm_fraction of the device memory free when the loop starts, after it reserves
+ * buffers for the largest request; at most max_batch_seqs sequences), runs them
  * as one query batch, splits the answer by request and hands each request its pairs
  * (y = n_seqs + the request's own row) through the callback. A request larger than the budget
  * runs in pieces. results[i] receives the admission and completion times (seconds since the

@@ -129,15 +129,19 @@ def test_serving_loop_matches_direct_queries(index_setup):
         d = 1 if rng.random() < 0.7 else 2
         m = 1 if i % 5 == 4 else 0
         reqs.append((c, o, d, m, float(rng.uniform(0, 0.05))))
-    stats, outs = ix.serve(reqs, max_batch_seqs=1000, realtime=True)
-    batches = set()
-    for (c, o, d, m, t), st, out in zip(reqs, stats, outs):
-        assert st["status"] == 0
-        assert st["admitted_s"] >= t - 1e-6 and st["done_s"] >= st["admitted_s"]
-        exp = ix.query(c, o, distance=d, measure=m)
-        assert np.array_equal(out.pairs, exp.pairs)
-        assert np.array_equal(out.distances, exp.distances)
-        assert st["n_out"] == len(exp.pairs)
-        batches.add(st["batch"])
-    assert len(batches) < len(reqs)  # requests were batched together
-    assert sum(len(out.pairs) for out in outs) > 0
+    expected = [ix.query(c, o, distance=d, measure=m) for c, o, d, m, _ in reqs]
+    assert sum(len(e.pairs) for e in expected) > 0
+    # in real time (arrival times honoured), then with every request ready at once, so that
+    # requests of one (distance, measure) share batches and the large one is split
+    for realtime in (True, False):
+        stats, outs = ix.serve(reqs, max_batch_seqs=1000, realtime=realtime)
+        for (c, o, d, m, t), st, out, exp in zip(reqs, stats, outs, expected):
+            assert st["status"] == 0
+            if realtime:
+                assert st["admitted_s"] >= t - 1e-6
+            assert st["done_s"] >= st["admitted_s"]
+            assert np.array_equal(out.pairs, exp.pairs)
+            assert np.array_equal(out.distances, exp.distances)
+            assert st["n_out"] == len(exp.pairs)
+        if not realtime:
+            assert len({st["batch"] for st in stats}) < len(reqs)

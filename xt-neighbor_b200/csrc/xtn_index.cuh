@@ -111,13 +111,9 @@ __global__ void k_query_count(const uint64_t* __restrict__ qh, int64_t Vq, const
         if ((recs[m] >> idbits) < lo_key) a = m + 1;
         else z = m;
     }
+    // runs of equal hash are short: walk to the end of the (hash, deletions <= d) range
     const uint32_t first = a;
-    z = hi;
-    while (a < z) {
-        const uint32_t m = (a + z) >> 1;
-        if ((recs[m] >> idbits) <= hi_key) a = m + 1;
-        else z = m;
-    }
+    while (a < hi && (recs[a] >> idbits) <= hi_key) a++;
     lb[r] = first;
     cnt[r] = a - first;
 }
@@ -328,6 +324,37 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
     return XTN_SUCCESS;
 }
 
+// Grows the query buffers for a batch of nq sequences with `chars` residues at distance d, so
+// that a serving loop does not reallocate device memory between requests (candidate buffers
+// are sized for one candidate per query variant and grow if a batch needs more).
+static int index_reserve(xtn_index* ix, int64_t nq, int64_t chars, int d) {
+    xtn_context* c = ix->c;
+    const int64_t Vq = nq * (d >= 2 ? 172 : 19);
+    XTN_TRY(ensure(c->chars, (size_t)chars + 16));
+    XTN_TRY(ensure(c->offs, sizeof(uint32_t) * (nq + 1)));
+    XTN_TRY(ensure(c->keys, sizeof(u128) * nq));
+    XTN_TRY(ensure(c->klen, (size_t)nq));
+    XTN_TRY(ensure(c->vcnt, sizeof(uint32_t) * nq));
+    XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (nq + 1)));
+    XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * nq));
+    XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)nq));
+    XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(Vq + 1)));
+    XTN_TRY(ensure(ix->qh, sizeof(uint64_t) * Vq));
+    XTN_TRY(ensure(ix->qrow, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(ix->qlb, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(ix->qcnt, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(ix->qcoff, sizeof(uint64_t) * (Vq + 1)));
+    XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Vq + 64));
+    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Vq + 64));
+    XTN_TRY(ensure(c->dist, (size_t)Vq));
+    XTN_TRY(ensure(c->flag, (size_t)Vq));
+    XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Vq + 1)));
+    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * std::max(radix_scratch_elems(Vq), scan_scratch_elems(Vq))));
+    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * (size_t)Vq / 4 + 16));
+    XTN_TRY(ensure(c->out_dist, (size_t)Vq / 4 + 16));
+    return XTN_SUCCESS;
+}
+
 static int index_create_common(int device, int dmax, xtn_index** out, xtn_index** ix) {
     if (!out) {
         set_err("null output pointer");
@@ -517,6 +544,28 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
     const bool realtime = !opt || opt->realtime;
     xtn_context* c = ix->c;
     XTN_CK(cudaSetDevice(c->device));
+    {
+        // device memory for the largest batch the loop can form, reserved before the clock starts
+        int64_t big = 0, big_chars = 0;
+        int dbig = 1;
+        for (int i = 0; i < n_reqs; i++) {
+            big = std::max<int64_t>(big, reqs[i].n_seqs);
+            big_chars = std::max<int64_t>(big_chars, reqs[i].offsets[reqs[i].n_seqs] - reqs[i].offsets[0]);
+            dbig = std::max(dbig, reqs[i].distance);
+        }
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const int64_t cap0 = std::max<int64_t>(
+            1, std::min<int64_t>(max_batch, (int64_t)((double)free_b * frac / (double)query_bytes_per_seq(dbig))));
+        const int64_t nres = std::min(std::max<int64_t>(big, std::min<int64_t>(cap0, 1 << 16)), cap0);
+        XTN_TRY(index_reserve(ix, nres, std::max<int64_t>(big_chars, nres * 24), dbig));
+    }
+    // The memory budget is read once: a device-memory query can take tens of milliseconds,
+    // far longer than a small batch. Only this loop allocates on the index's device while it
+    // runs, so free memory changes only when a batch outgrows the reservation.
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const double budget = (double)free_b * frac;
     // requests in arrival order
     std::vector<int> order(n_reqs);
     for (int i = 0; i < n_reqs; i++) order[i] = i;
@@ -539,11 +588,9 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
         }
         // admission: the oldest ready request fixes (distance, measure); requests of the same
         // kind join while the batch fits the memory budget
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
         const int d = reqs[ready[0]].distance, m = reqs[ready[0]].measure;
-        const int64_t cap = std::max<int64_t>(
-            1, std::min<int64_t>(max_batch, (int64_t)((double)free_b * frac / (double)query_bytes_per_seq(d))));
+        const int64_t cap =
+            std::max<int64_t>(1, std::min<int64_t>(max_batch, (int64_t)(budget / (double)query_bytes_per_seq(d))));
         std::vector<int> batch, rest;
         int64_t seqs = 0;
         for (int r : ready) {
@@ -582,11 +629,9 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
                 Piece& pc = pieces[p1];
                 pc.row0 = rows;
                 const xtn_request& q = reqs[pc.req];
-                for (int i = 0; i < pc.count; i++) {
-                    const uint32_t a = q.offsets[pc.first + i], b = q.offsets[pc.first + i + 1];
-                    hchars.insert(hchars.end(), q.seqs + a, q.seqs + b);
-                    hoffs.push_back((uint32_t)(hoffs.back() + (b - a)));
-                }
+                const uint32_t a0 = q.offsets[pc.first], base = hoffs.back();
+                hchars.insert(hchars.end(), q.seqs + a0, q.seqs + q.offsets[pc.first + pc.count]);
+                for (int i = 1; i <= pc.count; i++) hoffs.push_back(base + (q.offsets[pc.first + i] - a0));
                 rows += pc.count;
                 p1++;
             }
