@@ -8,15 +8,17 @@
 //                              (variants generated and hashed, not stored)
 //   offsets  k_bucket_colscan  per bucket: exclusive prefix over tiles, bucket totals
 //   scatter  k_bucket_scatter_staged
-//                              the variants again, 8192 at a time in shared memory (made by
-//                              balanced tasks, for_each_task_variant), counting-sorted by
-//                              bucket there and written out as contiguous runs: every
-//                              global store is part of a coalesced run, so L2 receives
-//                              whole sectors instead of read-modify-writing partial ones
+//                              the variants again (hashed from the key tables by balanced
+//                              tasks), up to 4096 at a time in shared memory, ranked within
+//                              their bucket as they are made, reordered by bucket and
+//                              written out as contiguous runs: every global store is part of
+//                              a coalesced run, so L2 receives whole sectors instead of
+//                              read-modify-writing partial ones
 //   plan     k_bucket_plan     buckets that fit in shared memory go straight to grouping;
 //                              larger ones are split by their next hash bits
 //   split    k_bucket_split_staged
-//                              the same staged partition, per bucket, into sub-buckets
+//                              per oversized bucket, the same staged partition into
+//                              sub-buckets (chunks arrive by bulk copy)
 //   group    k_bucket_group    one CTA per (sub-)bucket: TMA bulk copy into shared memory,
 //                              a bitmap filter that drops records without a partner, a
 //                              counting sort of the rest, runs of equal hashes, then every id
@@ -155,15 +157,11 @@ template <class C>
 struct StageSmem {
     uint64_t rec[C::kChunk + 2]; // records of the chunk, in arrival order (+ bulk-copy alignment)
     uint64_t sorted[C::kChunk];  // the same records grouped by bucket
-    uint16_t bkt[C::kChunk];     // bucket of rec[i]
     uint16_t sbkt[C::kChunk];    // bucket of sorted[i]
     uint32_t cnt[C::kFan];
     uint32_t lstart[C::kFan];
     uint32_t gcur[C::kFan];      // next global position of each bucket for this CTA
-    uint16_t rel_v[C::kChunk];   // voff of the chunk's sequences, relative to the chunk
-    uint16_t rel_t[C::kChunk];   // toff of the chunk's sequences, relative to the chunk
     uint32_t warp_sums[C::kThreads / 32 + 1];
-    uint32_t seq_end;
     uint32_t wait_failed;
     unsigned long long mbar;     // completion barrier of the chunk bulk copies (split)
 };
@@ -175,50 +173,9 @@ constexpr int stage_ctas_per_sm() {
     return (int)((228u * 1024u) / (sizeof(StageSmem<C>) + 1024u));
 }
 
-// Writes rec[0..m) (bucket bkt[]) to dst, each bucket's records appended at gcur[bucket],
-// as contiguous runs from consecutive threads.
-template <class C>
-__device__ __forceinline__ void stage_partition(StageSmem<C>& S, int nb, uint32_t m, uint64_t* __restrict__ dst) {
-    constexpr int kStageThreads = C::kThreads, kFanPer = C::kFanPer;
-    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
-    __syncthreads();
-    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[S.bkt[p]], 1u);
-    __syncthreads();
-    {
-        uint32_t tot, loc[kFanPer], sum = 0;
-        const int b0 = threadIdx.x * kFanPer;
-#pragma unroll
-        for (int k = 0; k < kFanPer; k++) {
-            loc[k] = sum;
-            sum += (b0 + k < nb) ? S.cnt[b0 + k] : 0u;
-        }
-        const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
-#pragma unroll
-        for (int k = 0; k < kFanPer; k++)
-            if (b0 + k < nb) {
-                S.lstart[b0 + k] = ex + loc[k];
-                S.cnt[b0 + k] = ex + loc[k];
-            }
-    }
-    __syncthreads();
-    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
-        const uint16_t b = S.bkt[p];
-        const uint32_t q = atomicAdd(&S.cnt[b], 1u);
-        S.sorted[q] = S.rec[p];
-        S.sbkt[q] = b;
-    }
-    __syncthreads();
-    for (uint32_t q = threadIdx.x; q < m; q += kStageThreads) {
-        const uint16_t b = S.sbkt[q];
-        dst[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
-    __syncthreads();
-}
-
-// Split form of stage_partition: the chunk's records are r[0..m) and their bucket is
-// r[p] >> shift; after_rank() runs once every thread is done reading r.
+// Staged partition of a split chunk: the chunk's records are r[0..m), the bucket of r[p] is
+// r[p] >> shift; each bucket's records are appended at gcur[bucket] as contiguous runs written by
+// consecutive threads. after_rank() runs once every thread is done reading r.
 template <class C, class Hook>
 __device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r, int shift,
                                                 uint64_t* __restrict__ dst, Hook&& after_rank) {
@@ -287,102 +244,164 @@ __device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void* src, ui
                  : "memory");
 }
 
-// Tasks per sequence for the staged scatter: for d = 2, 2 * ceil(runs / 2) balanced tasks
-// (task_items); for d = 1 one task per variant (the key, then the single deletion of each
-// run), so a chunk's table loads are spread over all threads.
-__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, int d, uint32_t* __restrict__ tcnt) {
+// Tasks per sequence for the staged scatter at d = 2: 2 * ceil(runs / 2) balanced tasks
+// (task_items). (At d = 1 each sequence is one task and needs no map.)
+__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint32_t* __restrict__ tcnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t R = (uint32_t)popc32((uint32_t)runinfo[i]);
-    tcnt[i] = d >= 2 ? 2u * ((R + 1u) >> 1) : 1u + R;
+    tcnt[i] = 2u * ((R + 1u) >> 1);
 }
 
-// First-level scatter for d <= 2. The tile's sequences go through shared memory 4096
-// variants at a time; each chunk's variants are produced by tasks (at d = 2 balanced tasks of
-// about R/2 + 1 variants, at d = 1 single variants; one table load and one add per variant
-// hash), written at their index within the sequence; then the staged partition writes them out
-// by bucket. runinfo[i] is key_run_info of sequence i, tab its key_table; toff is the
-// exclusive scan of k_task_counts.
+// Task -> sequence map of the staged scatter: the k_task_counts tasks of sequence i occupy
+// task_seq[toff[i] .. toff[i+1]).
+__global__ void k_task_seq(const uint64_t* __restrict__ toff, int n, uint32_t* __restrict__ task_seq) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint64_t g = toff[i], e = toff[i + 1]; g < e; g++) task_seq[g] = (uint32_t)i;
+}
+
+constexpr int kMaxVariantsD2 = 1 + kKeyLen + kKeyLen * (kKeyLen - 1) / 2;  // 172: all runs of length 1
+constexpr int kScatterChunksPerRound = 1024;
+
 template <class C>
-__global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_scatter_staged(
+struct ScatterSmem {
+    uint64_t rec[C::kChunk];     // records of the chunk, at their sequence's slots
+    uint64_t sorted[C::kChunk];  // the same records grouped by bucket
+    uint16_t bkt[C::kChunk];     // bucket of rec[i]
+    uint16_t rank[C::kChunk];    // rank of rec[i] among the chunk's records of its bucket
+    uint16_t sbkt[C::kChunk];    // bucket of sorted[i]
+    uint32_t cnt[C::kFan];       // records of each bucket in the chunk
+    uint32_t lstart[C::kFan];    // first slot of each bucket in `sorted`
+    uint32_t gcur[C::kFan];      // next global position of each bucket for this CTA
+    uint32_t cstart[kScatterChunksPerRound + 1];
+    uint32_t warp_sums[C::kThreads / 32 + 1];
+};
+
+template <class SM>
+constexpr int ctas_per_sm_for() {
+    return (int)((228u * 1024u) / (sizeof(SM) + 1024u));
+}
+
+// First-level scatter for d <= 2. The CTA's tile of sequences is cut into chunks of at most
+// C::kChunk variants by a rule every thread can apply alone: chunk k holds the sequences whose
+// first variant lies in [k * span, (k + 1) * span) from the tile's first variant, with
+// span = C::kChunk - 172 (a key has at most 172 variants at d <= 2), so no chunk overflows
+// and none is empty. For each chunk:
+//   1. the chunk's generation tasks hash their variants from the key tables (one load and one
+//      add per variant), write each record at its sequence's slot and take its rank within
+//      its bucket with one shared-memory atomic. At d = 2 the tasks are k_task_counts'
+//      balanced halves of run pairs and task_seq maps a task to its sequence; at d = 1
+//      (task_seq null) a task is a whole sequence: its table row is loaded into registers
+//      at once and the key and single deletions are emitted by an unrolled loop;
+//   2. an exclusive scan of the bucket counts, a rank-ordered copy into `sorted`, and
+//      coalesced writes of each bucket's run at the CTA's cursor (gcur).
+// runinfo[i] is key_run_info of sequence i, tab its key_table; voff and toff are exclusive
+// scans of the variant and task counts (toff = sequence index at d = 1).
+template <class C>
+__global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()) k_bucket_scatter_staged(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
-    const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, int n, int tile, int d, int b1, int idbits,
-    const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs) {
-    constexpr int kStageThreads = C::kThreads, kStageChunk = C::kChunk;
+    const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
+    int tile, int d, int b1, int idbits, const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart,
+    uint64_t* __restrict__ recs) {
+    constexpr int T = C::kThreads, kFanPer = C::kFanPer;
+    constexpr uint64_t kSpan = (uint64_t)(C::kChunk - kMaxVariantsD2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
+    ScatterSmem<C>& S = *reinterpret_cast<ScatterSmem<C>*>(smem_raw);
     const int nb = 1 << b1;
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
-    for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] = (uint32_t)bstart[b] + off[b];
+    for (int b = threadIdx.x; b < nb; b += T) {
+        S.gcur[b] = (uint32_t)bstart[b] + off[b];
+        S.cnt[b] = 0;
+    }
     const int t0 = blockIdx.x * tile;
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
-    constexpr int kPer = C::kPer;  // task slots per thread in the scan
-    __syncthreads();
-    for (int s0 = t0; s0 < t1;) {
-        // chunk end: the largest s1 <= t1 with voff[s1] - voff[s0] <= chunk, found by all threads
-        // reading consecutive voff entries (coalesced) instead of one thread's binary search
-        const uint64_t base = voff[s0], tbase = toff[s0];
-        if (threadIdx.x == 0) S.seq_end = (uint32_t)(s0 + 1);
-        for (int f = threadIdx.x; f < kStageChunk; f += kStageThreads) S.sbkt[f] = 0;
-        __syncthreads();
-        for (int r0 = s0 + 1; r0 <= t1; r0 += kStageThreads) {
-            const int idx = r0 + threadIdx.x;
-            if (idx <= t1 && voff[idx] - base <= (uint64_t)kStageChunk) atomicMax(&S.seq_end, (uint32_t)idx);
-            __syncthreads();
-            if ((int)S.seq_end < r0 + kStageThreads - 1 || r0 + kStageThreads > t1) break;
-            __syncthreads();
+    for (int r0 = t0; r0 < t1;) {
+        // chunk starts of this round (at most kScatterChunksPerRound chunks)
+        const uint64_t base = voff[r0];
+        const uint64_t last = (voff[t1 - 1] - base) / kSpan;
+        const int nch = last + 1 < (uint64_t)kScatterChunksPerRound ? (int)(last + 1) : kScatterChunksPerRound;
+        for (int s = r0 + threadIdx.x; s < t1; s += T) {
+            const uint64_t k = (voff[s] - base) / kSpan;
+            if (k > (uint64_t)nch) break;
+            if (s == r0 || (voff[s - 1] - base) / kSpan != k) S.cstart[k] = (uint32_t)s;
         }
-        const int s1 = (int)S.seq_end;
-        const uint32_t m = (uint32_t)(voff[s1] - base);
-        const uint32_t nt = (uint32_t)(toff[s1] - tbase);  // <= m (a sequence has >= its task count of variants)
-        // per-sequence offsets into smem; task -> owning sequence: mark each sequence's first
-        // task, then an inclusive scan
-        for (int i = s0 + threadIdx.x; i < s1; i += kStageThreads) {
-            const uint32_t rv = (uint32_t)(voff[i] - base), rt = (uint32_t)(toff[i] - tbase);
-            S.rel_v[i - s0] = (uint16_t)rv;
-            S.rel_t[i - s0] = (uint16_t)rt;
-            if (i > s0) S.sbkt[rt] = 1;
-        }
+        if (threadIdx.x == 0 && (uint64_t)nch == last + 1) S.cstart[nch] = (uint32_t)t1;
         __syncthreads();
-        {
-            const int f0 = threadIdx.x * kPer;
-            uint32_t loc[kPer], sum = 0;
+        for (int c = 0; c < nch; c++) {
+            const int s0 = (int)S.cstart[c], s1 = (int)S.cstart[c + 1];
+            const uint64_t vbase = voff[s0];
+            const uint64_t tb = task_seq ? toff[s0] : (uint64_t)s0;
+            const uint32_t m = (uint32_t)(voff[s1] - vbase);
+            const uint32_t nt = (uint32_t)((task_seq ? toff[s1] : (uint64_t)s1) - tb);
+            for (uint32_t tau = threadIdx.x; tau < nt; tau += T) {
+                const uint64_t g = tb + tau;
+                const int i = task_seq ? (int)task_seq[g] : (int)g;
+                const int t = task_seq ? (int)(g - toff[i]) : 0;
+                const uint32_t vb = (uint32_t)(voff[i] - vbase);
+                const uint64_t id = (uint64_t)i;
+                auto put = [&](int v, uint64_t h) {
+                    const uint32_t b = (uint32_t)(h >> shift);
+                    const uint32_t pos = vb + (uint32_t)v;
+                    S.rank[pos] = (uint16_t)atomicAdd(&S.cnt[b], 1u);
+                    S.bkt[pos] = (uint16_t)b;
+                    S.rec[pos] = ((h << b1) & hi_mask) | id;
+                };
+                const uint64_t* row = tab + (size_t)i * kTabLen;
+                if (d >= 2) {
+                    for_each_task_hash(row, klen[i], runinfo[i], d, t, put);
+                } else {
+                    // the key, then the single deletion of each run: r G[p] + r^-1 P_L
+                    uint64_t G[kKeyLen];
 #pragma unroll
-            for (int k = 0; k < kPer; k++) {
-                sum += S.sbkt[f0 + k];
-                loc[k] = sum;
-            }
-            uint32_t tot;
-            const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
+                    for (int q = 0; q < kKeyLen; q++) G[q] = row[kTabG + q];
+                    const uint64_t PL = row[kTabKey];
+                    const uint32_t rs = (uint32_t)runinfo[i];
+                    put(0, hash_fin(PL));
+                    const uint64_t single = kPolyRI * PL;
+                    int v = 1;
 #pragma unroll
-            for (int k = 0; k < kPer; k++) S.sbkt[f0 + k] = (uint16_t)(ex + loc[k]);
-        }
-        __syncthreads();
-        for (uint32_t tau = threadIdx.x; tau < nt; tau += kStageThreads) {
-            const int li = S.sbkt[tau];
-            const int i = s0 + li;
-            const int t = (int)(tau - S.rel_t[li]);
-            const uint32_t vb = S.rel_v[li];
-            const uint64_t id = (uint64_t)i;
-            auto put = [&](int v, uint64_t h) {
-                S.bkt[vb + v] = (uint16_t)(h >> shift);
-                S.rec[vb + v] = ((h << b1) & hi_mask) | id;
-            };
-            const uint64_t* row = tab + (size_t)i * kTabLen;
-            if (d >= 2) {
-                for_each_task_hash(row, klen[i], runinfo[i], d, t, put);
-            } else if (t == 0) {
-                put(0, hash_fin(row[kTabKey]));
-            } else {  // single deletion of run t - 1: r G[p] + r^-1 P_L
-                const int p = select_bit((uint32_t)runinfo[i], t - 1);
-                put(t, hash_fin(kPolyR * row[kTabG + p] + kPolyRI * row[kTabKey]));
+                    for (int q = 0; q < kKeyLen; q++)
+                        if ((rs >> q) & 1u) put(v++, hash_fin(kPolyR * G[q] + single));
+                }
             }
+            __syncthreads();
+            {
+                uint32_t tot, loc[kFanPer], sum = 0;
+                const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++) {
+                    loc[k] = sum;
+                    sum += (b0 + k < nb) ? S.cnt[b0 + k] : 0u;
+                }
+                const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++)
+                    if (b0 + k < nb) S.lstart[b0 + k] = ex + loc[k];
+            }
+            __syncthreads();
+            for (uint32_t p = threadIdx.x; p < m; p += T) {
+                const uint32_t b = S.bkt[p];
+                const uint32_t q = S.lstart[b] + S.rank[p];
+                S.sorted[q] = S.rec[p];
+                S.sbkt[q] = (uint16_t)b;
+            }
+            __syncthreads();
+            for (uint32_t q = threadIdx.x; q < m; q += T) {
+                const uint32_t b = S.sbkt[q];
+                recs[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
+            }
+            __syncthreads();
+            for (int b = threadIdx.x; b < nb; b += T) {
+                S.gcur[b] += S.cnt[b];
+                S.cnt[b] = 0;
+            }
+            __syncthreads();
         }
+        r0 = (int)S.cstart[nch];
         __syncthreads();
-        stage_partition(S, nb, m, recs);
-        s0 = s1;
     }
 }
 

@@ -322,7 +322,7 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
-    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab;
+    DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab, tseq;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
     bool attrs_set = false;
@@ -489,7 +489,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     const int nb = 1 << b1;
     const bool small = c->stage_chunk == 2048;
     const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
-                                              : (small ? stage_ctas_per_sm<StageSmall>() : stage_ctas_per_sm<StageLarge>());
+                                              : (small ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
+                                                       : ctas_per_sm_for<ScatterSmem<StageLarge>>());
     const int64_t wave = (int64_t)c->sms * per_sm;
     const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
     const int tile = (n + ntiles - 1) / ntiles;
@@ -504,9 +505,9 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem<StageLarge>)));
+                                    (int)sizeof(ScatterSmem<StageLarge>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem<StageSmall>)));
+                                    (int)sizeof(ScatterSmem<StageSmall>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(StageSmem<StageLarge>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -523,23 +524,30 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
     const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
     if (d <= 2 && (1 << b1) <= stage_fan && c->key_tables) {
-        XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
-        XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
-        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n, d,
-                                                                                   P<uint32_t>(c->tcnt)));
-        XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
+        const uint32_t* tseq = nullptr;  // d = 1: one task per sequence
+        if (d >= 2) {
+            XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
+            XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
+            XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
+                                                                                       P<uint32_t>(c->tcnt)));
+            XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
+            XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * V + 16));  // tasks <= variants
+            XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->toff), n,
+                                                                                 P<uint32_t>(c->tseq)));
+            tseq = P<uint32_t>(c->tseq);
+        }
         if (small)
             XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageSmall><<<ntiles, StageSmall::kThreads, sizeof(StageSmem<StageSmall>), s>>>(
+                       k_bucket_scatter_staged<StageSmall><<<ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), n, tile, d, b1, idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart),
-                           P<uint64_t>(c->recA)));
+                           P<uint64_t>(c->toff), tseq, n, tile, d, b1, idbits, P<uint32_t>(c->boffs),
+                           P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
         else
             XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageLarge><<<ntiles, StageLarge::kThreads, sizeof(StageSmem<StageLarge>), s>>>(
+                       k_bucket_scatter_staged<StageLarge><<<ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), n, tile, d, b1, idbits, P<uint32_t>(c->boffs), P<uint64_t>(c->bstart),
-                           P<uint64_t>(c->recA)));
+                           P<uint64_t>(c->toff), tseq, n, tile, d, b1, idbits, P<uint32_t>(c->boffs),
+                           P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
     } else
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
@@ -1188,7 +1196,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info};
+                      &c->ktab,    &c->info,     &c->tseq};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
