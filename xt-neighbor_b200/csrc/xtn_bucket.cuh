@@ -268,9 +268,8 @@ template <class C>
 struct ScatterSmem {
     uint64_t rec[C::kChunk];     // records of the chunk, at their sequence's slots
     uint64_t sorted[C::kChunk];  // the same records grouped by bucket
-    uint16_t bkt[C::kChunk];     // bucket of rec[i]
-    uint16_t rank[C::kChunk];    // rank of rec[i] among the chunk's records of its bucket
-    uint16_t sbkt[C::kChunk];    // bucket of sorted[i]
+    uint32_t br[C::kChunk];      // bucket << 16 | rank of rec[i] among the chunk's records of its bucket
+    uint32_t dst[C::kChunk];     // global position of sorted[i]
     uint32_t cnt[C::kFan];       // records of each bucket in the chunk
     uint32_t lstart[C::kFan];    // first slot of each bucket in `sorted`
     uint32_t gcur[C::kFan];      // next global position of each bucket for this CTA
@@ -345,8 +344,7 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
                 auto put = [&](int v, uint64_t h) {
                     const uint32_t b = (uint32_t)(h >> shift);
                     const uint32_t pos = vb + (uint32_t)v;
-                    S.rank[pos] = (uint16_t)atomicAdd(&S.cnt[b], 1u);
-                    S.bkt[pos] = (uint16_t)b;
+                    S.br[pos] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
                     S.rec[pos] = ((h << b1) & hi_mask) | id;
                 };
                 const uint64_t* row = tab + (size_t)i * kTabLen;
@@ -383,16 +381,13 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
             }
             __syncthreads();
             for (uint32_t p = threadIdx.x; p < m; p += T) {
-                const uint32_t b = S.bkt[p];
-                const uint32_t q = S.lstart[b] + S.rank[p];
+                const uint32_t br = S.br[p], b = br >> 16, r = br & 0xffffu;
+                const uint32_t q = S.lstart[b] + r;
                 S.sorted[q] = S.rec[p];
-                S.sbkt[q] = (uint16_t)b;
+                S.dst[q] = S.gcur[b] + r;
             }
             __syncthreads();
-            for (uint32_t q = threadIdx.x; q < m; q += T) {
-                const uint32_t b = S.sbkt[q];
-                recs[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
-            }
+            for (uint32_t q = threadIdx.x; q < m; q += T) recs[S.dst[q]] = S.sorted[q];
             __syncthreads();
             for (int b = threadIdx.x; b < nb; b += T) {
                 S.gcur[b] += S.cnt[b];
