@@ -294,6 +294,24 @@ def ncu_traffic(kernel: str, workload: str):
     return None
 
 
+def reduce_max(values, pg, device):
+    """Element-wise maximum over the ranks of a process group (None: one process). Every rank
+    calls it with the same number of values; the replicas' step time is the slowest rank's."""
+    if pg is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def replica_throughput(units_per_rank: int, world: int, ms_max: float) -> float:
+    """Whole-job throughput of `world` independent replicas: all ranks' units over the slowest
+    rank's time."""
+    return world * units_per_rank / (ms_max / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -388,10 +406,7 @@ def run_ours(args, w):
     e2e_ms = sum(e2e_times) / len(e2e_times)
     assert len(res.pairs) == n_out
 
-    if pg:
-        t = torch.tensor([ms_step, e2e_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_step, e2e_ms = float(t[0]), float(t[1])
+    ms_step, e2e_ms = reduce_max([ms_step, e2e_ms], pg, "cuda")
     if rank != 0:
         ctx.close()
         if pg:
@@ -408,7 +423,7 @@ def run_ours(args, w):
     total_kernel_ms = sum(v[0] for v in ktimes.values())
     line = {
         "metric": METRIC,
-        "value": world * n / (ms_step / 1e3),
+        "value": replica_throughput(n, world, ms_step),
         "unit": "seqs/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -436,7 +451,7 @@ def run_ours(args, w):
         "output_entries": n_out,
         "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_out")},
         "e2e": {
-            "value": world * n / (e2e_ms / 1e3),
+            "value": replica_throughput(n, world, e2e_ms),
             "unit": "seqs/s",
             "ms_per_step": e2e_ms,
             "h2d_bytes_per_step": int(len(chars) + 4 * len(offs) + (12 * n if overlap else 0)),
