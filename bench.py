@@ -348,6 +348,9 @@ def run_ours(args, w):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     ext = torch.cuda.ExternalStream(ctx.stream())
     torch.cuda.synchronize()
+    tuned = None
+    if args.autotune and not overlap:  # outside the timed region
+        tuned = ctx.autotune(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
 
     def step():
         if overlap:
@@ -445,6 +448,7 @@ def run_ours(args, w):
             "engine": args.engine,
             "options": {o.split("=", 1)[0]: int(o.split("=", 1)[1]) for o in args.opt},
             "l2": "flushed between steps (256 MiB write)",
+            "autotuned": tuned,
         },
         "pairs_per_s": None if overlap else world * n_out / (ms_step / 1e3),
         "verified_pairs": stats["n_verified_pairs"] if overlap else n_out,
@@ -628,6 +632,8 @@ def main():
     ap.add_argument("--engine", choices=["bucket", "sort"], default="bucket",
                     help="key grouping: shared-memory hash buckets (default) or full radix sort")
     ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the bucket-engine shape by timing on the workload first (xtn_context_autotune)")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
                     help="context option (xtn_context_set_option), repeatable")
     args = ap.parse_args()

@@ -166,6 +166,15 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *                     0 = hash each variant key directly (same hash values, slower) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
+/* Autotuner: times the search on these device-resident inputs (the caller's data, so its length
+ * distribution and duplicate structure) for each bucket-engine shape - first-level and split
+ * stage chunks, first-level bucket bits, then bulk-copy or plain loads in the grouping kernel -
+ * taking the best of `repeats` runs after a warm-up, and leaves the fastest shape set on the
+ * context. `report` (may be NULL) receives the choice and its time. No counterpart in the
+ * reference, which has fixed chunk sizes (xtneighbor_streaming/src/xtn.cu:21-26). */
+int xtn_context_autotune(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                         int32_t n_seqs, int32_t repeats, char* report, int32_t report_cap);
+
 /* ------------------------------------------------------------------ resident index and serving */
 
 /* A resident deletion index: every deletion variant (at most max_distance <= 2 deletions) of

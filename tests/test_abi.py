@@ -60,3 +60,11 @@ def test_index_argument_errors_need_no_device():
     assert lib.xtn_index_create(0, chars.ctypes.data, offs.ctypes.data, 2, 3, ctypes.byref(h)) == xtn.ERR_ARG
     assert b"maximum distance" in lib.xtn_last_error()
     assert lib.xtn_index_serve(None, None, 0, None, None, xtn.REQUEST_CALLBACK(0), None) == xtn.ERR_ARG
+
+
+def test_autotune_argument_errors_need_no_device():
+    lib = xtn.load()
+    args = xtn.Args(1, 0, 0, 0)
+    import ctypes
+
+    assert lib.xtn_context_autotune(None, ctypes.byref(args), None, None, 0, 1, None, 0) == xtn.ERR_ARG

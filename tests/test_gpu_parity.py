@@ -187,3 +187,18 @@ def test_overlap_device_entry(ctx):
     bad[7, 1] = len(reps)
     with pytest.raises(xtn.XtnError, match="out of range at row 7$"):
         ctx.perform(chars, offs, distance=1, info=bad, n_reps=len(reps))
+
+
+def test_autotune_keeps_results_exact():
+    """The autotuner picks a bucket-engine shape by timing; the search stays bit-exact."""
+    import torch
+
+    chars, offs = xtn.synth_clusters(seed=13, n=50_000)
+    ctx = xtn.Context(0)
+    dch = torch.from_numpy(chars).cuda()
+    dof = torch.from_numpy(offs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    report = ctx.autotune(dch.data_ptr(), dof.data_ptr(), len(offs) - 1, distance=2, repeats=1)
+    assert "stage_chunk=" in report and "best of" in report
+    check_nn(ctx, chars, offs, 2, 0, "after autotune")
+    ctx.close()

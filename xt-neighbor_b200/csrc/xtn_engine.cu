@@ -1309,6 +1309,92 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     return XTN_SUCCESS;
 }
 
+int xtn_context_autotune(xtn_context* c, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                         int32_t n, int32_t repeats, char* report, int32_t report_cap) {
+    if (!c || !d_seqs || !d_offsets || n < 1) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    XTN_CK(cudaSetDevice(c->device));
+    if (repeats < 1) repeats = 2;
+    // the bucket engine's shapes: first-level and split stage chunks, first-level bucket bits,
+    // bulk copy or plain loads in the grouping kernel
+    struct Shape {
+        int stage, split, bits, tma;
+    };
+    std::vector<Shape> shapes;
+    for (int stage : {4096, 2048})
+        for (int split : {4096, 2048})
+            for (int bits : {9, 10}) {
+                if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
+                shapes.push_back(Shape{stage, split, bits, 1});
+            }
+    const Shape saved{c->stage_chunk, c->split_chunk, c->bucket_bits_max, c->group_tma};
+    const int saved_engine = c->engine;
+    c->engine = 0;
+    auto apply = [&](const Shape& sh) {
+        c->stage_chunk = sh.stage;
+        c->split_chunk = sh.split;
+        c->bucket_bits_max = sh.bits;
+        c->group_tma = sh.tma;
+    };
+    auto time_shape = [&](const Shape& sh, float* ms) -> int {
+        apply(sh);
+        float best = 1e30f;
+        for (int r = 0; r <= repeats; r++) {  // the first run is a warm-up
+            begin_run(c);
+            int st = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance,
+                            args->measure);
+            end_run(c);
+            if (st != XTN_SUCCESS) return st;
+            float t = (float)c->stats.ms_total;
+            if (r > 0) best = std::min(best, t);
+        }
+        *ms = best;
+        return XTN_SUCCESS;
+    };
+    Shape best_shape = shapes[0];
+    float best_ms = 1e30f;
+    int tried = 0;
+    for (const Shape& sh : shapes) {
+        float ms = 0;
+        int st = time_shape(sh, &ms);
+        if (st != XTN_SUCCESS) {
+            apply(saved);
+            c->engine = saved_engine;
+            return st;
+        }
+        tried++;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_shape = sh;
+        }
+    }
+    {  // the grouping kernel's load path, on the best shape
+        Shape sh = best_shape;
+        sh.tma = 0;
+        float ms = 0;
+        int st = time_shape(sh, &ms);
+        if (st != XTN_SUCCESS) {
+            apply(saved);
+            c->engine = saved_engine;
+            return st;
+        }
+        tried++;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_shape = sh;
+        }
+    }
+    apply(best_shape);
+    if (report && report_cap > 0)
+        snprintf(report, (size_t)report_cap,
+                 "stage_chunk=%d split_chunk=%d bucket_bits_max=%d group_tma=%d: %.3f ms (best of %d shapes)",
+                 best_shape.stage, best_shape.split, best_shape.bits, best_shape.tma, best_ms, tried);
+    return XTN_SUCCESS;
+}
+
 int xtn_context_set_profiling(xtn_context* c, int on) {
     if (!c) return XTN_ERR_ARG;
     c->prof.on = on != 0;

@@ -46,6 +46,7 @@ SYMBOLS = (
     "xtn_context_stream",
     "xtn_context_stats",
     "xtn_context_set_option",
+    "xtn_context_autotune",
     "xtn_context_set_profiling",
     "xtn_context_kernel_times",
     "xtn_last_error",
@@ -171,6 +172,8 @@ def load():
     lib.xtn_context_overlap_device.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P,
                                                ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_fetch.argtypes = [P, P, P, P, ctypes.c_int64]
+    lib.xtn_context_autotune.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, ctypes.c_int32, P,
+                                         ctypes.c_int32]
     lib.xtn_index_create.argtypes = [ctypes.c_int, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(P)]
     lib.xtn_index_create_device.argtypes = [ctypes.c_int, P, P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(P)]
     lib.xtn_index_destroy.argtypes = [P]
@@ -328,6 +331,15 @@ class Context:
             )
         )
         return Result(pairs, None, sums)
+
+    def autotune(self, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN, repeats=2) -> str:
+        """Times the bucket engine's shapes on these device inputs and keeps the fastest on the
+        context (xtn_context_autotune); returns the choice as text."""
+        args = Args(distance, measure, 0, 0)
+        buf = ctypes.create_string_buffer(256)
+        _check(self.lib.xtn_context_autotune(self.h, ctypes.byref(args), ctypes.c_void_p(d_chars),
+                                             ctypes.c_void_p(d_offsets), n, repeats, buf, 256))
+        return buf.value.decode()
 
     def fetch(self, n: int) -> Result:
         pairs = np.zeros((n, 2), np.int32)
