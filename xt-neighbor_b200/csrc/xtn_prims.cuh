@@ -188,7 +188,7 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 
 __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(const uint64_t* __restrict__ keys, int64_t n, int shift,
