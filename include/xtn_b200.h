@@ -160,6 +160,9 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *   "stage_chunk"     2048 | 4096: records per shared-memory chunk of the first-level scatter
  *                     (default 4096: two CTAs per SM; 2048: four)
  *   "split_chunk"     2048 | 4096: the same for the split of large buckets (default 4096)
+ *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
+ *                     CTAs take slices of the bucket and merge their histograms through
+ *                     distributed shared memory)
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
  *                     (default), 0 = with plain 16-byte loads from every thread
  *   "key_tables"      1 = for d <= 2, hash variants from per-sequence tables (default),

@@ -29,6 +29,8 @@
 #pragma once
 #include <cstdint>
 
+#include <cooperative_groups.h>
+
 #include "xtn_common.cuh"
 
 namespace xtn {
@@ -40,6 +42,7 @@ constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp
 // boundary sectors complete in L2.
 constexpr int kMaxFirstLevelBits = 9;  // default bound; the large stage shape takes up to 10
 constexpr int kMaxSplitBits = 10;
+constexpr int kSplitSlices = 8;        // CTAs (one thread-block cluster) per split bucket
 
 // Shape of a staged partition: threads per CTA, records per chunk, largest fan-out.
 template <int THREADS, int CHUNK, int FAN>
@@ -448,30 +451,45 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
     }
 }
 
-// One CTA per split job: histogram of the record's top `bits` bits (the next hash bits),
-// sub-bucket descriptors, then the bucket's records, chunk by chunk, through the staged
-// partition into buffer B at the same range. Sub-buckets that fit are listed for grouping;
-// larger ones go to the fallback list. counters[5] counts CTAs whose chunk copy did not
+// Split of the oversized first-level buckets. Each job (bucket) is handled by a cluster of
+// kSlices CTAs, each taking a contiguous slice of the bucket's records:
+//   1. each CTA histograms its slice by the records' top `bits` bits (the next hash bits);
+//   2. after a cluster barrier, each CTA reads every slice's histogram from its peers' shared
+//      memory (distributed shared memory, plain loads) and derives the sub-bucket totals, their
+//      starts and its own offset inside each sub-bucket; rank 0 lists the sub-buckets (those
+//      that fit for grouping, larger ones for the fallback); a second barrier ends the remote
+//      reads;
+//   3. each CTA streams its slice chunk by chunk (bulk copy, the next chunk in flight during the
+//      write-out) through the staged partition into buffer B at the bucket's range.
+// With kSlices CTAs per bucket, few buckets are in flight at a time, so the second read of a
+// slice comes from L2 rather than DRAM. counters[5] counts CTAs whose chunk copy did not
 // complete within the wait bound (their output is incomplete; the host reports an error).
-template <class C>
-__global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_split_staged(
-    const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t group_cap,
-    BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
+template <class C, int kSlices>
+__global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
+    k_bucket_split_staged(const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in,
+                          uint64_t* __restrict__ out, uint32_t group_cap, BucketDesc* __restrict__ desc,
+                          BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
     constexpr int kStageThreads = C::kThreads, kStageChunk = C::kChunk, kFanPer = C::kFanPer;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
-    const SplitJob job = jobs[blockIdx.x];
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const SplitJob job = jobs[blockIdx.x / kSlices];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;
     const bool priv = nsub <= kPrivFan;
-    const uint64_t* src = in + job.start;
-    // Chunk c of the job reaches S.rec by one bulk copy from the 16-byte boundary at or below
+    const uint32_t s_lo = (uint32_t)((uint64_t)job.size * rank / kSlices);
+    const uint32_t s_hi = (uint32_t)((uint64_t)job.size * (rank + 1) / kSlices);
+    const uint32_t size = s_hi - s_lo;
+    const uint64_t* src = in + job.start + s_lo;
+    // Chunk c of the slice reaches S.rec by one bulk copy from the 16-byte boundary at or below
     // its first record (the record buffers carry 16 bytes of padding), completing on S.mbar
     // with parity c & 1. The copy of chunk c + 1 is issued as soon as chunk c's records are
     // ranked, so it overlaps chunk c's write-out.
     const uint32_t mbar = smem_u32(&S.mbar);
     auto issue = [&](uint32_t c0) {
-        const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
+        const uint32_t m = min((uint32_t)kStageChunk, size - c0);
         const uint64_t* a = src + c0;
         const uint32_t lead = (uint32_t)(((uintptr_t)a & 15u) >> 3);
         bulk_load(smem_u32(&S.rec[0]), a - lead, ((lead + m) * 8u + 15u) & ~15u, mbar);
@@ -480,18 +498,19 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
         S.wait_failed = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        if (job.size > 0) issue(0);
+        if (size > 0) issue(0);
     }
-    // histogram: per-warp copies (in `sorted`, unused until the first chunk) for small fan-outs
-    uint32_t* hist = priv ? reinterpret_cast<uint32_t*>(S.sorted) + (threadIdx.x >> 5) * kPrivFan : S.cnt;
+    // 1. slice histogram into S.lstart (per-warp copies in `sorted`, unused until the first
+    //    chunk, for small fan-outs)
+    uint32_t* hist = priv ? reinterpret_cast<uint32_t*>(S.sorted) + (threadIdx.x >> 5) * kPrivFan : S.lstart;
     for (int i = threadIdx.x; i < (priv ? kPrivFan * (kStageThreads / 32) : nsub); i += kStageThreads)
-        (priv ? reinterpret_cast<uint32_t*>(S.sorted) : S.cnt)[i] = 0;
+        (priv ? reinterpret_cast<uint32_t*>(S.sorted) : S.lstart)[i] = 0;
     __syncthreads();
     {
-        // 16-byte loads, four in flight per thread (job.start is 8-byte aligned: peel one)
-        const uint32_t lead = (uint32_t)(((uintptr_t)src & 15u) >> 3);
-        if (lead && threadIdx.x == 0 && job.size > 0) atomicAdd(&hist[src[0] >> shift], 1u);
-        const uint32_t nv = (job.size - lead) >> 1;
+        // 16-byte loads, four in flight per thread (the slice is 8-byte aligned: peel one)
+        const uint32_t lead = size > 0 ? (uint32_t)(((uintptr_t)src & 15u) >> 3) : 0u;
+        if (lead && threadIdx.x == 0) atomicAdd(&hist[src[0] >> shift], 1u);
+        const uint32_t nv = (size - lead) >> 1;
         const uint4* v = reinterpret_cast<const uint4*>(src + lead);
         uint32_t i = threadIdx.x;
         for (; i + 3 * kStageThreads < nv; i += 4 * kStageThreads) {
@@ -508,43 +527,53 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
             atomicAdd(&hist[(((uint64_t)a.y << 32) | a.x) >> shift], 1u);
             atomicAdd(&hist[(((uint64_t)a.w << 32) | a.z) >> shift], 1u);
         }
-        if (threadIdx.x == 0 && ((job.size - lead) & 1u)) atomicAdd(&hist[src[job.size - 1] >> shift], 1u);
+        if (threadIdx.x == 0 && ((size - lead) & 1u)) atomicAdd(&hist[src[size - 1] >> shift], 1u);
     }
     __syncthreads();
     if (priv) {
         for (int b = threadIdx.x; b < nsub; b += kStageThreads) {
             uint32_t t = 0;
             for (int w = 0; w < kStageThreads / 32; w++) t += reinterpret_cast<uint32_t*>(S.sorted)[w * kPrivFan + b];
-            S.cnt[b] = t;
+            S.lstart[b] = t;
         }
-        __syncthreads();
     }
+    cluster.sync();
+    // 2. sub-bucket totals, starts and this slice's offsets from every slice's histogram
     {
-        uint32_t tot, loc[kFanPer], sum = 0;
+        uint32_t tot_b[kFanPer], mine_b[kFanPer], loc[kFanPer], sum = 0;
         const int b0 = threadIdx.x * kFanPer;
 #pragma unroll
         for (int k = 0; k < kFanPer; k++) {
+            tot_b[k] = mine_b[k] = 0;
+            if (b0 + k < nsub)
+                for (int r = 0; r < kSlices; r++) {
+                    const uint32_t c = cluster.map_shared_rank(S.lstart, r)[b0 + k];
+                    tot_b[k] += c;
+                    if (r < rank) mine_b[k] += c;
+                }
             loc[k] = sum;
-            sum += (b0 + k < nsub) ? S.cnt[b0 + k] : 0u;
+            sum += tot_b[k];
         }
+        uint32_t tot;
         const uint32_t ex = block_scan_ex<uint32_t, kStageThreads>(sum, &tot, S.warp_sums);
 #pragma unroll
         for (int k = 0; k < kFanPer; k++) {
             const int b = b0 + k;
             if (b >= nsub) continue;
-            const uint32_t c = S.cnt[b], st = ex + loc[k];
-            S.gcur[b] = (uint32_t)job.start + st;
-            if (c >= 2) {
-                BucketDesc bd{job.start + st, c, 1};
-                if (c <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
+            const uint32_t st = ex + loc[k];
+            S.gcur[b] = (uint32_t)job.start + st + mine_b[k];
+            if (rank == 0 && tot_b[k] >= 2) {
+                BucketDesc bd{job.start + st, tot_b[k], 1};
+                if (tot_b[k] <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
                 else fallback[atomicAdd(&counters[3], 1u)] = bd;
             }
         }
     }
-    __syncthreads();
+    cluster.sync();  // no remote reads after this point: S.lstart is free again
+    // 3. the slice through the staged partition
     uint32_t parity = 0;
-    for (uint32_t c0 = 0; c0 < job.size; c0 += kStageChunk, parity ^= 1u) {
-        const uint32_t m = min((uint32_t)kStageChunk, job.size - c0);
+    for (uint32_t c0 = 0; c0 < size; c0 += kStageChunk, parity ^= 1u) {
+        const uint32_t m = min((uint32_t)kStageChunk, size - c0);
         const uint32_t lead = (uint32_t)(((uintptr_t)(src + c0) & 15u) >> 3);
         if (threadIdx.x == 0) {
             uint32_t polls = 0;
@@ -568,7 +597,7 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>()) k_bucket_
             return;
         }
         split_partition(S, nsub, m, S.rec + lead, shift, out, [&] {
-            if (threadIdx.x == 0 && c0 + kStageChunk < job.size) issue(c0 + kStageChunk);
+            if (threadIdx.x == 0 && c0 + kStageChunk < size) issue(c0 + kStageChunk);
         });
     }
 }

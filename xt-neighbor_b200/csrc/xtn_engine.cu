@@ -332,6 +332,7 @@ struct xtn_context {
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
     int split_chunk = 4096;  // the same for the split (2048 | 4096)
+    int split_slices = kSplitSlices;  // CTAs (one cluster) per split bucket: 1 | kSplitSlices
     uint32_t group_cap = kGroupCap;
     uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
     // results
@@ -508,10 +509,14 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
                                     (int)sizeof(ScatterSmem<StageLarge>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(ScatterSmem<StageSmall>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(StageSmem<StageLarge>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, kSplitSlices>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageLarge>)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(StageSmem<SplitSmall>)));
+        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, kSplitSlices>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<SplitSmall>)));
         XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
         c->attrs_set = true;
     }
@@ -571,16 +576,21 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_CK(cudaStreamSynchronize(s));
     memcpy(cnt, c->h_scalar, 32);
     if (cnt[1] > 0) {
-        if (c->split_chunk == 2048)
-            XTN_LAUNCH("bucket_split",
-                       k_bucket_split_staged<SplitSmall><<<cnt[1], SplitSmall::kThreads, sizeof(StageSmem<SplitSmall>), s>>>(
-                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
-                           P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
-        else
-            XTN_LAUNCH("bucket_split",
-                       k_bucket_split_staged<StageLarge><<<cnt[1], StageLarge::kThreads, sizeof(StageSmem<StageLarge>), s>>>(
-                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
-                           P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)));
+        // one CTA per bucket, or a cluster of kSplitSlices CTAs per bucket
+        const bool sliced = c->split_slices > 1;
+        const unsigned grid = cnt[1] * (sliced ? kSplitSlices : 1);
+#define XTN_SPLIT(CFG, SL)                                                                                         \
+    XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
+                                   P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
+                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)))
+        if (c->split_chunk == 2048) {
+            if (sliced) XTN_SPLIT(SplitSmall, kSplitSlices);
+            else XTN_SPLIT(SplitSmall, 1);
+        } else {
+            if (sliced) XTN_SPLIT(StageLarge, kSplitSlices);
+            else XTN_SPLIT(StageLarge, 1);
+        }
+#undef XTN_SPLIT
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1302,6 +1312,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
+    else if (!strcmp(name, "split_slices") && (v == 1 || v == kSplitSlices)) c->split_slices = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
         return XTN_ERR_ARG;
