@@ -79,6 +79,20 @@ def test_single_and_identical(ctx):
     check_nn(ctx, chars, offs, 1, 0, "identical")
 
 
+def test_every_sequence_twice(ctx):
+    """Each of 40,000 sequences (10% of them mutants of others) appears twice, shuffled, so
+    every variant hash is a run of >= 2 records: a first-level bucket or sub-bucket of ~2,500
+    records then lists ~1,250 runs, more than the grouping CTA holds, and goes to the
+    sort-based regrouping."""
+    bc, bo = xtn.synth_mutants(seed=31, n=40_000, mutant_frac=0.10)
+    base = [bytes(bc[bo[i] : bo[i + 1]]).decode() for i in range(len(bo) - 1)]
+    rng = np.random.default_rng(31)
+    seqs = [base[i] for i in rng.permutation(np.repeat(np.arange(len(base)), 2))]
+    chars, offs = csr(seqs)
+    got = check_nn(ctx, chars, offs, 1, xtn.LEVENSHTEIN, "every sequence twice")
+    assert (got.distances == 0).sum() >= 40_000 and (got.distances == 1).sum() > 1000
+
+
 def test_short_sequences_large_d(ctx):
     """d >= L: the empty variant is shared by every short sequence."""
     rng = np.random.default_rng(1)
