@@ -166,7 +166,11 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
  *                     (default), 0 = with plain 16-byte loads from every thread
  *   "key_tables"      1 = for d <= 2, hash variants from per-sequence tables (default),
- *                     0 = hash each variant key directly (same hash values, slower) */
+ *                     0 = hash each variant key directly (same hash values, slower)
+ *   "onesweep"        1 = radix sorts of up to 2^24 keys (candidate pairs, fallback buckets)
+ *                     by single-sweep passes with decoupled look-back (default; larger sorts
+ *                     keep the classic passes), 0 = classic passes for every sort (per-tile
+ *                     counts, a scan, a scatter) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length

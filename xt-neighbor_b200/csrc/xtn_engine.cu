@@ -322,9 +322,12 @@ struct xtn_context {
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
+    DevBuf os_scratch, os_status, dev_err;  // single-sweep sort scratch, status words, wait-error count
+    uint32_t os_epoch = 0;
     DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab, tseq;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
+    int onesweep = 1;       // radix sorts by single-sweep passes (0: classic passes)
     bool attrs_set = false;
     int bucket_bits_max = kMaxFirstLevelBits;
     int scatter_ctas_per_sm = 0;  // 0: as many as the stage shape's shared memory allows
@@ -402,13 +405,65 @@ static int scan_u64(xtn_context* c, const uint64_t* in, uint64_t* out, int64_t n
     return XTN_SUCCESS;
 }
 
-static int sort_u64(xtn_context* c, DevBuf& a, DevBuf& b, int64_t n, int lo, int hi, uint64_t** result, const char* up,
-                    const char* down) {
-    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
-    *result = radix_sort_u64(P<uint64_t>(a), P<uint64_t>(b), n, lo, hi, P<uint32_t>(c->scratch32), c->stream, up, down);
+// Kernel names of one sort (classic passes or single-sweep passes).
+struct SortNames {
+    const char* up;
+    const char* down;
+    const char* hist;
+    const char* pass;
+};
+#define XTN_SORT_NAMES(p) (SortNames{p "_upsweep", p "_downsweep", p "_hist", p "_pass"})
+
+// Single-sweep passes are used up to this many keys. They save the classic passes' count
+// kernels, scans and launches, which dominate small sorts. Above it the classic passes were
+// measured faster on B200 (55M candidate pairs: 2.6 ms against 3.2 ms), because each tile's
+// look-back latency is exposed at five CTAs per SM.
+constexpr int64_t kOsMaxKeys = int64_t(1) << 24;
+
+static int ensure_err_word(xtn_context* c) {
+    if (c->dev_err.p) return XTN_SUCCESS;
+    XTN_TRY(ensure(c->dev_err, 16));
+    XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, c->stream));
     return XTN_SUCCESS;
 }
 
+// Sorts n keys by bits [lo, hi): single-sweep passes (look-back) up to kOsMaxKeys keys, else
+// the classic count / scan / scatter passes.
+static int sort_u64(xtn_context* c, DevBuf& a, DevBuf& b, int64_t n, int lo, int hi, uint64_t** result,
+                    SortNames names) {
+    const int passes = (hi - lo + kRadixBits - 1) / kRadixBits;
+    const int64_t words = onesweep_status_words(n);
+    if (c->onesweep && n <= kOsMaxKeys && passes <= kOsMaxPasses) {
+        XTN_TRY(ensure(c->os_scratch, sizeof(uint32_t) * kOsScratchWords));
+        XTN_TRY(ensure_err_word(c));
+        if (c->os_status.cap < sizeof(unsigned long long) * (size_t)words) {
+            XTN_TRY(ensure(c->os_status, sizeof(unsigned long long) * (size_t)words));
+            XTN_CK(cudaMemsetAsync(c->os_status.p, 0, c->os_status.cap, c->stream));
+        }
+        *result = onesweep_sort_u64(P<uint64_t>(a), P<uint64_t>(b), n, lo, hi, P<uint32_t>(c->os_scratch),
+                                    P<unsigned long long>(c->os_status), (int64_t)(c->os_status.cap / 8), &c->os_epoch,
+                                    P<unsigned int>(c->dev_err), c->sms, c->stream, names.hist, names.pass);
+        return XTN_SUCCESS;
+    }
+    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
+    *result = radix_sort_u64(P<uint64_t>(a), P<uint64_t>(b), n, lo, hi, P<uint32_t>(c->scratch32), c->stream, names.up,
+                             names.down);
+    return XTN_SUCCESS;
+}
+
+// Reads (after the stream has drained up to here) and clears the count of device waits that
+// gave up; nonzero means a result computed since the last check is unreliable.
+static int check_err_word(xtn_context* c) {
+    if (!c->dev_err.p) return XTN_SUCCESS;
+    uint64_t e = 0;
+    XTN_TRY(read_scalar(c, c->dev_err.p, 4, &e));
+    if (e != 0) {
+        XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, c->stream));
+        set_err("radix sort: " + std::to_string(e) + " look-back waits did not complete in time");
+        return XTN_ERR_CUDA;
+    }
+    return XTN_SUCCESS;
+}
 
 // Grows a buffer keeping its first `used` bytes.
 static int ensure_keep(xtn_context* c, DevBuf& b, size_t bytes, size_t used) {
@@ -475,7 +530,7 @@ static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t 
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
     uint64_t* recs = nullptr;
-    XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, "key_sort_upsweep", "key_sort_downsweep"));
+    XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, XTN_SORT_NAMES("key_sort")));
     XTN_CK(cudaEventRecord(c->ev[3], s));
     XTN_TRY(group_sorted(c, recs, (int64_t)V, idbits, 0, Pc));
     XTN_CK(cudaEventRecord(c->ev[4], s));
@@ -645,8 +700,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
             const uint64_t* srcbuf = f.src ? P<uint64_t>(c->recB) : P<uint64_t>(c->recA);
             XTN_CK(cudaMemcpyAsync(c->fbA.p, srcbuf + f.start, sizeof(uint64_t) * f.size, cudaMemcpyDeviceToDevice, s));
             uint64_t* sorted = nullptr;
-            XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, "fallback_sort_upsweep",
-                             "fallback_sort_downsweep"));
+            XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, XTN_SORT_NAMES("fallback_sort")));
             uint64_t more = 0;
             XTN_TRY(group_sorted(c, sorted, f.size, idbits, total, &more));
             total += more;
@@ -708,8 +762,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_CK(cudaEventRecord(c->ev[5], s));
     uint64_t* pairs = P<uint64_t>(c->pairA);
     if (Pc > 1)
-        XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, 2 * idbits, &pairs, "pair_sort_upsweep",
-                         "pair_sort_downsweep"));
+        XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, 2 * idbits, &pairs, XTN_SORT_NAMES("pair_sort")));
     XTN_CK(cudaEventRecord(c->ev[6], s));
 
     // verify + compact
@@ -737,7 +790,14 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
                                                                P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist)));
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[8], s));
+    if (c->dev_err.p) XTN_CK(cudaMemcpyAsync(c->h_scalar + 7, c->dev_err.p, 8, cudaMemcpyDeviceToHost, s));
     XTN_CK(cudaStreamSynchronize(s));
+    if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
+        XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
+        set_err("radix sort: " + std::to_string((uint32_t)c->h_scalar[7]) +
+                " look-back waits did not complete in time");
+        return XTN_ERR_CUDA;
+    }
     c->n_out = (int64_t)nout;
     c->overlap_result = false;
     st.n_out = (int64_t)nout;
@@ -1206,7 +1266,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->tseq};
+                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1309,6 +1369,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "group_cap") && v >= 2 && v <= kGroupCap) c->group_cap = (uint32_t)v;
     else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 0 && v <= 4) c->scatter_ctas_per_sm = (int)v;
     else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
+    else if (!strcmp(name, "onesweep") && (v == 0 || v == 1)) c->onesweep = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;

@@ -214,8 +214,7 @@ static int index_build(xtn_index* ix, int n, int dmax) {
                                 P<uint64_t>(c->voff), n, dmax, ix->idbits, P<uint64_t>(ix->recs)));
     XTN_CK(cudaGetLastError());
     uint64_t* sorted = nullptr;
-    XTN_TRY(sort_u64(c, ix->recs, c->recB, (int64_t)V, ix->idbits, 64, &sorted, "index_sort_upsweep",
-                     "index_sort_downsweep"));
+    XTN_TRY(sort_u64(c, ix->recs, c->recB, (int64_t)V, ix->idbits, 64, &sorted, XTN_SORT_NAMES("index_sort")));
     if (sorted != P<uint64_t>(ix->recs))
         XTN_CK(cudaMemcpyAsync(ix->recs.p, sorted, sizeof(uint64_t) * V, cudaMemcpyDeviceToDevice, s));
     int B = 1;
@@ -229,11 +228,12 @@ static int index_build(xtn_index* ix, int n, int dmax) {
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(e1, s));
     XTN_CK(cudaStreamSynchronize(s));
+    XTN_TRY(check_err_word(c));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     ix->ms_build = ms;
     // the build's scratch is not needed by queries
-    DevBuf* tmp[] = {&c->recB, &c->keys, &c->ktab, &c->scratch32};
+    DevBuf* tmp[] = {&c->recB, &c->keys, &c->ktab, &c->scratch32, &c->os_status};
     for (DevBuf* b : tmp) release(*b);
     return XTN_SUCCESS;
 }
@@ -297,8 +297,7 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
         XTN_CK(cudaGetLastError());
         uint64_t* pairs = P<uint64_t>(c->pairA);
         if (Pc > 1)
-            XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, ix->idbits + qbits, &pairs, "pair_sort_upsweep",
-                             "pair_sort_downsweep"));
+            XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, ix->idbits + qbits, &pairs, XTN_SORT_NAMES("pair_sort")));
         XTN_TRY(ensure(c->dist, Pc));
         XTN_TRY(ensure(c->flag, Pc));
         XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Pc + 1)));
@@ -318,7 +317,13 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
                                             P<int8_t>(c->out_dist)));
         XTN_CK(cudaGetLastError());
     }
+    if (c->dev_err.p) XTN_CK(cudaMemcpyAsync(c->h_scalar + 7, c->dev_err.p, 8, cudaMemcpyDeviceToHost, s));
     XTN_CK(cudaStreamSynchronize(s));
+    if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
+        XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
+        set_err("radix sort: a look-back wait did not complete in time");
+        return XTN_ERR_CUDA;
+    }
     c->n_out = (int64_t)nout;
     c->stats.n_out = (int64_t)nout;
     return XTN_SUCCESS;

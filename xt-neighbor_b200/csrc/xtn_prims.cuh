@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 namespace xtn {
@@ -297,6 +298,225 @@ inline uint64_t* radix_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo
         XTN_LAUNCH(up_name, k_radix_upsweep<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(src, n, shift, counts, ntiles));
         scan_exclusive<uint32_t, uint32_t>(counts, offsets, m, sscratch, stream);
         XTN_LAUNCH(down_name, k_radix_downsweep<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(src, dst, n, shift, offsets, ntiles));
+        uint64_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// ------------------------------------------------------------------ single-sweep LSD radix sort
+// The passes of radix_sort_u64 with each pass's count kernel and count-matrix scan replaced by
+// a chained scan (Adinets & Merrill, "Onesweep: a faster least significant digit radix sort
+// for GPUs", 2022):
+//   1. k_onesweep_hist reads the keys once and counts every pass's digit at the same time; the
+//      last CTA to finish turns the counts into each pass's digit starts;
+//   2. per pass, k_onesweep_pass: a CTA takes the next tile in start order (an atomic ticket),
+//      ranks the tile's keys by digit, publishes its per-digit counts in a status word per
+//      (tile, digit), sums the counts of all earlier tiles by looking back through their
+//      status words (decoupled look-back) and writes each digit run at its global position.
+// A tile only waits for tiles whose tickets were taken earlier, by CTAs already running, and
+// those publish their counts before they look back themselves, so every wait ends; each is
+// still bounded (kOsPollLimit polls), after which the CTA counts an error in *err and goes on
+// with the sum it has (the host reports the error and discards the result).
+// Status word: bits 62-63 flag (1: this tile's count, 2: the count of tiles 0..this one),
+// bits 32-61 epoch (a per-pass tag: words of earlier passes read as unset, so the array is
+// never cleared between passes), bits 0-31 the count.
+constexpr int kOsMaxPasses = 8;
+constexpr uint32_t kOsPollLimit = 1u << 22;
+constexpr uint32_t kOsMaxEpoch = (1u << 30) - 1u;
+constexpr unsigned long long kOsFlagCount = 1ull << 62;
+constexpr unsigned long long kOsFlagPrefix = 2ull << 62;
+
+// Scratch of one sort (u32 words): digit starts [passes][256], then the counts [passes][256],
+// a ticket per pass and the finished-CTA counter, which are cleared before every sort.
+constexpr int kOsStartWords = kOsMaxPasses * kRadix;
+constexpr int kOsClearWords = kOsMaxPasses * kRadix + kOsMaxPasses + 1;
+constexpr int kOsScratchWords = kOsStartWords + kOsClearWords;
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_onesweep_hist(const uint64_t* __restrict__ keys, int64_t n, int lo_bit,
+                                                                int passes, uint32_t* __restrict__ dstart,
+                                                                uint32_t* __restrict__ counts,
+                                                                unsigned int* __restrict__ done) {
+    __shared__ uint32_t h[kOsMaxPasses][kRadix];
+    __shared__ int last;
+#pragma unroll
+    for (int p = 0; p < kOsMaxPasses; p++) h[p][threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * kSortThreads;
+    for (int64_t i = (int64_t)blockIdx.x * kSortThreads + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i] >> lo_bit;
+        for (int p = 0; p < passes; p++) atomicAdd(&h[p][(k >> (kRadixBits * p)) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    for (int p = 0; p < passes; p++) {
+        const uint32_t v = h[p][threadIdx.x];
+        if (v) atomicAdd(&counts[p * kRadix + threadIdx.x], v);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int p = 0; p < passes; p++) {
+        uint32_t tot;
+        const uint32_t v = __ldcg(&counts[p * kRadix + threadIdx.x]);
+        dstart[p * kRadix + threadIdx.x] = block_exclusive_scan<uint32_t, kSortThreads>(v, &tot);
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                                                int64_t n, int shift, const uint32_t* __restrict__ dstart,
+                                                                unsigned long long* __restrict__ status, uint32_t epoch,
+                                                                unsigned int* __restrict__ ticket,
+                                                                unsigned int* __restrict__ err) {
+    __shared__ uint64_t s_keys[kSortTile];
+    __shared__ uint32_t s_cnt[kSortWarps][kRadix + 1];
+    __shared__ uint32_t s_start[kRadix];
+    __shared__ uint32_t s_base[kRadix];
+    __shared__ uint32_t s_tile;
+    __shared__ int s_failed;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(ticket, 1u);
+        s_failed = 0;
+    }
+    for (int i = threadIdx.x; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&s_cnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int64_t tile_base = (int64_t)tile * kSortTile;
+    const int64_t valid64 = n - tile_base;
+    const int valid = valid64 > kSortTile ? kSortTile : (int)valid64;
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t key[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        const int pos = warp * (32 * kSortItems) + k * 32 + lane;  // warp-contiguous tile order
+        const bool ok = pos < valid;
+        const uint64_t kv = ok ? in[tile_base + pos] : 0ull;
+        const unsigned dg = ok ? (unsigned)((kv >> shift) & (kRadix - 1)) : (unsigned)kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+        const int leader = __ffs(peers) - 1;
+        uint32_t before = 0;
+        if (lane == leader) {
+            before = s_cnt[warp][dg];
+            s_cnt[warp][dg] = before + __popc(peers);
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        key[k] = kv;
+        rank[k] = before + __popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+    const int d = threadIdx.x;  // kSortThreads == kRadix: one digit per thread
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+        const uint32_t c = s_cnt[w][d];
+        s_cnt[w][d] = tot;
+        tot += c;
+    }
+    // publish this tile's counts, then look back one predecessor at a time until an inclusive
+    // count is met (tile 0 always publishes one), then publish this tile's inclusive count
+    unsigned long long* mine = status + (size_t)tile * kRadix + d;
+    const unsigned long long tag = (unsigned long long)epoch << 32;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        st_relaxed_u64(mine, kOsFlagPrefix | tag | tot);
+    } else {
+        st_relaxed_u64(mine, kOsFlagCount | tag | tot);
+        const unsigned long long* q = mine - kRadix;
+        uint32_t polls = 0;
+        for (int64_t j = (int64_t)tile - 1;;) {
+            const unsigned long long w = ld_relaxed_u64(q);
+            if ((w >> 62) == 0ull || (uint32_t)((w >> 32) & kOsMaxEpoch) != epoch) {
+                if (++polls > kOsPollLimit) {
+                    atomicAdd(err, 1u);
+                    s_failed = 1;
+                    break;
+                }
+                if (polls > 64) __nanosleep(64);
+                continue;
+            }
+            excl += (uint32_t)w;
+            if ((w >> 62) == 2ull) break;
+            if (--j < 0) {  // past tile 0 without an inclusive count: cannot happen, but never loops
+                atomicAdd(err, 1u);
+                s_failed = 1;
+                break;
+            }
+            q -= kRadix;
+        }
+        st_relaxed_u64(mine, kOsFlagPrefix | tag | (excl + tot));
+    }
+    uint32_t all;
+    const uint32_t start = block_exclusive_scan<uint32_t, kSortThreads>(tot, &all);
+    s_start[d] = start;
+    s_base[d] = dstart[d] + excl - start;  // global index of local slot i of digit d: s_base[d] + i
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        const int pos = warp * (32 * kSortItems) + k * 32 + lane;
+        if (pos < valid) {
+            const unsigned dg = (unsigned)((key[k] >> shift) & (kRadix - 1));
+            s_keys[s_start[dg] + s_cnt[warp][dg] + rank[k]] = key[k];
+        }
+    }
+    __syncthreads();
+    if (s_failed) return;  // this tile's positions are unknown: nothing is written
+    for (int i = threadIdx.x; i < valid; i += kSortThreads) {
+        const uint64_t kv = s_keys[i];
+        const unsigned dg = (unsigned)((kv >> shift) & (kRadix - 1));
+        const uint32_t at = s_base[dg] + (uint32_t)i;
+        if (at < (uint64_t)n) out[at] = kv;
+    }
+}
+
+// Status words a single-sweep sort of n keys uses.
+inline int64_t onesweep_status_words(int64_t n) { return radix_tiles(n) * kRadix; }
+
+// Same contract as radix_sort_u64, for n < 2^32 and at most kOsMaxPasses passes. `scratch`
+// holds kOsScratchWords u32; `status` onesweep_status_words(n) words, all of whose epochs are
+// below *epoch + 1 (zero-filled at allocation); *epoch advances by one per pass, and when it
+// would pass kOsMaxEpoch the whole status array (status_cap words) is cleared and it restarts.
+// *err counts look-back waits that gave up.
+inline uint64_t* onesweep_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int hi_bit, uint32_t* scratch,
+                                   unsigned long long* status, int64_t status_cap, uint32_t* epoch, unsigned int* err,
+                                   int sms, cudaStream_t stream, const char* hist_name, const char* pass_name) {
+    if (n <= 1 || hi_bit <= lo_bit) return keys;
+    const int passes = (hi_bit - lo_bit + kRadixBits - 1) / kRadixBits;
+    const int64_t ntiles = radix_tiles(n);
+    uint32_t* dstart = scratch;
+    uint32_t* counts = scratch + kOsStartWords;
+    unsigned int* tickets = counts + kOsMaxPasses * kRadix;
+    unsigned int* done = tickets + kOsMaxPasses;
+    cudaMemsetAsync(counts, 0, sizeof(uint32_t) * kOsClearWords, stream);
+    if (*epoch + (uint32_t)passes > kOsMaxEpoch) {
+        cudaMemsetAsync(status, 0, sizeof(unsigned long long) * status_cap, stream);
+        *epoch = 0;
+    }
+    const int64_t hist_blocks = std::min<int64_t>((n + kSortTile - 1) / kSortTile, (int64_t)sms * 8);
+    XTN_LAUNCH(hist_name, k_onesweep_hist<<<(unsigned)hist_blocks, kSortThreads, 0, stream>>>(keys, n, lo_bit, passes, dstart,
+                                                                                           counts, done));
+    uint64_t* src = keys;
+    uint64_t* dst = alt;
+    for (int p = 0; p < passes; p++) {
+        *epoch += 1;
+        XTN_LAUNCH(pass_name, k_onesweep_pass<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(
+                                  src, dst, n, lo_bit + kRadixBits * p, dstart + p * kRadix, status, *epoch,
+                                  tickets + p, err));
         uint64_t* t = src;
         src = dst;
         dst = t;
