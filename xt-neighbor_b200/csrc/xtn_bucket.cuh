@@ -622,6 +622,7 @@ struct GroupSmem {
     uint32_t cnt[kDigits];     // digit counts -> digit ends
     uint32_t warp_sums[kGroupThreads / 32 + 1];
     uint32_t wait_failed;
+    uint32_t n_cand;
     unsigned long long base;
     unsigned long long mbar;
 };
@@ -633,11 +634,12 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 // Groups one bucket. Records of equal hash (record >> idbits) form a run; every pair of
 // positions in a run is written as (min id << idbits) | max id.
 //   1. a two-bitmap filter over kBitmapBits hash bits keeps only records that can have a
-//      partner (every record of a run of >= 2 survives; ~1 in 20 singletons does too);
+//      partner (every record of a run of >= 2 survives; ~1 in 20 singletons does too); the
+//      survivors are collected in any order, one shared atomic per warp;
 //   2. the survivors are counting-sorted by kDigitBits further hash bits;
 //   3. each survivor checks its digit: it heads a run when no earlier survivor of the digit
-//      has its hash, and the run's size is the number with that hash (two passes: count,
-//      then write at block-scanned offsets);
+//      has its hash, and the run's size is the number with that hash (found once, kept per
+//      slot, then written at block-scanned offsets);
 //   4. the CTA reserves its output range with one atomic on `cursor` and spreads the pairs
 //      over its threads. Entries at or past `cap` are counted but not written, so the caller
 //      can grow the buffer to the exact size and run again.
@@ -717,19 +719,26 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         const uint32_t bit = 1u << (b & 31);
         if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
     }
+    if (threadIdx.x == 0) S.n_cand = 0;
     __syncthreads();
-    uint32_t my_c = 0;
-    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
-        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
-        my_c += (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
-    }
-    uint32_t m;
-    uint32_t c_off = block_scan_ex<uint32_t, kGroupThreads>(my_c, &m, S.warp_sums);
-    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
-        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
-        if ((S.u.bm.twice[b >> 5] >> (b & 31)) & 1u) S.cand[c_off++] = (uint16_t)i;
+    // candidates in any order (one shared atomic per warp and round)
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t i0 = threadIdx.x & ~31u; i0 < n; i0 += kGroupThreads) {
+        const uint32_t i = i0 + lane;
+        bool hit = false;
+        if (i < n) {
+            const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+            hit = (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, hit);
+        if (mask == 0u) continue;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&S.n_cand, (uint32_t)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (hit) S.cand[base + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)i;
     }
     __syncthreads();  // the bitmaps are dead from here on
+    const uint32_t m = S.n_cand;
 
     // 2. counting sort of the candidates by kDigitBits hash bits above the bitmap bits
     for (uint32_t c = threadIdx.x; c < m; c += kGroupThreads)
@@ -772,13 +781,18 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         contiguous = (sz == b - a) ? 1u : 0u;
         return sz >= 2;
     };
+    // each slot's run word (contiguous << 15 | size for a run head, 0 otherwise) is kept in
+    // `cand`, which the counting sort no longer needs, for the second pass
     uint32_t my_runs = 0, my_pairs = 0;
     for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {
         uint32_t sz, ct;
+        uint16_t word = 0;
         if (scan_pos(i, sz, ct)) {
             my_runs++;
             my_pairs += sz * (sz - 1) / 2;
+            word = (uint16_t)((ct << 15) | sz);  // size <= kGroupCap < 2^15
         }
+        S.cand[i] = word;
     }
     uint32_t nr, total;
     uint32_t run_off = block_scan_ex<uint32_t, kGroupThreads>(my_runs, &nr, S.warp_sums);
@@ -787,9 +801,10 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         if (threadIdx.x == 0) overflow[atomicAdd(n_overflow, 1u)] = bd;
         return;
     }
-    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {
-        uint32_t sz, ct;
-        if (scan_pos(i, sz, ct)) {
+    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {  // the same slots as above
+        const uint32_t word = S.cand[i];
+        if (word) {
+            const uint32_t sz = word & 0x7fffu, ct = word >> 15;
             S.u.gr.runs[run_off] = (ct << 31) | (sz << 16) | i;  // head slot < 2^13, size < 2^15
             S.u.gr.poff[run_off] = pair_off;
             run_off++;
