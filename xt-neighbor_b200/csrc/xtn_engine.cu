@@ -227,26 +227,59 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
     return dv;
 }
 
-__global__ void k_verify(const uint64_t* __restrict__ pairs, int64_t P, int idbits, const uint8_t* __restrict__ chars,
-                         const uint32_t* __restrict__ offs, const int32_t* __restrict__ rows, int d, int measure,
-                         int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    uint64_t p = pairs[i];
-    bool keep = false;
-    int dv = 0;
-    if (i == 0 || pairs[i - 1] != p) {
-        const uint64_t idmask = (1ull << idbits) - 1ull;
-        uint32_t x = (uint32_t)(p >> idbits), y = (uint32_t)(p & idmask);
-        if (x != y) {
-            int rx = rows ? rows[x] : (int)x, ry = rows ? rows[y] : (int)y;
-            uint32_t sa = offs[rx], sb = offs[ry];
-            dv = pair_distance(chars + sa, (int)(offs[rx + 1] - sa), chars + sb, (int)(offs[ry + 1] - sb), d, measure,
-                               &keep);
+// Verification of the sorted candidate pairs. Only the first of each run of equal pairs, with
+// x != y, is verified; the others get distance 0 and are not kept. Most candidates are repeats
+// (a close pair shares many deletion variants), so each warp takes kVerifyPer * 32 consecutive
+// candidates, lists the ones to verify in shared memory and spreads them over its lanes.
+constexpr int kVerifyPer = 4;
+constexpr int kVerifyWarps = kThreads / 32;
+
+__global__ void __launch_bounds__(kThreads) k_verify(const uint64_t* __restrict__ pairs, int64_t P, int idbits,
+                                                     const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
+                                                     const int32_t* __restrict__ rows, int d, int measure,
+                                                     int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
+    __shared__ uint64_t s_pair[kVerifyWarps][32 * kVerifyPer];
+    __shared__ uint8_t s_slot[kVerifyWarps][32 * kVerifyPer];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = ((int64_t)blockIdx.x * kVerifyWarps + warp) * (32 * kVerifyPer);
+    if (base >= P) return;  // whole warp
+    const uint64_t idmask = (1ull << idbits) - 1ull;
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t carry = base > 0 ? pairs[base - 1] : 0ull;  // the candidate before each row's lane 0
+    uint32_t n_work = 0;
+#pragma unroll
+    for (int k = 0; k < kVerifyPer; k++) {
+        const int64_t i = base + k * 32 + lane;
+        const bool in = i < P;
+        const uint64_t p = in ? pairs[i] : 0ull;
+        uint64_t prev = __shfl_up_sync(0xffffffffu, p, 1);
+        if (lane == 0) prev = carry;
+        carry = __shfl_sync(0xffffffffu, p, 31);
+        const bool need = in && (i == 0 || prev != p) && (p >> idbits) != (p & idmask);
+        const unsigned mask = __ballot_sync(0xffffffffu, need);
+        if (need) {
+            const uint32_t w = n_work + __popc(mask & lt);
+            s_pair[warp][w] = p;
+            s_slot[warp][w] = (uint8_t)(k * 32 + lane);
+        } else if (in) {
+            dist[i] = 0;
+            flag[i] = 0;
         }
+        n_work += __popc(mask);
     }
-    dist[i] = (int8_t)dv;
-    flag[i] = keep ? 1 : 0;
+    __syncwarp();
+    for (uint32_t w = lane; w < n_work; w += 32) {
+        const uint64_t p = s_pair[warp][w];
+        const int64_t i = base + s_slot[warp][w];
+        const uint32_t x = (uint32_t)(p >> idbits), y = (uint32_t)(p & idmask);
+        const int rx = rows ? rows[x] : (int)x, ry = rows ? rows[y] : (int)y;
+        const uint32_t sa = offs[rx], sb = offs[ry];
+        bool keep = false;
+        const int dv = pair_distance(chars + sa, (int)(offs[rx + 1] - sa), chars + sb, (int)(offs[ry + 1] - sb), d,
+                                     measure, &keep);
+        dist[i] = (int8_t)dv;
+        flag[i] = keep ? 1 : 0;
+    }
 }
 
 __global__ void k_compact(const uint64_t* __restrict__ pairs, int64_t P, int idbits, const int8_t* __restrict__ dist,
@@ -771,7 +804,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Pc + 1)));
     uint64_t nout = 0;
     if (Pc > 0) {
-        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
+        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
                                                               P<int8_t>(c->dist), P<uint8_t>(c->flag)));
         XTN_CK(cudaGetLastError());
         XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * scan_scratch_elems((int64_t)Pc)));
@@ -1645,7 +1678,7 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
         uint64_t* pairs = Pc > 1 ? radix_sort_u64(pairA, pairB, (int64_t)Pc, 0, 2 * idbits, pscratch, s,
                                                   "pair_sort_upsweep", "pair_sort_downsweep")
                                  : pairA;
-        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars,
+        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars,
                                                                                     offs, nullptr, d, measure, dist, flag));
         scan_exclusive<uint8_t, uint32_t>(flag, fpos, (int64_t)Pc, pscratch, s);
         XTN_TRY(read_u64(fpos + Pc, 4, s, &nout));
