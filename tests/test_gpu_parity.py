@@ -95,6 +95,20 @@ def test_every_sequence_twice(ctx):
     assert (got.distances == 0).sum() >= 40_000 and (got.distances == 1).sum() > 1000
 
 
+def test_invalid_offsets_rejected(ctx):
+    """A sequence of 0 or more than 500 residues is rejected with its index, and the context
+    stays usable."""
+    chars, offs = csr(["CASSLF", "CASS", "CASSLG"])
+    bad = offs.copy()
+    bad[2] = bad[1]  # sequence 1 empty
+    with pytest.raises(xtn.XtnError, match="sequence 1 has an invalid length"):
+        ctx.perform(chars, bad, distance=1)
+    lc, lo = csr(["CASSLF", "A" * 501])
+    with pytest.raises(xtn.XtnError, match="sequence 1 has an invalid length"):
+        ctx.perform(lc, lo, distance=1)
+    check_nn(ctx, chars, offs, 1, 0, "after rejected inputs")
+
+
 def test_short_sequences_large_d(ctx):
     """d >= L: the empty variant is shared by every short sequence."""
     rng = np.random.default_rng(1)

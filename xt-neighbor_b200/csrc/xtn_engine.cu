@@ -861,7 +861,13 @@ static int check_args(const xtn_args* a) {
     return XTN_SUCCESS;
 }
 
+// Every sequence must have 1..kMaxInputLength residues. The scan has no early exit so that the
+// compiler vectorises it; the first bad index is searched for only when one exists.
 static int check_offsets(const uint32_t* offs, int n) {
+    uint32_t bad = 0;
+    for (int i = 0; i < n; i++)
+        bad |= (uint32_t)(offs[i + 1] <= offs[i]) | (uint32_t)(offs[i + 1] - offs[i] > (uint32_t)kMaxInputLength);
+    if (!bad) return XTN_SUCCESS;
     for (int i = 0; i < n; i++) {
         if (offs[i + 1] <= offs[i] || offs[i + 1] - offs[i] > (uint32_t)kMaxInputLength) {
             set_err("sequence " + std::to_string(i) + " has an invalid length");
@@ -1366,9 +1372,17 @@ int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, 
         return XTN_ERR_ARG;
     }
     XTN_TRY(check_args(args));
-    XTN_TRY(check_offsets(offsets, n));
+    // the total bounds the upload; the per-sequence check then runs while the copies are in flight
+    if ((uint64_t)offsets[n] > (uint64_t)n * kMaxInputLength + offsets[0]) {
+        set_err("the offsets describe more residues than n_seqs sequences can hold");
+        return XTN_ERR_ARG;
+    }
     XTN_CK(cudaSetDevice(c->device));
     XTN_TRY(upload(c, seqs, offsets, n));
+    if (check_offsets(offsets, n) != XTN_SUCCESS) {
+        cudaStreamSynchronize(c->stream);  // the copies read the caller's buffers
+        return XTN_ERR_ARG;
+    }
     const uint8_t* dch = P<uint8_t>(c->chars);
     const uint32_t* dof = P<uint32_t>(c->offs);
     int r;

@@ -130,24 +130,55 @@ __global__ void k_query_emit(const uint32_t* __restrict__ qrow, int64_t Vq, cons
     for (uint32_t k = s; k < e; k++) pairs[o++] = ((recs[k] & idmask) << qbits) | q;
 }
 
-// Unique (index row, query row) pairs, verified on the full strings of the two stores.
-__global__ void k_query_verify(const uint64_t* __restrict__ pairs, int64_t P, int qbits,
-                               const uint8_t* __restrict__ ichars, const uint32_t* __restrict__ ioffs,
-                               const uint8_t* __restrict__ qchars, const uint32_t* __restrict__ qoffs, int d,
-                               int measure, int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    const uint64_t p = pairs[i];
-    bool keep = false;
-    int dv = 0;
-    if (i == 0 || pairs[i - 1] != p) {
+// Unique (index row, query row) pairs, verified on the full strings of the two stores. As in
+// k_verify, each warp lists the first of each run of equal pairs among its kVerifyPer * 32
+// candidates and spreads them over its lanes; repeats get distance 0 and are not kept.
+__global__ void __launch_bounds__(kThreads) k_query_verify(const uint64_t* __restrict__ pairs, int64_t P, int qbits,
+                                                           const uint8_t* __restrict__ ichars,
+                                                           const uint32_t* __restrict__ ioffs,
+                                                           const uint8_t* __restrict__ qchars,
+                                                           const uint32_t* __restrict__ qoffs, int d, int measure,
+                                                           int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
+    __shared__ uint64_t s_pair[kVerifyWarps][32 * kVerifyPer];
+    __shared__ uint8_t s_slot[kVerifyWarps][32 * kVerifyPer];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = ((int64_t)blockIdx.x * kVerifyWarps + warp) * (32 * kVerifyPer);
+    if (base >= P) return;  // whole warp
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t carry = base > 0 ? pairs[base - 1] : 0ull;
+    uint32_t n_work = 0;
+#pragma unroll
+    for (int k = 0; k < kVerifyPer; k++) {
+        const int64_t i = base + k * 32 + lane;
+        const bool in = i < P;
+        const uint64_t p = in ? pairs[i] : 0ull;
+        uint64_t prev = __shfl_up_sync(0xffffffffu, p, 1);
+        if (lane == 0) prev = carry;
+        carry = __shfl_sync(0xffffffffu, p, 31);
+        const bool need = in && (i == 0 || prev != p);
+        const unsigned mask = __ballot_sync(0xffffffffu, need);
+        if (need) {
+            const uint32_t w = n_work + __popc(mask & lt);
+            s_pair[warp][w] = p;
+            s_slot[warp][w] = (uint8_t)(k * 32 + lane);
+        } else if (in) {
+            dist[i] = 0;
+            flag[i] = 0;
+        }
+        n_work += __popc(mask);
+    }
+    __syncwarp();
+    for (uint32_t w = lane; w < n_work; w += 32) {
+        const uint64_t p = s_pair[warp][w];
+        const int64_t i = base + s_slot[warp][w];
         const uint32_t x = (uint32_t)(p >> qbits), y = (uint32_t)(p & ((1ull << qbits) - 1ull));
         const uint32_t sa = ioffs[x], sb = qoffs[y];
-        dv = pair_distance(ichars + sa, (int)(ioffs[x + 1] - sa), qchars + sb, (int)(qoffs[y + 1] - sb), d, measure,
-                           &keep);
+        bool keep = false;
+        const int dv = pair_distance(ichars + sa, (int)(ioffs[x + 1] - sa), qchars + sb, (int)(qoffs[y + 1] - sb), d,
+                                     measure, &keep);
+        dist[i] = (int8_t)dv;
+        flag[i] = keep ? 1 : 0;
     }
-    dist[i] = (int8_t)dv;
-    flag[i] = keep ? 1 : 0;
 }
 
 __global__ void k_query_compact(const uint64_t* __restrict__ pairs, int64_t P, int qbits, int n_index,
@@ -302,7 +333,7 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
         XTN_TRY(ensure(c->flag, Pc));
         XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Pc + 1)));
         XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * scan_scratch_elems((int64_t)Pc)));
-        XTN_LAUNCH("query_verify", k_query_verify<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
+        XTN_LAUNCH("query_verify", k_query_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(
                                        pairs, (int64_t)Pc, qbits, P<uint8_t>(ix->chars), P<uint32_t>(ix->offs), qchars,
                                        qoffs, d, measure, P<int8_t>(c->dist), P<uint8_t>(c->flag)));
         scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc,

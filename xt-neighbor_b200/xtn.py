@@ -290,12 +290,16 @@ class Context:
             None,
         )
         _check(rc)
-        pairs = np.concatenate(chunks_p) if chunks_p else np.zeros((0, 2), np.int32)
+
+        def joined(chunks, empty):
+            if not chunks:
+                return empty
+            return chunks[0] if len(chunks) == 1 else np.concatenate(chunks)
+
+        pairs = joined(chunks_p, np.zeros((0, 2), np.int32))
         if overlap:
-            vals = np.concatenate(chunks_v) if chunks_v else np.zeros(0, np.uint64)
-            return Result(pairs, None, vals)
-        vals = np.concatenate(chunks_v) if chunks_v else np.zeros(0, np.int8)
-        return Result(pairs, vals, None)
+            return Result(pairs, None, joined(chunks_v, np.zeros(0, np.uint64)))
+        return Result(pairs, joined(chunks_v, np.zeros(0, np.int8)), None)
 
     def nn_device(self, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN) -> int:
         """Search on device pointers; returns the number of output pairs (kept on device)."""
