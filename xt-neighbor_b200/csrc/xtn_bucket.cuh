@@ -475,6 +475,7 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
+    if (blockIdx.x / kSlices >= counters[1]) return;  // no such job (the whole cluster leaves)
     const SplitJob job = jobs[blockIdx.x / kSlices];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;

@@ -660,13 +660,11 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
-    XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
-    XTN_CK(cudaStreamSynchronize(s));
-    memcpy(cnt, c->h_scalar, 32);
-    if (cnt[1] > 0) {
-        // one CTA per bucket, or a cluster of kSplitSlices CTAs per bucket
+    {
+        // one CTA per bucket, or a cluster of kSplitSlices CTAs per bucket, launched for every
+        // bucket without waiting for the plan: those past the plan's job count exit at once
         const bool sliced = c->split_slices > 1;
-        const unsigned grid = cnt[1] * (sliced ? kSplitSlices : 1);
+        const unsigned grid = (unsigned)nb * (sliced ? kSplitSlices : 1);
 #define XTN_SPLIT(CFG, SL)                                                                                         \
     XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
                                    P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
@@ -699,8 +697,10 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     for (int attempt = 0; attempt < 2; attempt++) {
         XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * cap + 64));
         XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
-        XTN_CK(cudaMemsetAsync(P<unsigned int>(c->bcnt) + 3, 0, 4, s));
-        XTN_CK(cudaMemcpyAsync(P<unsigned int>(c->bcnt) + 3, &nfall_split, 4, cudaMemcpyHostToDevice, s));
+        if (attempt > 0) {  // the overflow list restarts after the split's fallback buckets
+            c->h_scalar[5] = nfall_split;
+            XTN_CK(cudaMemcpyAsync(P<unsigned int>(c->bcnt) + 3, c->h_scalar + 5, 4, cudaMemcpyHostToDevice, s));
+        }
         if (ndesc > 0)
             XTN_LAUNCH("bucket_group", k_bucket_group<<<ndesc, kGroupThreads, sizeof(GroupSmem), s>>>(
                                            P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
@@ -811,20 +811,23 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc,
                                           P<uint32_t>(c->scratch32), s);
         XTN_CK(cudaEventRecord(c->ev[7], s));
-        XTN_TRY(read_scalar(c, P<uint32_t>(c->fpos) + Pc, 4, &nout));
-    } else {
-        XTN_CK(cudaEventRecord(c->ev[7], s));
-    }
-    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * nout));
-    XTN_TRY(ensure(c->out_dist, (size_t)nout));
-    if (nout > 0)
+        // the output arrays hold every candidate, so the verified count (fpos[Pc]) is only read
+        // with the final synchronisation
+        XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * Pc));
+        XTN_TRY(ensure(c->out_dist, (size_t)Pc));
         XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, P<int8_t>(c->dist),
                                                                P<uint8_t>(c->flag), P<uint32_t>(c->fpos),
                                                                P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist)));
+        c->h_scalar[6] = 0;
+        XTN_CK(cudaMemcpyAsync(c->h_scalar + 6, P<uint32_t>(c->fpos) + Pc, 4, cudaMemcpyDeviceToHost, s));
+    } else {
+        XTN_CK(cudaEventRecord(c->ev[7], s));
+    }
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[8], s));
     if (c->dev_err.p) XTN_CK(cudaMemcpyAsync(c->h_scalar + 7, c->dev_err.p, 8, cudaMemcpyDeviceToHost, s));
     XTN_CK(cudaStreamSynchronize(s));
+    if (Pc > 0) nout = c->h_scalar[6];
     if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
         XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
         set_err("radix sort: " + std::to_string((uint32_t)c->h_scalar[7]) +
