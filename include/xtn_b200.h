@@ -170,7 +170,10 @@ int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double*
  *   "onesweep"        1 = radix sorts of up to 2^24 keys (candidate pairs, fallback buckets)
  *                     by single-sweep passes with decoupled look-back (default; larger sorts
  *                     keep the classic passes), 0 = classic passes for every sort (per-tile
- *                     counts, a scan, a scatter) */
+ *                     counts, a scan, a scatter)
+ *   "pair_dedup"      1 = candidate pairs go through a hash set in HBM before the pair sort, so
+ *                     only distinct pairs are sorted and verified (default; used from 2^15
+ *                     candidates and for n <= 2^24), 0 = every candidate is sorted */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length

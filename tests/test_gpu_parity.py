@@ -21,9 +21,9 @@ ENGINES = {
     "bucket_split_fallback": {"bucket_bits_max": 4, "group_cap": 64, "split_chunk": 2048},
     # buckets loaded into shared memory by plain loads instead of a TMA bulk copy; the larger
     # first-level stage shape; one CTA per split bucket instead of a cluster; classic radix
-    # sort passes instead of single-sweep ones
+    # sort passes instead of single-sweep ones; every candidate pair sorted (no hash set)
     "bucket_plain_loads": {"group_tma": 0, "scatter_ctas_per_sm": 1, "stage_chunk": 4096, "split_slices": 1,
-                           "onesweep": 0},
+                           "onesweep": 0, "pair_dedup": 0},
     # every variant key hashed directly (the d > 2 and no-allocation form) instead of from
     # per-sequence tables; direct first-level scatter
     "bucket_key_hash": {"key_tables": 0},

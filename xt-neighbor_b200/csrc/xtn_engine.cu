@@ -227,6 +227,71 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
     return dv;
 }
 
+// ------------------------------------------------------------------ candidate dedup
+// Most candidate pairs are repeats (a close pair shares many deletion variants). Before the
+// pair sort they go through a hash set in HBM (open addressing, linear probing, load <= 1/2):
+// the first insertion of a pair appends it to `uniq`; repeats and self pairs are dropped, so
+// only distinct pairs are sorted and verified. A slot holds tag | pair, the tag being the
+// search's epoch in the top kDedupTagBits bits; a slot with another epoch is free, so the table
+// is cleared only when allocated and when the epoch wraps. Pairs must fit in kDedupKeyBits
+// bits (2 * id_bits <= 48, n <= 2^24). Slot hash: the SplitMix64 finaliser (Steele, Lea and
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014).
+constexpr int kDedupKeyBits = 48;
+constexpr int kDedupTagBits = 64 - kDedupKeyBits;
+constexpr uint64_t kDedupTagMask = ~((1ull << kDedupKeyBits) - 1ull);
+constexpr int64_t kDedupMinPairs = int64_t(1) << 15;  // below this the plain sort is as fast
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restrict__ pairs, int64_t P, int idbits,
+                                                         unsigned long long* __restrict__ table, uint64_t tmask,
+                                                         uint64_t tag, uint64_t* __restrict__ uniq,
+                                                         unsigned long long* __restrict__ n_uniq,
+                                                         unsigned int* __restrict__ err) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31u;
+    bool fresh = false;
+    uint64_t p = 0;
+    if (i < P) {
+        p = pairs[i];
+        const uint64_t idmask = (1ull << idbits) - 1ull;
+        if ((p >> idbits) != (p & idmask)) {
+            const unsigned long long want = tag | p;
+            uint64_t h = mix64(p) & tmask;
+            unsigned long long v = ld_relaxed_u64(table + h);
+            for (uint64_t probes = 0;;) {
+                if ((v & kDedupTagMask) != tag) {  // free in this search
+                    const unsigned long long old = atomicCAS(table + h, v, want);
+                    if (old == v) {
+                        fresh = true;
+                        break;
+                    }
+                    v = old;  // taken meanwhile: it now holds a pair of this search
+                    continue;
+                }
+                if (v == want) break;  // a repeat
+                h = (h + 1) & tmask;
+                if (++probes > tmask) {  // cannot happen at load <= 1/2, but never loops
+                    atomicAdd(err, 1u);
+                    break;
+                }
+                v = ld_relaxed_u64(table + h);
+            }
+        }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, fresh);
+    if (mask == 0u) return;
+    unsigned long long base = 0;
+    const int leader = __ffs(mask) - 1;
+    if ((int)lane == leader) base = atomicAdd(n_uniq, (unsigned long long)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (fresh) uniq[base + __popc(mask & ((1u << lane) - 1u))] = p;
+}
+
 // Verification of the sorted candidate pairs. Only the first of each run of equal pairs, with
 // x != y, is verified; the others get distance 0 and are not kept. Most candidates are repeats
 // (a close pair shares many deletion variants), so each warp takes kVerifyPer * 32 consecutive
@@ -357,6 +422,9 @@ struct xtn_context {
     DevBuf scratch64, scratch32, counter;
     DevBuf os_scratch, os_status, dev_err;  // single-sweep sort scratch, status words, wait-error count
     uint32_t os_epoch = 0;
+    DevBuf dd_table;         // candidate-pair hash set (tag | pair per slot)
+    uint32_t dd_epoch = 0;
+    int pair_dedup = 1;      // distinct candidate pairs through the hash set before the pair sort
     DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab, tseq;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
@@ -743,6 +811,30 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     return XTN_SUCCESS;
 }
 
+// Distinct non-self candidate pairs of pairA[0..Pc) into pairB[0..*U), in no particular order.
+static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
+    cudaStream_t s = c->stream;
+    uint64_t T = 2;
+    while (T < 2 * Pc) T <<= 1;
+    if (c->dd_table.cap < sizeof(uint64_t) * T) {
+        XTN_TRY(ensure(c->dd_table, sizeof(uint64_t) * T));
+        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
+        c->dd_epoch = 0;
+    }
+    if (++c->dd_epoch >= (1u << kDedupTagBits)) {
+        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
+        c->dd_epoch = 1;
+    }
+    XTN_TRY(ensure_err_word(c));
+    XTN_CK(cudaMemsetAsync(c->counter.p, 0, 8, s));
+    XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
+                                 P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table), T - 1,
+                                 (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB),
+                                 P<unsigned long long>(c->counter), P<unsigned int>(c->dev_err)));
+    XTN_CK(cudaGetLastError());
+    return read_scalar(c, c->counter.p, 8, U);
+}
+
 // The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
 // -> CSR row. On success the result is in c->out_pairs / c->out_dist, c->n_out entries; the
 // verified pair list in sorted (x, y) order of search indexes.
@@ -794,8 +886,16 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc + 64));
     XTN_CK(cudaEventRecord(c->ev[5], s));
     uint64_t* pairs = P<uint64_t>(c->pairA);
-    if (Pc > 1)
+    if (c->pair_dedup && (int64_t)Pc >= kDedupMinPairs && 2 * idbits <= kDedupKeyBits) {
+        // from here on Pc counts the distinct pairs (in pairB), which alone are sorted and verified
+        XTN_TRY(dedup_pairs(c, Pc, idbits, &Pc));
+        st.n_unique = (int64_t)Pc;
+        pairs = P<uint64_t>(c->pairB);
+        if (Pc > 1)
+            XTN_TRY(sort_u64(c, c->pairB, c->pairA, (int64_t)Pc, 0, 2 * idbits, &pairs, XTN_SORT_NAMES("pair_sort")));
+    } else if (Pc > 1) {
         XTN_TRY(sort_u64(c, c->pairA, c->pairB, (int64_t)Pc, 0, 2 * idbits, &pairs, XTN_SORT_NAMES("pair_sort")));
+    }
     XTN_CK(cudaEventRecord(c->ev[6], s));
 
     // verify + compact
@@ -830,8 +930,8 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     if (Pc > 0) nout = c->h_scalar[6];
     if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
         XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
-        set_err("radix sort: " + std::to_string((uint32_t)c->h_scalar[7]) +
-                " look-back waits did not complete in time");
+        set_err(std::to_string((uint32_t)c->h_scalar[7]) +
+                " device-side waits or probes reached their bound (radix-sort look-back, pair hash set)");
         return XTN_ERR_CUDA;
     }
     c->n_out = (int64_t)nout;
@@ -1308,7 +1408,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err};
+                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1420,6 +1520,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 0 && v <= 4) c->scatter_ctas_per_sm = (int)v;
     else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
     else if (!strcmp(name, "onesweep") && (v == 0 || v == 1)) c->onesweep = (int)v;
+    else if (!strcmp(name, "pair_dedup") && (v == 0 || v == 1)) c->pair_dedup = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
