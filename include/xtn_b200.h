@@ -145,6 +145,10 @@ int xtn_context_stats(const xtn_context* ctx, xtn_stats* out);
  * distinct kernels (entries written: at most cap). */
 int xtn_context_set_profiling(xtn_context* ctx, int on);
 int xtn_context_kernel_times(const xtn_context* ctx, const char** names, double* ms, int64_t* launches, int cap);
+/* Restricts profiling to the launches of one kernel name (as xtn_context_kernel_times reports
+ * it), so that a timed run carries one pair of events per launch of that kernel only; NULL or
+ * "" brackets every launch again. */
+int xtn_context_profile_only(xtn_context* ctx, const char* name);
 
 /* Tuning and engine options of a context (0 on success, XTN_ERR_ARG for an unknown name or
  * a value out of range):

@@ -1624,6 +1624,12 @@ int xtn_context_set_profiling(xtn_context* c, int on) {
     return XTN_SUCCESS;
 }
 
+int xtn_context_profile_only(xtn_context* c, const char* name) {
+    if (!c) return XTN_ERR_ARG;
+    c->prof.only = name ? name : "";
+    return XTN_SUCCESS;
+}
+
 int xtn_context_kernel_times(const xtn_context* c, const char** names, double* ms, int64_t* launches, int cap) {
     if (!c) return -XTN_ERR_ARG;
     int n = (int)c->kt_names.size();

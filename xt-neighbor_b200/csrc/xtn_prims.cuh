@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 namespace xtn {
@@ -16,6 +17,8 @@ namespace xtn {
 // caller can read per-kernel device time after the run.
 struct KernelProfiler {
     bool on = false;
+    std::string only;  // when set, only launches of this kernel name are bracketed
+    bool skipping = false;
     int64_t launches = 0;
     struct Rec {
         const char* name;
@@ -31,7 +34,8 @@ struct KernelProfiler {
     }
     void begin(const char* name) {
         launches++;
-        if (!on) return;
+        skipping = !on || (!only.empty() && only != name);
+        if (skipping) return;
         if (used == recs.size()) {
             Rec r{name, nullptr, nullptr};
             cudaEventCreate(&r.a);
@@ -42,7 +46,7 @@ struct KernelProfiler {
         cudaEventRecord(recs[used].a, stream);
     }
     void end() {
-        if (!on) return;
+        if (skipping) return;
         cudaEventRecord(recs[used].b, stream);
         used++;
     }

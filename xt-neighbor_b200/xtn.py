@@ -49,6 +49,7 @@ SYMBOLS = (
     "xtn_context_autotune",
     "xtn_context_set_profiling",
     "xtn_context_kernel_times",
+    "xtn_context_profile_only",
     "xtn_last_error",
     "xtn_version",
 )
@@ -190,6 +191,7 @@ def load():
     lib.xtn_context_stream.restype = P
     lib.xtn_context_stats.argtypes = [P, ctypes.POINTER(Stats)]
     lib.xtn_context_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.xtn_context_profile_only.argtypes = [P, ctypes.c_char_p]
     lib.xtn_context_set_option.argtypes = [P, ctypes.c_char_p, ctypes.c_int64]
     lib.xtn_context_kernel_times.argtypes = [P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
@@ -358,8 +360,10 @@ class Context:
     def stream(self) -> int:
         return self.lib.xtn_context_stream(self.h) or 0
 
-    def set_profiling(self, on: bool):
+    def set_profiling(self, on: bool, only: str = None):
+        """Brackets kernel launches with CUDA events; `only` restricts that to one kernel name."""
         _check(self.lib.xtn_context_set_profiling(self.h, 1 if on else 0))
+        _check(self.lib.xtn_context_profile_only(self.h, only.encode() if only else None))
 
     def kernel_times(self) -> dict:
         """{kernel name: (total ms, launches)} of the last run (profiling on)."""
