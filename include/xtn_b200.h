@@ -177,7 +177,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     counts, a scan, a scatter)
  *   "pair_dedup"      1 = candidate pairs go through a hash set in HBM before the pair sort, so
  *                     only distinct pairs are sorted and verified (default; used from 2^15
- *                     candidates and for n <= 2^24), 0 = every candidate is sorted */
+ *                     candidates and for n <= 2^24), 0 = every candidate is sorted,
+ *                     2 = as 1 with the table always sized from the previous search's share
+ *                     of distinct pairs (the sizing used above 256 MiB of table) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length

@@ -95,6 +95,21 @@ def test_every_sequence_twice(ctx):
     assert (got.distances == 0).sum() >= 40_000 and (got.distances == 1).sum() > 1000
 
 
+def test_hash_set_regrows():
+    """Large candidate hash sets are sized from the previous search's share of distinct pairs
+    (pair_dedup=2 applies that sizing at any size). A search where every pair repeats ~100
+    times (400 copies of one sequence, d=2) leaves a share of about 1 %; the next search, with
+    far more distinct pairs than that table holds, must redo the pass with a larger one."""
+    ctx = xtn.Context(0, pair_dedup=2)
+    chars, offs = csr(["CASSLGQGAYEQYF"] * 400)
+    check_nn(ctx, chars, offs, 2, 0, "400 copies")
+    # ~180k distinct pairs: more than the 2^16-slot table the copies' share asks for
+    chars, offs = xtn.synth_clusters(seed=7, n=150_000, cluster_frac=0.2, dup_frac=0.02)
+    got = check_nn(ctx, chars, offs, 2, 0, "after the copies")
+    assert len(got.pairs) > 40_000
+    ctx.close()
+
+
 def test_invalid_offsets_rejected(ctx):
     """A sequence of 0 or more than 500 residues is rejected with its index, and the context
     stays usable."""

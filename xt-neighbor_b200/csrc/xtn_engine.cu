@@ -229,7 +229,7 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
 
 // ------------------------------------------------------------------ candidate dedup
 // Most candidate pairs are repeats (a close pair shares many deletion variants). Before the
-// pair sort they go through a hash set in HBM (open addressing, linear probing, load <= 1/2):
+// pair sort they go through a hash set in HBM (open addressing, linear probing):
 // the first insertion of a pair appends it to `uniq`; repeats and self pairs are dropped, so
 // only distinct pairs are sorted and verified. A slot holds tag | pair, the tag being the
 // search's epoch in the top kDedupTagBits bits; a slot with another epoch is free, so the table
@@ -240,6 +240,9 @@ constexpr int kDedupKeyBits = 48;
 constexpr int kDedupTagBits = 64 - kDedupKeyBits;
 constexpr uint64_t kDedupTagMask = ~((1ull << kDedupKeyBits) - 1ull);
 constexpr int64_t kDedupMinPairs = int64_t(1) << 15;  // below this the plain sort is as fast
+// An insertion that probes this many slots gives up and asks for a larger table (the table is
+// sized from the previous search's share of distinct pairs, which may not hold for this one).
+constexpr uint32_t kDedupMaxProbes = 256;
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
                                                          unsigned long long* __restrict__ table, uint64_t tmask,
                                                          uint64_t tag, uint64_t* __restrict__ uniq,
                                                          unsigned long long* __restrict__ n_uniq,
-                                                         unsigned int* __restrict__ err) {
+                                                         unsigned long long* __restrict__ n_full) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned lane = threadIdx.x & 31u;
     bool fresh = false;
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
             const unsigned long long want = tag | p;
             uint64_t h = mix64(p) & tmask;
             unsigned long long v = ld_relaxed_u64(table + h);
-            for (uint64_t probes = 0;;) {
+            for (uint32_t probes = 0;;) {
                 if ((v & kDedupTagMask) != tag) {  // free in this search
                     const unsigned long long old = atomicCAS(table + h, v, want);
                     if (old == v) {
@@ -275,8 +278,8 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
                 }
                 if (v == want) break;  // a repeat
                 h = (h + 1) & tmask;
-                if (++probes > tmask) {  // cannot happen at load <= 1/2, but never loops
-                    atomicAdd(err, 1u);
+                if (++probes > kDedupMaxProbes) {  // table too full: the host reruns with a larger one
+                    atomicAdd(n_full, 1ull);
                     break;
                 }
                 v = ld_relaxed_u64(table + h);
@@ -424,7 +427,8 @@ struct xtn_context {
     uint32_t os_epoch = 0;
     DevBuf dd_table;         // candidate-pair hash set (tag | pair per slot)
     uint32_t dd_epoch = 0;
-    int pair_dedup = 1;      // distinct candidate pairs through the hash set before the pair sort
+    double dd_share = 1.0;   // distinct share of the previous search's candidates (table sizing)
+    int pair_dedup = 1;      // candidate pairs through the hash set before the pair sort (2: table always sized by share)
     DevBuf bcounts, boffs, btotals, bstart, bdesc, bjobs, bfall, bcnt, fbA, fbB, runinfo, tcnt, toff, ktab, tseq;
     int sms = 148;
     int engine = 0;         // 0: hash buckets, 1: full radix sort of the records
@@ -812,27 +816,50 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
 }
 
 // Distinct non-self candidate pairs of pairA[0..Pc) into pairB[0..*U), in no particular order.
+// Table size: two slots per candidate while that is at most kDedupWideBytes. Above that, two
+// slots per expected distinct pair, the expectation being 1.25 x the previous search's distinct
+// share (all candidates for the first search). Measured on B200: 5.56M candidates (1.22M
+// distinct) take 0.12 ms with 2^24 slots and 0.17 ms with 2^22; 55M candidates take 2.3 ms with
+// 2^27 slots and 1.7 ms with 2^25. If an insertion runs past kDedupMaxProbes slots, the pass is
+// repeated with four times the slots under a new epoch.
+constexpr uint64_t kDedupWideBytes = uint64_t(256) << 20;
+
 static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
     cudaStream_t s = c->stream;
-    uint64_t T = 2;
-    while (T < 2 * Pc) T <<= 1;
-    if (c->dd_table.cap < sizeof(uint64_t) * T) {
-        XTN_TRY(ensure(c->dd_table, sizeof(uint64_t) * T));
-        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
-        c->dd_epoch = 0;
+    const double share = std::min(1.0, c->dd_share * 1.25);
+    uint64_t want = 2 * Pc;
+    if (sizeof(uint64_t) * want > kDedupWideBytes || c->pair_dedup == 2)
+        want = std::max<uint64_t>((uint64_t)(2.0 * share * (double)Pc),
+                                  c->pair_dedup == 2 ? (1u << 16) : kDedupWideBytes / sizeof(uint64_t));
+    for (int attempt = 0; attempt < 3; attempt++) {
+        uint64_t T = 2;
+        while (T < want) T <<= 1;
+        if (c->dd_table.cap < sizeof(uint64_t) * T) {
+            XTN_TRY(ensure(c->dd_table, sizeof(uint64_t) * T));
+            XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
+            c->dd_epoch = 0;
+        }
+        if (++c->dd_epoch >= (1u << kDedupTagBits)) {
+            XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
+            c->dd_epoch = 1;
+        }
+        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
+        XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
+                                     P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table),
+                                     T - 1, (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB),
+                                     P<unsigned long long>(c->counter), P<unsigned long long>(c->counter) + 1));
+        XTN_CK(cudaGetLastError());
+        XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        if (c->h_scalar[1] == 0) {
+            *U = c->h_scalar[0];
+            c->dd_share = Pc ? std::max(0.01, (double)*U / (double)Pc) : 1.0;
+            return XTN_SUCCESS;
+        }
+        want = std::max<uint64_t>(4 * T, 2 * Pc);  // too full: enough room for every candidate
     }
-    if (++c->dd_epoch >= (1u << kDedupTagBits)) {
-        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
-        c->dd_epoch = 1;
-    }
-    XTN_TRY(ensure_err_word(c));
-    XTN_CK(cudaMemsetAsync(c->counter.p, 0, 8, s));
-    XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
-                                 P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table), T - 1,
-                                 (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB),
-                                 P<unsigned long long>(c->counter), P<unsigned int>(c->dev_err)));
-    XTN_CK(cudaGetLastError());
-    return read_scalar(c, c->counter.p, 8, U);
+    set_err("candidate pair hash set: insertions did not find a free slot");
+    return XTN_ERR_CUDA;
 }
 
 // The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
@@ -930,8 +957,8 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     if (Pc > 0) nout = c->h_scalar[6];
     if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
         XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
-        set_err(std::to_string((uint32_t)c->h_scalar[7]) +
-                " device-side waits or probes reached their bound (radix-sort look-back, pair hash set)");
+        set_err("radix sort: " + std::to_string((uint32_t)c->h_scalar[7]) +
+                " look-back waits did not complete in time");
         return XTN_ERR_CUDA;
     }
     c->n_out = (int64_t)nout;
@@ -1520,7 +1547,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "scatter_ctas_per_sm") && v >= 0 && v <= 4) c->scatter_ctas_per_sm = (int)v;
     else if (!strcmp(name, "group_tma") && (v == 0 || v == 1)) c->group_tma = (int)v;
     else if (!strcmp(name, "onesweep") && (v == 0 || v == 1)) c->onesweep = (int)v;
-    else if (!strcmp(name, "pair_dedup") && (v == 0 || v == 1)) c->pair_dedup = (int)v;
+    else if (!strcmp(name, "pair_dedup") && v >= 0 && v <= 2) c->pair_dedup = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
