@@ -424,6 +424,7 @@ struct xtn_context {
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
     DevBuf os_scratch, os_status, dev_err;  // single-sweep sort scratch, status words, wait-error count
+    DevBuf scan_status;      // single-pass scan status words
     uint32_t os_epoch = 0;
     DevBuf dd_table;         // candidate-pair hash set (tag | pair per slot)
     uint32_t dd_epoch = 0;
@@ -498,16 +499,25 @@ static void end_run(xtn_context* c) {
     }
 }
 
-static int scan_u32_to_u64(xtn_context* c, const uint32_t* in, uint64_t* out, int64_t n) {
-    XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(n)));
-    scan_exclusive<uint32_t, uint64_t>(in, out, n, P<uint64_t>(c->scratch64), c->stream);
+static int ensure_err_word(xtn_context* c);
+
+// Single-pass scans (scan_exclusive_1p); their status words live in c->scan_status and a wait
+// that reaches its bound is counted in c->dev_err, which each entry point checks at its end.
+template <typename In, typename Out>
+static int scan_1p(xtn_context* c, const In* in, Out* out, int64_t n) {
+    XTN_TRY(ensure(c->scan_status, sizeof(unsigned long long) * scan_1p_words(n)));
+    XTN_TRY(ensure_err_word(c));
+    scan_exclusive_1p<In, Out>(in, out, n, P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err),
+                               c->stream);
     return XTN_SUCCESS;
 }
 
+static int scan_u32_to_u64(xtn_context* c, const uint32_t* in, uint64_t* out, int64_t n) {
+    return scan_1p<uint32_t, uint64_t>(c, in, out, n);
+}
+
 static int scan_u64(xtn_context* c, const uint64_t* in, uint64_t* out, int64_t n) {
-    XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(n)));
-    scan_exclusive<uint64_t, uint64_t>(in, out, n, P<uint64_t>(c->scratch64), c->stream);
-    return XTN_SUCCESS;
+    return scan_1p<uint64_t, uint64_t>(c, in, out, n);
 }
 
 // Kernel names of one sort (classic passes or single-sweep passes).
@@ -564,7 +574,7 @@ static int check_err_word(xtn_context* c) {
     XTN_TRY(read_scalar(c, c->dev_err.p, 4, &e));
     if (e != 0) {
         XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, c->stream));
-        set_err("radix sort: " + std::to_string(e) + " look-back waits did not complete in time");
+        set_err(std::to_string(e) + " look-back waits (radix sort or scan) did not complete in time");
         return XTN_ERR_CUDA;
     }
     return XTN_SUCCESS;
@@ -934,9 +944,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
                                                               P<int8_t>(c->dist), P<uint8_t>(c->flag)));
         XTN_CK(cudaGetLastError());
-        XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * scan_scratch_elems((int64_t)Pc)));
-        scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc,
-                                          P<uint32_t>(c->scratch32), s);
+        XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc)));
         XTN_CK(cudaEventRecord(c->ev[7], s));
         // the output arrays hold every candidate, so the verified count (fpos[Pc]) is only read
         // with the final synchronisation
@@ -957,8 +965,8 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     if (Pc > 0) nout = c->h_scalar[6];
     if (c->dev_err.p && (uint32_t)c->h_scalar[7] != 0) {
         XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
-        set_err("radix sort: " + std::to_string((uint32_t)c->h_scalar[7]) +
-                " look-back waits did not complete in time");
+        set_err(std::to_string((uint32_t)c->h_scalar[7]) +
+                " look-back waits (radix sort or scan) did not complete in time");
         return XTN_ERR_CUDA;
     }
     c->n_out = (int64_t)nout;
@@ -1435,7 +1443,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table};
+                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);

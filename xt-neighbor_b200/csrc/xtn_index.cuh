@@ -336,8 +336,7 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
         XTN_LAUNCH("query_verify", k_query_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(
                                        pairs, (int64_t)Pc, qbits, P<uint8_t>(ix->chars), P<uint32_t>(ix->offs), qchars,
                                        qoffs, d, measure, P<int8_t>(c->dist), P<uint8_t>(c->flag)));
-        scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc,
-                                          P<uint32_t>(c->scratch32), s);
+        XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc)));
         XTN_TRY(read_scalar(c, P<uint32_t>(c->fpos) + Pc, 4, &nout));
         XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * (nout + 1)));
         XTN_TRY(ensure(c->out_dist, nout + 1));

@@ -86,6 +86,17 @@ __device__ __forceinline__ T warp_inclusive_scan(T v) {
     return v;
 }
 
+// Relaxed loads and stores of status words that other CTAs poll (gpu scope, no L1 caching).
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Exclusive scan of one value per thread across the block; returns the block total in *total.
 template <typename T, int BLOCK>
 __device__ __forceinline__ T block_exclusive_scan(T v, T* total) {
@@ -183,6 +194,105 @@ void scan_exclusive(const In* in, Out* out, int64_t n, Out* scratch, cudaStream_
     XTN_LAUNCH("scan_reduce", (k_scan_reduce<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, sums, n)));
     scan_exclusive<Out, Out>(sums, offs, tiles, scratch + 2 * tiles + 1, stream);
     XTN_LAUNCH("scan_tiles", (k_scan_tiles<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, offs, n, true)));
+}
+
+// Single-pass exclusive scan (decoupled look-back, as in Merrill & Garland, "Single-pass
+// parallel prefix scan with decoupled look-back", 2016): a CTA takes the next tile in start order
+// (an atomic ticket), publishes its tile total in a status word, and warp 0 sums the totals of
+// earlier tiles 32 at a time, back to the nearest inclusive prefix, before publishing its own.
+// A tile waits only for tiles taken earlier by running CTAs, which publish before they look
+// back, so the waits end; each is still bounded (kScanPollLimit rounds), after which *err is
+// incremented and the tile continues with the sum it has (the host reports the error). One
+// launch instead of scan_exclusive's three or more; `status` holds scan_1p_words(n) words that
+// the call clears first. Status word: bits 62-63 flag (1: tile total, 2: inclusive prefix),
+// bits 0-61 the value.
+constexpr unsigned long long kScanFlagTotal = 1ull << 62;
+constexpr unsigned long long kScanFlagPrefix = 2ull << 62;
+constexpr unsigned long long kScanValueMask = (1ull << 62) - 1ull;
+constexpr uint32_t kScanPollLimit = 1u << 22;
+
+inline int64_t scan_1p_words(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+template <typename In, typename Out>
+__global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ in, Out* __restrict__ out, int64_t n,
+                                                        unsigned long long* __restrict__ status,
+                                                        unsigned int* __restrict__ err) {
+    __shared__ uint32_t s_tile;
+    __shared__ Out s_excl;
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(status);  // word 0; tiles from word 1
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    Out v[kScanItems];
+    Out sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const int64_t i = base + k;
+        v[k] = i < n ? (Out)in[i] : Out(0);
+        sum += v[k];
+    }
+    Out total;
+    const Out ex = block_exclusive_scan<Out, kScanBlock>(sum, &total);
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        unsigned long long* words = status + 1;
+        Out excl = 0;
+        if (tile == 0) {
+            if (lane == 0) st_relaxed_u64(words, kScanFlagPrefix | (unsigned long long)total);
+        } else {
+            if (lane == 0) st_relaxed_u64(words + tile, kScanFlagTotal | (unsigned long long)total);
+            uint32_t polls = 0;
+            for (int64_t j = (int64_t)tile - 1; j >= 0; j -= 32) {
+                const int64_t t = j - lane;  // lane 0 reads the nearest tile
+                unsigned long long w = t >= 0 ? ld_relaxed_u64(words + t) : kScanFlagPrefix;
+                while (__any_sync(0xffffffffu, (w >> 62) == 0ull) && ++polls <= kScanPollLimit) {
+                    if (polls > 64) __nanosleep(64);
+                    if ((w >> 62) == 0ull) w = ld_relaxed_u64(words + t);
+                }
+                if (polls > kScanPollLimit) {
+                    if (lane == 0) atomicAdd(err, 1u);
+                    break;
+                }
+                const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2ull);
+                const int stop = pm ? __ffs(pm) - 1 : 31;  // nearest inclusive prefix
+                Out part = lane <= stop ? (Out)(w & kScanValueMask) : Out(0);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+                excl += __shfl_sync(0xffffffffu, part, 0);
+                if (pm) break;
+            }
+            if (lane == 0) st_relaxed_u64(words + tile, kScanFlagPrefix | (unsigned long long)(excl + total));
+        }
+        if (lane == 0) s_excl = excl;
+    }
+    __syncthreads();
+    Out run = s_excl + ex;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (tile == gridDim.x - 1 && threadIdx.x == 0) out[n] = s_excl + total;
+}
+
+// Exclusive scan of n items into out[0..n), with out[n] = total, in one launch (plus the clear
+// of `status`). Asynchronous on `stream`.
+template <typename In, typename Out>
+void scan_exclusive_1p(const In* in, Out* out, int64_t n, unsigned long long* status, unsigned int* err,
+                       cudaStream_t stream) {
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, sizeof(Out), stream);
+        return;
+    }
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles == 1) {
+        XTN_LAUNCH("scan_tiles", (k_scan_tiles<In, Out><<<1, kScanBlock, 0, stream>>>(in, out, nullptr, n, true)));
+        return;
+    }
+    cudaMemsetAsync(status, 0, sizeof(unsigned long long) * scan_1p_words(n), stream);
+    XTN_LAUNCH("scan_1p", (k_scan_1p<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, n, status, err)));
 }
 
 // ------------------------------------------------------------------ LSD radix sort (u64 keys)
@@ -337,16 +447,6 @@ constexpr unsigned long long kOsFlagPrefix = 2ull << 62;
 constexpr int kOsStartWords = kOsMaxPasses * kRadix;
 constexpr int kOsClearWords = kOsMaxPasses * kRadix + kOsMaxPasses + 1;
 constexpr int kOsScratchWords = kOsStartWords + kOsClearWords;
-
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
 
 __global__ void __launch_bounds__(kSortThreads) k_onesweep_hist(const uint64_t* __restrict__ keys, int64_t n, int lo_bit,
                                                                 int passes, uint32_t* __restrict__ dstart,
