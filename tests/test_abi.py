@@ -68,3 +68,15 @@ def test_autotune_argument_errors_need_no_device():
     import ctypes
 
     assert lib.xtn_context_autotune(None, ctypes.byref(args), None, None, 0, 1, None, 0) == xtn.ERR_ARG
+
+
+def test_every_option_is_documented():
+    """The names xtn_context_set_option accepts are exactly the ones the header documents."""
+    src = open(os.path.join(ROOT, "xt-neighbor_b200", "csrc", "xtn_engine.cu")).read()
+    fn = src[src.index("int xtn_context_set_option(") :]
+    fn = fn[: fn.index("\n}\n")]
+    accepted = set(re.findall(r'strcmp\(name, "(\w+)"\)', fn))
+    hdr = open(HEADER).read()
+    block = hdr[hdr.index("Tuning and engine options") : hdr.index("int xtn_context_set_option")]
+    documented = set(re.findall(r'^ \*   "(\w+)"', block, flags=re.M))
+    assert accepted and accepted == documented
