@@ -130,3 +130,14 @@ int hc_share_variant(const char* a, int la, const char* b, int lb, int d) {
 
 uint64_t hc_tri_row_start(uint64_t i, uint64_t s) { return tri_row_start(i, s); }
 }
+
+extern "C" {
+
+// The candidate hash set's sizing rule (table slots after the power-of-two rounding).
+uint64_t hc_dedup_first_table(uint64_t Pc, double prev_share, int share_sizing) {
+    return pow2_at_least(dedup_first_slots(Pc, prev_share, share_sizing != 0));
+}
+
+uint64_t hc_dedup_regrow_table(uint64_t T, uint64_t Pc) { return pow2_at_least(dedup_regrow_slots(T, Pc)); }
+
+}  // extern "C"

@@ -167,3 +167,33 @@ def test_triangle_rows(hc):
         for i in range(s - 1):
             assert hc.hc_tri_row_start(i, s) == l
             l += s - 1 - i
+
+
+def test_hash_set_sizing(hc):
+    """The candidate hash set's table sizes (the rule the engine applies; the sizes measured
+    on B200 for the 1M and 10M workloads are the first two cases)."""
+    first = hc.hc_dedup_first_table
+    first.restype = ctypes.c_uint64
+    first.argtypes = [ctypes.c_uint64, ctypes.c_double, ctypes.c_int]
+    regrow = hc.hc_dedup_regrow_table
+    regrow.restype = ctypes.c_uint64
+    regrow.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+    # 1M: two slots per candidate fit in 256 MiB
+    assert first(5_557_204, 1.0, 0) == 1 << 24
+    assert first(5_557_204, 0.22, 0) == 1 << 24
+    # 10M: above 256 MiB the previous search's distinct share sizes it (first search: all)
+    assert first(55_000_000, 0.22, 0) == 1 << 25
+    assert first(55_000_000, 1.0, 0) == 1 << 27
+    # forced share sizing, with its 2^16-slot floor
+    assert first(1000, 0.01, 1) == 1 << 16
+    assert first(1_000_000, 0.5, 1) == 1 << 21
+    for pc in (2, 1000, 1 << 20, 3_000_000, 40_000_000):
+        for share in (0.01, 0.2, 0.8, 1.0):
+            for forced in (0, 1):
+                t = first(pc, share, forced)
+                assert t & (t - 1) == 0 and t >= 2
+                # at least two slots per expected distinct pair (1.25 x the share)
+                assert t >= min(2 * pc, 2 * min(1.0, 1.25 * share) * pc)
+    # a rerun gets four times the slots, and never fewer than two per candidate
+    assert regrow(1 << 16, 1_000_000) == 1 << 21
+    assert regrow(1 << 25, 1_000_000) == 1 << 27

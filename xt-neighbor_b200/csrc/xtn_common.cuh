@@ -415,6 +415,36 @@ XTN_HD void for_each_hash(const uint64_t* tab, int L, uint64_t info, int d, F&& 
 // Row i of a group of size s owns pairs (i, i+1..s-1); it starts at local index r(i).
 XTN_HD uint64_t tri_row_start(uint64_t i, uint64_t s) { return i * (2 * s - i - 1) / 2; }
 
+// ------------------------------------------------------------------ candidate hash set sizing
+// Slots (before rounding up to a power of two) for the candidate-pair hash set of Pc candidates:
+// two per candidate while that is at most kDedupWideBytes of table; above that, or when
+// share_sizing is set, two per expected distinct pair, the expectation being 1.25 x
+// prev_share (the previous search's distinct share; 1 for a first search) x Pc, with a floor
+// of kDedupWideBytes of table (2^16 slots under share_sizing). Measured on B200: 5.56M
+// candidates (1.22M distinct) take 0.12 ms with 2^24 slots and 0.17 ms with 2^22; 55M
+// candidates take 2.3 ms with 2^27 slots and 1.7 ms with 2^25.
+constexpr uint64_t kDedupWideBytes = uint64_t(256) << 20;
+
+inline uint64_t dedup_first_slots(uint64_t Pc, double prev_share, bool share_sizing) {
+    const double share = prev_share * 1.25 < 1.0 ? prev_share * 1.25 : 1.0;
+    uint64_t want = 2 * Pc;
+    if (sizeof(uint64_t) * want > kDedupWideBytes || share_sizing) {
+        const uint64_t floor = share_sizing ? (uint64_t(1) << 16) : kDedupWideBytes / sizeof(uint64_t);
+        const uint64_t by_share = (uint64_t)(2.0 * share * (double)Pc);
+        want = by_share > floor ? by_share : floor;
+    }
+    return want;
+}
+
+// Slots for the rerun after an insertion ran out of probes in a table of T slots.
+inline uint64_t dedup_regrow_slots(uint64_t T, uint64_t Pc) { return 4 * T > 2 * Pc ? 4 * T : 2 * Pc; }
+
+inline uint64_t pow2_at_least(uint64_t x) {
+    uint64_t t = 2;
+    while (t < x) t <<= 1;
+    return t;
+}
+
 // ------------------------------------------------------------------ distances
 // Levenshtein distance by Myers' bit-vector algorithm in Hyyro's global form
 // (G. Myers, J. ACM 46(3) 1999; H. Hyyro, 2001). `a` is the pattern (1 <= m <= 64).

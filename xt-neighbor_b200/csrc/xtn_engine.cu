@@ -826,24 +826,13 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
 }
 
 // Distinct non-self candidate pairs of pairA[0..Pc) into pairB[0..*U), in no particular order.
-// Table size: two slots per candidate while that is at most kDedupWideBytes. Above that, two
-// slots per expected distinct pair, the expectation being 1.25 x the previous search's distinct
-// share (all candidates for the first search). Measured on B200: 5.56M candidates (1.22M
-// distinct) take 0.12 ms with 2^24 slots and 0.17 ms with 2^22; 55M candidates take 2.3 ms with
-// 2^27 slots and 1.7 ms with 2^25. If an insertion runs past kDedupMaxProbes slots, the pass is
-// repeated with four times the slots under a new epoch.
-constexpr uint64_t kDedupWideBytes = uint64_t(256) << 20;
-
+// Table size: dedup_first_slots (xtn_common.cuh). If an insertion runs past kDedupMaxProbes
+// slots, the pass is repeated with dedup_regrow_slots under a new epoch.
 static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
     cudaStream_t s = c->stream;
-    const double share = std::min(1.0, c->dd_share * 1.25);
-    uint64_t want = 2 * Pc;
-    if (sizeof(uint64_t) * want > kDedupWideBytes || c->pair_dedup == 2)
-        want = std::max<uint64_t>((uint64_t)(2.0 * share * (double)Pc),
-                                  c->pair_dedup == 2 ? (1u << 16) : kDedupWideBytes / sizeof(uint64_t));
+    uint64_t want = dedup_first_slots(Pc, c->dd_share, c->pair_dedup == 2);
     for (int attempt = 0; attempt < 3; attempt++) {
-        uint64_t T = 2;
-        while (T < want) T <<= 1;
+        const uint64_t T = pow2_at_least(want);
         if (c->dd_table.cap < sizeof(uint64_t) * T) {
             XTN_TRY(ensure(c->dd_table, sizeof(uint64_t) * T));
             XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, s));
@@ -866,7 +855,7 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
             c->dd_share = Pc ? std::max(0.01, (double)*U / (double)Pc) : 1.0;
             return XTN_SUCCESS;
         }
-        want = std::max<uint64_t>(4 * T, 2 * Pc);  // too full: enough room for every candidate
+        want = dedup_regrow_slots(T, Pc);  // too full
     }
     set_err("candidate pair hash set: insertions did not find a free slot");
     return XTN_ERR_CUDA;
