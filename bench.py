@@ -184,8 +184,14 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
         return 8.0 * V + 25.0 * n
     if kernel == "find_groups":
         return 8.0 * V
+    U = st.get("n_unique") or Pc  # pairs sorted and verified (distinct ones after the hash set)
+    if kernel == "pair_dedup":
+        return 8.0 * Pc + 16.0 * U  # candidates read; each distinct pair written to its slot and the list
+    if kernel == "pair_sort_pass":
+        passes = -(-2 * st["id_bits"] // 8)
+        return 16.0 * U * passes  # each pass reads and writes every key
     if kernel == "verify":
-        return 10.0 * Pc + 2.0 * (n_chars / max(n, 1) + 8.0) * Pc
+        return 10.0 * U + 2.0 * (n_chars / max(n, 1) + 8.0) * U
     return None
 
 
