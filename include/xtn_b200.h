@@ -116,7 +116,10 @@ int xtn_context_perform(xtn_context* ctx, const xtn_args* args, const char* seqs
 
 /* Nearest-neighbour search on inputs already in device memory (d_seqs, d_offsets as in
  * xtn_perform). The result stays on the device; *n_out receives its length. Read it with
- * xtn_context_fetch or xtn_context_result_device. */
+ * xtn_context_fetch or xtn_context_result_device. The offsets are checked on the device
+ * before any kernel uses a length: a sequence outside 1..500 residues returns XTN_ERR_ARG
+ * (the same check as xtn_perform's; the device-resident overlap and index entry points below
+ * make it too). */
 int xtn_context_nn_device(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
                           int32_t n_seqs, int64_t* n_out);
 
@@ -179,7 +182,14 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     only distinct pairs are sorted and verified (default; used from 2^15
  *                     candidates and for n <= 2^24), 0 = every candidate is sorted,
  *                     2 = as 1 with the table always sized from the previous search's share
- *                     of distinct pairs (the sizing used above 256 MiB of table) */
+ *                     of distinct pairs (the sizing used above 256 MiB of table)
+ *   "wait_polls"      1..4194304: bound on the polls of one look-back wait in the single-pass
+ *                     prefix sums (default 4194304); a wait that reaches it makes the call
+ *                     return XTN_ERR_CUDA and the result is discarded
+ *   "wait_fault_test" 1 = the next search's variant-offset prefix sum leaves its first tile's
+ *                     status word unset, so the later tiles' bounded waits run out: the call
+ *                     returns XTN_ERR_CUDA and the context stays usable (a test of the error
+ *                     path; reset to 0 after that one search) */
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length
@@ -282,7 +292,12 @@ int xtn_index_serve(xtn_index* index, const xtn_request* requests, int32_t n_req
  *
  * Limits and behaviour:
  *   - Scratch comes from one fixed 32 MiB device array inside the library, held by every GPU
- *     that loads it until the process exits.
+ *     that loads it until the process exits. The array is reserved when the library's device
+ *     code is loaded on a device; with CUDA's lazy module loading that can be during this
+ *     function's first call there, so a caller that must not see any allocation on its call
+ *     path makes one warm-up call per device first.
+ *   - The caller's offsets are checked on the device (1..500 residues per sequence); a bad
+ *     length returns XTN_ERR_ARG naming the first bad sequence.
  *   - At most 4096 sequences. Inputs whose variants, groups or candidate pairs do not fit the
  *     array, or whose result exceeds out_cap, return XTN_ERR_LIMIT with a message. For an
  *     oversized result, *n_out holds the needed size.

@@ -428,9 +428,28 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* _
     }
 }
 
+// Counter words shared by the plan, split and grouping kernels (unsigned int counters[16]).
+constexpr int kCntDesc = 0;      // descriptors listed for grouping
+constexpr int kCntJobs = 1;      // split jobs
+constexpr int kCntSub = 2;       // sub-buckets the split jobs produce
+constexpr int kCntFallback = 3;  // buckets grouped by sorting instead
+constexpr int kCntWaitFail = 5;  // split CTAs whose chunk copy did not complete in time
+constexpr int kCntDropped = 6;   // appends refused because a list was full (must stay 0)
+
+// Appends v to list[0..cap) at counters[which]; an append past the capacity is counted in
+// counters[kCntDropped] instead (the host then reports an error: the capacities are bounds
+// that the plan's arithmetic guarantees, so this never happens with consistent inputs).
+template <class T>
+__device__ __forceinline__ void bounded_append(T* __restrict__ list, uint32_t cap, unsigned int* __restrict__ counters,
+                                               int which, const T& v) {
+    const unsigned k = atomicAdd(&counters[which], 1u);
+    if (k < cap) list[k] = v;
+    else atomicAdd(&counters[kCntDropped], 1u);
+}
+
 // Sorts buckets into "group directly" descriptors and split jobs.
 __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint32_t group_cap,
-                              BucketDesc* __restrict__ desc, SplitJob* __restrict__ jobs,
+                              BucketDesc* __restrict__ desc, uint32_t desc_cap, SplitJob* __restrict__ jobs,
                               unsigned int* __restrict__ counters) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
@@ -438,16 +457,14 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint3
     uint32_t size = (uint32_t)(e - s);
     if (size < 2) return;
     if (size <= group_cap) {
-        unsigned k = atomicAdd(&counters[0], 1u);
-        desc[k] = BucketDesc{s, size, 0};
+        bounded_append(desc, desc_cap, counters, kCntDesc, BucketDesc{s, size, 0});
     } else {
         // sub-buckets aim at 7/8 of the shared-memory capacity (hash buckets are near-uniform)
         const uint32_t target = group_cap * 7 / 8;
         uint32_t bits = 1;
         while (bits < kMaxSplitBits && ((uint64_t)size >> bits) > (uint64_t)(target > 1 ? target : 1)) bits++;
-        unsigned k = atomicAdd(&counters[1], 1u);
-        jobs[k] = SplitJob{s, size, bits};
-        atomicAdd(&counters[2], 1u << bits);
+        bounded_append(jobs, (uint32_t)nb, counters, kCntJobs, SplitJob{s, size, bits});
+        atomicAdd(&counters[kCntSub], 1u << bits);
     }
 }
 
@@ -468,14 +485,14 @@ template <class C, int kSlices>
 __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
     k_bucket_split_staged(const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in,
                           uint64_t* __restrict__ out, uint32_t group_cap, BucketDesc* __restrict__ desc,
-                          BucketDesc* __restrict__ fallback, unsigned int* __restrict__ counters) {
+                          BucketDesc* __restrict__ fallback, uint32_t desc_cap, unsigned int* __restrict__ counters) {
     constexpr int kStageThreads = C::kThreads, kStageChunk = C::kChunk, kFanPer = C::kFanPer;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
-    if (blockIdx.x / kSlices >= counters[1]) return;  // no such job (the whole cluster leaves)
+    if (blockIdx.x / kSlices >= min(counters[kCntJobs], (unsigned)(gridDim.x / kSlices))) return;  // no such job
     const SplitJob job = jobs[blockIdx.x / kSlices];
     const int nsub = 1 << job.bits;
     const int shift = 64 - (int)job.bits;
@@ -565,8 +582,8 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
             S.gcur[b] = (uint32_t)job.start + st + mine_b[k];
             if (rank == 0 && tot_b[k] >= 2) {
                 BucketDesc bd{job.start + st, tot_b[k], 1};
-                if (tot_b[k] <= group_cap) desc[atomicAdd(&counters[0], 1u)] = bd;
-                else fallback[atomicAdd(&counters[3], 1u)] = bd;
+                if (tot_b[k] <= group_cap) bounded_append(desc, desc_cap, counters, kCntDesc, bd);
+                else bounded_append(fallback, desc_cap, counters, kCntFallback, bd);
             }
         }
     }
@@ -592,7 +609,7 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
             if (threadIdx.x == 0) {
                 uint32_t polls = 0;
                 while (!mbar_try_wait(mbar, parity) && ++polls < kWaitLimit) __nanosleep(64);
-                atomicAdd(&counters[5], 1u);
+                atomicAdd(&counters[kCntWaitFail], 1u);
             }
             __syncthreads();
             return;
@@ -652,7 +669,8 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
                                                                      unsigned long long* __restrict__ cursor,
                                                                      unsigned int* __restrict__ errors, int use_tma,
                                                                      BucketDesc* __restrict__ overflow,
-                                                                     unsigned int* __restrict__ n_overflow) {
+                                                                     uint32_t overflow_cap,
+                                                                     unsigned int* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem& S = *reinterpret_cast<GroupSmem*>(smem_raw);
     const BucketDesc bd = descs[blockIdx.x];
@@ -799,7 +817,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     uint32_t run_off = block_scan_ex<uint32_t, kGroupThreads>(my_runs, &nr, S.warp_sums);
     uint32_t pair_off = block_scan_ex<uint32_t, kGroupThreads>(my_pairs, &total, S.warp_sums);
     if (nr > (uint32_t)kMaxRuns) {  // too many runs to list: the bucket is regrouped by sorting
-        if (threadIdx.x == 0) overflow[atomicAdd(n_overflow, 1u)] = bd;
+        if (threadIdx.x == 0) bounded_append(overflow, overflow_cap, counters, kCntFallback, bd);
         return;
     }
     for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {  // the same slots as above

@@ -75,8 +75,10 @@ __global__ void __launch_bounds__(kPackThreads) k_pack(const uint8_t* __restrict
     if (live) {
         int r = rows ? rows[i] : i;
         uint32_t s = offs[r];
-        int L = (int)(offs[r + 1] - s);
-        int Lk = L < kKeyLen ? L : kKeyLen;
+        // lengths are validated by k_check_lengths before the host uses anything computed
+        // here; the clamp keeps an invalid one from steering the loop below
+        const uint32_t L = offs[r + 1] - s;
+        int Lk = L < (uint32_t)kKeyLen ? (int)L : kKeyLen;
         // the key's two 64-bit words (key_words), built with 64-bit shifts
         uint64_t wa = 0, wb = 0;
         for (int j = 0; j < Lk; j++) {
@@ -99,6 +101,20 @@ __global__ void __launch_bounds__(kPackThreads) k_pack(const uint8_t* __restrict
     if (cnt <= 0) return;
     uint64_t* dst = tab + (size_t)i0 * kTabLen;
     for (int k = lane; k < cnt * kTabLen; k += 32) dst[k] = s_tab[w][(k / kTabLen) * kPackRow + k % kTabLen];
+}
+
+// Device-side check of caller-provided offsets (the device-resident entry points never see
+// them on the host): every sequence must have 1..kMaxInputLength residues, as check_offsets
+// requires on the host path. *first_bad (preset to 0xffffffff) receives the smallest bad
+// index. Kernels that index by length (the verification's DP column, in particular) run only
+// after the host has read this word.
+__global__ void k_check_lengths(const uint32_t* __restrict__ offs, const int32_t* __restrict__ rows, int n,
+                                unsigned int* __restrict__ first_bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = rows ? rows[i] : i;
+    const uint32_t a = offs[r], b = offs[r + 1];
+    if (b <= a || b - a > (uint32_t)kMaxInputLength) atomicMin(first_bad, (unsigned int)i);
 }
 
 // One thread per sequence writes its variant records at voff[i]; d <= 2 hashes come from
@@ -419,7 +435,7 @@ struct xtn_context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[S_COUNT + 1] = {};
     // inputs (host-buffer API)
-    DevBuf chars, offs, info;
+    DevBuf chars, offs, info, lencheck;
     // pipeline
     DevBuf keys, klen, vcnt, voff, recA, recB, gstart, gsize, gcnt, goff, pairA, pairB, dist, flag, fpos;
     DevBuf scratch64, scratch32, counter;
@@ -439,6 +455,8 @@ struct xtn_context {
     int scatter_ctas_per_sm = 0;  // 0: as many as the stage shape's shared memory allows
     int group_tma = 1;
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
+    uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
+    int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
     int split_chunk = 4096;  // the same for the split (2048 | 4096)
     int split_slices = kSplitSlices;  // CTAs (one cluster) per split bucket: 1 | kSplitSlices
@@ -467,6 +485,24 @@ static int read_scalar(xtn_context* c, const void* dptr, size_t bytes, uint64_t*
     XTN_CK(cudaStreamSynchronize(c->stream));
     *out = *c->h_scalar;
     return XTN_SUCCESS;
+}
+
+// Length check of device-resident offsets (k_check_lengths) into c->lencheck; the caller reads
+// the word with its next synchronisation and passes it to length_check_result.
+static int launch_length_check(xtn_context* c, const uint32_t* offs, const int32_t* rows, int n) {
+    XTN_TRY(ensure(c->lencheck, 16));
+    XTN_CK(cudaMemsetAsync(c->lencheck.p, 0xff, 4, c->stream));
+    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, c->stream>>>(
+                                    offs, rows, n, P<unsigned int>(c->lencheck)));
+    XTN_CK(cudaGetLastError());
+    return XTN_SUCCESS;
+}
+
+static int length_check_result(xtn_context* c, uint32_t first_bad) {
+    (void)c;
+    if (first_bad == 0xffffffffu) return XTN_SUCCESS;
+    set_err("sequence " + std::to_string(first_bad) + " has an invalid length");
+    return XTN_ERR_ARG;
 }
 
 static void begin_run(xtn_context* c) {
@@ -503,12 +539,14 @@ static int ensure_err_word(xtn_context* c);
 
 // Single-pass scans (scan_exclusive_1p); their status words live in c->scan_status and a wait
 // that reaches its bound is counted in c->dev_err, which each entry point checks at its end.
+// withhold_tile0: the fault test of the bounded waits (context option "wait_fault_test"); only
+// the variant-offset scan takes it, whose result the host checks before anything consumes it.
 template <typename In, typename Out>
-static int scan_1p(xtn_context* c, const In* in, Out* out, int64_t n) {
+static int scan_1p(xtn_context* c, const In* in, Out* out, int64_t n, int withhold_tile0 = 0) {
     XTN_TRY(ensure(c->scan_status, sizeof(unsigned long long) * scan_1p_words(n)));
     XTN_TRY(ensure_err_word(c));
     scan_exclusive_1p<In, Out>(in, out, n, P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err),
-                               c->stream);
+                               c->stream, c->wait_polls, withhold_tile0);
     return XTN_SUCCESS;
 }
 
@@ -706,7 +744,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
             XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
                                                                                        P<uint32_t>(c->tcnt)));
             XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
-            XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * V + 16));  // tasks <= variants
+            // a sequence has at most kKeyLen runs, so at most kKeyLen tasks
+            XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * std::min<uint64_t>(V, (uint64_t)kKeyLen * n) + 16));
             XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->toff), n,
                                                                                  P<uint32_t>(c->tseq)));
             tseq = P<uint32_t>(c->tseq);
@@ -739,7 +778,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
                                   P<uint64_t>(c->bstart), nb, c->group_cap, P<BucketDesc>(c->bdesc),
-                                  P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
+                                  (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
@@ -750,7 +789,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
 #define XTN_SPLIT(CFG, SL)                                                                                         \
     XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
                                    P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
-                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), P<unsigned int>(c->bcnt)))
+                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,        \
+                                   P<unsigned int>(c->bcnt)))
         if (c->split_chunk == 2048) {
             if (sliced) XTN_SPLIT(SplitSmall, kSplitSlices);
             else XTN_SPLIT(SplitSmall, 1);
@@ -763,8 +803,12 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
         memcpy(cnt, c->h_scalar, 32);
-        if (cnt[5] != 0) {
-            set_err("bucket split: " + std::to_string(cnt[5]) + " chunk copies did not complete in time");
+        if (cnt[kCntWaitFail] != 0) {
+            set_err("bucket split: " + std::to_string(cnt[kCntWaitFail]) + " chunk copies did not complete in time");
+            return XTN_ERR_CUDA;
+        }
+        if (cnt[kCntDropped] != 0) {
+            set_err("bucket plan: " + std::to_string(cnt[kCntDropped]) + " descriptors beyond the list capacity");
             return XTN_ERR_CUDA;
         }
     }
@@ -788,14 +832,18 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
                                            P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
                                            P<uint64_t>(c->pairA), cap, P<unsigned long long>(c->counter),
                                            P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
-                                           P<unsigned int>(c->bcnt) + 3));
+                                           (uint32_t)desc_cap, P<unsigned int>(c->bcnt)));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
-        XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 16, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
         total = c->h_scalar[0];
         if ((c->h_scalar[1] & 0xffffffffu) != 0) {
             set_err("bucket grouping: a shared-memory bulk copy did not complete in time");
+            return XTN_ERR_CUDA;
+        }
+        if ((uint32_t)c->h_scalar[5] != 0) {  // bcnt[kCntDropped]: low half of the fourth word
+            set_err("bucket grouping: overflow list capacity exceeded");
             return XTN_ERR_CUDA;
         }
         if (total <= cap) break;
@@ -865,7 +913,7 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
 // -> CSR row. On success the result is in c->out_pairs / c->out_dist, c->n_out entries; the
 // verified pair list in sorted (x, y) order of search indexes.
 static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n, int d,
-                  int measure) {
+                  int measure, bool validate) {
     xtn_stats& st = c->stats;
     memset(&st, 0, sizeof st);
     st.n_seqs = n;
@@ -874,6 +922,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     st.id_bits = idbits;
     cudaStream_t s = c->stream;
     XTN_CK(cudaEventRecord(c->ev[0], s));
+    if (validate) XTN_TRY(launch_length_check(c, offs, rows, n));
 
     // pack + variant counts
     XTN_TRY(ensure(c->keys, sizeof(u128) * n));
@@ -887,10 +936,21 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
                                              P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo),
                                              tables ? P<uint64_t>(c->ktab) : nullptr));
     XTN_CK(cudaGetLastError());
-    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n));
+    XTN_TRY((scan_1p<uint32_t, uint64_t>(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n, c->wait_fault_test)));
+    c->wait_fault_test = 0;
     XTN_CK(cudaEventRecord(c->ev[1], s));
     uint64_t V = 0;
+    if (validate) XTN_CK(cudaMemcpyAsync(c->h_scalar + 1, c->lencheck.p, 4, cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->dev_err.p, 4, cudaMemcpyDeviceToHost, s));
     XTN_TRY(read_scalar(c, P<uint64_t>(c->voff) + n, 8, &V));
+    if (validate) XTN_TRY(length_check_result(c, (uint32_t)c->h_scalar[1]));
+    if ((uint32_t)c->h_scalar[2] != 0) {  // a look-back wait gave up: the offsets are unusable
+        XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        set_err(std::to_string((uint32_t)c->h_scalar[2]) +
+                " look-back waits (radix sort or scan) did not complete in time");
+        return XTN_ERR_CUDA;
+    }
     st.n_variants = (int64_t)V;
     if (V >= (uint64_t)UINT32_MAX) {
         set_err("too many deletion variants for one round (" + std::to_string(V) + ")");
@@ -1280,7 +1340,7 @@ __global__ void k_split_info(const xtn_seq_info* __restrict__ info, int n, int R
 
 // Overlap mode on device-resident inputs (d_info: one xtn_seq_info per row, row order).
 int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* d_info, int n, int d,
-                int measure, int R) {
+                int measure, int R, bool validate) {
     if (R > kMaxRepertoires) {
         set_err("overlap mode supports at most " + std::to_string(kMaxRepertoires) + " repertoires");
         return XTN_ERR_LIMIT;
@@ -1293,11 +1353,14 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     XTN_TRY(ensure(c->counter, 64));
     const int int_max = 0x7fffffff;
     XTN_CK(cudaMemcpyAsync(c->counter.p, &int_max, sizeof(int), cudaMemcpyHostToDevice, s));
+    if (validate) XTN_TRY(launch_length_check(c, offs, nullptr, n));
     XTN_LAUNCH("split_info", k_split_info<<<blocks_for(n), kThreads, 0, s>>>(d_info, n, R, P<int32_t>(b.freq),
                                                                               P<int32_t>(b.rep), P<int>(c->counter)));
     XTN_CK(cudaGetLastError());
     uint64_t bad = 0;
+    if (validate) XTN_CK(cudaMemcpyAsync(c->h_scalar + 1, c->lencheck.p, 4, cudaMemcpyDeviceToHost, s));
     XTN_TRY(read_scalar(c, c->counter.p, 4, &bad));
+    if (validate) XTN_TRY(length_check_result(c, (uint32_t)c->h_scalar[1]));
     if ((int)bad != int_max) {
         set_err("repertoire id out of range at row " + std::to_string((int)bad));
         return XTN_ERR_ARG;
@@ -1345,7 +1408,7 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     XTN_CK(cudaGetLastError());
 
     // 3. neighbours among the unique strings
-    XTN_TRY(run_nn(c, chars, offs, P<int32_t>(b.rep_row), (int)U, d, measure));
+    XTN_TRY(run_nn(c, chars, offs, P<int32_t>(b.rep_row), (int)U, d, measure, false));
     const int64_t nverified = c->n_out;
 
     // 4. cross term
@@ -1424,6 +1487,7 @@ int xtn_context_create(int device, xtn_context** out) {
 
 void xtn_context_destroy(xtn_context* c) {
     if (!c) return;
+    if (current_profiler() == &c->prof) current_profiler() = nullptr;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->chars,   &c->offs,     &c->keys,      &c->klen,      &c->vcnt,     &c->voff,
@@ -1432,7 +1496,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
+                      &c->ktab,    &c->info,     &c->lencheck, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1466,7 +1530,8 @@ int xtn_context_nn_device(xtn_context* c, const xtn_args* args, const char* d_se
     XTN_TRY(check_args(args));
     XTN_CK(cudaSetDevice(c->device));
     begin_run(c);
-    int r = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance, args->measure);
+    int r = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance, args->measure,
+                   true);
     end_run(c);
     if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
     return r;
@@ -1486,7 +1551,7 @@ int xtn_context_overlap_device(xtn_context* c, const xtn_args* args, const char*
     XTN_CK(cudaSetDevice(c->device));
     begin_run(c);
     int r = run_overlap(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, d_info, n, args->distance, args->measure,
-                        args->info_len);
+                        args->info_len, true);
     end_run(c);
     if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
     return r;
@@ -1512,18 +1577,27 @@ int xtn_context_perform(xtn_context* c, const xtn_args* args, const char* seqs, 
     }
     const uint8_t* dch = P<uint8_t>(c->chars);
     const uint32_t* dof = P<uint32_t>(c->offs);
+    if (info && args->info_len < 1) {
+        set_err("invalid info length");
+        return XTN_ERR_ARG;
+    }
     int r;
-    begin_run(c);
+    begin_run(c);  // every path below reaches end_run
     if (info) {
-        if (args->info_len < 1) {
-            set_err("invalid info length");
-            return XTN_ERR_ARG;
+        r = ensure(c->info, sizeof(xtn_seq_info) * (size_t)n);
+        if (r == XTN_SUCCESS) {
+            const cudaError_t e = cudaMemcpyAsync(c->info.p, info, sizeof(xtn_seq_info) * (size_t)n,
+                                                  cudaMemcpyHostToDevice, c->stream);
+            if (e != cudaSuccess) {
+                set_err(std::string("copy of the sequence info failed: ") + cudaGetErrorString(e));
+                r = XTN_ERR_CUDA;
+            }
         }
-        XTN_TRY(ensure(c->info, sizeof(xtn_seq_info) * (size_t)n));
-        XTN_CK(cudaMemcpyAsync(c->info.p, info, sizeof(xtn_seq_info) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-        r = run_overlap(c, dch, dof, P<xtn_seq_info>(c->info), n, args->distance, args->measure, args->info_len);
+        if (r == XTN_SUCCESS)
+            r = run_overlap(c, dch, dof, P<xtn_seq_info>(c->info), n, args->distance, args->measure, args->info_len,
+                            false);
     } else {
-        r = run_nn(c, dch, dof, nullptr, n, args->distance, args->measure);
+        r = run_nn(c, dch, dof, nullptr, n, args->distance, args->measure, false);
     }
     end_run(c);
     if (r != XTN_SUCCESS) return r;
@@ -1549,6 +1623,8 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
     else if (!strcmp(name, "split_slices") && (v == 1 || v == kSplitSlices)) c->split_slices = (int)v;
+    else if (!strcmp(name, "wait_polls") && v >= 1 && v <= (int64_t)kScanPollLimit) c->wait_polls = (uint32_t)v;
+    else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
         return XTN_ERR_ARG;
@@ -1592,7 +1668,7 @@ int xtn_context_autotune(xtn_context* c, const xtn_args* args, const char* d_seq
         for (int r = 0; r <= repeats; r++) {  // the first run is a warm-up
             begin_run(c);
             int st = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance,
-                            args->measure);
+                            args->measure, true);
             end_run(c);
             if (st != XTN_SUCCESS) return st;
             float t = (float)c->stats.ms_total;
@@ -1775,14 +1851,25 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
     uint32_t* vcnt;
     uint64_t *voff, *runinfo, *scan64;
     unsigned long long* counter;
+    unsigned int* lenbad;
     if (!cv.take(&keys, n) || !cv.take(&klen, n) || !cv.take(&vcnt, n) || !cv.take(&voff, n + 1) ||
-        !cv.take(&runinfo, n) || !cv.take(&scan64, scan_scratch_elems(n)) || !cv.take(&counter, 2))
+        !cv.take(&runinfo, n) || !cv.take(&scan64, scan_scratch_elems(n)) || !cv.take(&counter, 2) ||
+        !cv.take(&lenbad, 1))
         return arena_full("sequence tables");
+    // the caller's offsets are checked on the device (1..500 residues each) before any kernel
+    // that indexes by length runs
+    XTN_CK(cudaMemsetAsync(lenbad, 0xff, 4, s));
+    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, s>>>(offs, nullptr, n, lenbad));
     XTN_LAUNCH("pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(chars, offs, nullptr, n, d, keys, klen, vcnt, runinfo,
                                                                  nullptr));
     XTN_CK(cudaGetLastError());
     scan_exclusive<uint32_t, uint64_t>(vcnt, voff, n, scan64, s);
-    uint64_t V = 0;
+    uint64_t V = 0, bad = 0;
+    XTN_TRY(read_u64(lenbad, 4, s, &bad));
+    if ((uint32_t)bad != 0xffffffffu) {
+        set_err("sequence " + std::to_string((uint32_t)bad) + " has an invalid length");
+        return XTN_ERR_ARG;
+    }
     XTN_TRY(read_u64(voff + n, 8, s, &V));
     uint64_t *recA, *recB;
     uint32_t* rscratch;

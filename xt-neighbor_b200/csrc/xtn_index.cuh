@@ -206,7 +206,7 @@ struct xtn_index {
 
 namespace xtn {
 
-static int index_build(xtn_index* ix, int n, int dmax) {
+static int index_build(xtn_index* ix, int n, int dmax, bool validate) {
     xtn_context* c = ix->c;
     cudaStream_t s = c->stream;
     cudaEvent_t e0 = c->ev[0], e1 = c->ev[1];
@@ -226,13 +226,16 @@ static int index_build(xtn_index* ix, int n, int dmax) {
     XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (n + 1)));
     XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * n));
     XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)n));
+    if (validate) XTN_TRY(launch_length_check(c, offs, nullptr, n));
     XTN_LAUNCH("index_pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(
                                  chars, offs, nullptr, n, dmax, P<u128>(c->keys), P<uint8_t>(c->klen),
                                  P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab)));
     XTN_CK(cudaGetLastError());
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n));
     uint64_t V = 0;
+    if (validate) XTN_CK(cudaMemcpyAsync(c->h_scalar + 1, c->lencheck.p, 4, cudaMemcpyDeviceToHost, s));
     XTN_TRY(read_scalar(c, P<uint64_t>(c->voff) + n, 8, &V));
+    if (validate) XTN_TRY(length_check_result(c, (uint32_t)c->h_scalar[1]));
     if (V >= (uint64_t)UINT32_MAX) {
         set_err("index has too many deletion variants (" + std::to_string(V) + ")");
         return XTN_ERR_LIMIT;
@@ -271,7 +274,8 @@ static int index_build(xtn_index* ix, int n, int dmax) {
 
 // One query batch on device inputs; the result (pairs (index row, n_index + query row), int8
 // distances) is left in the context's output buffers, c->n_out entries.
-static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qoffs, int nq, int d, int measure) {
+static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qoffs, int nq, int d, int measure,
+                       bool validate) {
     xtn_context* c = ix->c;
     cudaStream_t s = c->stream;
     c->stats = xtn_stats{};
@@ -288,13 +292,16 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
     XTN_TRY(ensure(c->voff, sizeof(uint64_t) * (nq + 1)));
     XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * nq));
     XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)nq));
+    if (validate) XTN_TRY(launch_length_check(c, qoffs, nullptr, nq));
     XTN_LAUNCH("query_pack", k_pack<<<blocks_for(nq, kPackThreads), kPackThreads, 0, s>>>(
                                  qchars, qoffs, nullptr, nq, d, P<u128>(c->keys), P<uint8_t>(c->klen),
                                  P<uint32_t>(c->vcnt), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab)));
     XTN_CK(cudaGetLastError());
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), nq));
     uint64_t Vq = 0;
+    if (validate) XTN_CK(cudaMemcpyAsync(c->h_scalar + 1, c->lencheck.p, 4, cudaMemcpyDeviceToHost, s));
     XTN_TRY(read_scalar(c, P<uint64_t>(c->voff) + nq, 8, &Vq));
+    if (validate) XTN_TRY(length_check_result(c, (uint32_t)c->h_scalar[1]));
     c->stats.n_variants = (int64_t)Vq;
     XTN_TRY(ensure(ix->qh, sizeof(uint64_t) * Vq));
     XTN_TRY(ensure(ix->qrow, sizeof(uint32_t) * Vq));
@@ -461,7 +468,7 @@ int xtn_index_create(int device, const char* seqs, const uint32_t* offsets, int3
     }
     if (r == XTN_SUCCESS) {
         begin_run(ix->c);
-        r = index_build(ix, n_seqs, max_distance);
+        r = index_build(ix, n_seqs, max_distance, false);
         end_run(ix->c);
     }
     if (r != XTN_SUCCESS) {
@@ -498,7 +505,7 @@ int xtn_index_create_device(int device, const char* d_seqs, const uint32_t* d_of
     }
     if (r == XTN_SUCCESS) {
         begin_run(ix->c);
-        r = index_build(ix, n_seqs, max_distance);
+        r = index_build(ix, n_seqs, max_distance, true);
         end_run(ix->c);
     }
     if (r != XTN_SUCCESS) {
@@ -534,7 +541,7 @@ int xtn_index_query_device(xtn_index* ix, const xtn_args* args, const char* d_se
     XTN_CK(cudaSetDevice(ix->c->device));
     begin_run(ix->c);
     int r = index_query(ix, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n_queries, args->distance,
-                        args->measure);
+                        args->measure, true);
     end_run(ix->c);
     if (r == XTN_SUCCESS && n_out) *n_out = ix->c->n_out;
     return r;
@@ -552,7 +559,8 @@ int xtn_index_query(xtn_index* ix, const xtn_args* args, const char* seqs, const
     XTN_CK(cudaSetDevice(c->device));
     XTN_TRY(upload(c, seqs, offsets, n_queries));
     begin_run(c);
-    int r = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), n_queries, args->distance, args->measure);
+    int r = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), n_queries, args->distance, args->measure,
+                        false);
     end_run(c);
     if (r != XTN_SUCCESS) return r;
     return deliver(c, cb, user);
@@ -673,7 +681,7 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
             status = upload(c, hchars.data(), hoffs.data(), (int)rows);
             if (status == XTN_SUCCESS) {
                 begin_run(c);
-                status = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), (int)rows, d, m);
+                status = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), (int)rows, d, m, false);
                 end_run(c);
             }
             if (status != XTN_SUCCESS) break;

@@ -201,11 +201,13 @@ void scan_exclusive(const In* in, Out* out, int64_t n, Out* scratch, cudaStream_
 // (an atomic ticket), publishes its tile total in a status word, and warp 0 sums the totals of
 // earlier tiles 32 at a time, back to the nearest inclusive prefix, before publishing its own.
 // A tile waits only for tiles taken earlier by running CTAs, which publish before they look
-// back, so the waits end; each is still bounded (kScanPollLimit rounds), after which *err is
-// incremented and the tile continues with the sum it has (the host reports the error). One
-// launch instead of scan_exclusive's three or more; `status` holds scan_1p_words(n) words that
-// the call clears first. Status word: bits 62-63 flag (1: tile total, 2: inclusive prefix),
-// bits 0-61 the value.
+// back, so the waits end; each is still bounded (poll_limit rounds, kScanPollLimit by default),
+// after which *err is incremented and the tile continues with the sum it has (the host reports
+// the error and discards the result). One launch instead of scan_exclusive's three or more;
+// `status` holds scan_1p_words(n) words that the call clears first. Status word: bits 62-63
+// flag (1: tile total, 2: inclusive prefix), bits 0-61 the value. withhold_tile0 != 0 makes tile
+// 0 skip publishing its prefix: a status word that nothing sets, so that a test can make the
+// later tiles' bounded waits run out and check that the error reaches the caller.
 constexpr unsigned long long kScanFlagTotal = 1ull << 62;
 constexpr unsigned long long kScanFlagPrefix = 2ull << 62;
 constexpr unsigned long long kScanValueMask = (1ull << 62) - 1ull;
@@ -216,7 +218,8 @@ inline int64_t scan_1p_words(int64_t n) { return (n + kScanTile - 1) / kScanTile
 template <typename In, typename Out>
 __global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ in, Out* __restrict__ out, int64_t n,
                                                         unsigned long long* __restrict__ status,
-                                                        unsigned int* __restrict__ err) {
+                                                        unsigned int* __restrict__ err, uint32_t poll_limit,
+                                                        int withhold_tile0) {
     __shared__ uint32_t s_tile;
     __shared__ Out s_excl;
     unsigned int* ticket = reinterpret_cast<unsigned int*>(status);  // word 0; tiles from word 1
@@ -239,18 +242,18 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ i
         unsigned long long* words = status + 1;
         Out excl = 0;
         if (tile == 0) {
-            if (lane == 0) st_relaxed_u64(words, kScanFlagPrefix | (unsigned long long)total);
+            if (lane == 0 && !withhold_tile0) st_relaxed_u64(words, kScanFlagPrefix | (unsigned long long)total);
         } else {
             if (lane == 0) st_relaxed_u64(words + tile, kScanFlagTotal | (unsigned long long)total);
             uint32_t polls = 0;
             for (int64_t j = (int64_t)tile - 1; j >= 0; j -= 32) {
                 const int64_t t = j - lane;  // lane 0 reads the nearest tile
                 unsigned long long w = t >= 0 ? ld_relaxed_u64(words + t) : kScanFlagPrefix;
-                while (__any_sync(0xffffffffu, (w >> 62) == 0ull) && ++polls <= kScanPollLimit) {
+                while (__any_sync(0xffffffffu, (w >> 62) == 0ull) && ++polls <= poll_limit) {
                     if (polls > 64) __nanosleep(64);
                     if ((w >> 62) == 0ull) w = ld_relaxed_u64(words + t);
                 }
-                if (polls > kScanPollLimit) {
+                if (polls > poll_limit) {
                     if (lane == 0) atomicAdd(err, 1u);
                     break;
                 }
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ i
 // of `status`). Asynchronous on `stream`.
 template <typename In, typename Out>
 void scan_exclusive_1p(const In* in, Out* out, int64_t n, unsigned long long* status, unsigned int* err,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, uint32_t poll_limit = kScanPollLimit, int withhold_tile0 = 0) {
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(Out), stream);
         return;
@@ -292,7 +295,8 @@ void scan_exclusive_1p(const In* in, Out* out, int64_t n, unsigned long long* st
         return;
     }
     cudaMemsetAsync(status, 0, sizeof(unsigned long long) * scan_1p_words(n), stream);
-    XTN_LAUNCH("scan_1p", (k_scan_1p<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, n, status, err)));
+    XTN_LAUNCH("scan_1p", (k_scan_1p<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, n, status, err,
+                                                                                          poll_limit, withhold_tile0)));
 }
 
 // ------------------------------------------------------------------ LSD radix sort (u64 keys)
