@@ -1,14 +1,19 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 symmetric-deletion neighbour search.
 
-One step = one full nearest-neighbour search (pack, variant generation, key sort,
-grouping, candidate emission, pair sort, verification, compaction) over the workload's
+One step = one full nearest-neighbour search (pack, variant generation, key grouping,
+candidate emission, pair dedup and sort, verification, compaction) over the workload's
 sequences, inputs resident in HBM (`value`); `e2e` is the same search through the C ABI's
 host-buffer entry point (xtn_context_perform) with the host->device copy of the sequences
 and the device->host copy of the result pairs inside the timed region.
 
-Workload (default): 1,000,000 synthetic CDR3 sequences, 20% in mutant clusters, 2% exact
-duplicates, Levenshtein d = 2, seeded generator (xtn.synth_clusters).
+Workload (default): 10,000,000 synthetic CDR3 sequences, 20% in mutant clusters, 2% exact
+duplicates, Levenshtein d = 2, seeded generator (xtn.synth_clusters). The 1,000,000-sequence
+workload of the same generator is measured too and reported under "extra_workloads".
+
+The reference arm (--impl reference) times the reference's own library entry point,
+xtn_perform, built from its sources for sm_100a (oracle/_ref/ref_perform), as a call in one
+process after a warm-up call, on workload files written by a separate generator process.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--workload NAME]
 
@@ -31,11 +36,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "xt-neighbor_b200")
 sys.path.insert(0, PKG)
 
+# expect_out: the output length on the workload, which the reference binary's and this
+# build's outputs share byte for byte (tests/test_gpu_reference_full_size.py); the reference
+# arm compares its own count with it
 WORKLOADS = {
-    "nn_1m_leven_d2": dict(kind="clusters", n=1_000_000, d=2, measure=0, seed=20241),
+    "nn_1m_leven_d2": dict(kind="clusters", n=1_000_000, d=2, measure=0, seed=20241, expect_out=314_584),
     "nn_10k_leven_d1": dict(kind="mutants", n=10_000, d=1, measure=0, seed=20240),
-    "nn_10m_leven_d2": dict(kind="clusters", n=10_000_000, d=2, measure=0, seed=20242),
-    "nn_10m_hamming_d2": dict(kind="clusters", n=10_000_000, d=2, measure=1, seed=20242),
+    "nn_10m_leven_d2": dict(kind="clusters", n=10_000_000, d=2, measure=0, seed=20242, expect_out=3_182_141),
+    "nn_10m_hamming_d2": dict(kind="clusters", n=10_000_000, d=2, measure=1, seed=20242, expect_out=890_373),
     # repertoire overlap: 64 repertoires, sizes log-uniform in [1e4, 2e6] (23.9M rows with this
     # seed), 5% of each drawn from a shared pool, power-law duplicate counts; Levenshtein d = 1
     "overlap_64rep_leven_d1": dict(kind="repertoires", n_reps=64, min=1e4, max=2e6, shared=0.05, d=1, measure=0,
@@ -47,7 +55,12 @@ SERVE_WORKLOADS = {
     "serve_5m_d2": dict(n_index=5_000_000, n_pool=1_000_000, seed=20245, rates=(10, 100, 1000), seconds=3.0,
                         max_size=100_000, p_d1=0.7),
 }
-DEFAULT_WORKLOAD = "nn_1m_leven_d2"
+DEFAULT_WORKLOAD = "nn_10m_leven_d2"
+EXTRA_WORKLOADS = {"nn_10m_leven_d2": ["nn_1m_leven_d2"]}
+SYNTH_CLI = os.path.join(PKG, "bin", "xtn_synth")
+REF_PERFORM = os.path.join(ROOT, "oracle", "_ref", "ref_perform")
+# the reference arm stops repeating the search once its timed calls have taken this long
+REF_MAX_SECONDS = 60.0
 METRIC = "seqs/s (symmetric-deletion NN search, whole job)"
 L2_FLUSH_BYTES = 256 << 20
 
@@ -492,8 +505,13 @@ def run_ours(args, w):
         "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(breakdown.items(), key=lambda kv: -kv[1][0])},
         "clocks": clocks,
     }
+    extras = {}
+    for name in ([] if args.no_extra else EXTRA_WORKLOADS.get(args.workload, [])):
+        extras[name] = measure_extra(ctx, WORKLOADS[name], args, flush, ext)
+    if extras:
+        line["extra_workloads"] = extras
     if world == 1 and not args.no_cli:
-        line["cli_process"] = cli_process(args, w, chars, offs, info, reps)
+        line["cli_process"] = cli_process(args, w, n)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(chars, offs, w, info, reps)
     ctx.close()
@@ -502,10 +520,56 @@ def run_ours(args, w):
     return line
 
 
+def measure_extra(ctx, w, args, flush, ext):
+    """A further nearest-neighbour workload on the same context, timed like the headline:
+    device-resident search (`value`) and host-buffer search with both copies (`e2e`)."""
+    import numpy as np
+    import torch
+
+    chars, offs, _, _ = gen_workload(w)
+    n = len(offs) - 1
+    d_chars = torch.from_numpy(chars).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    ctx.set_profiling(False)
+
+    def timed(fn, count):
+        out, ms = None, []
+        for _ in range(count):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            out = fn()
+            e1.record(ext)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return out, ms
+
+    dev = lambda: ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+    timed(dev, args.warmup)
+    n_out, ms = timed(dev, args.steps)
+    pin_c = torch.from_numpy(chars).pin_memory()
+    pin_o = torch.from_numpy(offs.view(np.int32)).pin_memory()
+    hc, ho = pin_c.numpy(), pin_o.numpy().view(np.uint32)
+    host = lambda: ctx.perform(hc, ho, distance=w["d"], measure=w["measure"])
+    timed(host, args.warmup)
+    res, ems = timed(host, args.steps)
+    assert len(res.pairs) == n_out
+    st = ctx.stats()
+    m, em = sum(ms) / len(ms), sum(ems) / len(ems)
+    return {"value": n / (m / 1e3), "unit": "seqs/s", "ms_per_step": m, "steps": args.steps,
+            "n_seqs": n, "distance": w["d"], "measure": "hamming" if w["measure"] else "leven",
+            "pairs_per_s": n_out / (m / 1e3), "output_entries": n_out,
+            "counts": {k: st[k] for k in ("n_variants", "n_candidates", "n_unique", "n_out")},
+            "e2e": {"value": n / (em / 1e3), "unit": "seqs/s", "ms_per_step": em,
+                    "h2d_bytes_per_step": int(len(chars) + 4 * len(offs)), "d2h_bytes_per_step": int(n_out * 9)}}
+
+
 def cpu_baseline(chars, offs, w, info=None, reps=None, max_seqs=2_000_000):
-    """The CPU oracle (multithreaded restatement of the reference algorithm) on the workload:
-    the whole input in nearest-neighbour mode; in overlap mode the leading repertoires up to
-    about max_seqs rows (a bounded sample of the same workload)."""
+    """The CPU oracle (multithreaded restatement of the reference algorithm) on a bounded sample
+    of the workload: its first max_seqs sequences in nearest-neighbour mode (the whole input
+    when it is smaller), the leading repertoires up to about max_seqs rows in overlap mode."""
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -514,8 +578,12 @@ def cpu_baseline(chars, offs, w, info=None, reps=None, max_seqs=2_000_000):
     n = len(offs) - 1
     t0 = time.perf_counter()
     if info is None:
-        orc.nn_search(chars, offs, w["d"], w["measure"])
-        sample, what = n, f"whole workload ({n} seqs), one search"
+        k = min(n, max_seqs)
+        sub_o = offs[: k + 1]
+        orc.nn_search(chars[: sub_o[-1]], sub_o, w["d"], w["measure"])
+        sample = k
+        what = (f"whole workload ({n} seqs), one search" if k == n else
+                f"first {k} of the workload's {n} sequences, one search")
     else:
         k = max(1, int(np.searchsorted(np.cumsum(reps), max_seqs, side="right")))
         rows = int(np.sum(reps[:k]))
@@ -533,104 +601,131 @@ def cpu_baseline(chars, offs, w, info=None, reps=None, max_seqs=2_000_000):
     }
 
 
-def cli_process(args, w, chars, offs, info=None, reps=None):
+def cli_process(args, w, n):
     """The xt_neighbor CLI as a whole process on the workload files (parse + search, no -o),
-    timed like the reference's published harness: wall clock around the process."""
+    timed like the reference's published harness: wall clock around the process. Its -V
+    stage lines (start-up, parse, search, output) give the breakdown of the last run."""
     import xtn
 
-    n = len(offs) - 1
     with tempfile.TemporaryDirectory() as td:
-        cmd = [xtn.CLI_PATH] + workload_files(td, w, chars, offs, info, reps)
-        times = []
-        for i in range(2 + 3):
+        cmd = [xtn.CLI_PATH] + workload_files(td, w)
+        runs = 3 if n <= 2_000_000 else 2
+        times, stages = [], None
+        for i in range(1 + runs):
             t0 = time.perf_counter()
-            p = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+            p = subprocess.run(cmd + ["-V"], capture_output=True, text=True, timeout=1800)
             dt = time.perf_counter() - t0
             if p.returncode != 0:
                 return {"error": p.stderr[-200:]}
-            if i >= 2:
+            if i >= 1:
                 times.append(dt)
+                stages = cli_stage_times(p.stdout)
     s = sum(times) / len(times)
     return {"value": n / s, "unit": "seqs/s", "ms_per_run": s * 1e3, "runs": len(times),
-            "what": "xt_neighbor CLI process: CSV parse + search, no -o, wall clock"}
+            "stages_ms": stages, "what": "xt_neighbor CLI process: CSV parse + search, no -o, wall clock"}
 
 
-def workload_files(td, w, chars, offs, info=None, reps=None):
-    """Writes the workload in the CLI's input format under td; returns the CLI arguments."""
-    n = len(offs) - 1
+def cli_stage_times(stdout: str):
+    """The `xtn_b200 stage <name> <ms>` lines the CLI prints under -V, as a dict."""
+    out = {}
+    for line in stdout.splitlines():
+        parts = line.split()
+        if len(parts) == 4 and parts[0] == "xtn_b200" and parts[1] == "stage":
+            try:
+                out[parts[2]] = float(parts[3])
+            except ValueError:
+                pass
+    return out or None
+
+
+def workload_files(td, w, prefix_rows: int = 0):
+    """Writes the workload in the CLI's input format under td with the generator command
+    (bin/xtn_synth: a separate process, so the caller loads no library of this build);
+    returns the CLI arguments. With prefix_rows, also writes the first rows to warm.csv."""
     path = os.path.join(td, "seqs.csv")
-    write_csv(chars, offs, path, None if info is None else info[:, 0])
-    cmd = ["-i", path, "-n", str(n), "-d", str(w["d"])] + (["-m", "hamming"] if w["measure"] else [])
-    if info is not None:
+    if w["kind"] == "repertoires":
         ipath = os.path.join(td, "info.csv")
-        with open(ipath, "w") as f:
-            f.write("size\n" + "".join(f"{int(r)}\n" for r in reps))
-        cmd += ["-I", ipath, "-N", str(len(reps))]
-    return cmd
-
-
-def write_csv(chars, offs, path, counts=None):
-    b = chars.tobytes()
-    with open(path, "wb") as f:
-        f.write(b"cdr3\n" if counts is None else b"cdr3,count\n")
-        out = bytearray()
-        for i in range(len(offs) - 1):
-            out += b[offs[i] : offs[i + 1]]
-            if counts is not None:
-                out += b",%d" % int(counts[i])
-            out += b"\n"
-            if len(out) > (64 << 20):
-                f.write(out)
-                out = bytearray()
-        f.write(out)
+        cmd = [SYNTH_CLI, "repertoires", str(w["seed"]), str(w["n_reps"]), repr(w["min"]), repr(w["max"]),
+               repr(w["shared"]), path, ipath]
+    elif w["kind"] == "clusters":
+        cmd = [SYNTH_CLI, "clusters", str(w["seed"]), str(w["n"]), "0.2", "0.02", path]
+    else:
+        cmd = [SYNTH_CLI, "mutants", str(w["seed"]), str(w["n"]), "0.1", path]
+    if prefix_rows and w["kind"] != "repertoires":
+        cmd += [str(prefix_rows), os.path.join(td, "warm.csv")]
+    p = subprocess.run(cmd, capture_output=True, text=True, check=True, timeout=1800)
+    n = int(p.stdout.strip().splitlines()[-1])
+    args = ["-i", path, "-n", str(n), "-d", str(w["d"])] + (["-m", "hamming"] if w["measure"] else [])
+    if w["kind"] == "repertoires":
+        with open(os.path.join(td, "info.csv")) as f:
+            n_reps = sum(1 for line in f) - 1
+        args += ["-I", os.path.join(td, "info.csv"), "-N", str(n_reps)]
+    return args
 
 
 def run_reference(args, w):
-    """The reference XTNeighbor-streaming (oracle/_ref/xt_neighbor_ref, its own CUDA CLI built
-    for sm_100a) on the same workload, timed as the reference's harness does: wall clock
-    around the whole process, no output file."""
+    """The reference XTNeighbor-streaming's own library entry point, xtn_perform, built from its
+    sources for sm_100a (oracle/_ref/ref_perform), timed as a call in one process: one warm-up
+    call on the workload's first 10,000 sequences, then up to --steps calls on the workload,
+    stopping once the timed calls have taken REF_MAX_SECONDS (at least one always runs). The
+    workload files come from the generator command, a separate process: this process loads no
+    library of this build. Rank 0 alone runs under torchrun."""
     world, rank, local = dist_setup()
     if rank != 0:
         return None
-    ref = os.path.join(ROOT, "oracle", "_ref", "xt_neighbor_ref")
-    chars, offs, info, reps = gen_workload(w)
-    n = len(offs) - 1
-    if not os.path.exists(ref):
-        return {"impl": "reference", "unavailable": "reference build oracle/_ref/xt_neighbor_ref missing"}
+    if w["kind"] == "repertoires":
+        return {"impl": "reference", "unavailable": "the in-process reference arm covers nearest-neighbour workloads"}
+    if not os.path.exists(REF_PERFORM):
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/ref_perform missing"}
+    warm_rows = 10_000
     with tempfile.TemporaryDirectory() as td:
-        cmd = [ref] + workload_files(td, w, chars, offs, info, reps)
+        cli = workload_files(td, w, prefix_rows=warm_rows)
+        n = int(cli[cli.index("-n") + 1])
+        cmd = [REF_PERFORM, os.path.join(td, "warm.csv"), str(min(warm_rows, n)), cli[cli.index("-i") + 1], str(n),
+               str(w["d"]), str(w["measure"]), str(max(1, args.steps)), str(REF_MAX_SECONDS)]
         env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
-        times = []
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
-            dt = time.perf_counter() - t0
-            if p.returncode != 0 or "Cuda error" in p.stdout:
-                return {"impl": "reference", "unavailable": f"reference exited {p.returncode}: {(p.stderr or p.stdout)[-200:]}"}
-            if i >= args.warmup:
-                times.append(dt)
-    s = sum(times) / len(times)
-    v = n / s
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=3600)
+        wall = time.perf_counter() - t0
+    steps, outputs, parse_s = [], [], None
+    for line in p.stdout.splitlines():
+        parts = line.split()
+        if parts and parts[0] == "step":
+            steps.append(float(parts[1]))
+            outputs.append(int(parts[2]))
+        elif parts and parts[0] == "parse":
+            parse_s = float(parts[1])
+    if p.returncode != 0 or not steps or "Cuda error" in p.stdout:
+        return {"impl": "reference", "unavailable": f"reference exited {p.returncode}: {(p.stderr or p.stdout)[-200:]}"}
+    sec = sum(steps) / len(steps)
+    v = n / sec
+    expect = w.get("expect_out")
     return {
         "impl": "reference",
         "metric": METRIC,
         "value": v,
         "unit": "seqs/s",
         "n_gpus": 1,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": s * 1e3,
+        "steps": len(steps),
+        "warmup": 1,
+        "ms_per_step": sec * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded CDR3 generator)",
         "config": {"workload": args.workload, "n_seqs": n, "distance": w["d"],
-                   "measure": "hamming" if w["measure"] else "leven", "mode": "nn" if info is None else "overlap",
-                   "parallelism": "single process"},
+                   "measure": "hamming" if w["measure"] else "leven", "mode": "nn",
+                   "parallelism": "single process", "steps_requested": args.steps,
+                   "warmup_call": f"first {min(warm_rows, n)} sequences of the workload",
+                   "stop_after_s": REF_MAX_SECONDS},
+        "outputs": outputs[-1],
+        "outputs_match_expected": (outputs[-1] == expect) if expect is not None else None,
+        "parse_s": parse_s,
+        "process_wall_s": wall,
         "cpu_baseline": {"value": v, "unit": "seqs/s", "cores": 1, "kind": "reference",
-                         "sample": "reference xt_neighbor (CUDA build, sm_100a) on this GPU; whole process: "
-                                   "parse + search, no -o, wall clock"},
+                         "sample": f"reference xtn_perform (its CUDA build, sm_100a, on this GPU; one host thread) "
+                                   f"on the whole workload, {len(steps)} timed call(s) after a warm-up call"},
         "e2e": {"value": v, "unit": "seqs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -646,6 +741,7 @@ def main():
     ap.add_argument("--engine", choices=["bucket", "sort"], default="bucket",
                     help="key grouping: shared-memory hash buckets (default) or full radix sort")
     ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
+    ap.add_argument("--no-extra", action="store_true", help="skip the extra workloads measured beside the headline")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the bucket-engine shape by timing on the workload first (xtn_context_autotune)")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",

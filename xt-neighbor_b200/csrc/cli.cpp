@@ -16,6 +16,7 @@
 //     error here, where the reference indexes its column table at -1;
 //   * a negative -n/-N is rejected like 0;
 //   * CUDA failures exit with status 1 (the reference prints them and continues).
+#include <chrono>
 #include <cerrno>
 #include <climits>
 #include <clocale>
@@ -426,7 +427,13 @@ void overlap_handler(const xtn_output* o, void* user) {
 
 }  // namespace
 
+// Host time since t0 in milliseconds (the -V stage breakdown).
+static double ms_since(const std::chrono::steady_clock::time_point& t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 int main(int argc, char** argv) {
+    const auto t_main = std::chrono::steady_clock::now();
     Args args;
     setlocale(LC_ALL, "");
     int rc = parse_args(argc, argv, &args);
@@ -447,6 +454,7 @@ int main(int argc, char** argv) {
     else rc = parse_input(args.seqPath, &seqs, &info, args.seqLen, overlap);
     if (rc != SUCCESS) return rc;
 
+    const double t_parse = ms_since(t_main);
     if (args.verbose) print_args(args);
     Sink sink;
     if (args.outputPath) {
@@ -454,11 +462,34 @@ int main(int argc, char** argv) {
         if (!sink.out) return print_err("output file opening failed");
     }
     xtn_args xa{args.distance, args.measure, args.verbose, args.infoLen};
-    int r = xtn_perform(&xa, seqs.chars.data(), seqs.offsets.data(), seqs.size(), overlap ? info.data() : nullptr,
-                        overlap ? overlap_handler : nn_handler, &sink);
+    // the library context: device selection, CUDA context creation, stream and pinned scalars
+    xtn_context* ctx = nullptr;
+    int r = xtn_context_create(0, &ctx);
+    const double t_init = ms_since(t_main);
+    double t_search = t_init;
+    xtn_stats st{};
+    if (r == XTN_SUCCESS) {
+        r = xtn_context_perform(ctx, &xa, seqs.chars.data(), seqs.offsets.data(), seqs.size(),
+                                overlap ? info.data() : nullptr, overlap ? overlap_handler : nn_handler, &sink);
+        t_search = ms_since(t_main);
+        xtn_context_stats(ctx, &st);
+    }
+    std::string err = r != XTN_SUCCESS ? xtn_last_error() : "";
+    xtn_context_destroy(ctx);
     if (sink.out && fclose(sink.out) != 0) sink.failed = true;
-    if (r != XTN_SUCCESS) return print_err(xtn_last_error());
+    if (r != XTN_SUCCESS) return print_err(err.c_str());
     if (sink.failed) return print_err("output file writing failed");
-    if (args.verbose) printf("total output length: %'lu\n", (unsigned long)sink.total);
+    if (args.verbose) {
+        // host-time breakdown of this process from main() on (the exec and library loading
+        // before main() and the exit after it are outside): input parse, CUDA start-up,
+        // search with output delivery (the device time of the search itself), release
+        const double t_end = ms_since(t_main);
+        printf("xtn_b200 stage parse %.3f\n", t_parse);
+        printf("xtn_b200 stage cuda_init %.3f\n", t_init - t_parse);
+        printf("xtn_b200 stage search_and_output %.3f\n", t_search - t_init);
+        printf("xtn_b200 stage device_search %.3f\n", st.ms_total);
+        printf("xtn_b200 stage release %.3f\n", t_end - t_search);
+        printf("total output length: %'lu\n", (unsigned long)sink.total);
+    }
     return SUCCESS;
 }

@@ -226,3 +226,72 @@ void synth_copy(void* h, char* chars, uint32_t* offs, int32_t* freq, int32_t* re
 }
 void synth_free(void* h) { delete static_cast<Synth*>(h); }
 }
+
+#ifdef XTN_SYNTH_MAIN
+// Command-line front end (bin/xtn_synth): writes a generated workload in the xt_neighbor CLI's
+// input format, so that a process can be given a workload file without loading this library.
+//   xtn_synth mutants     SEED N FRAC              OUT.csv [PREFIX_N PREFIX.csv]
+//   xtn_synth clusters    SEED N CLUSTER_FRAC DUP  OUT.csv [PREFIX_N PREFIX.csv]
+//   xtn_synth repertoires SEED R MIN MAX SHARED    OUT.csv INFO.csv
+// OUT.csv: header line, then one sequence per line ("seq,count" for repertoires); INFO.csv:
+// header line, then one repertoire size per line. PREFIX.csv holds the first PREFIX_N rows.
+#include <cstdio>
+#include <cstdlib>
+
+static bool write_rows(const Synth* s, int64_t rows, const char* path) {
+    FILE* f = fopen(path, "wb");
+    if (!f) return false;
+    const bool counts = !s->freq.empty();
+    std::string buf = counts ? "cdr3,count\n" : "cdr3\n";
+    for (int64_t i = 0; i < rows; i++) {
+        buf.append(s->chars.data() + s->offs[i], s->offs[i + 1] - s->offs[i]);
+        if (counts) {
+            buf.push_back(',');
+            buf.append(std::to_string(s->freq[i]));
+        }
+        buf.push_back('\n');
+        if (buf.size() > (size_t(32) << 20)) {
+            fwrite(buf.data(), 1, buf.size(), f);
+            buf.clear();
+        }
+    }
+    fwrite(buf.data(), 1, buf.size(), f);
+    return fclose(f) == 0;
+}
+
+int main(int argc, char** argv) {
+    const std::string kind = argc > 1 ? argv[1] : "";
+    Synth* s = nullptr;
+    int next = 0;
+    if (kind == "mutants" && argc >= 6) {
+        s = static_cast<Synth*>(synth_nn(strtoull(argv[2], nullptr, 10), atoll(argv[3]), 0, atof(argv[4]), 0.0));
+        next = 5;
+    } else if (kind == "clusters" && argc >= 7) {
+        s = static_cast<Synth*>(
+            synth_nn(strtoull(argv[2], nullptr, 10), atoll(argv[3]), 1, atof(argv[4]), atof(argv[5])));
+        next = 6;
+    } else if (kind == "repertoires" && argc >= 9) {
+        s = static_cast<Synth*>(
+            synth_overlap(strtoull(argv[2], nullptr, 10), atoi(argv[3]), atof(argv[4]), atof(argv[5]), atof(argv[6])));
+        next = 7;
+    } else {
+        fprintf(stderr, "usage: xtn_synth mutants|clusters|repertoires ... (see synth.cpp)\n");
+        return 1;
+    }
+    const int64_t n = (int64_t)s->offs.size() - 1;
+    if (!write_rows(s, n, argv[next])) return 1;
+    if (kind == "repertoires") {
+        FILE* f = fopen(argv[next + 1], "wb");
+        if (!f) return 1;
+        fputs("size\n", f);
+        for (int32_t r : s->rep_sizes) fprintf(f, "%d\n", r);
+        if (fclose(f) != 0) return 1;
+    } else if (argc > next + 2) {
+        const int64_t k = std::min<int64_t>(n, atoll(argv[next + 1]));
+        if (!write_rows(s, k, argv[next + 2])) return 1;
+    }
+    printf("%lld\n", (long long)n);
+    delete s;
+    return 0;
+}
+#endif
