@@ -74,7 +74,7 @@ typedef struct xtn_output {
 
 typedef void (*xtn_callback)(const xtn_output* output, void* user);
 
-/* Opaque reusable state: device, stream and device buffers that grow on demand. */
+/* Opaque reusable state: device, streams and device buffers that grow on demand. */
 typedef struct xtn_context xtn_context;
 
 /* Counters and stage timings of the last run on a context. */
@@ -88,9 +88,11 @@ typedef struct xtn_stats {
     int64_t n_verified_pairs;  /* verified sequence pairs (overlap mode) */
     int64_t n_launches;        /* kernel launches of the last run */
     int32_t id_bits;           /* bits used for a sequence id in packed records */
-    int32_t n_rounds;          /* key-space rounds the search ran in */
+    int32_t n_rounds;          /* rounds the search ran in (contiguous ranges of first-level
+                                  hash buckets sized to the memory budget; see memory_budget) */
     double ms_total;           /* device time of the last run, milliseconds */
     double ms_stage[8];        /* pack, gen, key sort, group, emit, pair sort, verify, output */
+    int64_t n_fallback;        /* buckets grouped by sorting (too large for shared memory) */
 } xtn_stats;
 
 /* ------------------------------------------------------------------ reference interface */
@@ -183,6 +185,19 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     candidates and for n <= 2^24), 0 = every candidate is sorted,
  *                     2 = as 1 with the table always sized from the previous search's share
  *                     of distinct pairs (the sizing used above 256 MiB of table)
+ *   "memory_budget"   bytes of device memory a search may hold (default 0: 80% of the free
+ *                     device memory plus what the context holds, read only when one round
+ *                     would need more than half of the device). A search whose variant
+ *                     records do not fit runs in rounds over contiguous ranges of first-level
+ *                     hash buckets (bucket engine; xtn_stats.n_rounds); a budget that cannot
+ *                     hold one bucket returns XTN_ERR_NOMEM. Replaces the reference's memory
+ *                     model and lower-bound rounds (xtneighbor_streaming/src/xtn.cu:21-26,
+ *                     64-157, 383-470)
+ *   "max_round_records" >= 0: at most this many variant records per round (default 0: no
+ *                     bound beyond the budget and 2^32 - 2^20)
+ *   "round_overlap"   1 = in a multi-round search, a round's candidate-pair dedup runs on a
+ *                     second stream while the next round generates (default), 0 = in turn on
+ *                     one stream
  *   "wait_polls"      1..4194304: bound on the polls of one look-back wait in the single-pass
  *                     prefix sums (default 4194304); a wait that reaches it makes the call
  *                     return XTN_ERR_CUDA and the result is discarded

@@ -12,6 +12,11 @@ properties that hold at any size.
   - For sampled query sequences, the exhaustive neighbour scan (oracle.brute_neighbors)
     finds exactly the reported pairs that involve them. This is completeness and soundness
     for those queries.
+  - Forced into eight rounds, the search returns exactly the one-round result (which the
+    reference binary matches byte for byte, tests/test_gpu_reference_full_size.py).
+
+10,000,000 sequences at d = 3 (about 5.8e9 deletion variants, more than one round can hold in
+32-bit positions): the search runs in rounds and its result has the same properties.
 """
 import numpy as np
 import pytest
@@ -102,3 +107,28 @@ def test_10m_hamming_within_levenshtein(ten_million_results):
     pos = np.searchsorted(lk, hk)
     assert (pos < len(lk)).all() and (lk[pos] == hk).all()
     assert (lev.distances[pos] <= ham.distances).all()
+
+
+def test_10m_rounds_equal_one_round(ten_million, ten_million_results):
+    chars, offs = ten_million
+    b = ten_million_results[xtn.LEVENSHTEIN]
+    ctx = xtn.Context(0)
+    ctx.set_option("max_round_records", 1_096_096_457 // 8 + 1)
+    r = ctx.perform(chars, offs, distance=2)
+    assert ctx.stats()["n_rounds"] >= 8
+    ctx.close()
+    assert_same_pairs(r.pairs, r.distances, b.pairs, b.distances, "10M, eight rounds vs one")
+
+
+def test_10m_d3_completes_in_rounds(ten_million):
+    chars, offs = ten_million
+    ctx = xtn.Context(0)
+    r = ctx.perform(chars, offs, distance=3)
+    st = ctx.stats()
+    ctx.close()
+    assert st["n_variants"] > 2**32 and st["n_rounds"] >= 2
+    assert len(r.pairs) > len(chars) // 100
+    check_sorted_unique(r.pairs)
+    assert (r.distances >= 0).all() and (r.distances <= 3).all()
+    check_sample_distances(chars, offs, r.pairs, r.distances, 0, k=1000)
+    check_queries(chars, offs, r.pairs, r.distances, 3, 0, n_random=8)

@@ -278,6 +278,7 @@ struct ScatterSmem {
     uint32_t gcur[C::kFan];      // next global position of each bucket for this CTA
     uint32_t cstart[kScatterChunksPerRound + 1];
     uint32_t warp_sums[C::kThreads / 32 + 1];
+    uint32_t m_in;               // records of the chunk inside the round's bucket range
 };
 
 template <class SM>
@@ -300,12 +301,15 @@ constexpr int ctas_per_sm_for() {
 //      coalesced writes of each bucket's run at the CTA's cursor (gcur).
 // runinfo[i] is key_run_info of sequence i, tab its key_table; voff and toff are exclusive
 // scans of the variant and task counts (toff = sequence index at d = 1).
+// Rounds: only the records of buckets [b_lo, b_lo + b_n) are kept, at their global position
+// minus `round_base` (the global position of bucket b_lo's first record); the others are
+// generated and dropped (b_lo = 0, b_n = 2^b1, round_base = 0: every record, one round).
 template <class C>
 __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()) k_bucket_scatter_staged(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
     int tile, int d, int b1, int idbits, const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart,
-    uint64_t* __restrict__ recs) {
+    uint32_t b_lo, uint32_t b_n, uint64_t round_base, uint64_t* __restrict__ recs) {
     constexpr int T = C::kThreads, kFanPer = C::kFanPer;
     constexpr uint64_t kSpan = (uint64_t)(C::kChunk - kMaxVariantsD2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     const int nb = 1 << b1;
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
     for (int b = threadIdx.x; b < nb; b += T) {
-        S.gcur[b] = (uint32_t)bstart[b] + off[b];
+        S.gcur[b] = (uint32_t)(bstart[b] - round_base) + off[b];  // used for buckets of the round only
         S.cnt[b] = 0;
     }
     const int t0 = blockIdx.x * tile;
@@ -347,6 +351,10 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
                 auto put = [&](int v, uint64_t h) {
                     const uint32_t b = (uint32_t)(h >> shift);
                     const uint32_t pos = vb + (uint32_t)v;
+                    if (b - b_lo >= b_n) {  // another round's bucket
+                        S.br[pos] = 0xffffffffu;
+                        return;
+                    }
                     S.br[pos] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
                     S.rec[pos] = ((h << b1) & hi_mask) | id;
                 };
@@ -381,16 +389,19 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
 #pragma unroll
                 for (int k = 0; k < kFanPer; k++)
                     if (b0 + k < nb) S.lstart[b0 + k] = ex + loc[k];
+                if (threadIdx.x == 0) S.m_in = tot;
             }
             __syncthreads();
             for (uint32_t p = threadIdx.x; p < m; p += T) {
                 const uint32_t br = S.br[p], b = br >> 16, r = br & 0xffffu;
+                if (br == 0xffffffffu) continue;
                 const uint32_t q = S.lstart[b] + r;
                 S.sorted[q] = S.rec[p];
                 S.dst[q] = S.gcur[b] + r;
             }
             __syncthreads();
-            for (uint32_t q = threadIdx.x; q < m; q += T) recs[S.dst[q]] = S.sorted[q];
+            const uint32_t m_in = S.m_in;
+            for (uint32_t q = threadIdx.x; q < m_in; q += T) recs[S.dst[q]] = S.sorted[q];
             __syncthreads();
             for (int b = threadIdx.x; b < nb; b += T) {
                 S.gcur[b] += S.cnt[b];
@@ -403,16 +414,18 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     }
 }
 
-// First-level scatter for any d: one thread per sequence, smem cursors, direct stores.
+// First-level scatter for any d: one thread per sequence, smem cursors, direct stores. Rounds
+// as in k_bucket_scatter_staged: buckets [b_lo, b_lo + b_n) only, positions minus `round_base`.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* __restrict__ keys,
                                                                    const uint8_t* __restrict__ klen, int n, int tile, int d,
                                                                    int b1, int idbits, const uint32_t* __restrict__ offsets,
-                                                                   const uint64_t* __restrict__ bstart,
+                                                                   const uint64_t* __restrict__ bstart, uint32_t b_lo,
+                                                                   uint32_t b_n, uint64_t round_base,
                                                                    uint64_t* __restrict__ recs) {
     extern __shared__ uint32_t s_cur[];
     const int nb = 1 << b1;
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) s_cur[i] = (uint32_t)bstart[i] + off[i];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) s_cur[i] = (uint32_t)(bstart[i] - round_base) + off[i];
     __syncthreads();
     const int base = blockIdx.x * tile;
     const int end = min(n, base + tile);
@@ -422,7 +435,9 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* _
         const uint64_t id = (uint64_t)i;
         for_each_variant(keys[i], klen[i], d, [&](u128 k) {
             uint64_t h = key_hash(k);
-            uint32_t pos = atomicAdd(&s_cur[h >> shift], 1u);
+            const uint32_t b = (uint32_t)(h >> shift);
+            if (b - b_lo >= b_n) return;
+            uint32_t pos = atomicAdd(&s_cur[b], 1u);
             recs[pos] = ((h << b1) & hi_mask) | id;
         });
     }
@@ -448,12 +463,14 @@ __device__ __forceinline__ void bounded_append(T* __restrict__ list, uint32_t ca
 }
 
 // Sorts buckets into "group directly" descriptors and split jobs.
-__global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint32_t group_cap,
+// bstart points at the round's first bucket; `base` is that bucket's global start, so the
+// descriptors hold positions in the round's record buffer.
+__global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint64_t base, uint32_t group_cap,
                               BucketDesc* __restrict__ desc, uint32_t desc_cap, SplitJob* __restrict__ jobs,
                               unsigned int* __restrict__ counters) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    uint64_t s = bstart[b], e = bstart[b + 1];
+    uint64_t s = bstart[b] - base, e = bstart[b + 1] - base;
     uint32_t size = (uint32_t)(e - s);
     if (size < 2) return;
     if (size <= group_cap) {

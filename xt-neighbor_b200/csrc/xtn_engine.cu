@@ -251,7 +251,8 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
 // search's epoch in the top kDedupTagBits bits; a slot with another epoch is free, so the table
 // is cleared only when allocated and when the epoch wraps. Pairs must fit in kDedupKeyBits
 // bits (2 * id_bits <= 48, n <= 2^24). Slot hash: the SplitMix64 finaliser (Steele, Lea and
-// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014).
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014). With uniq == nullptr
+// the pairs are only inserted (the rebuild of a grown table from the distinct list).
 constexpr int kDedupKeyBits = 48;
 constexpr int kDedupTagBits = 64 - kDedupKeyBits;
 constexpr uint64_t kDedupTagMask = ~((1ull << kDedupKeyBits) - 1ull);
@@ -302,6 +303,7 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
             }
         }
     }
+    if (uniq == nullptr) return;
     const unsigned mask = __ballot_sync(0xffffffffu, fresh);
     if (mask == 0u) return;
     unsigned long long base = 0;
@@ -461,7 +463,15 @@ struct xtn_context {
     int split_chunk = 4096;  // the same for the split (2048 | 4096)
     int split_slices = kSplitSlices;  // CTAs (one cluster) per split bucket: 1 | kSplitSlices
     uint32_t group_cap = kGroupCap;
-    uint64_t last_pc = 0;   // candidate count of the previous run (initial buffer size)
+    double last_pc_per_rec = 0;  // candidates per variant record of the previous run (buffer sizing)
+    // rounds: memory model and the second stream of the multi-round loop
+    int64_t memory_budget = 0;      // bytes a search may hold on the device; 0: 80% of what is free
+    int64_t max_round_records = 0;  // records per round at most; 0: from the budget
+    int round_overlap = 1;          // 1: a round's pair dedup runs on stream2 during the next round
+    size_t total_mem = 0;           // device memory size
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_round[2] = {};
+    DevBuf pairA2, ddcnt;
     // results
     DevBuf out_pairs, out_dist, out_freq;
     uint64_t* h_scalar = nullptr;  // pinned
@@ -631,8 +641,9 @@ static int ensure_keep(xtn_context* c, DevBuf& b, size_t bytes, size_t used) {
 }
 
 // Candidate pairs of a record array sorted by hash: runs of equal hash, every id pair of every
-// run appended to c->pairA at index `base`. *count receives the number appended.
-static int group_sorted(xtn_context* c, const uint64_t* recs, int64_t V, int idbits, uint64_t base, uint64_t* count) {
+// run appended to `out` at index `base`. *count receives the number appended.
+static int group_sorted(xtn_context* c, const uint64_t* recs, int64_t V, int idbits, DevBuf& out, uint64_t base,
+                        uint64_t* count) {
     cudaStream_t s = c->stream;
     XTN_TRY(ensure(c->counter, 64));
     int64_t gcap = std::max<int64_t>(1 << 16, V / 8);
@@ -661,11 +672,11 @@ static int group_sorted(xtn_context* c, const uint64_t* recs, int64_t V, int idb
     uint64_t Pc = 0;
     XTN_TRY(read_scalar(c, P<uint64_t>(c->goff) + G, 8, &Pc));
     if (Pc == 0) return XTN_SUCCESS;
-    XTN_TRY(ensure_keep(c, c->pairA, sizeof(uint64_t) * (base + Pc) + 64, sizeof(uint64_t) * base));
+    XTN_TRY(ensure_keep(c, out, sizeof(uint64_t) * (base + Pc) + 64, sizeof(uint64_t) * base));
     uint64_t threads = (Pc + kEmitPer - 1) / kEmitPer;
     XTN_LAUNCH("emit", k_emit<<<blocks_for((int64_t)threads), kThreads, 0, s>>>(
                            recs, P<uint64_t>(c->gstart), P<uint32_t>(c->gsize), P<uint64_t>(c->goff), (int64_t)G, Pc,
-                           idbits, P<uint64_t>(c->pairA) + base));
+                           idbits, P<uint64_t>(out) + base));
     XTN_CK(cudaGetLastError());
     *count = Pc;
     return XTN_SUCCESS;
@@ -685,99 +696,145 @@ static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t 
     uint64_t* recs = nullptr;
     XTN_TRY(sort_u64(c, c->recA, c->recB, (int64_t)V, idbits, 64, &recs, XTN_SORT_NAMES("key_sort")));
     XTN_CK(cudaEventRecord(c->ev[3], s));
-    XTN_TRY(group_sorted(c, recs, (int64_t)V, idbits, 0, Pc));
+    XTN_TRY(group_sorted(c, recs, (int64_t)V, idbits, c->pairA, 0, Pc));
     XTN_CK(cudaEventRecord(c->ev[4], s));
     return XTN_SUCCESS;
 }
 
-// Bucket engine (xtn_bucket.cuh).
-static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_t V, uint64_t* Pc) {
+// Bucket engine (xtn_bucket.cuh). A search's first-level plan (bucket bits, tiles, per-tile
+// bucket counts, bucket starts, the d = 2 task map) is made once; the records are then
+// produced, split and grouped in one or more rounds, each over a contiguous range of
+// first-level buckets (bucket_round).
+struct BucketPlan {
+    int b1 = 1, nb = 2, ntiles = 1, tile = 1;
+    bool small = false, staged = false;
+    const uint32_t* tseq = nullptr;
+};
+
+__global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+
+static int bucket_attrs(xtn_context* c) {
+    if (c->attrs_set) return XTN_SUCCESS;
+    XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<StageLarge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<StageSmall>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(StageSmem<StageLarge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, kSplitSlices>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageLarge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(StageSmem<SplitSmall>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, kSplitSlices>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<SplitSmall>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
+    c->attrs_set = true;
+    return XTN_SUCCESS;
+}
+
+// Largest first-level bucket bits: the staged scatter's fan-out bounds it for d <= 2 with key
+// tables; the direct scatter (d > 2, or per-key hashing) takes up to 2^14 buckets, which keeps
+// the buckets of very large variant counts (10M sequences at d = 3: ~6e9) small enough for the
+// split to bring them to shared-memory size.
+constexpr int kDirectBucketBitsMax = 14;
+
+// The first-level plan: count pass over every variant (per-tile histograms of the top b1 hash
+// bits), per-tile offsets inside each bucket, bucket starts (c->bstart, nb + 1 entries) and, for
+// the staged scatter at d = 2, the balanced task map.
+static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
     cudaStream_t s = c->stream;
-    int b1 = 1;
-    while (b1 < c->bucket_bits_max && (V >> b1) > 7000) b1++;
-    const int nb = 1 << b1;
     const bool small = c->stage_chunk == 2048;
+    const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
+    const bool tables = d <= 2 && c->key_tables;
+    const int bits_cap = tables ? c->bucket_bits_max : std::max(c->bucket_bits_max, kDirectBucketBitsMax);
+    int b1 = 1;
+    while (b1 < bits_cap && (V >> b1) > 7000) b1++;
+    const int nb = 1 << b1;
     const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
                                               : (small ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
                                                        : ctas_per_sm_for<ScatterSmem<StageLarge>>());
     const int64_t wave = (int64_t)c->sms * per_sm;
     const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
     const int tile = (n + ntiles - 1) / ntiles;
+    bp->b1 = b1;
+    bp->nb = nb;
+    bp->ntiles = ntiles;
+    bp->tile = tile;
+    bp->small = small;
+    bp->staged = tables && nb <= stage_fan;
+    bp->tseq = nullptr;
     const size_t hist_smem = sizeof(uint32_t) * nb;
     XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)ntiles * nb));
     XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)ntiles * nb));
     XTN_TRY(ensure(c->btotals, sizeof(uint32_t) * (nb + 1)));
     XTN_TRY(ensure(c->bstart, sizeof(uint64_t) * (nb + 1)));
-    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
-    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
-    if (!c->attrs_set) {
-        XTN_CK(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(ScatterSmem<StageLarge>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(ScatterSmem<StageSmall>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem<StageLarge>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, kSplitSlices>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageLarge>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(StageSmem<SplitSmall>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, kSplitSlices>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<SplitSmall>)));
-        XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
-        c->attrs_set = true;
-    }
+    XTN_TRY(bucket_attrs(c));
     XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                    P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
-                                   d <= 2 && c->key_tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1,
-                                   P<uint32_t>(c->bcounts)));
+                                   tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1, P<uint32_t>(c->bcounts)));
     XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
-    const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
-    if (d <= 2 && (1 << b1) <= stage_fan && c->key_tables) {
-        const uint32_t* tseq = nullptr;  // d = 1: one task per sequence
-        if (d >= 2) {
-            XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
-            XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
-            XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
-                                                                                       P<uint32_t>(c->tcnt)));
-            XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
-            // a sequence has at most kKeyLen runs, so at most kKeyLen tasks
-            XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * std::min<uint64_t>(V, (uint64_t)kKeyLen * n) + 16));
-            XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->toff), n,
-                                                                                 P<uint32_t>(c->tseq)));
-            tseq = P<uint32_t>(c->tseq);
-        }
-        if (small)
+    if (bp->staged && d >= 2) {
+        XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
+        XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
+        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
+                                                                                   P<uint32_t>(c->tcnt)));
+        XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
+        // a sequence has at most kKeyLen runs, so at most kKeyLen tasks
+        XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * std::min<uint64_t>(V, (uint64_t)kKeyLen * n) + 16));
+        XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->toff), n,
+                                                                             P<uint32_t>(c->tseq)));
+        bp->tseq = P<uint32_t>(c->tseq);
+    }
+    XTN_CK(cudaGetLastError());
+    return XTN_SUCCESS;
+}
+
+// One round: the records of first-level buckets [b_lo, b_lo + b_n), which hold Vr records at
+// global positions [base, base + Vr), are written to recA (positions minus base), oversized
+// buckets split into recB, and every bucket grouped; the candidate pairs are written to `out`
+// from index `at` (grown, keeping entries [0, at), when they do not fit). *Pc receives the
+// number of candidates of the round.
+static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int idbits, uint32_t b_lo, uint32_t b_n,
+                        uint64_t base, uint64_t Vr, DevBuf& out, uint64_t at, uint64_t* Pc) {
+    cudaStream_t s = c->stream;
+    const int b1 = bp.b1, nb = bp.nb;
+    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * Vr + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * Vr + 64));
+    const uint64_t* bstart = P<uint64_t>(c->bstart);
+    if (bp.staged) {
+        if (bp.small)
             XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageSmall><<<ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
+                       k_bucket_scatter_staged<StageSmall><<<bp.ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), tseq, n, tile, d, b1, idbits, P<uint32_t>(c->boffs),
-                           P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
+                           b_lo, b_n, base, P<uint64_t>(c->recA)));
         else
             XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageLarge><<<ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
+                       k_bucket_scatter_staged<StageLarge><<<bp.ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), tseq, n, tile, d, b1, idbits, P<uint32_t>(c->boffs),
-                           P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
-    } else
-        XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<ntiles, kBucketThreads, hist_smem, s>>>(
-                                         P<u128>(c->keys), P<uint8_t>(c->klen), n, tile, d, b1, idbits,
-                                         P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA)));
+                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
+                           b_lo, b_n, base, P<uint64_t>(c->recA)));
+    } else {
+        XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
+                                         P<u128>(c->keys), P<uint8_t>(c->klen), n, bp.tile, d, b1, idbits,
+                                         P<uint32_t>(c->boffs), bstart, b_lo, b_n, base, P<uint64_t>(c->recA)));
+    }
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
 
     // plan: buckets that fit go to grouping, the rest are split by the next hash bits
-    const size_t desc_cap = (size_t)nb * 3 + 4 * V / c->group_cap + 2048;
+    const size_t desc_cap = (size_t)b_n * 3 + 4 * Vr / c->group_cap + 2048;
     XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
-    XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * nb));
+    XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * b_n));
     XTN_TRY(ensure(c->bcnt, 64));
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
-    XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
-                                  P<uint64_t>(c->bstart), nb, c->group_cap, P<BucketDesc>(c->bdesc),
+    XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(b_n), kThreads, 0, s>>>(
+                                  bstart + b_lo, (int)b_n, base, c->group_cap, P<BucketDesc>(c->bdesc),
                                   (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
@@ -785,7 +842,7 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         // one CTA per bucket, or a cluster of kSplitSlices CTAs per bucket, launched for every
         // bucket without waiting for the plan: those past the plan's job count exit at once
         const bool sliced = c->split_slices > 1;
-        const unsigned grid = (unsigned)nb * (sliced ? kSplitSlices : 1);
+        const unsigned grid = (unsigned)b_n * (sliced ? kSplitSlices : 1);
 #define XTN_SPLIT(CFG, SL)                                                                                         \
     XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
                                    P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
@@ -813,24 +870,27 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         }
     }
     XTN_CK(cudaEventRecord(c->ev[3], s));
-    const uint32_t ndesc = cnt[0];
+    const uint32_t ndesc = cnt[kCntDesc];
 
     // group every listed bucket in shared memory; buckets with too many runs are appended
-    // to the fallback list (counter 3)
-    uint64_t cap = std::max<uint64_t>({c->last_pc + c->last_pc / 4, V / 16, (uint64_t)1 << 20});
-    uint64_t total = 0;
-    const uint32_t nfall_split = cnt[3];
+    // to the fallback list (counter kCntFallback); the cursor starts at `at`
+    const uint64_t want =
+        std::max<uint64_t>({c->last_pc_per_rec > 0 ? (uint64_t)(c->last_pc_per_rec * 1.25 * (double)Vr) : 0,
+                            Vr / 16, (uint64_t)1 << 20});
+    uint64_t cap = std::max<uint64_t>(at + want, out.cap / sizeof(uint64_t) > 8 ? out.cap / sizeof(uint64_t) - 8 : 0);
+    uint64_t total = at;
+    const uint32_t nfall_split = cnt[kCntFallback];
     for (int attempt = 0; attempt < 2; attempt++) {
-        XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * cap + 64));
-        XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
-        if (attempt > 0) {  // the overflow list restarts after the split's fallback buckets
-            c->h_scalar[5] = nfall_split;
-            XTN_CK(cudaMemcpyAsync(P<unsigned int>(c->bcnt) + 3, c->h_scalar + 5, 4, cudaMemcpyHostToDevice, s));
-        }
+        XTN_TRY(ensure_keep(c, out, sizeof(uint64_t) * cap + 64, sizeof(uint64_t) * at));
+        XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), (unsigned long long)at));
+        XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
+        if (attempt > 0)  // the overflow list restarts after the split's fallback buckets
+            XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->bcnt) + kCntFallback / 2,
+                                                               ((unsigned long long)nfall_split << 32) | cnt[2]));
         if (ndesc > 0)
             XTN_LAUNCH("bucket_group", k_bucket_group<<<ndesc, kGroupThreads, sizeof(GroupSmem), s>>>(
                                            P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
-                                           P<uint64_t>(c->pairA), cap, P<unsigned long long>(c->counter),
+                                           P<uint64_t>(out), cap, P<unsigned long long>(c->counter),
                                            P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
                                            (uint32_t)desc_cap, P<unsigned int>(c->bcnt)));
         XTN_CK(cudaGetLastError());
@@ -849,8 +909,8 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
         if (total <= cap) break;
         cap = total;
     }
-    const uint32_t nfall = (uint32_t)(c->h_scalar[3] >> 32);  // bcnt[3]: high half of the second word
-    c->stats.n_groups = ndesc;
+    const uint32_t nfall = (uint32_t)(c->h_scalar[3] >> 32);  // bcnt[kCntFallback]: high half of the second word
+    c->stats.n_groups += ndesc;
     XTN_CK(cudaEventRecord(c->ev[4], s));
 
     // buckets too large for shared memory: sorted and grouped in global memory
@@ -865,12 +925,19 @@ static int candidates_bucketed(xtn_context* c, int n, int d, int idbits, uint64_
             uint64_t* sorted = nullptr;
             XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, XTN_SORT_NAMES("fallback_sort")));
             uint64_t more = 0;
-            XTN_TRY(group_sorted(c, sorted, f.size, idbits, total, &more));
+            XTN_TRY(group_sorted(c, sorted, f.size, idbits, out, total, &more));
             total += more;
         }
     }
-    *Pc = total;
+    c->stats.n_fallback += nfall;
+    *Pc = total - at;
     return XTN_SUCCESS;
+}
+
+// Single-round bucket engine: every record of the search in one pass.
+static int candidates_bucketed(xtn_context* c, const BucketPlan& bp, int n, int d, int idbits, uint64_t V,
+                               uint64_t* Pc) {
+    return bucket_round(c, bp, n, d, idbits, 0, (uint32_t)bp.nb, 0, V, c->pairA, 0, Pc);
 }
 
 // Distinct non-self candidate pairs of pairA[0..Pc) into pairB[0..*U), in no particular order.
@@ -907,6 +974,197 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
     }
     set_err("candidate pair hash set: insertions did not find a free slot");
     return XTN_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------ rounds
+// A search whose variant records do not fit the memory budget (or a 32-bit position) runs in
+// rounds, each over a contiguous range of first-level buckets. Equal variants hash to the same
+// bucket, so every group of equal variants lies in one round; a candidate pair can still come
+// from several rounds (through different shared variants), so the rounds' candidates go through
+// one candidate-pair hash set that lives across the rounds: each distinct pair is appended to
+// the distinct list once, by whichever round meets it first. This replaces the reference's
+// lower-bound rounds over the min-id space (S/src/xtn.cu:383-470, cal_lowerbounds
+// S/src/xtn.cu:179-184,218-230), which bound the candidate pairs held in host RAM; here the
+// bound is on device memory, and the records are what grows with the input.
+struct Round {
+    uint32_t b_lo, b_n;  // first-level buckets [b_lo, b_lo + b_n)
+    uint64_t base, size; // their records: global positions [base, base + size)
+};
+
+// Device memory this context holds in its buffers.
+static size_t held_bytes(const xtn_context* c) {
+    const DevBuf* bufs[] = {&c->chars, &c->offs, &c->keys, &c->klen, &c->vcnt, &c->voff, &c->recA, &c->recB,
+                            &c->gstart, &c->gsize, &c->gcnt, &c->goff, &c->pairA, &c->pairB, &c->pairA2, &c->dist,
+                            &c->flag, &c->fpos, &c->scratch64, &c->scratch32, &c->out_pairs, &c->out_dist,
+                            &c->out_freq, &c->bcounts, &c->boffs, &c->bdesc, &c->bfall, &c->fbA, &c->fbB,
+                            &c->runinfo, &c->tcnt, &c->toff, &c->ktab, &c->tseq, &c->dd_table, &c->os_status};
+    size_t t = 0;
+    for (const DevBuf* b : bufs) t += b->cap;
+    return t;
+}
+
+// The memory model: the largest number of variant records one round may hold. The reference
+// sizes each of its stages from the free device memory with a 20% margin (S/src/xtn.cu:21-26,
+// 64-157); here the budget is the context option memory_budget, or else 80% of the free device
+// memory plus what the context already holds (free memory is queried only when one round of
+// the search would need more than half of the device). Per record of a round: 16 bytes of
+// record buffers and about 20 bytes per expected candidate (two candidate buffers with
+// headroom); per search: the per-sequence arrays and about 48 bytes per expected distinct pair
+// (distinct list, hash-set slots, sort buffer, verification and output). The expectations are
+// the previous search's ratios (6% candidates per record and all of them distinct at first).
+static uint64_t round_record_limit(xtn_context* c, int n, int d, uint64_t V) {
+    const double cpr = c->last_pc_per_rec > 0 ? c->last_pc_per_rec : 0.06;
+    const double share = std::min(1.0, 1.25 * c->dd_share);
+    const double per_rec = 16.0 + 20.0 * cpr;
+    const double fixed = (d <= 2 && c->key_tables ? 273.0 : 41.0) * (double)n;
+    const double pairs = 48.0 * share * cpr * (double)V;
+    double budget = (double)c->memory_budget;
+    if (budget <= 0 && fixed + pairs + per_rec * (double)V > 0.5 * (double)c->total_mem) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = 0.8 * (double)(free_b + held_bytes(c));
+        else cudaGetLastError();
+    }
+    uint64_t lim = UINT64_MAX;
+    if (budget > 0) {
+        const double room = budget - fixed - pairs;
+        lim = room > per_rec ? (uint64_t)(room / per_rec) : 1;
+    }
+    if (c->max_round_records > 0) lim = std::min<uint64_t>(lim, (uint64_t)c->max_round_records);
+    return std::min<uint64_t>(lim, (uint64_t)UINT32_MAX - (uint64_t(1) << 20));  // 32-bit positions in a round
+}
+
+// Contiguous bucket ranges of at most `limit` records each (bucket starts read from the device).
+static int plan_rounds(xtn_context* c, const BucketPlan& bp, uint64_t limit, std::vector<Round>* rounds) {
+    std::vector<uint64_t> bs(bp.nb + 1);
+    XTN_CK(cudaMemcpyAsync(bs.data(), c->bstart.p, sizeof(uint64_t) * (bp.nb + 1), cudaMemcpyDeviceToHost, c->stream));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    rounds->clear();
+    uint32_t lo = 0;
+    while (lo < (uint32_t)bp.nb) {
+        if (bs[lo + 1] - bs[lo] > limit) {
+            set_err("the memory budget cannot hold one first-level bucket (" + std::to_string(bs[lo + 1] - bs[lo]) +
+                    " variant records, at most " + std::to_string(limit) + " per round)");
+            return XTN_ERR_NOMEM;
+        }
+        uint32_t hi = lo + 1;
+        while (hi < (uint32_t)bp.nb && bs[hi + 1] - bs[lo] <= limit) hi++;
+        rounds->push_back(Round{lo, hi - lo, bs[lo], bs[hi] - bs[lo]});
+        lo = hi;
+    }
+    return XTN_SUCCESS;
+}
+
+// Candidate-pair hash set of a search: T slots (a power of two) of c->dd_table under a fresh
+// epoch, cleared on `st` when the table is (re)allocated or the epoch wraps.
+static int dedup_table(xtn_context* c, uint64_t want, cudaStream_t st, uint64_t* T, uint64_t* tag) {
+    *T = pow2_at_least(want);
+    if (c->dd_table.cap < sizeof(uint64_t) * *T) {
+        XTN_TRY(ensure(c->dd_table, sizeof(uint64_t) * *T));
+        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, st));
+        c->dd_epoch = 0;
+    }
+    if (++c->dd_epoch >= (1u << kDedupTagBits)) {
+        XTN_CK(cudaMemsetAsync(c->dd_table.p, 0, c->dd_table.cap, st));
+        c->dd_epoch = 1;
+    }
+    *tag = (uint64_t)c->dd_epoch << kDedupKeyBits;
+    return XTN_SUCCESS;
+}
+
+// Multi-round candidates. With the hash set, the distinct pairs of all rounds end in
+// c->pairB[0..*U) (*distinct = true): round r's candidates are written to one of two buffers
+// (pairA, pairA2) and de-duplicated on stream2 while round r + 1 generates and groups on the
+// main stream (round_overlap; otherwise everything runs on the main stream in turn). Without
+// the hash set (n > 2^24 or pair_dedup = 0) every round's candidates are appended to c->pairA
+// (*U = *Ptotal, *distinct = false), to be sorted and checked for repeats afterwards.
+static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d, int idbits, uint64_t V,
+                             const std::vector<Round>& rounds, uint64_t* Ptotal, uint64_t* U_out, bool* distinct) {
+    cudaStream_t s = c->stream;
+    uint64_t Ptot = 0;
+    *distinct = c->pair_dedup && 2 * idbits <= kDedupKeyBits;
+    if (!*distinct) {
+        for (const Round& r : rounds) {
+            uint64_t pc = 0;
+            XTN_TRY(bucket_round(c, bp, n, d, idbits, r.b_lo, r.b_n, r.base, r.size, c->pairA, Ptot, &pc));
+            Ptot += pc;
+        }
+        *Ptotal = *U_out = Ptot;
+        return XTN_SUCCESS;
+    }
+    const bool overlap = c->round_overlap != 0;
+    cudaStream_t sd = overlap ? c->stream2 : s;  // stream of the dedup passes
+    DevBuf* cand[2] = {&c->pairA, overlap ? &c->pairA2 : &c->pairA};
+    XTN_TRY(ensure(c->ddcnt, 64));
+    XTN_CK(cudaMemsetAsync(c->ddcnt.p, 0, 64, s));  // distinct count, insertions that ran out of probes
+    XTN_CK(cudaEventRecord(c->ev_round[0], s));
+    XTN_CK(cudaStreamWaitEvent(sd, c->ev_round[0], 0));
+    unsigned long long* n_uniq = P<unsigned long long>(c->ddcnt);
+    uint64_t T = 0, tag = 0, Pc_est = 0, U_now = 0;
+    uint64_t U_before[2] = {0, 0}, Pc_r[2] = {0, 0};
+    auto launch_dedup = [&](int slot) -> int {
+        if (Pc_r[slot] > 0)
+            XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc_r[slot]), kThreads, 0, sd>>>(
+                                         P<uint64_t>(*cand[slot]), (int64_t)Pc_r[slot], idbits,
+                                         P<unsigned long long>(c->dd_table), T - 1, tag, P<uint64_t>(c->pairB), n_uniq,
+                                         n_uniq + 1));
+        XTN_CK(cudaGetLastError());
+        XTN_CK(cudaMemcpyAsync(c->h_scalar + 8, c->ddcnt.p, 16, cudaMemcpyDeviceToHost, sd));
+        return XTN_SUCCESS;
+    };
+    // waits for the dedup of the round in `slot`; when an insertion ran out of probes, the table
+    // grows, is rebuilt from the distinct pairs of the earlier rounds, and the round is redone
+    auto settle = [&](int slot) -> int {
+        for (int attempt = 0;; attempt++) {
+            XTN_CK(cudaStreamSynchronize(sd));
+            if (c->h_scalar[9] == 0) {
+                U_now = c->h_scalar[8];
+                return XTN_SUCCESS;
+            }
+            if (attempt == 2) {
+                set_err("candidate pair hash set: insertions did not find a free slot");
+                return XTN_ERR_CUDA;
+            }
+            XTN_TRY(dedup_table(c, dedup_regrow_slots(T, Pc_est), sd, &T, &tag));
+            XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, sd>>>(n_uniq, (unsigned long long)U_before[slot]));
+            XTN_CK(cudaMemsetAsync(n_uniq + 1, 0, 8, sd));
+            if (U_before[slot] > 0)
+                XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)U_before[slot]), kThreads, 0, sd>>>(
+                                             P<uint64_t>(c->pairB), (int64_t)U_before[slot], idbits,
+                                             P<unsigned long long>(c->dd_table), T - 1, tag, nullptr, n_uniq,
+                                             n_uniq + 1));
+            XTN_TRY(launch_dedup(slot));
+        }
+    };
+    for (size_t r = 0; r < rounds.size(); r++) {
+        const int slot = (int)(r & 1);
+        uint64_t pc = 0;
+        XTN_TRY(bucket_round(c, bp, n, d, idbits, rounds[r].b_lo, rounds[r].b_n, rounds[r].base, rounds[r].size,
+                             *cand[slot], 0, &pc));
+        Ptot += pc;
+        if (pc >= (uint64_t)UINT32_MAX) {
+            set_err("too many candidate pairs in one round (" + std::to_string(pc) + ")");
+            return XTN_ERR_LIMIT;
+        }
+        if (overlap && r > 0) XTN_TRY(settle(slot ^ 1));  // its buffer is the next round's
+        if (r == 0) {
+            // the table is sized for the whole search, extrapolated from the first round
+            Pc_est = (uint64_t)((double)pc * (double)V / (double)std::max<uint64_t>(1, rounds[0].size) * 1.1) + 1;
+            XTN_TRY(dedup_table(c, dedup_first_slots(Pc_est, c->dd_share, c->pair_dedup == 2), sd, &T, &tag));
+        }
+        // the distinct list grows by at most this round's candidates (the dedup stream is idle)
+        XTN_TRY(ensure_keep(c, c->pairB, sizeof(uint64_t) * (U_now + pc) + 64, sizeof(uint64_t) * U_now));
+        U_before[slot] = U_now;
+        Pc_r[slot] = pc;
+        XTN_CK(cudaEventRecord(c->ev_round[slot], s));
+        XTN_CK(cudaStreamWaitEvent(sd, c->ev_round[slot], 0));
+        XTN_TRY(launch_dedup(slot));
+        if (!overlap) XTN_TRY(settle(slot));
+    }
+    if (overlap) XTN_TRY(settle((int)((rounds.size() - 1) & 1)));
+    *Ptotal = Ptot;
+    *U_out = U_now;
+    c->dd_share = Ptot ? std::max(0.01, (double)U_now / (double)Ptot) : 1.0;
+    return XTN_SUCCESS;
 }
 
 // The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
@@ -952,27 +1210,59 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         return XTN_ERR_CUDA;
     }
     st.n_variants = (int64_t)V;
-    if (V >= (uint64_t)UINT32_MAX) {
-        set_err("too many deletion variants for one round (" + std::to_string(V) + ")");
+    if (c->engine == 1 && V >= (uint64_t)UINT32_MAX) {
+        set_err("too many deletion variants for the sort engine's one round (" + std::to_string(V) + ")");
         return XTN_ERR_LIMIT;
     }
 
     // candidate pairs: every (min id, max id) of every group of equal variant hashes
     uint64_t Pc = 0;
     XTN_TRY(ensure(c->counter, 64));
-    if (c->engine == 1) XTN_TRY(candidates_sorted(c, n, d, idbits, V, &Pc));
-    else XTN_TRY(candidates_bucketed(c, n, d, idbits, V, &Pc));
-    c->last_pc = Pc;
-    st.n_candidates = (int64_t)Pc;
+    bool distinct = false;  // pairB already holds the distinct pairs (multi-round search)
+    if (c->engine == 1) {
+        XTN_TRY(candidates_sorted(c, n, d, idbits, V, &Pc));
+    } else {
+        BucketPlan bp;
+        XTN_TRY(bucket_prepare(c, n, d, V, &bp));
+        const uint64_t limit = round_record_limit(c, n, d, V);
+        if (V <= limit) {
+            XTN_TRY(candidates_bucketed(c, bp, n, d, idbits, V, &Pc));
+        } else {
+            std::vector<Round> rounds;
+            XTN_TRY(plan_rounds(c, bp, limit, &rounds));
+            st.n_rounds = (int32_t)rounds.size();
+            uint64_t U = 0;
+            XTN_TRY(candidates_rounds(c, bp, n, d, idbits, V, rounds, &Pc, &U, &distinct));
+            if (distinct) {
+                st.n_candidates = (int64_t)Pc;
+                c->last_pc_per_rec = V ? (double)Pc / (double)V : 0.0;
+                Pc = U;
+            }
+        }
+    }
+    if (!distinct) {
+        c->last_pc_per_rec = V ? (double)Pc / (double)V : 0.0;
+        st.n_candidates = (int64_t)Pc;
+    }
     if (Pc >= (uint64_t)UINT32_MAX) {
-        set_err("too many candidate pairs for one round (" + std::to_string(Pc) + ")");
+        set_err("too many " + std::string(distinct ? "distinct" : "candidate") + " pairs (" + std::to_string(Pc) + ")");
         return XTN_ERR_LIMIT;
     }
-    XTN_TRY(ensure_keep(c, c->pairA, sizeof(uint64_t) * Pc + 64, sizeof(uint64_t) * Pc));
-    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc + 64));
+    if (distinct) {
+        XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Pc + 64));  // the sort's second buffer
+    } else {
+        XTN_TRY(ensure_keep(c, c->pairA, sizeof(uint64_t) * Pc + 64, sizeof(uint64_t) * Pc));
+        XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc + 64));
+    }
     XTN_CK(cudaEventRecord(c->ev[5], s));
     uint64_t* pairs = P<uint64_t>(c->pairA);
-    if (c->pair_dedup && (int64_t)Pc >= kDedupMinPairs && 2 * idbits <= kDedupKeyBits) {
+    if (distinct) {
+        // the rounds' distinct pairs (pairB): only sorted and verified
+        st.n_unique = (int64_t)Pc;
+        pairs = P<uint64_t>(c->pairB);
+        if (Pc > 1)
+            XTN_TRY(sort_u64(c, c->pairB, c->pairA, (int64_t)Pc, 0, 2 * idbits, &pairs, XTN_SORT_NAMES("pair_sort")));
+    } else if (c->pair_dedup && (int64_t)Pc >= kDedupMinPairs && 2 * idbits <= kDedupKeyBits) {
         // from here on Pc counts the distinct pairs (in pairB), which alone are sorted and verified
         XTN_TRY(dedup_pairs(c, Pc, idbits, &Pc));
         st.n_unique = (int64_t)Pc;
@@ -1472,12 +1762,18 @@ int xtn_context_create(int device, xtn_context** out) {
     xtn_context* c = new xtn_context();
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&c->h_scalar, 64) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&c->h_scalar, 128) != cudaSuccess) {
         set_err("stream or pinned scalar allocation failed");
         delete c;
         return XTN_ERR_CUDA;
     }
     for (auto& ev : c->ev) cudaEventCreate(&ev);
+    for (auto& ev : c->ev_round) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    {
+        size_t free_b = 0;
+        cudaMemGetInfo(&free_b, &c->total_mem);
+    }
     c->overlap_bufs = new xtn_overlap_bufs();
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* e = getenv("XTN_ENGINE")) c->engine = (strcmp(e, "sort") == 0) ? 1 : 0;
@@ -1496,7 +1792,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
                       &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->lencheck, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
+                      &c->ktab,    &c->info,     &c->lencheck, &c->pairA2, &c->ddcnt, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
     for (DevBuf* b : bufs) release(*b);
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
@@ -1507,6 +1803,12 @@ void xtn_context_destroy(xtn_context* c) {
     }
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : c->ev_round)
+        if (ev) cudaEventDestroy(ev);
+    if (c->stream2) {
+        cudaStreamSynchronize(c->stream2);
+        cudaStreamDestroy(c->stream2);
+    }
     if (c->h_scalar) cudaFreeHost(c->h_scalar);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1624,6 +1926,9 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
     else if (!strcmp(name, "split_slices") && (v == 1 || v == kSplitSlices)) c->split_slices = (int)v;
     else if (!strcmp(name, "wait_polls") && v >= 1 && v <= (int64_t)kScanPollLimit) c->wait_polls = (uint32_t)v;
+    else if (!strcmp(name, "memory_budget") && v >= 0) c->memory_budget = v;
+    else if (!strcmp(name, "max_round_records") && v >= 0) c->max_round_records = v;
+    else if (!strcmp(name, "round_overlap") && (v == 0 || v == 1)) c->round_overlap = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);

@@ -95,6 +95,7 @@ class Stats(ctypes.Structure):
         ("n_rounds", ctypes.c_int32),
         ("ms_total", ctypes.c_double),
         ("ms_stage", ctypes.c_double * 8),
+        ("n_fallback", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
