@@ -16,7 +16,9 @@
 //     error here, where the reference indexes its column table at -1;
 //   * a negative -n/-N is rejected like 0;
 //   * CUDA failures exit with status 1 (the reference prints them and continues).
+#include <algorithm>
 #include <chrono>
+#include <thread>
 #include <cerrno>
 #include <climits>
 #include <clocale>
@@ -211,39 +213,200 @@ bool parse_int_field(const char* s, int* out) {
     return true;
 }
 
-// S/src/cli.cu:101-147
+// One fgets()-sized piece of the input: [begin, begin + len) of the file image.
+struct Piece {
+    size_t begin;
+    int len;
+};
+
+// Cuts file bytes [from, to) into the pieces fgets(buf, size, f) would return (a piece ends
+// after a newline or after size - 1 characters). `from` must be the start of a physical line
+// (or of the file), so that pieces of different segments never straddle.
+static void cut_pieces(const char* data, size_t from, size_t to, int size, std::vector<Piece>* out) {
+    const int maxp = size - 1;
+    size_t i = from;
+    while (i < to) {
+        const void* nl = memchr(data + i, '\n', std::min<size_t>(to - i, (size_t)maxp));
+        const size_t e = nl ? (size_t)((const char*)nl - data) + 1 : std::min(to, i + (size_t)maxp);
+        out->push_back(Piece{i, (int)(e - i)});
+        i = e;
+    }
+}
+
+// A piece as the C string fgets() leaves: it ends at the first NUL byte, if any.
+static int c_len(const char* s, int len) {
+    const void* z = memchr(s, '\0', (size_t)len);
+    return z ? (int)((const char*)z - s) : len;
+}
+
+// The reference skips the lines "\n" and " \n" (S/src/cli.cu:113-114).
+static bool blank_piece(const char* s, int len) {
+    len = c_len(s, len);
+    return (len == 1 && s[0] == '\n') || (len == 2 && s[0] == ' ' && s[1] == '\n');
+}
+
+// Outcome of a data piece (a non-blank piece after the header).
+enum PieceCheck { P_OK = 0, P_BAD_CHAR, P_EMPTY, P_NO_COMMA, P_BAD_NUMBER };
+
+// SeqArray::append (S/src/codec.cu:175-196) and the frequency field (S/src/cli.cu:122-137) of
+// one piece, without storing: the residues count, their validity, the frequency.
+static PieceCheck check_piece(const char* s, int len, bool doubleCol, int* seq_len, int* freq) {
+    len = c_len(s, len);
+    int i = 0;
+    while (i < 500 && i < len) {
+        const char c = s[i];
+        if (c == '\n' || c == ',' || c == '\t') break;
+        i++;
+        if (char_encode(c) == -1) return P_BAD_CHAR;
+    }
+    *seq_len = i;
+    if (i == 0) return P_EMPTY;
+    if (doubleCol) {
+        const void* comma = memchr(s, ',', (size_t)len);
+        if (!comma) return P_NO_COMMA;
+        char num[512];
+        const char* c1 = (const char*)comma + 1;
+        const int m = (int)(s + len - c1);
+        memcpy(num, c1, (size_t)m);
+        num[m] = '\0';
+        if (!parse_int_field(num, freq)) return P_BAD_NUMBER;
+    }
+    return P_OK;
+}
+
+// S/src/cli.cu:101-147, read in parallel. The file is loaded whole, cut into segments at
+// physical line starts, and each segment into fgets() pieces (so a line longer than 499
+// characters becomes several logical lines, as in the reference); the pieces are checked and
+// stored by several threads. The outcome is the sequential one: the first failing piece in
+// file order decides the message and its line number, and the row-count limit (-n) applies
+// at the data piece where a sequential reader would reach it.
 int parse_input(const char* path, SeqStore* seqs, std::vector<xtn_seq_info>* info, int len, bool doubleCol) {
     FILE* f = fopen(path, "r");
     if (!f) return print_err("input file reading failed");
-    PieceReader rd(f, 500);
-    int lineNumber = 1, count = 0;
-    rd.next();  // header
-    while (rd.next()) {
-        lineNumber++;
-        char* line = rd.line();
-        if (blank_line(line)) continue;
-        int r = seqs->append(line);
-        if (r != SUCCESS) {
-            fclose(f);
-            return print_err_line("input parsing error", lineNumber);
-        }
-        if (doubleCol) {
-            char* c = strchr(line, ',');
-            if (!c) {
-                fclose(f);
-                return print_err_line("input parsing error (comma expected)", lineNumber);
-            }
-            int v;
-            if (!parse_int_field(c + 1, &v)) {
-                fclose(f);
-                return print_err_line("input parsing error (invalid number)", lineNumber);
-            }
-            if (count < (int)info->size()) (*info)[count].frequency = v;
-        }
-        count++;
+    std::vector<char> data;
+    {
+        char buf[1 << 16];
+        size_t k;
+        while ((k = fread(buf, 1, sizeof buf, f)) > 0) data.insert(data.end(), buf, buf + k);
     }
     fclose(f);
+    // the header is the first piece
+    std::vector<Piece> head;
+    cut_pieces(data.data(), 0, std::min<size_t>(data.size(), 499), 500, &head);
+    const size_t body = head.empty() ? 0 : head[0].len;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 32u));
+    if (data.size() - body < (size_t(1) << 20)) nt = 1;
+    // segment bounds at physical line starts
+    std::vector<size_t> cut(nt + 1, data.size());
+    cut[0] = body;
+    for (unsigned t = 1; t < nt; t++) {
+        size_t at = body + (data.size() - body) * t / nt;
+        at = std::max(at, cut[t - 1]);
+        while (at < data.size() && at > body && data[at - 1] != '\n') at++;
+        cut[t] = at;
+    }
+    struct Seg {
+        std::vector<Piece> pieces;
+        std::vector<int> lens, freqs;  // per data piece
+        size_t chars = 0;
+        int64_t first_bad = -1;        // index into pieces of the first failing data piece
+        PieceCheck why = P_OK;
+        int64_t data_before_bad = 0;   // data pieces before it
+    };
+    std::vector<Seg> seg(nt);
+    auto work = [&](unsigned t) {
+        Seg& g = seg[t];
+        cut_pieces(data.data(), cut[t], cut[t + 1], 500, &g.pieces);
+        for (size_t k = 0; k < g.pieces.size(); k++) {
+            const char* s = data.data() + g.pieces[k].begin;
+            const int pl = g.pieces[k].len;
+            if (blank_piece(s, pl)) continue;
+            int sl = 0, fq = 0;
+            const PieceCheck r = check_piece(s, pl, doubleCol, &sl, &fq);
+            if (r != P_OK) {
+                g.first_bad = (int64_t)k;
+                g.why = r;
+                g.data_before_bad = (int64_t)g.lens.size();
+                return;
+            }
+            g.lens.push_back(sl);
+            if (doubleCol) g.freqs.push_back(fq);
+            g.chars += (size_t)sl;
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; t++) th.emplace_back(work, t);
+        work(0);
+        for (auto& x : th) x.join();
+    }
+    // sequential outcome: walk the segments in file order. A data piece first meets the row
+    // limit (SeqArray::append refuses the (len + 1)-th row), then its own checks.
+    int64_t count = 0, pieces_before = 0;
+    for (unsigned t = 0; t < nt; t++) {
+        const Seg& g = seg[t];
+        const int64_t room = (int64_t)len - count;
+        const int64_t ndata = g.first_bad >= 0 ? g.data_before_bad + 1 : (int64_t)g.lens.size();
+        if (ndata > room) {  // the limit is met at this segment's data piece number `room`
+            int64_t seen = 0;
+            for (size_t k = 0; k < g.pieces.size(); k++) {
+                if (blank_piece(data.data() + g.pieces[k].begin, g.pieces[k].len)) continue;
+                if (seen++ == room) {
+                    print_err("SeqArray exceeding max length");
+                    return print_err_line("input parsing error", (int)(2 + pieces_before + (int64_t)k));
+                }
+            }
+        }
+        if (g.first_bad >= 0) {
+            const int line = (int)(2 + pieces_before + g.first_bad);
+            switch (g.why) {
+                case P_BAD_CHAR:
+                    print_err("invalid char");
+                    return print_err_line("input parsing error", line);
+                case P_EMPTY: return print_err_line("input parsing error", line);
+                case P_NO_COMMA: return print_err_line("input parsing error (comma expected)", line);
+                default: return print_err_line("input parsing error (invalid number)", line);
+            }
+        }
+        pieces_before += (int64_t)g.pieces.size();
+        count += (int64_t)g.lens.size();
+    }
     if (count != len) return print_err("input length doesn't match with the actual");
+    // store: offsets by a prefix over the segments, characters copied by the threads
+    size_t total = 0;
+    std::vector<size_t> char_base(nt), row_base(nt);
+    int64_t rows = 0;
+    for (unsigned t = 0; t < nt; t++) {
+        char_base[t] = total;
+        row_base[t] = (size_t)rows;
+        total += seg[t].chars;
+        rows += (int64_t)seg[t].lens.size();
+    }
+    seqs->chars.resize(total);
+    seqs->offsets.resize((size_t)rows + 1);
+    seqs->offsets[0] = 0;
+    auto store = [&](unsigned t) {
+        const Seg& g = seg[t];
+        size_t c = char_base[t], row = row_base[t], di = 0;
+        for (size_t k = 0; k < g.pieces.size(); k++) {
+            const char* s = data.data() + g.pieces[k].begin;
+            if (blank_piece(s, g.pieces[k].len)) continue;
+            const int sl = g.lens[di];
+            memcpy(seqs->chars.data() + c, s, (size_t)sl);
+            c += (size_t)sl;
+            seqs->offsets[row + 1] = (uint32_t)c;
+            if (doubleCol && row < info->size()) (*info)[row].frequency = g.freqs[di];
+            row++;
+            di++;
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; t++) th.emplace_back(store, t);
+        store(0);
+        for (auto& x : th) x.join();
+    }
     return SUCCESS;
 }
 
@@ -439,6 +602,26 @@ int main(int argc, char** argv) {
     int rc = parse_args(argc, argv, &args);
     if (rc != SUCCESS) return rc;
 
+    // CUDA start-up (device selection, context, streams) runs on its own thread while the
+    // input is parsed; its outcome is looked at only once parsing has succeeded
+    xtn_context* ctx = nullptr;
+    int ctx_rc = XTN_SUCCESS;
+    double t_init_done = 0;
+    std::string init_err;  // the library's error text is per thread
+    std::thread init([&] {
+        ctx_rc = xtn_context_create(0, &ctx);
+        if (ctx_rc != XTN_SUCCESS) init_err = xtn_last_error();
+        t_init_done = ms_since(t_main);
+    });
+    struct Joiner {
+        std::thread& t;
+        xtn_context*& c;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+            xtn_context_destroy(c);
+        }
+    } joiner{init, ctx};
+
     bool overlap = args.infoPath != nullptr;
     SeqStore seqs;
     seqs.maxSize = args.seqLen;
@@ -462,9 +645,9 @@ int main(int argc, char** argv) {
         if (!sink.out) return print_err("output file opening failed");
     }
     xtn_args xa{args.distance, args.measure, args.verbose, args.infoLen};
-    // the library context: device selection, CUDA context creation, stream and pinned scalars
-    xtn_context* ctx = nullptr;
-    int r = xtn_context_create(0, &ctx);
+    init.join();
+    int r = ctx_rc;
+    if (r != XTN_SUCCESS) return print_err(init_err.c_str());
     const double t_init = ms_since(t_main);
     double t_search = t_init;
     xtn_stats st{};
@@ -476,16 +659,19 @@ int main(int argc, char** argv) {
     }
     std::string err = r != XTN_SUCCESS ? xtn_last_error() : "";
     xtn_context_destroy(ctx);
+    ctx = nullptr;
     if (sink.out && fclose(sink.out) != 0) sink.failed = true;
     if (r != XTN_SUCCESS) return print_err(err.c_str());
     if (sink.failed) return print_err("output file writing failed");
     if (args.verbose) {
         // host-time breakdown of this process from main() on (the exec and library loading
-        // before main() and the exit after it are outside): input parse, CUDA start-up,
-        // search with output delivery (the device time of the search itself), release
+        // before main() and the exit after it are outside): input parse, CUDA start-up (on
+        // its own thread during the parse) and what was left of it after the parse, search
+        // with output delivery (the device time of the search itself), release
         const double t_end = ms_since(t_main);
         printf("xtn_b200 stage parse %.3f\n", t_parse);
-        printf("xtn_b200 stage cuda_init %.3f\n", t_init - t_parse);
+        printf("xtn_b200 stage cuda_init %.3f\n", t_init_done);  // from main(), beside the parse
+        printf("xtn_b200 stage wait_for_cuda_init %.3f\n", t_init - t_parse);
         printf("xtn_b200 stage search_and_output %.3f\n", t_search - t_init);
         printf("xtn_b200 stage device_search %.3f\n", st.ms_total);
         printf("xtn_b200 stage release %.3f\n", t_end - t_search);
