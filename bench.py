@@ -505,6 +505,11 @@ def run_ours(args, w):
         "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(breakdown.items(), key=lambda kv: -kv[1][0])},
         "clocks": clocks,
     }
+    # the plain form (above: one launch sequence per search, sizes read back between stages)
+    # against the batched/persistent form (the search captured once into a CUDA graph and
+    # replayed, every size read on the device), same inputs, same timing
+    if not overlap and not args.no_forms:
+        line["forms"] = measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, ms_step, n_out)
     extras = {}
     for name in ([] if args.no_extra else EXTRA_WORKLOADS.get(args.workload, [])):
         extras[name] = measure_extra(ctx, WORKLOADS[name], args, flush, ext)
@@ -518,6 +523,35 @@ def run_ours(args, w):
     if pg:
         pg.destroy_process_group()
     return line
+
+
+def measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, plain_ms, plain_out):
+    import torch
+
+    ctx.set_profiling(False)
+    ctx.set_option("graph", 1)
+    fn = lambda: ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+    times, out = [], None
+    for i in range(1 + args.warmup + args.steps):  # the first search runs plain and captures
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        out = fn()
+        e1.record(ext)
+        e1.synchronize()
+        if i > args.warmup:
+            times.append(e0.elapsed_time(e1))
+    st = ctx.stats()
+    ctx.set_option("graph", 0)
+    assert out == plain_out, "graph form and plain form differ in output length"
+    g = sum(times) / len(times)
+    return {"plain": {"value": n / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                      "what": "one launch sequence per search, four host reads of sizes"},
+            "batched_graph": {"value": n / (g / 1e3), "ms_per_step": g, "launches_in_graph": st["n_launches"],
+                              "what": "whole search captured once in a CUDA graph, sizes read on the device, "
+                                      "grouping by persistent CTAs, one host read per search"},
+            "batched_over_plain": plain_ms / g}
 
 
 def measure_extra(ctx, w, args, flush, ext):
@@ -742,6 +776,7 @@ def main():
                     help="key grouping: shared-memory hash buckets (default) or full radix sort")
     ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
     ap.add_argument("--no-extra", action="store_true", help="skip the extra workloads measured beside the headline")
+    ap.add_argument("--no-forms", action="store_true", help="skip the plain-vs-graph form comparison")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the bucket-engine shape by timing on the workload first (xtn_context_autotune)")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",

@@ -198,6 +198,17 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *   "round_overlap"   1 = in a multi-round search, a round's candidate-pair dedup runs on a
  *                     second stream while the next round generates (default), 0 = in turn on
  *                     one stream
+ *   "graph"           1 = xtn_context_nn_device runs the batched/persistent form: the whole
+ *                     search (one round) is captured once per input (device pointers, size,
+ *                     distance, measure, shape options) into a CUDA graph whose kernels read
+ *                     every data-dependent size on the device (grouping by persistent CTAs
+ *                     that take bucket descriptors from a device-side queue), and each later
+ *                     search on that input replays it with one synchronisation at the end.
+ *                     Capacities come from the plain search that precedes the capture; a
+ *                     replay that exceeds one (or meets a bucket too large for shared memory)
+ *                     is redone by the plain form, which re-sizes the graph. 0 = the plain
+ *                     form (default): one launch sequence per search that reads sizes back to
+ *                     the host between its stages
  *   "wait_polls"      1..4194304: bound on the polls of one look-back wait in the single-pass
  *                     prefix sums (default 4194304); a wait that reaches it makes the call
  *                     return XTN_ERR_CUDA and the result is discarded

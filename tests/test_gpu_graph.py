@@ -1,0 +1,80 @@
+"""The batched/persistent form (context option "graph"): the whole search captured into one
+CUDA graph whose kernels read every data-dependent size on the device, replayed per search.
+It must return exactly what the plain form returns (which the parity suite pins to the oracle
+and the reference), on first use (plain search, then capture), on every replay, after the
+input changes in place (a replay that outgrows its capacities is redone by the plain form),
+and it must reject invalid lengths like the plain form.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import xtn
+from conftest import assert_same_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def on_device(torch, chars, offs, pad=0):
+    dch = torch.zeros(len(chars) + 64 + pad, dtype=torch.uint8, device="cuda")
+    dch[: len(chars)] = torch.from_numpy(chars).cuda()
+    dof = torch.from_numpy(offs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    return dch, dof
+
+
+@pytest.mark.parametrize("kind,n,d,measure", [("clusters", 60_000, 2, 0), ("clusters", 60_000, 2, 1),
+                                              ("mutants", 10_000, 1, 0), ("mutants", 10_000, 3, 0)])
+def test_graph_form_equals_oracle_on_every_replay(kind, n, d, measure):
+    import torch
+
+    chars, offs = (xtn.synth_clusters(seed=7, n=n) if kind == "clusters" else xtn.synth_mutants(seed=42, n=n))
+    exp_p, exp_d, _ = orc.nn_search(chars, offs, d, measure)
+    dch, dof = on_device(torch, chars, offs)
+    with xtn.Context(0, graph=1) as ctx:
+        for rep in range(4):  # plain + capture, then three replays
+            m = ctx.nn_device(dch.data_ptr(), dof.data_ptr(), n, d, measure)
+            got = ctx.fetch(m)
+            assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, f"graph form, search {rep}")
+        st = ctx.stats()
+        assert st["n_launches"] > 10 and st["n_out"] == len(exp_p)
+
+
+def test_graph_form_redoes_a_replay_that_outgrows_its_capacities():
+    """Same device buffers, new contents: a replay whose variants or candidates exceed the
+    captured capacities is redone by the plain form (and the graph re-sized)."""
+    import torch
+
+    small_c, small_o = xtn.synth_mutants(seed=5, n=20_000, mutant_frac=0.01)
+    big_c, big_o = xtn.synth_clusters(seed=6, n=20_000, cluster_frac=0.9, dup_frac=0.2)
+    dch, dof = on_device(torch, small_c, small_o, pad=max(0, len(big_c) - len(small_c)))
+    with xtn.Context(0, graph=1) as ctx:
+        for c_, o_ in ((small_c, small_o), (big_c, big_o), (big_c, big_o), (small_c, small_o)):
+            dch[: len(c_)] = torch.from_numpy(c_).cuda()
+            dof.copy_(torch.from_numpy(o_.view(np.int32)).cuda())
+            torch.cuda.synchronize()
+            exp_p, exp_d, _ = orc.nn_search(c_, o_, 2, 0)
+            m = ctx.nn_device(dch.data_ptr(), dof.data_ptr(), len(o_) - 1, 2, 0)
+            got = ctx.fetch(m)
+            assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, "graph form after new contents")
+
+
+def test_graph_form_rejects_bad_lengths():
+    import torch
+
+    chars, offs = xtn.synth_mutants(seed=9, n=5000)
+    dch, dof = on_device(torch, chars, offs)
+    with xtn.Context(0, graph=1) as ctx:
+        ctx.nn_device(dch.data_ptr(), dof.data_ptr(), 5000, 2, 0)  # plain + capture
+        bad = offs.copy()
+        bad[1001] = bad[1000]  # sequence 1000 empty
+        dof.copy_(torch.from_numpy(bad.view(np.int32)).cuda())
+        torch.cuda.synchronize()
+        with pytest.raises(xtn.XtnError, match="sequence 1000 has an invalid length"):
+            ctx.nn_device(dch.data_ptr(), dof.data_ptr(), 5000, 2, 0)
+        dof.copy_(torch.from_numpy(offs.view(np.int32)).cuda())
+        torch.cuda.synchronize()
+        m = ctx.nn_device(dch.data_ptr(), dof.data_ptr(), 5000, 2, 0)
+        exp_p, exp_d, _ = orc.nn_search(chars, offs, 2, 0)
+        got = ctx.fetch(m)
+        assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, "graph form after a rejected input")

@@ -309,8 +309,10 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
     int tile, int d, int b1, int idbits, const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart,
-    uint32_t b_lo, uint32_t b_n, uint64_t round_base, uint64_t* __restrict__ recs) {
+    uint32_t b_lo, uint32_t b_n, uint64_t round_base, uint64_t* __restrict__ recs,
+    const unsigned int* __restrict__ abort) {
     constexpr int T = C::kThreads, kFanPer = C::kFanPer;
+    if (abort && *abort) return;  // graph form: the records would not fit their buffer
     constexpr uint64_t kSpan = (uint64_t)(C::kChunk - kMaxVariantsD2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem<C>& S = *reinterpret_cast<ScatterSmem<C>*>(smem_raw);
@@ -421,7 +423,9 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* _
                                                                    int b1, int idbits, const uint32_t* __restrict__ offsets,
                                                                    const uint64_t* __restrict__ bstart, uint32_t b_lo,
                                                                    uint32_t b_n, uint64_t round_base,
-                                                                   uint64_t* __restrict__ recs) {
+                                                                   uint64_t* __restrict__ recs,
+                                                                   const unsigned int* __restrict__ abort) {
+    if (abort && *abort) return;
     extern __shared__ uint32_t s_cur[];
     const int nb = 1 << b1;
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
@@ -465,11 +469,13 @@ __device__ __forceinline__ void bounded_append(T* __restrict__ list, uint32_t ca
 // Sorts buckets into "group directly" descriptors and split jobs.
 // bstart points at the round's first bucket; `base` is that bucket's global start, so the
 // descriptors hold positions in the round's record buffer.
+// abort (graph form, may be null): when set, nothing is listed, so the split and grouping that
+// follow have no work.
 __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint64_t base, uint32_t group_cap,
                               BucketDesc* __restrict__ desc, uint32_t desc_cap, SplitJob* __restrict__ jobs,
-                              unsigned int* __restrict__ counters) {
+                              unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+    if (b >= nb || (abort && *abort)) return;
     uint64_t s = bstart[b] - base, e = bstart[b + 1] - base;
     uint32_t size = (uint32_t)(e - s);
     if (size < 2) return;
@@ -679,6 +685,12 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 //      over its threads. Entries at or past `cap` are counted but not written, so the caller
 //      can grow the buffer to the exact size and run again.
 // A bucket with more than kMaxRuns runs is appended to `overflow` (grouped later by sorting).
+// With n_desc null, CTA i groups descriptor i (the grid has one CTA per descriptor). Otherwise
+// the CTAs are persistent: they take descriptors from a queue (counters[kCntNext]) until the
+// device-side count *n_desc (at most overflow_cap) is reached, so the grid needs no host-side
+// count (the graph form).
+constexpr int kCntNext = 7;  // the persistent grouping's queue position
+
 __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketDesc* __restrict__ descs,
                                                                      const uint64_t* __restrict__ buf_a,
                                                                      const uint64_t* __restrict__ buf_b, int idbits,
@@ -687,10 +699,24 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
                                                                      unsigned int* __restrict__ errors, int use_tma,
                                                                      BucketDesc* __restrict__ overflow,
                                                                      uint32_t overflow_cap,
-                                                                     unsigned int* __restrict__ counters) {
+                                                                     unsigned int* __restrict__ counters,
+                                                                     const unsigned int* __restrict__ n_desc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem& S = *reinterpret_cast<GroupSmem*>(smem_raw);
-    const BucketDesc bd = descs[blockIdx.x];
+    const uint32_t mbar = smem_u32(&S.mbar);
+    if (use_tma && threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const uint32_t count = n_desc ? min(*n_desc, overflow_cap) : gridDim.x;
+    uint32_t phase = 0;
+    for (uint32_t iter = 0;; iter++, phase ^= 1u) {
+    __syncthreads();  // the previous descriptor is done with the shared memory
+    if (threadIdx.x == 0) S.n_cand = n_desc ? atomicAdd(&counters[kCntNext], 1u) : (iter == 0 ? blockIdx.x : count);
+    __syncthreads();
+    const uint32_t di = S.n_cand;
+    if (di >= count) return;
+    const BucketDesc bd = descs[di];
     const uint32_t n = bd.size;
     const uint64_t* src = (bd.src ? buf_b : buf_a) + bd.start;
     // The bucket goes to shared memory either by one TMA bulk copy (use_tma) or by plain
@@ -700,12 +726,9 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     const uint32_t lead = (uint32_t)(((uintptr_t)src & 15u) >> 3);
     const uint64_t* src16 = src - lead;
     const uint32_t bytes = ((lead + n) * 8u + 15u) & ~15u;
-    const uint32_t mbar = smem_u32(&S.mbar);
     if (threadIdx.x == 0) S.wait_failed = 0;
     if (use_tma) {
         if (threadIdx.x == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
             asm volatile(
@@ -727,7 +750,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     if (use_tma && threadIdx.x == 0) {
         // one thread polls the barrier (sleeping between polls); the others wait at __syncthreads
         uint32_t polls = 0;
-        while (!mbar_try_wait(mbar, 0)) {
+        while (!mbar_try_wait(mbar, phase)) {
             if (++polls > kWaitLimit) {
                 S.wait_failed = 1;
                 break;
@@ -740,7 +763,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         // one more bounded wait for the copy to land before the shared memory is released
         if (threadIdx.x == 0) {
             uint32_t polls = 0;
-            while (!mbar_try_wait(mbar, 0) && ++polls < kWaitLimit) __nanosleep(64);
+            while (!mbar_try_wait(mbar, phase) && ++polls < kWaitLimit) __nanosleep(64);
             atomicAdd(errors, 1u);
         }
         __syncthreads();
@@ -755,7 +778,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         const uint32_t bit = 1u << (b & 31);
         if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
     }
-    if (threadIdx.x == 0) S.n_cand = 0;
+    if (threadIdx.x == 0) S.n_cand = 0;  // (read as the descriptor index before the first barrier)
     __syncthreads();
     // candidates in any order (one shared atomic per warp and round)
     const unsigned lane = threadIdx.x & 31u;
@@ -835,7 +858,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     uint32_t pair_off = block_scan_ex<uint32_t, kGroupThreads>(my_pairs, &total, S.warp_sums);
     if (nr > (uint32_t)kMaxRuns) {  // too many runs to list: the bucket is regrouped by sorting
         if (threadIdx.x == 0) bounded_append(overflow, overflow_cap, counters, kCntFallback, bd);
-        return;
+        continue;
     }
     for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {  // the same slots as above
         const uint32_t word = S.cand[i];
@@ -890,6 +913,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
         if (q < cap)
             pairs[q] = pack_pair(rec[S.u.gr.perm[pi]] & idmask, rec[S.u.gr.perm[pj]] & idmask, idbits);
     }
+    }  // descriptors
 }
 
 }  // namespace xtn

@@ -271,46 +271,52 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
                                                          unsigned long long* __restrict__ table, uint64_t tmask,
                                                          uint64_t tag, uint64_t* __restrict__ uniq,
                                                          unsigned long long* __restrict__ n_uniq,
-                                                         unsigned long long* __restrict__ n_full) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                                                         unsigned long long* __restrict__ n_full,
+                                                         const unsigned long long* __restrict__ P_dev) {
+    // P_dev (graph form): the count is read on the device (at most P) and the grid strides
+    if (P_dev) P = (int64_t)min((unsigned long long)P, *P_dev);
     const unsigned lane = threadIdx.x & 31u;
-    bool fresh = false;
-    uint64_t p = 0;
-    if (i < P) {
-        p = pairs[i];
-        const uint64_t idmask = (1ull << idbits) - 1ull;
-        if ((p >> idbits) != (p & idmask)) {
-            const unsigned long long want = tag | p;
-            uint64_t h = mix64(p) & tmask;
-            unsigned long long v = ld_relaxed_u64(table + h);
-            for (uint32_t probes = 0;;) {
-                if ((v & kDedupTagMask) != tag) {  // free in this search
-                    const unsigned long long old = atomicCAS(table + h, v, want);
-                    if (old == v) {
-                        fresh = true;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t w0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < P; w0 += stride) {
+        const int64_t i = w0 + lane;
+        bool fresh = false;
+        uint64_t p = 0;
+        if (i < P) {
+            p = pairs[i];
+            const uint64_t idmask = (1ull << idbits) - 1ull;
+            if ((p >> idbits) != (p & idmask)) {
+                const unsigned long long want = tag | p;
+                uint64_t h = mix64(p) & tmask;
+                unsigned long long v = ld_relaxed_u64(table + h);
+                for (uint32_t probes = 0;;) {
+                    if ((v & kDedupTagMask) != tag) {  // free in this search
+                        const unsigned long long old = atomicCAS(table + h, v, want);
+                        if (old == v) {
+                            fresh = true;
+                            break;
+                        }
+                        v = old;  // taken meanwhile: it now holds a pair of this search
+                        continue;
+                    }
+                    if (v == want) break;  // a repeat
+                    h = (h + 1) & tmask;
+                    if (++probes > kDedupMaxProbes) {  // table too full: the host reruns with a larger one
+                        atomicAdd(n_full, 1ull);
                         break;
                     }
-                    v = old;  // taken meanwhile: it now holds a pair of this search
-                    continue;
+                    v = ld_relaxed_u64(table + h);
                 }
-                if (v == want) break;  // a repeat
-                h = (h + 1) & tmask;
-                if (++probes > kDedupMaxProbes) {  // table too full: the host reruns with a larger one
-                    atomicAdd(n_full, 1ull);
-                    break;
-                }
-                v = ld_relaxed_u64(table + h);
             }
         }
+        if (uniq == nullptr) continue;
+        const unsigned mask = __ballot_sync(0xffffffffu, fresh);
+        if (mask == 0u) continue;
+        unsigned long long base = 0;
+        const int leader = __ffs(mask) - 1;
+        if ((int)lane == leader) base = atomicAdd(n_uniq, (unsigned long long)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (fresh) uniq[base + __popc(mask & ((1u << lane) - 1u))] = p;
     }
-    if (uniq == nullptr) return;
-    const unsigned mask = __ballot_sync(0xffffffffu, fresh);
-    if (mask == 0u) return;
-    unsigned long long base = 0;
-    const int leader = __ffs(mask) - 1;
-    if ((int)lane == leader) base = atomicAdd(n_uniq, (unsigned long long)__popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (fresh) uniq[base + __popc(mask & ((1u << lane) - 1u))] = p;
 }
 
 // Verification of the sorted candidate pairs. Only the first of each run of equal pairs, with
@@ -323,9 +329,11 @@ constexpr int kVerifyWarps = kThreads / 32;
 __global__ void __launch_bounds__(kThreads) k_verify(const uint64_t* __restrict__ pairs, int64_t P, int idbits,
                                                      const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
                                                      const int32_t* __restrict__ rows, int d, int measure,
-                                                     int8_t* __restrict__ dist, uint8_t* __restrict__ flag) {
+                                                     int8_t* __restrict__ dist, uint8_t* __restrict__ flag,
+                                                     const unsigned long long* __restrict__ P_dev) {
     __shared__ uint64_t s_pair[kVerifyWarps][32 * kVerifyPer];
     __shared__ uint8_t s_slot[kVerifyWarps][32 * kVerifyPer];
+    if (P_dev) P = (int64_t)min((unsigned long long)P, *P_dev);  // graph form: grid sized for P at most
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = ((int64_t)blockIdx.x * kVerifyWarps + warp) * (32 * kVerifyPer);
     if (base >= P) return;  // whole warp
@@ -370,7 +378,8 @@ __global__ void __launch_bounds__(kThreads) k_verify(const uint64_t* __restrict_
 
 __global__ void k_compact(const uint64_t* __restrict__ pairs, int64_t P, int idbits, const int8_t* __restrict__ dist,
                           const uint8_t* __restrict__ flag, const uint32_t* __restrict__ pos, xtn_int2* __restrict__ out,
-                          int8_t* __restrict__ out_dist) {
+                          int8_t* __restrict__ out_dist, const unsigned long long* __restrict__ P_dev) {
+    if (P_dev) P = (int64_t)min((unsigned long long)P, *P_dev);
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P || !flag[i]) return;
     uint64_t p = pairs[i];
@@ -472,6 +481,9 @@ struct xtn_context {
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_round[2] = {};
     DevBuf pairA2, ddcnt;
+    // graph form of the device-resident search (option "graph")
+    int graph_mode = 0;
+    void* graph = nullptr;  // GraphState (below)
     // results
     DevBuf out_pairs, out_dist, out_freq;
     uint64_t* h_scalar = nullptr;  // pinned
@@ -743,8 +755,8 @@ constexpr int kDirectBucketBitsMax = 14;
 // The first-level plan: count pass over every variant (per-tile histograms of the top b1 hash
 // bits), per-tile offsets inside each bucket, bucket starts (c->bstart, nb + 1 entries) and, for
 // the staged scatter at d = 2, the balanced task map.
-static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
-    cudaStream_t s = c->stream;
+// The first-level shape for n sequences and V variant records (no device work).
+static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
     const bool small = c->stage_chunk == 2048;
     const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
     const bool tables = d <= 2 && c->key_tables;
@@ -757,19 +769,37 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
                                                        : ctas_per_sm_for<ScatterSmem<StageLarge>>());
     const int64_t wave = (int64_t)c->sms * per_sm;
     const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
-    const int tile = (n + ntiles - 1) / ntiles;
     bp->b1 = b1;
     bp->nb = nb;
     bp->ntiles = ntiles;
-    bp->tile = tile;
+    bp->tile = (n + ntiles - 1) / ntiles;
     bp->small = small;
     bp->staged = tables && nb <= stage_fan;
     bp->tseq = nullptr;
+}
+
+// Reserves the buffers bucket_prepare uses for this shape.
+static int bucket_reserve(xtn_context* c, const BucketPlan& bp, int n, int d, uint64_t V) {
+    XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)bp.ntiles * bp.nb));
+    XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)bp.ntiles * bp.nb));
+    XTN_TRY(ensure(c->btotals, sizeof(uint32_t) * (bp.nb + 1)));
+    XTN_TRY(ensure(c->bstart, sizeof(uint64_t) * (bp.nb + 1)));
+    if (bp.staged && d >= 2) {
+        XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
+        XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
+        // a sequence has at most kKeyLen runs, so at most kKeyLen tasks
+        XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * std::min<uint64_t>(V, (uint64_t)kKeyLen * n) + 16));
+    }
+    return XTN_SUCCESS;
+}
+
+static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
+    cudaStream_t s = c->stream;
+    bucket_shape(c, n, d, V, bp);
+    const int b1 = bp->b1, nb = bp->nb, ntiles = bp->ntiles, tile = bp->tile;
+    const bool tables = d <= 2 && c->key_tables;
     const size_t hist_smem = sizeof(uint32_t) * nb;
-    XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)ntiles * nb));
-    XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)ntiles * nb));
-    XTN_TRY(ensure(c->btotals, sizeof(uint32_t) * (nb + 1)));
-    XTN_TRY(ensure(c->bstart, sizeof(uint64_t) * (nb + 1)));
+    XTN_TRY(bucket_reserve(c, *bp, n, d, V));
     XTN_TRY(bucket_attrs(c));
     XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                    P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
@@ -778,13 +808,9 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
     if (bp->staged && d >= 2) {
-        XTN_TRY(ensure(c->tcnt, sizeof(uint32_t) * n));
-        XTN_TRY(ensure(c->toff, sizeof(uint64_t) * (n + 1)));
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
                                                                                    P<uint32_t>(c->tcnt)));
         XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
-        // a sequence has at most kKeyLen runs, so at most kKeyLen tasks
-        XTN_TRY(ensure(c->tseq, sizeof(uint32_t) * std::min<uint64_t>(V, (uint64_t)kKeyLen * n) + 16));
         XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->toff), n,
                                                                              P<uint32_t>(c->tseq)));
         bp->tseq = P<uint32_t>(c->tseq);
@@ -811,17 +837,18 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
                        k_bucket_scatter_staged<StageSmall><<<bp.ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
                            P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           b_lo, b_n, base, P<uint64_t>(c->recA)));
+                           b_lo, b_n, base, P<uint64_t>(c->recA), nullptr));
         else
             XTN_LAUNCH("bucket_scatter",
                        k_bucket_scatter_staged<StageLarge><<<bp.ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
                            P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
                            P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           b_lo, b_n, base, P<uint64_t>(c->recA)));
+                           b_lo, b_n, base, P<uint64_t>(c->recA), nullptr));
     } else {
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, bp.tile, d, b1, idbits,
-                                         P<uint32_t>(c->boffs), bstart, b_lo, b_n, base, P<uint64_t>(c->recA)));
+                                         P<uint32_t>(c->boffs), bstart, b_lo, b_n, base, P<uint64_t>(c->recA),
+                                         nullptr));
     }
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
@@ -835,7 +862,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(b_n), kThreads, 0, s>>>(
                                   bstart + b_lo, (int)b_n, base, c->group_cap, P<BucketDesc>(c->bdesc),
-                                  (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt)));
+                                  (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), nullptr));
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
@@ -892,7 +919,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
                                            P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
                                            P<uint64_t>(out), cap, P<unsigned long long>(c->counter),
                                            P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
-                                           (uint32_t)desc_cap, P<unsigned int>(c->bcnt)));
+                                           (uint32_t)desc_cap, P<unsigned int>(c->bcnt), nullptr));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
@@ -961,7 +988,8 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
         XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
                                      P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table),
                                      T - 1, (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB),
-                                     P<unsigned long long>(c->counter), P<unsigned long long>(c->counter) + 1));
+                                     P<unsigned long long>(c->counter), P<unsigned long long>(c->counter) + 1,
+                                     nullptr));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1106,7 +1134,7 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
             XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc_r[slot]), kThreads, 0, sd>>>(
                                          P<uint64_t>(*cand[slot]), (int64_t)Pc_r[slot], idbits,
                                          P<unsigned long long>(c->dd_table), T - 1, tag, P<uint64_t>(c->pairB), n_uniq,
-                                         n_uniq + 1));
+                                         n_uniq + 1, nullptr));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 8, c->ddcnt.p, 16, cudaMemcpyDeviceToHost, sd));
         return XTN_SUCCESS;
@@ -1131,7 +1159,7 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
                 XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)U_before[slot]), kThreads, 0, sd>>>(
                                              P<uint64_t>(c->pairB), (int64_t)U_before[slot], idbits,
                                              P<unsigned long long>(c->dd_table), T - 1, tag, nullptr, n_uniq,
-                                             n_uniq + 1));
+                                             n_uniq + 1, nullptr));
             XTN_TRY(launch_dedup(slot));
         }
     };
@@ -1281,7 +1309,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     uint64_t nout = 0;
     if (Pc > 0) {
         XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
-                                                              P<int8_t>(c->dist), P<uint8_t>(c->flag)));
+                                                              P<int8_t>(c->dist), P<uint8_t>(c->flag), nullptr));
         XTN_CK(cudaGetLastError());
         XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc)));
         XTN_CK(cudaEventRecord(c->ev[7], s));
@@ -1291,7 +1319,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         XTN_TRY(ensure(c->out_dist, (size_t)Pc));
         XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, P<int8_t>(c->dist),
                                                                P<uint8_t>(c->flag), P<uint32_t>(c->fpos),
-                                                               P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist)));
+                                                               P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist), nullptr));
         c->h_scalar[6] = 0;
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 6, P<uint32_t>(c->fpos) + Pc, 4, cudaMemcpyDeviceToHost, s));
     } else {
@@ -1319,6 +1347,325 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     }
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[S_COUNT]);
     st.ms_total = ms;
+    return XTN_SUCCESS;
+}
+
+// ------------------------------------------------------------------ graph form
+// The batched/persistent form of a search on device-resident inputs: the whole single-round
+// launch sequence (length check, pack, variant offsets, count, scatter, plan, split, grouping
+// by persistent CTAs that take bucket descriptors from a device-side queue, candidate-pair
+// dedup, sort, verification, compaction) is captured once into a CUDA graph and replayed, with
+// every data-dependent size read on the device. Buffers are sized from the previous plain
+// search on the same input with headroom; the host reads one status block per replay. A replay
+// that outgrows a capacity, meets a bucket too large for shared memory or a hash set too full,
+// is redone by the plain form, which also re-sizes the graph. The plain form
+// (run_nn) waits for the device four times per search to size its buffers and grids.
+struct GraphState {
+    const uint8_t* chars = nullptr;
+    const uint32_t* offs = nullptr;
+    int n = 0, d = 0, measure = 0;
+    int64_t sig = 0;                 // options the capture depends on
+    uint64_t Vcap = 0, Pcap = 0, Ucap = 0, T = 0;
+    int b1 = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t* result = nullptr;      // where the sorted distinct pairs end (pairB or pairA)
+    int64_t launches = 0;
+    DevBuf status, table, os_status;
+    uint32_t os_epoch = 0;
+};
+
+// Status block of one replay (device words, copied to the pinned host scalars 16..31).
+enum {
+    GS_V, GS_ABORT, GS_LENBAD, GS_CAND, GS_GROUP_ERR, GS_SPLIT_ERR, GS_DROPPED, GS_FALLBACK, GS_UNIQUE,
+    GS_FULL, GS_LOOKBACK_ERR, GS_OUT, GS_NDESC, GS_WORDS
+};
+
+// Sets the abort word when the variant records exceed their capacity or a length is invalid.
+__global__ void k_graph_guard(const uint64_t* __restrict__ V, uint64_t Vcap, const unsigned int* __restrict__ lenbad,
+                              unsigned int* __restrict__ abort) {
+    *abort = (*V > Vcap || *lenbad != 0xffffffffu) ? 1u : 0u;
+}
+
+__global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned int* __restrict__ abort,
+                               const unsigned int* __restrict__ lenbad, const unsigned long long* __restrict__ cursor,
+                               const unsigned int* __restrict__ bcnt, const unsigned long long* __restrict__ ddcnt,
+                               const unsigned int* __restrict__ dev_err, const uint32_t* __restrict__ fpos,
+                               uint64_t Ucap, uint64_t* __restrict__ st) {
+    const unsigned long long U = ddcnt[0];
+    st[GS_V] = *V;
+    st[GS_ABORT] = *abort;
+    st[GS_LENBAD] = *lenbad;
+    st[GS_CAND] = cursor[0];
+    st[GS_GROUP_ERR] = reinterpret_cast<const unsigned int*>(cursor)[2];
+    st[GS_SPLIT_ERR] = bcnt[kCntWaitFail];
+    st[GS_DROPPED] = bcnt[kCntDropped];
+    st[GS_FALLBACK] = bcnt[kCntFallback];
+    st[GS_UNIQUE] = U;
+    st[GS_FULL] = ddcnt[1];
+    st[GS_LOOKBACK_ERR] = dev_err ? *dev_err : 0u;
+    st[GS_OUT] = fpos[U < Ucap ? U : Ucap];
+    st[GS_NDESC] = bcnt[kCntDesc];
+}
+
+static int64_t graph_signature(const xtn_context* c) {
+    return ((int64_t)c->stage_chunk << 40) ^ ((int64_t)c->split_chunk << 28) ^ ((int64_t)c->bucket_bits_max << 20) ^
+           ((int64_t)c->group_cap << 4) ^ ((int64_t)c->group_tma << 1) ^ ((int64_t)c->key_tables << 2) ^
+           ((int64_t)c->split_slices << 16) ^ ((int64_t)c->scatter_ctas_per_sm << 48) ^ ((int64_t)c->pair_dedup << 52);
+}
+
+static void graph_release(GraphState* g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->exec = nullptr;
+    g->graph = nullptr;
+}
+
+// Enqueues the whole search for the capacities in g (no host waits, no allocations: every
+// buffer is reserved beforehand).
+static int graph_enqueue(xtn_context* c, GraphState* g) {
+    cudaStream_t s = c->stream;
+    const int n = g->n, d = g->d;
+    const int idbits = id_bits_for(n);
+    const bool tables = d <= 2 && c->key_tables;
+    unsigned int* abort = P<unsigned int>(c->lencheck) + 1;
+    XTN_CK(cudaMemsetAsync(c->lencheck.p, 0xff, 4, s));
+    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, s>>>(g->offs, nullptr, n,
+                                                                                    P<unsigned int>(c->lencheck)));
+    XTN_LAUNCH("pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(
+                           g->chars, g->offs, nullptr, n, d, P<u128>(c->keys), P<uint8_t>(c->klen), P<uint32_t>(c->vcnt),
+                           P<uint64_t>(c->runinfo), tables ? P<uint64_t>(c->ktab) : nullptr));
+    XTN_TRY((scan_1p<uint32_t, uint64_t>(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n)));
+    XTN_LAUNCH("graph_guard", k_graph_guard<<<1, 1, 0, s>>>(P<uint64_t>(c->voff) + n, g->Vcap,
+                                                            P<unsigned int>(c->lencheck), abort));
+    BucketPlan bp;
+    XTN_TRY(bucket_prepare(c, n, d, g->Vcap, &bp));
+    if (bp.b1 != g->b1) {
+        set_err("graph capture: first-level bucket bits changed");
+        return XTN_ERR_CUDA;
+    }
+    const int nb = bp.nb;
+    const uint64_t* bstart = P<uint64_t>(c->bstart);
+    if (bp.staged) {
+        if (bp.small)
+            XTN_LAUNCH("bucket_scatter",
+                       k_bucket_scatter_staged<StageSmall><<<bp.ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
+                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
+                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, bp.b1, idbits, P<uint32_t>(c->boffs), bstart,
+                           0u, (uint32_t)nb, 0ull, P<uint64_t>(c->recA), abort));
+        else
+            XTN_LAUNCH("bucket_scatter",
+                       k_bucket_scatter_staged<StageLarge><<<bp.ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
+                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
+                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, bp.b1, idbits, P<uint32_t>(c->boffs), bstart,
+                           0u, (uint32_t)nb, 0ull, P<uint64_t>(c->recA), abort));
+    } else {
+        XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
+                                         P<u128>(c->keys), P<uint8_t>(c->klen), n, bp.tile, d, bp.b1, idbits,
+                                         P<uint32_t>(c->boffs), bstart, 0u, (uint32_t)nb, 0ull, P<uint64_t>(c->recA),
+                                         abort));
+    }
+    const size_t desc_cap = (size_t)nb * 3 + 4 * g->Vcap / c->group_cap + 2048;
+    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
+    XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
+                                  bstart, nb, 0ull, c->group_cap, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
+                                  P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
+    {
+        const bool sliced = c->split_slices > 1;
+        const unsigned grid = (unsigned)nb * (sliced ? kSplitSlices : 1);
+#define XTN_SPLIT(CFG, SL)                                                                                         \
+    XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
+                                   P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
+                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,        \
+                                   P<unsigned int>(c->bcnt)))
+        if (c->split_chunk == 2048) {
+            if (sliced) XTN_SPLIT(SplitSmall, kSplitSlices);
+            else XTN_SPLIT(SplitSmall, 1);
+        } else {
+            if (sliced) XTN_SPLIT(StageLarge, kSplitSlices);
+            else XTN_SPLIT(StageLarge, 1);
+        }
+#undef XTN_SPLIT
+    }
+    XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
+    XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
+    XTN_LAUNCH("bucket_group", k_bucket_group<<<(unsigned)c->sms * 3, kGroupThreads, sizeof(GroupSmem), s>>>(
+                                   P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
+                                   P<uint64_t>(c->pairA), g->Pcap, P<unsigned long long>(c->counter),
+                                   P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
+                                   (uint32_t)desc_cap, P<unsigned int>(c->bcnt), P<unsigned int>(c->bcnt) + kCntDesc));
+    // candidate pairs -> distinct pairs (the table is cleared every replay: a fixed epoch)
+    unsigned long long* ddcnt = P<unsigned long long>(c->ddcnt);
+    XTN_CK(cudaMemsetAsync(c->ddcnt.p, 0, 16, s));
+    XTN_CK(cudaMemsetAsync(g->table.p, 0, sizeof(uint64_t) * g->T, s));
+    XTN_LAUNCH("pair_dedup", k_pair_dedup<<<(unsigned)std::min<int64_t>(blocks_for((int64_t)g->Pcap), (int64_t)c->sms * 16),
+                                            kThreads, 0, s>>>(
+                                 P<uint64_t>(c->pairA), (int64_t)g->Pcap, idbits, P<unsigned long long>(g->table), g->T - 1,
+                                 1ull << kDedupKeyBits, P<uint64_t>(c->pairB), ddcnt, ddcnt + 1,
+                                 P<unsigned long long>(c->counter)));
+    uint64_t* pairs = P<uint64_t>(c->pairB);
+    pairs = onesweep_sort_u64(P<uint64_t>(c->pairB), P<uint64_t>(c->pairA), (int64_t)g->Ucap, 0, 2 * idbits,
+                              P<uint32_t>(c->os_scratch), P<unsigned long long>(g->os_status),
+                              (int64_t)(g->os_status.cap / 8), &g->os_epoch, P<unsigned int>(c->dev_err), c->sms, s,
+                              "pair_sort_hist", "pair_sort_pass", ddcnt);
+    g->result = pairs;
+    XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)g->Ucap, kThreads * kVerifyPer), kThreads, 0, s>>>(
+                             pairs, (int64_t)g->Ucap, idbits, g->chars, g->offs, nullptr, d, g->measure,
+                             P<int8_t>(c->dist), P<uint8_t>(c->flag), ddcnt));
+    scan_exclusive_1p<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)g->Ucap,
+                                         P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err), s,
+                                         c->wait_polls, 0, ddcnt);
+    XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)g->Ucap), kThreads, 0, s>>>(
+                              pairs, (int64_t)g->Ucap, idbits, P<int8_t>(c->dist), P<uint8_t>(c->flag),
+                              P<uint32_t>(c->fpos), P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist), ddcnt));
+    XTN_LAUNCH("graph_status", k_graph_status<<<1, 1, 0, s>>>(
+                                   P<uint64_t>(c->voff) + n, abort, P<unsigned int>(c->lencheck),
+                                   P<unsigned long long>(c->counter), P<unsigned int>(c->bcnt), ddcnt,
+                                   P<unsigned int>(c->dev_err), P<uint32_t>(c->fpos), g->Ucap, P<uint64_t>(g->status)));
+    XTN_CK(cudaMemcpyAsync(c->h_scalar + 16, g->status.p, sizeof(uint64_t) * GS_WORDS, cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaGetLastError());
+    return XTN_SUCCESS;
+}
+
+// Capacities from the plain search just run on this input, buffers reserved, graph captured.
+static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, const uint32_t* offs, int n, int d,
+                       int measure) {
+    graph_release(g);
+    const xtn_stats& st = c->stats;
+    if (c->engine != 0 || st.n_rounds != 1 || !c->pair_dedup || 2 * id_bits_for(n) > kDedupKeyBits) return XTN_ERR_LIMIT;
+    g->chars = chars;
+    g->offs = offs;
+    g->n = n;
+    g->d = d;
+    g->measure = measure;
+    g->sig = graph_signature(c);
+    const uint64_t V = (uint64_t)st.n_variants, Pc = (uint64_t)st.n_candidates;
+    const uint64_t U = st.n_unique > 0 ? (uint64_t)st.n_unique : Pc;
+    g->Vcap = V + V / 32 + 4096;
+    g->Pcap = Pc + Pc / 8 + 65536;
+    g->Ucap = std::min<uint64_t>(g->Pcap, U + U / 4 + 65536);
+    if (g->Ucap > (uint64_t)kOsMaxKeys || g->Vcap >= (uint64_t)UINT32_MAX || g->Pcap >= (uint64_t)UINT32_MAX)
+        return XTN_ERR_LIMIT;
+    g->T = pow2_at_least(2 * g->Ucap);
+    // the first-level shape the capacity implies, and every buffer reserved (the capture must
+    // not allocate)
+    BucketPlan bp;
+    bucket_shape(c, n, d, g->Vcap, &bp);
+    g->b1 = bp.b1;
+    XTN_TRY(bucket_reserve(c, bp, n, d, g->Vcap));
+    const int nb = bp.nb;
+    const size_t desc_cap = (size_t)nb * 3 + 4 * g->Vcap / c->group_cap + 2048;
+    XTN_TRY(ensure(c->lencheck, 16));
+    XTN_TRY(ensure(c->recA, sizeof(uint64_t) * g->Vcap + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * g->Vcap + 64));
+    XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
+    XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
+    XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * nb));
+    XTN_TRY(ensure(c->bcnt, 64));
+    XTN_TRY(ensure(c->counter, 64));
+    XTN_TRY(ensure(c->ddcnt, 64));
+    XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * g->Pcap + 64));
+    XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * g->Pcap + 64));
+    XTN_TRY(ensure(c->dist, (size_t)g->Ucap + 64));
+    XTN_TRY(ensure(c->flag, (size_t)g->Ucap + 64));
+    XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (g->Ucap + 1)));
+    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * g->Ucap + 64));
+    XTN_TRY(ensure(c->out_dist, (size_t)g->Ucap + 64));
+    XTN_TRY(ensure(c->os_scratch, sizeof(uint32_t) * kOsScratchWords));
+    XTN_TRY(ensure_err_word(c));
+    XTN_TRY(ensure(c->scan_status, sizeof(unsigned long long) * scan_1p_words((int64_t)std::max<uint64_t>(g->Ucap, n))));
+    XTN_TRY(ensure(g->status, sizeof(uint64_t) * GS_WORDS));
+    XTN_TRY(ensure(g->table, sizeof(uint64_t) * g->T));
+    XTN_TRY(ensure(g->os_status, sizeof(unsigned long long) * (size_t)onesweep_status_words((int64_t)g->Ucap)));
+    XTN_TRY(bucket_attrs(c));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    // capture (launches counted, no per-launch events)
+    KernelProfiler counting;
+    KernelProfiler* saved = current_profiler();
+    current_profiler() = &counting;
+    XTN_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int r = graph_enqueue(c, g);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    current_profiler() = saved;
+    if (r != XTN_SUCCESS || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (r == XTN_SUCCESS) set_err(std::string("graph capture failed: ") + cudaGetErrorString(e));
+        return r != XTN_SUCCESS ? r : XTN_ERR_CUDA;
+    }
+    g->graph = graph;
+    g->launches = counting.launches;
+    XTN_CK(cudaGraphInstantiate(&g->exec, graph, 0));
+    return XTN_SUCCESS;
+}
+
+// One search by the graph form; *redo is set when the plain form has to run instead.
+static int graph_replay(xtn_context* c, GraphState* g, bool* redo) {
+    cudaStream_t s = c->stream;
+    xtn_stats& st = c->stats;
+    memset(&st, 0, sizeof st);
+    st.n_seqs = g->n;
+    st.n_rounds = 1;
+    st.id_bits = id_bits_for(g->n);
+    XTN_CK(cudaEventRecord(c->ev[0], s));
+    XTN_CK(cudaGraphLaunch(g->exec, s));
+    XTN_CK(cudaEventRecord(c->ev[8], s));
+    XTN_CK(cudaStreamSynchronize(s));
+    const uint64_t* h = c->h_scalar + 16;
+    *redo = false;
+    if ((uint32_t)h[GS_LENBAD] != 0xffffffffu) return length_check_result(c, (uint32_t)h[GS_LENBAD]);
+    if (h[GS_GROUP_ERR] || h[GS_SPLIT_ERR] || h[GS_LOOKBACK_ERR]) {
+        XTN_CK(cudaMemsetAsync(c->dev_err.p, 0, 16, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        set_err("graph form: a bounded device wait did not complete in time");
+        return XTN_ERR_CUDA;
+    }
+    if (h[GS_DROPPED]) {
+        set_err("graph form: descriptors beyond the list capacity");
+        return XTN_ERR_CUDA;
+    }
+    if (h[GS_ABORT] || h[GS_CAND] > g->Pcap || h[GS_FALLBACK] || h[GS_FULL] || h[GS_UNIQUE] > g->Ucap) {
+        *redo = true;  // a capacity or a shared-memory bound was exceeded
+        return XTN_SUCCESS;
+    }
+    st.n_variants = (int64_t)h[GS_V];
+    st.n_groups = (int64_t)h[GS_NDESC];
+    st.n_candidates = (int64_t)h[GS_CAND];
+    st.n_unique = (int64_t)h[GS_UNIQUE];
+    st.n_out = (int64_t)h[GS_OUT];
+    st.n_launches = g->launches;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[8]);
+    st.ms_total = ms;
+    c->n_out = st.n_out;
+    c->overlap_result = false;
+    return XTN_SUCCESS;
+}
+
+// The device-resident search in the graph form (option "graph" = 1).
+static int nn_graph(xtn_context* c, const uint8_t* chars, const uint32_t* offs, int n, int d, int measure) {
+    if (!c->graph) c->graph = new GraphState();
+    GraphState* g = static_cast<GraphState*>(c->graph);
+    const bool same = g->exec && g->chars == chars && g->offs == offs && g->n == n && g->d == d &&
+                      g->measure == measure && g->sig == graph_signature(c);
+    if (same) {
+        bool redo = false;
+        XTN_TRY(graph_replay(c, g, &redo));
+        if (!redo) return XTN_SUCCESS;
+    }
+    // the plain form, then a graph sized from it for the next search on this input
+    begin_run(c);
+    int r = run_nn(c, chars, offs, nullptr, n, d, measure, true);
+    end_run(c);
+    if (r != XTN_SUCCESS) return r;
+    const xtn_stats keep = c->stats;
+    const int64_t keep_out = c->n_out;
+    const int b = graph_build(c, g, chars, offs, n, d, measure);
+    if (b != XTN_SUCCESS && b != XTN_ERR_LIMIT) return b;
+    if (b == XTN_ERR_LIMIT) graph_release(g);  // this input stays in the plain form
+    c->stats = keep;
+    c->n_out = keep_out;
     return XTN_SUCCESS;
 }
 
@@ -1763,7 +2110,7 @@ int xtn_context_create(int device, xtn_context** out) {
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&c->h_scalar, 128) != cudaSuccess) {
+        cudaMallocHost(&c->h_scalar, 256) != cudaSuccess) {
         set_err("stream or pinned scalar allocation failed");
         delete c;
         return XTN_ERR_CUDA;
@@ -1794,6 +2141,14 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
                       &c->ktab,    &c->info,     &c->lencheck, &c->pairA2, &c->ddcnt, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
     for (DevBuf* b : bufs) release(*b);
+    if (c->graph) {
+        GraphState* g = static_cast<GraphState*>(c->graph);
+        graph_release(g);
+        release(g->status);
+        release(g->table);
+        release(g->os_status);
+        delete g;
+    }
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
         DevBuf* obufs[] = {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
@@ -1831,10 +2186,15 @@ int xtn_context_nn_device(xtn_context* c, const xtn_args* args, const char* d_se
     }
     XTN_TRY(check_args(args));
     XTN_CK(cudaSetDevice(c->device));
-    begin_run(c);
-    int r = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance, args->measure,
+    int r;
+    if (c->graph_mode) {
+        r = nn_graph(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n, args->distance, args->measure);
+    } else {
+        begin_run(c);
+        r = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance, args->measure,
                    true);
-    end_run(c);
+        end_run(c);
+    }
     if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
     return r;
 }
@@ -1929,6 +2289,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "memory_budget") && v >= 0) c->memory_budget = v;
     else if (!strcmp(name, "max_round_records") && v >= 0) c->max_round_records = v;
     else if (!strcmp(name, "round_overlap") && (v == 0 || v == 1)) c->round_overlap = (int)v;
+    else if (!strcmp(name, "graph") && (v == 0 || v == 1)) c->graph_mode = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
@@ -2219,7 +2580,8 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
                                                   "pair_sort_upsweep", "pair_sort_downsweep")
                                  : pairA;
         XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars,
-                                                                                    offs, nullptr, d, measure, dist, flag));
+                                                                                    offs, nullptr, d, measure, dist, flag,
+                                                                                    nullptr));
         scan_exclusive<uint8_t, uint32_t>(flag, fpos, (int64_t)Pc, pscratch, s);
         XTN_TRY(read_u64(fpos + Pc, 4, s, &nout));
         if ((int64_t)nout > out_cap) {
@@ -2230,7 +2592,7 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
         if (nout > 0)
             XTN_LAUNCH("compact", k_compact<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits,
                                                                                           dist, flag, fpos, out_pairs,
-                                                                                          out_dist));
+                                                                                          out_dist, nullptr));
     }
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaStreamSynchronize(s));

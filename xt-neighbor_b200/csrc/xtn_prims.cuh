@@ -215,17 +215,25 @@ constexpr uint32_t kScanPollLimit = 1u << 22;
 
 inline int64_t scan_1p_words(int64_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
+// n_dev (graph form, may be null): n is a capacity and the item count is read on the device;
+// tiles past it leave at once (no later tile is real) and the last real tile writes out[n].
 template <typename In, typename Out>
 __global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ in, Out* __restrict__ out, int64_t n,
                                                         unsigned long long* __restrict__ status,
                                                         unsigned int* __restrict__ err, uint32_t poll_limit,
-                                                        int withhold_tile0) {
+                                                        int withhold_tile0, const unsigned long long* __restrict__ n_dev) {
     __shared__ uint32_t s_tile;
     __shared__ Out s_excl;
     unsigned int* ticket = reinterpret_cast<unsigned int*>(status);  // word 0; tiles from word 1
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
+    uint32_t last_tile = gridDim.x - 1;
+    if (n_dev) {
+        n = (int64_t)min((unsigned long long)n, *n_dev);
+        last_tile = n > 0 ? (uint32_t)((n - 1) / kScanTile) : 0u;
+        if (tile > last_tile) return;
+    }
     const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
     Out v[kScanItems];
     Out sum = 0;
@@ -277,14 +285,22 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_1p(const In* __restrict__ i
         if (i < n) out[i] = run;
         run += v[k];
     }
-    if (tile == gridDim.x - 1 && threadIdx.x == 0) out[n] = s_excl + total;
+    if (tile == last_tile && threadIdx.x == 0) out[n] = s_excl + total;
 }
 
 // Exclusive scan of n items into out[0..n), with out[n] = total, in one launch (plus the clear
 // of `status`). Asynchronous on `stream`.
 template <typename In, typename Out>
 void scan_exclusive_1p(const In* in, Out* out, int64_t n, unsigned long long* status, unsigned int* err,
-                       cudaStream_t stream, uint32_t poll_limit = kScanPollLimit, int withhold_tile0 = 0) {
+                       cudaStream_t stream, uint32_t poll_limit = kScanPollLimit, int withhold_tile0 = 0,
+                       const unsigned long long* n_dev = nullptr) {
+    if (n_dev) {  // graph form: always the look-back kernel, sized for n items at most
+        const int64_t tiles = std::max<int64_t>(1, (n + kScanTile - 1) / kScanTile);
+        cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (tiles + 1), stream);
+        XTN_LAUNCH("scan_1p", (k_scan_1p<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(
+                                  in, out, std::max<int64_t>(n, 1), status, err, poll_limit, 0, n_dev)));
+        return;
+    }
     if (n <= 0) {
         cudaMemsetAsync(out, 0, sizeof(Out), stream);
         return;
@@ -296,7 +312,8 @@ void scan_exclusive_1p(const In* in, Out* out, int64_t n, unsigned long long* st
     }
     cudaMemsetAsync(status, 0, sizeof(unsigned long long) * scan_1p_words(n), stream);
     XTN_LAUNCH("scan_1p", (k_scan_1p<In, Out><<<(unsigned)tiles, kScanBlock, 0, stream>>>(in, out, n, status, err,
-                                                                                          poll_limit, withhold_tile0)));
+                                                                                          poll_limit, withhold_tile0,
+                                                                                          nullptr)));
 }
 
 // ------------------------------------------------------------------ LSD radix sort (u64 keys)
@@ -455,9 +472,11 @@ constexpr int kOsScratchWords = kOsStartWords + kOsClearWords;
 __global__ void __launch_bounds__(kSortThreads) k_onesweep_hist(const uint64_t* __restrict__ keys, int64_t n, int lo_bit,
                                                                 int passes, uint32_t* __restrict__ dstart,
                                                                 uint32_t* __restrict__ counts,
-                                                                unsigned int* __restrict__ done) {
+                                                                unsigned int* __restrict__ done,
+                                                                const unsigned long long* __restrict__ n_dev) {
     __shared__ uint32_t h[kOsMaxPasses][kRadix];
     __shared__ int last;
+    if (n_dev) n = (int64_t)min((unsigned long long)n, *n_dev);  // graph form: count on the device
 #pragma unroll
     for (int p = 0; p < kOsMaxPasses; p++) h[p][threadIdx.x] = 0;
     __syncthreads();
@@ -488,7 +507,8 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
                                                                 int64_t n, int shift, const uint32_t* __restrict__ dstart,
                                                                 unsigned long long* __restrict__ status, uint32_t epoch,
                                                                 unsigned int* __restrict__ ticket,
-                                                                unsigned int* __restrict__ err) {
+                                                                unsigned int* __restrict__ err,
+                                                                const unsigned long long* __restrict__ n_dev) {
     __shared__ uint64_t s_keys[kSortTile];
     __shared__ uint32_t s_cnt[kSortWarps][kRadix + 1];
     __shared__ uint32_t s_start[kRadix];
@@ -504,6 +524,12 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
     __syncthreads();
     const uint32_t tile = s_tile;
     const int64_t tile_base = (int64_t)tile * kSortTile;
+    // graph form: the grid covers n keys at most and the count is read on the device; tiles past
+    // it leave before publishing (no later tile is real, so none waits for them)
+    if (n_dev) {
+        n = (int64_t)min((unsigned long long)n, *n_dev);
+        if (tile_base >= n) return;
+    }
     const int64_t valid64 = n - tile_base;
     const int valid = valid64 > kSortTile ? kSortTile : (int)valid64;
     const unsigned lt = (1u << lane) - 1u;
@@ -600,10 +626,13 @@ inline int64_t onesweep_status_words(int64_t n) { return radix_tiles(n) * kRadix
 // below *epoch + 1 (zero-filled at allocation); *epoch advances by one per pass, and when it
 // would pass kOsMaxEpoch the whole status array (status_cap words) is cleared and it restarts.
 // *err counts look-back waits that gave up.
+// n_dev (graph form, may be null): n is a capacity, the key count is read on the device, and
+// the status words are cleared by the call (a replayed graph repeats its epochs).
 inline uint64_t* onesweep_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int hi_bit, uint32_t* scratch,
                                    unsigned long long* status, int64_t status_cap, uint32_t* epoch, unsigned int* err,
-                                   int sms, cudaStream_t stream, const char* hist_name, const char* pass_name) {
-    if (n <= 1 || hi_bit <= lo_bit) return keys;
+                                   int sms, cudaStream_t stream, const char* hist_name, const char* pass_name,
+                                   const unsigned long long* n_dev = nullptr) {
+    if ((!n_dev && n <= 1) || hi_bit <= lo_bit) return keys;
     const int passes = (hi_bit - lo_bit + kRadixBits - 1) / kRadixBits;
     const int64_t ntiles = radix_tiles(n);
     uint32_t* dstart = scratch;
@@ -611,20 +640,23 @@ inline uint64_t* onesweep_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int
     unsigned int* tickets = counts + kOsMaxPasses * kRadix;
     unsigned int* done = tickets + kOsMaxPasses;
     cudaMemsetAsync(counts, 0, sizeof(uint32_t) * kOsClearWords, stream);
-    if (*epoch + (uint32_t)passes > kOsMaxEpoch) {
+    if (n_dev) {
+        cudaMemsetAsync(status, 0, sizeof(unsigned long long) * std::min<int64_t>(status_cap, ntiles * kRadix), stream);
+        *epoch = 0;
+    } else if (*epoch + (uint32_t)passes > kOsMaxEpoch) {
         cudaMemsetAsync(status, 0, sizeof(unsigned long long) * status_cap, stream);
         *epoch = 0;
     }
-    const int64_t hist_blocks = std::min<int64_t>((n + kSortTile - 1) / kSortTile, (int64_t)sms * 8);
+    const int64_t hist_blocks = std::max<int64_t>(1, std::min<int64_t>((n + kSortTile - 1) / kSortTile, (int64_t)sms * 8));
     XTN_LAUNCH(hist_name, k_onesweep_hist<<<(unsigned)hist_blocks, kSortThreads, 0, stream>>>(keys, n, lo_bit, passes, dstart,
-                                                                                           counts, done));
+                                                                                           counts, done, n_dev));
     uint64_t* src = keys;
     uint64_t* dst = alt;
     for (int p = 0; p < passes; p++) {
         *epoch += 1;
-        XTN_LAUNCH(pass_name, k_onesweep_pass<<<(unsigned)ntiles, kSortThreads, 0, stream>>>(
+        XTN_LAUNCH(pass_name, k_onesweep_pass<<<(unsigned)std::max<int64_t>(1, ntiles), kSortThreads, 0, stream>>>(
                                   src, dst, n, lo_bit + kRadixBits * p, dstart + p * kRadix, status, *epoch,
-                                  tickets + p, err));
+                                  tickets + p, err, n_dev));
         uint64_t* t = src;
         src = dst;
         dst = t;
