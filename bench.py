@@ -208,68 +208,80 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
     return None
 
 
-def run_serve(args, w):
-    """Serving loop on a resident deletion index (xtn_index_serve): Poisson request arrivals at
-    each rate, request sizes log-uniform in [1, max_size] sequences, d = 1 with probability p_d1
-    else 2, Levenshtein. Latency = completion - arrival of each request (host clock, the
-    request's pairs delivered to the host)."""
+def serve_trace(ix, pool_c, pool_o, w, rate, rng, slots=2):
+    """One Poisson trace against a resident index: `rate` req/s for w["seconds"] seconds,
+    request sizes log-uniform in [1, max_size], d = 1 with probability p_d1 else 2,
+    Levenshtein. Latency = completion - arrival of each request (host clock, the request's
+    pairs delivered to the host)."""
     import numpy as np
-    import torch
+
+    n_pool = len(pool_o) - 1
+    n_req = max(5, int(rate * w["seconds"]))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    sizes = np.minimum(np.exp(rng.uniform(0, np.log(w["max_size"]), n_req)).astype(np.int64), w["max_size"])
+    sizes = np.maximum(sizes, 1)
+    dists = np.where(rng.random(n_req) < w["p_d1"], 1, 2)
+    reqs = []
+    for k in range(n_req):
+        a = int(rng.integers(0, n_pool - sizes[k] + 1))
+        o = (pool_o[a : a + sizes[k] + 1] - pool_o[a]).astype(np.uint32)
+        reqs.append((pool_c[pool_o[a] : pool_o[a + sizes[k]]], o, int(dists[k]), 0, float(arrivals[k])))
+    # warm-up, untimed: the three largest requests of each distance
+    warm = [reqs[k] for dd in (1, 2) for k in np.argsort(-sizes * (dists == dd))[:3]]
+    ix.serve(warm, realtime=False, keep_results=False, slots=slots)
+    stats, _ = ix.serve(reqs, realtime=True, keep_results=False, slots=slots)
+    lat = np.array([(st["done_s"] - t) * 1e3 for st, (_, _, _, _, t) in zip(stats, reqs)])
+    span = max(st["done_s"] for st in stats) - float(arrivals[0])
+    small_d1 = np.array([l for l, (_, o, d, _, _) in zip(lat, reqs) if d == 1 and len(o) - 1 <= 1000])
+    return {
+        "rate_req_per_s": rate,
+        "slots": slots,
+        "requests": n_req,
+        "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "p50_ms_d1": float(np.percentile(lat[dists == 1], 50)),
+        "p99_ms_d1": float(np.percentile(lat[dists == 1], 99)),
+        "p99_ms_d2": float(np.percentile(lat[dists == 2], 99)) if (dists == 2).any() else None,
+        "p99_ms_d1_le_1k_seqs": float(np.percentile(small_d1, 99)) if len(small_d1) else None,
+        "seqs_per_s": float(sizes.sum() / span),
+        "batches": len({st["batch"] for st in stats}),
+        "pairs": int(sum(st["n_out"] for st in stats)),
+        "slowest": [{"seqs": int(sizes[k]), "d": int(dists[k]), "queue_ms": (stats[k]["admitted_s"] - arrivals[k]) * 1e3,
+                     "service_ms": (stats[k]["done_s"] - stats[k]["admitted_s"]) * 1e3, "batch": stats[k]["batch"]}
+                    for k in np.argsort(-lat)[:5]],
+    }
+
+
+def serve_setup(w, device):
+    """The resident index over the first n_index generator rows and the request pool."""
+    import numpy as np
 
     import xtn
+
+    chars, offs = xtn.synth_clusters(w["seed"], w["n_index"] + w["n_pool"], 0.20, 0.02)
+    ni = w["n_index"]
+    t0 = time.perf_counter()
+    ix = xtn.Index(chars[: offs[ni]], offs[: ni + 1], max_distance=2, device=device)
+    build_wall = time.perf_counter() - t0
+    pool_c, pool_o = chars[offs[ni] :], (offs[ni:] - offs[ni]).astype(np.uint32)
+    return ix, pool_c, pool_o, build_wall
+
+
+def run_serve(args, w):
+    """Serving loop on a resident deletion index (xtn_index_serve) at each rate of the workload."""
+    import numpy as np
+    import torch
 
     world, rank, local = dist_setup()
     if rank != 0:
         return None
     torch.cuda.set_device(local)
-    chars, offs = xtn.synth_clusters(w["seed"], w["n_index"] + w["n_pool"], 0.20, 0.02)
-    ni = w["n_index"]
-    t0 = time.perf_counter()
-    ix = xtn.Index(chars[: offs[ni]], offs[: ni + 1], max_distance=2, device=local)
-    build_wall = time.perf_counter() - t0
+    ix, pool_c, pool_o, build_wall = serve_setup(w, local)
     info = ix.info()
-    pool_c, pool_o = chars[offs[ni] :], (offs[ni:] - offs[ni]).astype(np.uint32)
-    n_pool = len(pool_o) - 1
     rng = np.random.default_rng(w["seed"] + 1)
     sampler = ClockSampler(local)
     sampler.start()
-    per_rate = {}
-    total_seqs, total_busy = 0, 0.0
-    for rate in w["rates"]:
-        n_req = max(5, int(rate * w["seconds"]))
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-        sizes = np.minimum(np.exp(rng.uniform(0, np.log(w["max_size"]), n_req)).astype(np.int64), w["max_size"])
-        sizes = np.maximum(sizes, 1)
-        dists = np.where(rng.random(n_req) < w["p_d1"], 1, 2)
-        reqs = []
-        for k in range(n_req):
-            a = int(rng.integers(0, n_pool - sizes[k] + 1))
-            o = (pool_o[a : a + sizes[k] + 1] - pool_o[a]).astype(np.uint32)
-            reqs.append((pool_c[pool_o[a] : pool_o[a + sizes[k]]], o, int(dists[k]), 0, float(arrivals[k])))
-        # warm-up, untimed: the three largest requests of each distance
-        warm = [reqs[k] for dd in (1, 2) for k in np.argsort(-sizes * (dists == dd))[:3]]
-        ix.serve(warm, realtime=False, keep_results=False)
-        stats, _ = ix.serve(reqs, realtime=True, keep_results=False)
-        lat = np.array([(st["done_s"] - t) * 1e3 for st, (_, _, _, _, t) in zip(stats, reqs)])
-        span = max(st["done_s"] for st in stats) - float(arrivals[0])
-        small_d1 = np.array([l for l, (_, o, d, _, _) in zip(lat, reqs) if d == 1 and len(o) - 1 <= 1000])
-        per_rate[str(rate)] = {
-            "requests": n_req,
-            "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)),
-            "p50_ms_d1": float(np.percentile(lat[dists == 1], 50)),
-            "p99_ms_d1": float(np.percentile(lat[dists == 1], 99)),
-            "p99_ms_d2": float(np.percentile(lat[dists == 2], 99)) if (dists == 2).any() else None,
-            "p99_ms_d1_le_1k_seqs": float(np.percentile(small_d1, 99)) if len(small_d1) else None,
-            "seqs_per_s": float(sizes.sum() / span),
-            "batches": len({st["batch"] for st in stats}),
-            "pairs": int(sum(st["n_out"] for st in stats)),
-            "slowest": [{"seqs": int(sizes[k]), "d": int(dists[k]), "queue_ms": (stats[k]["admitted_s"] - arrivals[k]) * 1e3,
-                         "service_ms": (stats[k]["done_s"] - stats[k]["admitted_s"]) * 1e3, "batch": stats[k]["batch"]}
-                        for k in np.argsort(-lat)[:5]],
-        }
-        total_seqs += int(sizes.sum())
-        total_busy += span
+    per_rate = {str(rate): serve_trace(ix, pool_c, pool_o, w, rate, rng) for rate in w["rates"]}
     clocks = sampler.stop()
     ix.close()
     top = per_rate[str(max(w["rates"]))]
@@ -286,7 +298,7 @@ def run_serve(args, w):
         "vs_baseline": None,
         "dtype": "u64",
         "data": "synthetic (seeded CDR3 generator)",
-        "config": {"workload": args.workload, "index_seqs": ni, "index_max_distance": 2,
+        "config": {"workload": args.workload, "index_seqs": w["n_index"], "index_max_distance": 2,
                    "request_sizes": f"log-uniform 1..{w['max_size']}", "p_d1": w["p_d1"],
                    "rates_req_per_s": list(w["rates"]), "seconds_per_rate": w["seconds"],
                    "value_is": f"p99 at {w['rates'][len(w['rates']) // 2]} req/s"},
@@ -296,6 +308,19 @@ def run_serve(args, w):
                   "build_ms_device": info["ms_build"], "build_s_wall": build_wall},
         "clocks": clocks,
     }
+
+
+def serving_line(local):
+    """The serving configuration at one rate (100 req/s, 3 s), for the default bench line."""
+    import numpy as np
+
+    w = SERVE_WORKLOADS["serve_5m_d2"]
+    ix, pool_c, pool_o, build_wall = serve_setup(w, local)
+    out = serve_trace(ix, pool_c, pool_o, w, 100, np.random.default_rng(w["seed"] + 1))
+    out["index_seqs"] = w["n_index"]
+    out["index_build_ms_device"] = ix.info()["ms_build"]
+    ix.close()
+    return out
 
 
 def ncu_traffic(kernel: str, workload: str):
@@ -515,6 +540,8 @@ def run_ours(args, w):
         extras[name] = measure_extra(ctx, WORKLOADS[name], args, flush, ext)
     if extras:
         line["extra_workloads"] = extras
+    if world == 1 and not args.no_serving and not overlap:
+        line["serving"] = serving_line(local)
     if world == 1 and not args.no_cli:
         line["cli_process"] = cli_process(args, w, n)
     if world == 1 and not args.no_cpu_baseline:
@@ -777,6 +804,7 @@ def main():
     ap.add_argument("--no-cli", action="store_true", help="skip timing the xt_neighbor CLI process")
     ap.add_argument("--no-extra", action="store_true", help="skip the extra workloads measured beside the headline")
     ap.add_argument("--no-forms", action="store_true", help="skip the plain-vs-graph form comparison")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving trace in the default line")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the bucket-engine shape by timing on the workload first (xtn_context_autotune)")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",

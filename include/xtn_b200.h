@@ -267,15 +267,21 @@ int xtn_index_query(xtn_index* index, const xtn_args* args, const char* seqs, co
 int xtn_index_query_device(xtn_index* index, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
                            int32_t n_queries, int64_t* n_out);
 
-/* Serving loop. Requests (host buffers) arrive at arrival_s seconds after the call starts
- * (realtime) or all at once. Whenever the device is free, the loop admits the ready requests
- * of the oldest one's (distance, measure) in arrival order while the batch fits the memory
- * budget (hbm_fraction of the device memory free when the loop starts, after it reserves
- * buffers for the largest request; at most max_batch_seqs sequences), runs them
- * as one query batch, splits the answer by request and hands each request its pairs
- * (y = n_seqs + the request's own row) through the callback. A request larger than the budget
- * runs in pieces. results[i] receives the admission and completion times (seconds since the
- * call started), the pair count and the status of request i. */
+/* Serving loop with continuous batching. Requests (host buffers) arrive at arrival_s seconds
+ * after the call starts (realtime) or all at once. The loop runs `slots` batches at a time, each
+ * slot on its own stream and host thread with its own query scratch (slot 0 uses the index's
+ * context); the index itself is shared, read only. Whenever a slot is free it admits the ready
+ * requests of the oldest one's (distance, measure) in arrival order while the batch fits the
+ * slot's memory budget (hbm_fraction of the device memory free when the loop starts, split
+ * over the slots, after buffers for the largest request are reserved in each slot; at most
+ * max_batch_seqs sequences), runs them as one query batch, splits the answer by request and
+ * hands each request its pairs (y = n_seqs + the request's own row) through the callback. So a
+ * request that arrives while another slot runs a large batch starts at once, and their work
+ * overlaps on the device. A request larger than the budget runs in pieces. A request's
+ * answer does not depend on the batch it joins (each pair is found and verified from the
+ * request's own sequences). Callbacks come from the loop's threads, one at a time.
+ * results[i] receives the admission and completion times (seconds since the call started), the
+ * batch, the pair count and the status of request i. */
 typedef struct {
     const char* seqs;
     const uint32_t* offsets;
@@ -295,8 +301,9 @@ typedef struct {
 
 typedef struct {
     int64_t max_batch_seqs; /* <= 0: 2^20 */
-    double hbm_fraction;    /* of free device memory a batch may use; <= 0: 0.5 */
+    double hbm_fraction;    /* of free device memory the batches may use; <= 0: 0.5 */
     int32_t realtime;       /* 1: honour arrival_s; 0: every request is ready at once */
+    int32_t slots;          /* batches in flight at a time, 1..8; <= 0: 2 */
 } xtn_serve_options;
 
 typedef void (*xtn_request_callback)(int32_t request, const xtn_output* out, void* user);

@@ -145,3 +145,76 @@ def test_serving_loop_matches_direct_queries(index_setup):
             assert st["n_out"] == len(exp.pairs)
         if not realtime:
             assert len({st["batch"] for st in stats}) < len(reqs)
+
+
+@pytest.mark.parametrize("slots", [1, 2, 4])
+def test_serving_slots_results_alone_and_in_the_mix(index_setup, slots):
+    """Continuous batching: with several slots, batches run at the same time on their own
+    streams. Each request's answer equals the same request queried alone, whatever batch and
+    slot it joined."""
+    ix, index_seqs = index_setup
+    rng = np.random.default_rng(31 + slots)
+    reqs = []
+    for i in range(40):
+        size = int(rng.integers(1, 300)) if i % 9 else 3000
+        q = make_queries(index_seqs, size, seed=500 + i)
+        c, o = csr(q)
+        reqs.append((c, o, 1 if rng.random() < 0.7 else 2, 0, float(rng.uniform(0, 0.03))))
+    expected = [ix.query(c, o, distance=d, measure=m) for c, o, d, m, _ in reqs]
+    for realtime in (True, False):
+        stats, outs = ix.serve(reqs, realtime=realtime, slots=slots)
+        for st, out, exp in zip(stats, outs, expected):
+            assert st["status"] == 0
+            assert np.array_equal(out.pairs, exp.pairs) and np.array_equal(out.distances, exp.distances)
+
+
+def test_small_request_overtakes_a_large_one(index_setup):
+    """A large d = 2 batch occupies one slot; small d = 1 requests that arrive while it runs are
+    admitted by the other slot and finish before it."""
+    ix, index_seqs = index_setup
+    big = csr(make_queries(index_seqs, 60_000, seed=1))
+    smalls = [csr(make_queries(index_seqs, 20, seed=600 + i)) for i in range(6)]
+    reqs = [(big[0], big[1], 2, 0, 0.0)] + [(c, o, 1, 0, 0.001 + 0.0005 * i) for i, (c, o) in enumerate(smalls)]
+    ix.serve(reqs, realtime=True, slots=2, keep_results=False)  # warm-up of the slots' buffers
+    stats, outs = ix.serve(reqs, realtime=True, slots=2)
+    big_done = stats[0]["done_s"]
+    assert any(st["done_s"] < big_done for st in stats[1:]), [st["done_s"] for st in stats]
+    assert len({st["batch"] for st in stats}) >= 2
+    for (c, o, d, m, _), out in zip(reqs, outs):
+        exp = ix.query(c, o, distance=d, measure=m)
+        assert np.array_equal(out.pairs, exp.pairs) and np.array_equal(out.distances, exp.distances)
+
+
+def test_serving_on_the_5m_index_equals_offline_runs():
+    """The serving configuration's index (5,000,000 generator sequences, d = 2): requests of
+    mixed sizes and distances, served with two slots, each equal to the offline search on
+    (index sequences followed by the request) restricted to the pairs with one side in each."""
+    import torch
+
+    chars, offs = xtn.synth_clusters(20245, 5_300_000, 0.20, 0.02)
+    ni = 5_000_000
+    ic, io = chars[: offs[ni]], offs[: ni + 1]
+    pool_c, pool_o = chars[offs[ni]:], (offs[ni:] - offs[ni]).astype(np.uint32)
+    rng = np.random.default_rng(7)
+    reqs = []
+    for k in range(10):
+        size = int(np.exp(rng.uniform(0, np.log(50_000))))
+        a = int(rng.integers(0, len(pool_o) - 1 - size))
+        o = (pool_o[a : a + size + 1] - pool_o[a]).astype(np.uint32)
+        reqs.append((pool_c[pool_o[a] : pool_o[a + size]], o, 1 if k % 3 else 2, 0, 0.002 * k))
+    with xtn.Index(ic, io, max_distance=2) as ix:
+        stats, outs = ix.serve(reqs, realtime=True, slots=2)
+    ctx = xtn.Context(0)
+    for (c, o, d, m, _), st, out in zip(reqs, stats, outs):
+        assert st["status"] == 0
+        uc = np.concatenate([ic, c])
+        uo = np.concatenate([io, o[1:] + io[-1]]).astype(np.uint32)
+        dch = torch.from_numpy(uc).cuda()
+        dof = torch.from_numpy(uo.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        m_out = ctx.nn_device(dch.data_ptr(), dof.data_ptr(), len(uo) - 1, d, m)
+        r = ctx.fetch(m_out)
+        sel = (r.pairs[:, 0] < ni) & (r.pairs[:, 1] >= ni)
+        assert np.array_equal(out.pairs, r.pairs[sel])
+        assert np.array_equal(out.distances, r.distances[sel])
+    ctx.close()

@@ -195,12 +195,18 @@ __global__ void k_query_compact(const uint64_t* __restrict__ pairs, int64_t P, i
 
 }  // namespace xtn
 
+// Query scratch of one serving slot (a slot also has its own context: stream, search scratch
+// and result buffers).
+struct xtn_query_bufs {
+    DevBuf qh, qrow, qlb, qcnt, qcoff;
+};
+
 struct xtn_index {
     xtn_context* c = nullptr;  // stream, scratch and the query result buffers
     int n = 0, dmax = 0, idbits = 0, dir_bits = 0;
     uint64_t V = 0;
     DevBuf chars, offs, recs, dir;
-    DevBuf qh, qrow, qlb, qcnt, qcoff;
+    xtn_query_bufs qb;
     double ms_build = 0;
 };
 
@@ -274,9 +280,8 @@ static int index_build(xtn_index* ix, int n, int dmax, bool validate) {
 
 // One query batch on device inputs; the result (pairs (index row, n_index + query row), int8
 // distances) is left in the context's output buffers, c->n_out entries.
-static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qoffs, int nq, int d, int measure,
-                       bool validate) {
-    xtn_context* c = ix->c;
+static int index_query(xtn_index* ix, xtn_context* c, xtn_query_bufs& qb, const uint8_t* qchars,
+                       const uint32_t* qoffs, int nq, int d, int measure, bool validate) {
     cudaStream_t s = c->stream;
     c->stats = xtn_stats{};
     c->stats.n_seqs = nq;
@@ -303,21 +308,21 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
     XTN_TRY(read_scalar(c, P<uint64_t>(c->voff) + nq, 8, &Vq));
     if (validate) XTN_TRY(length_check_result(c, (uint32_t)c->h_scalar[1]));
     c->stats.n_variants = (int64_t)Vq;
-    XTN_TRY(ensure(ix->qh, sizeof(uint64_t) * Vq));
-    XTN_TRY(ensure(ix->qrow, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qlb, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qcnt, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qcoff, sizeof(uint64_t) * (Vq + 1)));
+    XTN_TRY(ensure(qb.qh, sizeof(uint64_t) * Vq));
+    XTN_TRY(ensure(qb.qrow, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qlb, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qcnt, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qcoff, sizeof(uint64_t) * (Vq + 1)));
     XTN_LAUNCH("query_gen", k_query_gen<<<blocks_for(nq), kThreads, 0, s>>>(
                                 P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
-                                P<uint64_t>(c->voff), nq, d, P<uint64_t>(ix->qh), P<uint32_t>(ix->qrow)));
+                                P<uint64_t>(c->voff), nq, d, P<uint64_t>(qb.qh), P<uint32_t>(qb.qrow)));
     XTN_LAUNCH("query_count", k_query_count<<<blocks_for((int64_t)Vq), kThreads, 0, s>>>(
-                                  P<uint64_t>(ix->qh), (int64_t)Vq, P<uint64_t>(ix->recs), P<uint32_t>(ix->dir),
-                                  ix->dir_bits, ix->idbits, d, P<uint32_t>(ix->qlb), P<uint32_t>(ix->qcnt)));
+                                  P<uint64_t>(qb.qh), (int64_t)Vq, P<uint64_t>(ix->recs), P<uint32_t>(ix->dir),
+                                  ix->dir_bits, ix->idbits, d, P<uint32_t>(qb.qlb), P<uint32_t>(qb.qcnt)));
     XTN_CK(cudaGetLastError());
-    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(ix->qcnt), P<uint64_t>(ix->qcoff), (int64_t)Vq));
+    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(qb.qcnt), P<uint64_t>(qb.qcoff), (int64_t)Vq));
     uint64_t Pc = 0;
-    XTN_TRY(read_scalar(c, P<uint64_t>(ix->qcoff) + Vq, 8, &Pc));
+    XTN_TRY(read_scalar(c, P<uint64_t>(qb.qcoff) + Vq, 8, &Pc));
     c->stats.n_candidates = (int64_t)Pc;
     const int qbits = id_bits_for(nq);
     if (Pc >= (uint64_t)UINT32_MAX || ix->idbits + qbits > 64) {
@@ -329,8 +334,8 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
         XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Pc + 64));
         XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Pc + 64));
         XTN_LAUNCH("query_emit", k_query_emit<<<blocks_for((int64_t)Vq), kThreads, 0, s>>>(
-                                     P<uint32_t>(ix->qrow), (int64_t)Vq, P<uint64_t>(ix->recs), P<uint32_t>(ix->qlb),
-                                     P<uint32_t>(ix->qcnt), P<uint64_t>(ix->qcoff), ix->idbits, qbits,
+                                     P<uint32_t>(qb.qrow), (int64_t)Vq, P<uint64_t>(ix->recs), P<uint32_t>(qb.qlb),
+                                     P<uint32_t>(qb.qcnt), P<uint64_t>(qb.qcoff), ix->idbits, qbits,
                                      P<uint64_t>(c->pairA)));
         XTN_CK(cudaGetLastError());
         uint64_t* pairs = P<uint64_t>(c->pairA);
@@ -369,8 +374,9 @@ static int index_query(xtn_index* ix, const uint8_t* qchars, const uint32_t* qof
 // Grows the query buffers for a batch of nq sequences with `chars` residues at distance d, so
 // that a serving loop does not reallocate device memory between requests (candidate buffers
 // are sized for one candidate per query variant and grow if a batch needs more).
-static int index_reserve(xtn_index* ix, int64_t nq, int64_t chars, int d) {
-    xtn_context* c = ix->c;
+constexpr int kMaxServeSlots = 8;
+
+static int index_reserve(xtn_context* c, xtn_query_bufs& qb, int64_t nq, int64_t chars, int d) {
     const int64_t Vq = nq * (d >= 2 ? 172 : 19);
     XTN_TRY(ensure(c->chars, (size_t)chars + 16));
     XTN_TRY(ensure(c->offs, sizeof(uint32_t) * (nq + 1)));
@@ -381,11 +387,11 @@ static int index_reserve(xtn_index* ix, int64_t nq, int64_t chars, int d) {
     XTN_TRY(ensure(c->runinfo, sizeof(uint64_t) * nq));
     XTN_TRY(ensure(c->ktab, sizeof(uint64_t) * kTabLen * (size_t)nq));
     XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * scan_scratch_elems(Vq + 1)));
-    XTN_TRY(ensure(ix->qh, sizeof(uint64_t) * Vq));
-    XTN_TRY(ensure(ix->qrow, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qlb, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qcnt, sizeof(uint32_t) * Vq));
-    XTN_TRY(ensure(ix->qcoff, sizeof(uint64_t) * (Vq + 1)));
+    XTN_TRY(ensure(qb.qh, sizeof(uint64_t) * Vq));
+    XTN_TRY(ensure(qb.qrow, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qlb, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qcnt, sizeof(uint32_t) * Vq));
+    XTN_TRY(ensure(qb.qcoff, sizeof(uint64_t) * (Vq + 1)));
     XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * Vq + 64));
     XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * Vq + 64));
     XTN_TRY(ensure(c->dist, (size_t)Vq));
@@ -419,7 +425,8 @@ static void index_free(xtn_index* ix) {
     if (ix->c) {
         cudaSetDevice(ix->c->device);
         cudaStreamSynchronize(ix->c->stream);
-        DevBuf* bufs[] = {&ix->chars, &ix->offs, &ix->recs, &ix->dir, &ix->qh, &ix->qrow, &ix->qlb, &ix->qcnt, &ix->qcoff};
+        DevBuf* bufs[] = {&ix->chars, &ix->offs, &ix->recs, &ix->dir, &ix->qb.qh, &ix->qb.qrow, &ix->qb.qlb,
+                          &ix->qb.qcnt, &ix->qb.qcoff};
         for (DevBuf* b : bufs) release(*b);
         xtn_context_destroy(ix->c);
     }
@@ -540,8 +547,8 @@ int xtn_index_query_device(xtn_index* ix, const xtn_args* args, const char* d_se
     XTN_TRY(check_args(args));
     XTN_CK(cudaSetDevice(ix->c->device));
     begin_run(ix->c);
-    int r = index_query(ix, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n_queries, args->distance,
-                        args->measure, true);
+    int r = index_query(ix, ix->c, ix->qb, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n_queries,
+                        args->distance, args->measure, true);
     end_run(ix->c);
     if (r == XTN_SUCCESS && n_out) *n_out = ix->c->n_out;
     return r;
@@ -559,8 +566,8 @@ int xtn_index_query(xtn_index* ix, const xtn_args* args, const char* seqs, const
     XTN_CK(cudaSetDevice(c->device));
     XTN_TRY(upload(c, seqs, offsets, n_queries));
     begin_run(c);
-    int r = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), n_queries, args->distance, args->measure,
-                        false);
+    int r = index_query(ix, c, ix->qb, P<uint8_t>(c->chars), P<uint32_t>(c->offs), n_queries, args->distance,
+                        args->measure, false);
     end_run(c);
     if (r != XTN_SUCCESS) return r;
     return deliver(c, cb, user);
@@ -585,10 +592,42 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
     const int64_t max_batch = opt && opt->max_batch_seqs > 0 ? opt->max_batch_seqs : (int64_t)1 << 20;
     const double frac = opt && opt->hbm_fraction > 0 && opt->hbm_fraction <= 1 ? opt->hbm_fraction : 0.5;
     const bool realtime = !opt || opt->realtime;
-    xtn_context* c = ix->c;
-    XTN_CK(cudaSetDevice(c->device));
+    const int nslots = opt && opt->slots > 0 ? std::min(opt->slots, kMaxServeSlots) : 2;
+    const int device = ix->c->device;
+    XTN_CK(cudaSetDevice(device));
+    // slot 0 is the index's own context; the others get a context (stream, scratch) each
+    struct Slot {
+        xtn_context* c = nullptr;
+        xtn_query_bufs own;
+        xtn_query_bufs* qb = nullptr;
+    };
+    std::vector<Slot> slots(nslots);
+    slots[0].c = ix->c;
+    slots[0].qb = &ix->qb;
+    auto free_slots = [&]() {
+        for (int k = 1; k < nslots; k++) {
+            if (!slots[k].c) continue;
+            cudaStreamSynchronize(slots[k].c->stream);
+            DevBuf* b[] = {&slots[k].own.qh, &slots[k].own.qrow, &slots[k].own.qlb, &slots[k].own.qcnt,
+                           &slots[k].own.qcoff};
+            for (DevBuf* x : b) release(*x);
+            xtn_context_destroy(slots[k].c);
+            slots[k].c = nullptr;
+        }
+    };
+    for (int k = 1; k < nslots; k++) {
+        const int r = xtn_context_create(device, &slots[k].c);
+        if (r != XTN_SUCCESS) {
+            free_slots();
+            return r;
+        }
+        slots[k].qb = &slots[k].own;
+    }
+    // device memory for the largest batch a slot can form, reserved before the clock starts; the
+    // memory budget is split over the slots and read once (a device-memory query can take tens
+    // of milliseconds, far longer than a small batch)
+    int64_t cap_by_d[3] = {0, 0, 0};
     {
-        // device memory for the largest batch the loop can form, reserved before the clock starts
         int64_t big = 0, big_chars = 0;
         int dbig = 1;
         for (int i = 0; i < n_reqs; i++) {
@@ -598,153 +637,197 @@ int xtn_index_serve(xtn_index* ix, const xtn_request* reqs, int32_t n_reqs, cons
         }
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        const int64_t cap0 = std::max<int64_t>(
-            1, std::min<int64_t>(max_batch, (int64_t)((double)free_b * frac / (double)query_bytes_per_seq(dbig))));
+        const double per_slot = (double)free_b * frac / nslots;
+        const int64_t cap0 =
+            std::max<int64_t>(1, std::min<int64_t>(max_batch, (int64_t)(per_slot / (double)query_bytes_per_seq(dbig))));
         const int64_t nres = std::min(std::max<int64_t>(big, std::min<int64_t>(cap0, 1 << 16)), cap0);
-        XTN_TRY(index_reserve(ix, nres, std::max<int64_t>(big_chars, nres * 24), dbig));
+        for (int k = 0; k < nslots; k++) {
+            const int r = index_reserve(slots[k].c, *slots[k].qb, nres, std::max<int64_t>(big_chars, nres * 24), dbig);
+            if (r != XTN_SUCCESS) {
+                free_slots();
+                return r;
+            }
+        }
+        for (int dd = 1; dd <= 2; dd++)
+            cap_by_d[dd] = std::max<int64_t>(
+                1, std::min<int64_t>(max_batch, (int64_t)(per_slot / (double)query_bytes_per_seq(dd))));
     }
-    // The memory budget is read once: a device-memory query can take tens of milliseconds,
-    // far longer than a small batch. Only this loop allocates on the index's device while it
-    // runs, so free memory changes only when a batch outgrows the reservation.
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    const double budget = (double)free_b * frac;
-    // requests in arrival order
+    // requests in arrival order; a free slot takes the oldest ready request and the ready ones
+    // of the same (distance, measure) that fit its budget, so a request that arrives while
+    // another slot is busy with a large batch starts at once
     std::vector<int> order(n_reqs);
     for (int i = 0; i < n_reqs; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].arrival_s < reqs[b].arrival_s; });
-    const double t0 = now_s();
+    std::mutex mu, cb_mu;
+    std::condition_variable cv;
     size_t next = 0;
     std::vector<int> ready;
-    std::vector<char> hchars;
-    std::vector<uint32_t> hoffs;
-    std::vector<xtn_int2> hp;
-    std::vector<int8_t> hd;
-    int batch_id = 0;
-    while (next < order.size() || !ready.empty()) {
-        double now = now_s() - t0;
-        while (next < order.size() && (!realtime || reqs[order[next]].arrival_s <= now)) ready.push_back(order[next++]);
-        if (ready.empty()) {
-            const double wait = reqs[order[next]].arrival_s - now;
-            if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
-            continue;
-        }
-        // admission: the oldest ready request fixes (distance, measure); requests of the same
-        // kind join while the batch fits the memory budget
-        const int d = reqs[ready[0]].distance, m = reqs[ready[0]].measure;
-        const int64_t cap =
-            std::max<int64_t>(1, std::min<int64_t>(max_batch, (int64_t)(budget / (double)query_bytes_per_seq(d))));
-        std::vector<int> batch, rest;
-        int64_t seqs = 0;
-        for (int r : ready) {
-            const xtn_request& q = reqs[r];
-            if (q.distance == d && q.measure == m && (batch.empty() || seqs + q.n_seqs <= cap)) {
-                batch.push_back(r);
-                seqs += q.n_seqs;
-            } else {
-                rest.push_back(r);
-            }
-        }
-        ready.swap(rest);
-        const double admitted = now_s() - t0;
-        // one request larger than the budget runs in pieces of at most `cap` sequences
-        struct Piece {
-            int req, first, count;
-            int64_t row0;
-        };
-        std::vector<Piece> pieces;
-        for (int r : batch) {
-            for (int f = 0; f < reqs[r].n_seqs; f += (int)cap)
-                pieces.push_back(Piece{r, f, (int)std::min<int64_t>(cap, reqs[r].n_seqs - f), 0});
-        }
-        std::vector<std::vector<xtn_int2>> rp(batch.size());
-        std::vector<std::vector<int8_t>> rd(batch.size());
-        std::vector<int> slot(n_reqs, -1);
-        for (size_t k = 0; k < batch.size(); k++) slot[batch[k]] = (int)k;
-        int status = XTN_SUCCESS;
-        for (size_t p0 = 0; p0 < pieces.size() && status == XTN_SUCCESS;) {
-            // pieces p0..p1 form one device round of at most `cap` sequences
-            size_t p1 = p0;
-            int64_t rows = 0;
-            hchars.clear();
-            hoffs.assign(1, 0);
-            while (p1 < pieces.size() && (p1 == p0 || rows + pieces[p1].count <= cap)) {
-                Piece& pc = pieces[p1];
-                pc.row0 = rows;
-                const xtn_request& q = reqs[pc.req];
-                const uint32_t a0 = q.offsets[pc.first], base = hoffs.back();
-                hchars.insert(hchars.end(), q.seqs + a0, q.seqs + q.offsets[pc.first + pc.count]);
-                for (int i = 1; i <= pc.count; i++) hoffs.push_back(base + (q.offsets[pc.first + i] - a0));
-                rows += pc.count;
-                p1++;
-            }
-            status = upload(c, hchars.data(), hoffs.data(), (int)rows);
-            if (status == XTN_SUCCESS) {
-                begin_run(c);
-                status = index_query(ix, P<uint8_t>(c->chars), P<uint32_t>(c->offs), (int)rows, d, m, false);
-                end_run(c);
-            }
-            if (status != XTN_SUCCESS) break;
-            const int64_t nout = c->n_out;
-            hp.resize((size_t)nout);
-            hd.resize((size_t)nout);
-            if (nout > 0) {
-                XTN_CK(cudaMemcpyAsync(hp.data(), c->out_pairs.p, sizeof(xtn_int2) * nout, cudaMemcpyDeviceToHost,
-                                       c->stream));
-                XTN_CK(cudaMemcpyAsync(hd.data(), c->out_dist.p, (size_t)nout, cudaMemcpyDeviceToHost, c->stream));
-                XTN_CK(cudaStreamSynchronize(c->stream));
-            }
-            // split by request: rows [row0, row0 + count) of the round belong to piece k
-            std::vector<int64_t> starts;
-            for (size_t k = p0; k < p1; k++) starts.push_back(pieces[k].row0);
-            for (int64_t i = 0; i < nout; i++) {
-                const int64_t row = hp[i].y - ix->n;
-                const size_t k = p0 + (size_t)(std::upper_bound(starts.begin(), starts.end(), row) - starts.begin()) - 1;
-                const Piece& pc = pieces[k];
-                const int s = slot[pc.req];
-                rp[s].push_back(xtn_int2{hp[i].x, (int32_t)(ix->n + pc.first + (row - pc.row0))});
-                rd[s].push_back(hd[i]);
-            }
-            p0 = p1;
-        }
-        for (size_t k = 0; k < batch.size(); k++) {
-            const int r = batch[k];
-            xtn_request_result& res = results[r];
-            res.admitted_s = admitted;
-            res.batch = batch_id;
-            res.status = status;
-            if (status == XTN_SUCCESS) {
-                // a request split into pieces collects its pairs piece by piece: restore (x, y) order
-                std::vector<xtn_int2>& P2 = rp[k];
-                std::vector<int8_t>& D2 = rd[k];
-                bool sorted = true;
-                for (size_t i = 1; i < P2.size() && sorted; i++)
-                    sorted = P2[i - 1].x < P2[i].x || (P2[i - 1].x == P2[i].x && P2[i - 1].y < P2[i].y);
-                if (!sorted) {
-                    std::vector<size_t> idx(P2.size());
-                    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
-                    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-                        return P2[a].x < P2[b].x || (P2[a].x == P2[b].x && P2[a].y < P2[b].y);
-                    });
-                    std::vector<xtn_int2> p3(P2.size());
-                    std::vector<int8_t> d3(D2.size());
-                    for (size_t i = 0; i < idx.size(); i++) {
-                        p3[i] = P2[idx[i]];
-                        d3[i] = D2[idx[i]];
+    int batch_counter = 0, first_status = XTN_SUCCESS;
+    std::string first_error;
+    const double t0 = now_s();
+    auto worker = [&](int k) {
+        Slot& sl = slots[k];
+        xtn_context* c = sl.c;
+        if (cudaSetDevice(device) != cudaSuccess) return;
+        std::vector<char> hchars;
+        std::vector<uint32_t> hoffs;
+        std::vector<xtn_int2> hp;
+        std::vector<int8_t> hd;
+        for (;;) {
+            std::vector<int> batch;
+            int d = 1, m = 0, batch_id = 0;
+            int64_t cap = 1;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                for (;;) {
+                    if (first_status != XTN_SUCCESS) return;
+                    const double now = now_s() - t0;
+                    while (next < order.size() && (!realtime || reqs[order[next]].arrival_s <= now))
+                        ready.push_back(order[next++]);
+                    if (!ready.empty()) break;
+                    if (next >= order.size()) return;  // every request admitted
+                    const double wait = reqs[order[next]].arrival_s - now;
+                    cv.wait_for(lk, std::chrono::duration<double>(std::max(wait, 0.0)));
+                }
+                d = reqs[ready[0]].distance;
+                m = reqs[ready[0]].measure;
+                cap = cap_by_d[d];
+                std::vector<int> rest;
+                int64_t seqs = 0;
+                for (int r : ready) {
+                    const xtn_request& q = reqs[r];
+                    if (q.distance == d && q.measure == m && (batch.empty() || seqs + q.n_seqs <= cap)) {
+                        batch.push_back(r);
+                        seqs += q.n_seqs;
+                    } else {
+                        rest.push_back(r);
                     }
-                    P2.swap(p3);
-                    D2.swap(d3);
                 }
-                res.n_out = (int64_t)P2.size();
-                if (cb) {
-                    xtn_output o{P2.data(), D2.data(), nullptr, (int64_t)P2.size()};
-                    cb(r, &o, user);
-                }
+                ready.swap(rest);
+                batch_id = batch_counter++;
             }
-            res.done_s = now_s() - t0;
+            cv.notify_all();
+            const double admitted = now_s() - t0;
+            // a request larger than the budget runs in pieces of at most `cap` sequences
+            struct Piece {
+                int req, first, count;
+                int64_t row0;
+            };
+            std::vector<Piece> pieces;
+            for (int r : batch)
+                for (int f = 0; f < reqs[r].n_seqs; f += (int)cap)
+                    pieces.push_back(Piece{r, f, (int)std::min<int64_t>(cap, reqs[r].n_seqs - f), 0});
+            std::vector<std::vector<xtn_int2>> rp(batch.size());
+            std::vector<std::vector<int8_t>> rd(batch.size());
+            std::vector<int> slot_of(n_reqs, -1);
+            for (size_t q = 0; q < batch.size(); q++) slot_of[batch[q]] = (int)q;
+            int status = XTN_SUCCESS;
+            for (size_t p0 = 0; p0 < pieces.size() && status == XTN_SUCCESS;) {
+                // pieces p0..p1 form one device round of at most `cap` sequences
+                size_t p1 = p0;
+                int64_t rows = 0;
+                hchars.clear();
+                hoffs.assign(1, 0);
+                while (p1 < pieces.size() && (p1 == p0 || rows + pieces[p1].count <= cap)) {
+                    Piece& pc = pieces[p1];
+                    pc.row0 = rows;
+                    const xtn_request& q = reqs[pc.req];
+                    const uint32_t a0 = q.offsets[pc.first], base = hoffs.back();
+                    hchars.insert(hchars.end(), q.seqs + a0, q.seqs + q.offsets[pc.first + pc.count]);
+                    for (int i = 1; i <= pc.count; i++) hoffs.push_back(base + (q.offsets[pc.first + i] - a0));
+                    rows += pc.count;
+                    p1++;
+                }
+                status = upload(c, hchars.data(), hoffs.data(), (int)rows);
+                if (status == XTN_SUCCESS) {
+                    begin_run(c);
+                    status = index_query(ix, c, *sl.qb, P<uint8_t>(c->chars), P<uint32_t>(c->offs), (int)rows, d, m,
+                                         false);
+                    end_run(c);
+                }
+                if (status != XTN_SUCCESS) break;
+                const int64_t nout = c->n_out;
+                hp.resize((size_t)nout);
+                hd.resize((size_t)nout);
+                if (nout > 0 &&
+                    (cudaMemcpyAsync(hp.data(), c->out_pairs.p, sizeof(xtn_int2) * nout, cudaMemcpyDeviceToHost,
+                                     c->stream) != cudaSuccess ||
+                     cudaMemcpyAsync(hd.data(), c->out_dist.p, (size_t)nout, cudaMemcpyDeviceToHost, c->stream) !=
+                         cudaSuccess ||
+                     cudaStreamSynchronize(c->stream) != cudaSuccess)) {
+                    set_err("copy of a batch result failed");
+                    status = XTN_ERR_CUDA;
+                    break;
+                }
+                // split by request: rows [row0, row0 + count) of the round belong to piece k
+                std::vector<int64_t> starts;
+                for (size_t k2 = p0; k2 < p1; k2++) starts.push_back(pieces[k2].row0);
+                for (int64_t i = 0; i < nout; i++) {
+                    const int64_t row = hp[i].y - ix->n;
+                    const size_t k2 = p0 + (size_t)(std::upper_bound(starts.begin(), starts.end(), row) - starts.begin()) - 1;
+                    const Piece& pc = pieces[k2];
+                    const int sq = slot_of[pc.req];
+                    rp[sq].push_back(xtn_int2{hp[i].x, (int32_t)(ix->n + pc.first + (row - pc.row0))});
+                    rd[sq].push_back(hd[i]);
+                }
+                p0 = p1;
+            }
+            std::lock_guard<std::mutex> lk(cb_mu);  // callbacks come one at a time
+            for (size_t q = 0; q < batch.size(); q++) {
+                const int r = batch[q];
+                xtn_request_result& res = results[r];
+                res.admitted_s = admitted;
+                res.batch = batch_id;
+                res.status = status;
+                if (status == XTN_SUCCESS) {
+                    // a request split into pieces collects its pairs piece by piece: restore (x, y) order
+                    std::vector<xtn_int2>& P2 = rp[q];
+                    std::vector<int8_t>& D2 = rd[q];
+                    bool sorted = true;
+                    for (size_t i = 1; i < P2.size() && sorted; i++)
+                        sorted = P2[i - 1].x < P2[i].x || (P2[i - 1].x == P2[i].x && P2[i - 1].y < P2[i].y);
+                    if (!sorted) {
+                        std::vector<size_t> idx(P2.size());
+                        for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
+                        std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+                            return P2[a].x < P2[b].x || (P2[a].x == P2[b].x && P2[a].y < P2[b].y);
+                        });
+                        std::vector<xtn_int2> p3(P2.size());
+                        std::vector<int8_t> d3(D2.size());
+                        for (size_t i = 0; i < idx.size(); i++) {
+                            p3[i] = P2[idx[i]];
+                            d3[i] = D2[idx[i]];
+                        }
+                        P2.swap(p3);
+                        D2.swap(d3);
+                    }
+                    res.n_out = (int64_t)P2.size();
+                    if (cb) {
+                        xtn_output o{P2.data(), D2.data(), nullptr, (int64_t)P2.size()};
+                        cb(r, &o, user);
+                    }
+                }
+                res.done_s = now_s() - t0;
+            }
+            if (status != XTN_SUCCESS) {
+                std::lock_guard<std::mutex> lk2(mu);
+                if (first_status == XTN_SUCCESS) {
+                    first_status = status;
+                    first_error = xtn_last_error();
+                }
+                cv.notify_all();
+                return;
+            }
         }
-        batch_id++;
-        if (status != XTN_SUCCESS) return status;
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nslots; k++) th.emplace_back(worker, k);
+    worker(0);
+    for (auto& t : th) t.join();
+    free_slots();
+    if (first_status != XTN_SUCCESS) {
+        set_err(first_error);
+        return first_status;
     }
     return XTN_SUCCESS;
 }

@@ -140,7 +140,8 @@ class RequestResult(ctypes.Structure):
 
 
 class ServeOptions(ctypes.Structure):
-    _fields_ = [("max_batch_seqs", ctypes.c_int64), ("hbm_fraction", ctypes.c_double), ("realtime", ctypes.c_int32)]
+    _fields_ = [("max_batch_seqs", ctypes.c_int64), ("hbm_fraction", ctypes.c_double), ("realtime", ctypes.c_int32),
+                ("slots", ctypes.c_int32)]
 
 
 REQUEST_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_int32, ctypes.POINTER(Output), ctypes.c_void_p)
@@ -502,7 +503,7 @@ class Index:
                                                ctypes.c_void_p(d_offsets), n, ctypes.byref(nout)))
         return nout.value
 
-    def serve(self, requests, max_batch_seqs=0, hbm_fraction=0.5, realtime=True, keep_results=True):
+    def serve(self, requests, max_batch_seqs=0, hbm_fraction=0.5, realtime=True, keep_results=True, slots=0):
         """requests: list of (chars, offsets, distance, measure, arrival_s). Returns (per-request
         dicts with admitted_s, done_s, n_out, batch, status; per-request Result or None)."""
         keep = [(np.ascontiguousarray(c, dtype=np.uint8), np.ascontiguousarray(o, dtype=np.uint32))
@@ -525,7 +526,7 @@ class Index:
                              np.ctypeslib.as_array(o.pairwise_distances, shape=(o.len,)).copy(), None)
 
         ccb = REQUEST_CALLBACK(cb)
-        opt = ServeOptions(max_batch_seqs, hbm_fraction, 1 if realtime else 0)
+        opt = ServeOptions(max_batch_seqs, hbm_fraction, 1 if realtime else 0, slots)
         _check(self.lib.xtn_index_serve(self.h, arr, len(requests), ctypes.byref(opt), res, ccb, None))
         stats = [{k: getattr(res[i], k) for k, _ in RequestResult._fields_} for i in range(len(requests))]
         return stats, outs
