@@ -1843,6 +1843,26 @@ __global__ void k_uniq_build(const uint64_t* __restrict__ recs, const uint8_t* _
     if (i == n - 1) occ_start[uidx[n]] = (uint32_t)n;
 }
 
+// Unique strings renumbered in row order (the order of their first occurrence), so that the
+// search over them reads the character store in order: row_head[row] marks first occurrences;
+// after an exclusive scan row_uid[row] is the row-order number of a first occurrence, and
+// k_uniq_row_order fills row_rep (row-order number -> row, ascending) and row_map (row-order
+// number -> hash-order number, which indexes the occurrence lists).
+__global__ void k_uniq_row_heads(const int32_t* __restrict__ rep_row, int U, uint8_t* __restrict__ row_head) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < U) row_head[rep_row[u]] = 1;
+}
+
+__global__ void k_uniq_row_order(const int32_t* __restrict__ rep_row, int U, const uint32_t* __restrict__ row_uid,
+                                 int32_t* __restrict__ row_rep, uint32_t* __restrict__ row_map) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= U) return;
+    const int32_t row = rep_row[u];
+    const uint32_t v = row_uid[row];
+    row_rep[v] = row;
+    row_map[v] = (uint32_t)u;
+}
+
 __device__ __forceinline__ uint64_t freq_product(int32_t a, int32_t b) {
     return (uint64_t)(int64_t)a * (uint64_t)(int64_t)b;
 }
@@ -1898,7 +1918,7 @@ __global__ void k_diag(const uint32_t* __restrict__ occ_start, const uint32_t* _
 __global__ void k_cross(const xtn_int2* __restrict__ pairs, int64_t np, const uint32_t* __restrict__ occ_start,
                         const uint32_t* __restrict__ srow, const int32_t* __restrict__ freq,
                         const int32_t* __restrict__ rep, int R, unsigned long long* __restrict__ M,
-                        uint8_t* __restrict__ present) {
+                        uint8_t* __restrict__ present, const uint32_t* __restrict__ row_map) {
     extern __shared__ unsigned long long s_m[];
     const bool local = R <= kSmemReps;
     uint8_t* s_p = reinterpret_cast<uint8_t*>(s_m + (local ? R * R : 0));
@@ -1910,9 +1930,10 @@ __global__ void k_cross(const xtn_int2* __restrict__ pairs, int64_t np, const ui
         __syncthreads();
     }
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
-        xtn_int2 pr = pairs[t];
-        uint32_t s1 = occ_start[pr.x], e1 = occ_start[pr.x + 1];
-        uint32_t s2 = occ_start[pr.y], e2 = occ_start[pr.y + 1];
+        const xtn_int2 pr = pairs[t];
+        const uint32_t ux = row_map[pr.x], uy = row_map[pr.y];  // row-order -> hash-order numbers
+        uint32_t s1 = occ_start[ux], e1 = occ_start[ux + 1];
+        uint32_t s2 = occ_start[uy], e2 = occ_start[uy + 1];
         for (uint32_t a = s1; a < e1; a++) {
             uint32_t ra = srow[a];
             int qa = rep[ra];
@@ -1958,6 +1979,7 @@ __global__ void k_matrix_compact(const unsigned long long* __restrict__ M, const
 
 struct xtn_overlap_bufs {
     DevBuf freq, rep, recA, recB, head, uidx, rep_row, occ_start, srow, M, present, mpos, scratch;
+    DevBuf row_head, row_uid, row_rep, row_map;  // unique strings numbered in row order
 };
 
 namespace xtn {
@@ -2027,6 +2049,19 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     XTN_LAUNCH("uniq_build", k_uniq_build<<<blocks_for(n), kThreads, 0, s>>>(recs, P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, idbits,
                                                     P<int32_t>(b.rep_row), P<uint32_t>(b.occ_start), P<uint32_t>(b.srow)));
     XTN_CK(cudaGetLastError());
+    // row-order numbering of the unique strings
+    XTN_TRY(ensure(b.row_head, (size_t)n));
+    XTN_TRY(ensure(b.row_uid, sizeof(uint32_t) * (n + 1)));
+    XTN_TRY(ensure(b.row_rep, sizeof(int32_t) * (U + 1)));
+    XTN_TRY(ensure(b.row_map, sizeof(uint32_t) * (U + 1)));
+    XTN_CK(cudaMemsetAsync(b.row_head.p, 0, (size_t)n, s));
+    XTN_LAUNCH("uniq_row_heads", k_uniq_row_heads<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
+                                     P<int32_t>(b.rep_row), (int)U, P<uint8_t>(b.row_head)));
+    XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(b.row_head), P<uint32_t>(b.row_uid), n)));
+    XTN_LAUNCH("uniq_row_order", k_uniq_row_order<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
+                                     P<int32_t>(b.rep_row), (int)U, P<uint32_t>(b.row_uid), P<int32_t>(b.row_rep),
+                                     P<uint32_t>(b.row_map)));
+    XTN_CK(cudaGetLastError());
 
     // 2. diagonal term
     size_t RR = (size_t)R * R;
@@ -2046,7 +2081,7 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     XTN_CK(cudaGetLastError());
 
     // 3. neighbours among the unique strings
-    XTN_TRY(run_nn(c, chars, offs, P<int32_t>(b.rep_row), (int)U, d, measure, false));
+    XTN_TRY(run_nn(c, chars, offs, P<int32_t>(b.row_rep), (int)U, d, measure, false));
     const int64_t nverified = c->n_out;
 
     // 4. cross term
@@ -2055,7 +2090,7 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
         int64_t blocks = std::min<int64_t>((nverified + kThreads - 1) / kThreads, (int64_t)c->sms * 4);
         XTN_LAUNCH("cross", k_cross<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, smem, s>>>(
             P<xtn_int2>(c->out_pairs), nverified, P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), P<int32_t>(b.freq),
-            P<int32_t>(b.rep), R, P<unsigned long long>(b.M), P<uint8_t>(b.present)));
+            P<int32_t>(b.rep), R, P<unsigned long long>(b.M), P<uint8_t>(b.present), P<uint32_t>(b.row_map)));
         XTN_CK(cudaGetLastError());
     }
 
@@ -2153,7 +2188,8 @@ void xtn_context_destroy(xtn_context* c) {
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
         DevBuf* obufs[] = {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
-                           &ob->occ_start, &ob->srow, &ob->M, &ob->present, &ob->mpos, &ob->scratch};
+                           &ob->occ_start, &ob->srow, &ob->M, &ob->present, &ob->mpos, &ob->scratch,
+                           &ob->row_head, &ob->row_uid, &ob->row_rep, &ob->row_map};
         for (DevBuf* b : obufs) release(*b);
         delete ob;
     }
