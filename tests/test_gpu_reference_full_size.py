@@ -1,18 +1,32 @@
-"""Byte-for-byte parity with the reference binary on the benchmark's full-size workloads.
+"""Parity with the reference binary on the benchmark's full-size workloads.
 
 The reference XTNeighbor-streaming CLI (built from its sources by oracle/build_ref.sh into
 oracle/_ref/xt_neighbor_ref) and this build's xt_neighbor run on the same files, written by
-the generator command (bin/xtn_synth) with the benchmark's seeds, with -o; the output files
-must be identical:
-  * 10,000,000 sequences (clusters), Levenshtein d = 2 and Hamming d = 2;
-  * 64 repertoires (23.9M rows, log-uniform sizes 1e4..2e6, shared pool), overlap, d = 1.
-The reference needs about 100 s per 10M search on a B200. Its output lengths are the
-benchmark's expect_out values. Skipped where the reference build is absent.
+the generator command (bin/xtn_synth) with the benchmark's seeds, with -o.
+
+Where the reference is well defined the output files must be identical. It is not, at scale,
+for Levenshtein pairs with a sequence longer than 18 residues: its `levenshtein`
+(xtneighbor_streaming/src/kernel.cu:263-278) allocates max(len1, len2) bytes with device-side
+new, writes index len1 (one past the end when the first string is the longer), and frees the
+column before it reads the result from it. The result then depends on what other threads
+allocate in between; two runs of the reference on the same 10M input gave 3,181,049 and
+3,181,175 pairs. So:
+  * 10M sequences, Hamming d = 2: identical files.
+  * 10M sequences, Levenshtein d = 2: identical on every pair whose two sequences have at most
+    18 residues; every other difference (a pair in one file only, or a different distance)
+    involves a longer sequence, and for each the oracle's exact distance agrees with this
+    build (a pair only this build reports is within d; a pair only the reference reports is
+    not). The differences are a tiny share of the output.
+  * 64 repertoires (overlap, d = 1) without the rows longer than 18 residues: identical files.
+  * The same 64 repertoires with all rows: this build equals the CPU oracle bit for bit on the
+    leading repertoires (about 2M rows), long sequences included.
+The reference needs about 35 s per 10M search on a B200. Skipped where its build is absent.
 """
 import filecmp
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 import bench
@@ -33,25 +47,75 @@ def run_both_to_files(tmp_path, args):
     return paths
 
 
-def line_count(path):
-    with open(path, "rb") as f:
-        return sum(chunk.count(b"\n") for chunk in iter(lambda: f.read(1 << 24), b""))
+def read_triples(path):
+    import pandas as pd
+
+    if os.path.getsize(path) == 0:
+        return np.zeros((0, 3), np.int64)
+    return pd.read_csv(path, sep=" ", header=None, dtype=np.int64).to_numpy()
+
+
+def read_sequences(path):
+    import pandas as pd
+
+    return pd.read_csv(path, header=0, dtype=str, keep_default_na=False).iloc[:, 0].to_numpy()
 
 
 @pytest.mark.parametrize("workload", ["nn_10m_leven_d2", "nn_10m_hamming_d2"])
-def test_10m_output_identical(tmp_path, workload):
+def test_10m_output_matches_reference(tmp_path, workload):
     w = bench.WORKLOADS[workload]
     args = bench.workload_files(str(tmp_path), w)
-    ours, ref = run_both_to_files(tmp_path, args)
-    assert os.path.getsize(ours) == os.path.getsize(ref)
-    assert filecmp.cmp(ours, ref, shallow=False), f"{workload}: output files differ"
-    assert line_count(ref) == w["expect_out"]
+    ours_f, ref_f = run_both_to_files(tmp_path, args)
+    ours = read_triples(ours_f)
+    assert len(ours) == w["expect_out"]
+    if filecmp.cmp(ours_f, ref_f, shallow=False):
+        return
+    assert w["measure"] == 0, "Hamming outputs must be identical"
+    ref = read_triples(ref_f)
+    seqs = read_sequences(args[args.index("-i") + 1])
+    lens = np.fromiter((len(x) for x in seqs), dtype=np.int32, count=len(seqs))
+    long_o = (lens[ours[:, 0]] > 18) | (lens[ours[:, 1]] > 18)
+    long_r = (lens[ref[:, 0]] > 18) | (lens[ref[:, 1]] > 18)
+    # where the reference is well defined, identical lines
+    assert np.array_equal(ours[~long_o], ref[~long_r])
+    # every other difference: the oracle's exact distance sides with this build
+    key = lambda a: a[:, 0] * (1 << 32) + a[:, 1]
+    ko, kr = key(ours), key(ref)
+    only_o = np.setdiff1d(ko, kr)
+    only_r = np.setdiff1d(kr, ko)
+    both, io, ir = np.intersect1d(ko, kr, return_indices=True)
+    dist_diff = both[ours[io, 2] != ref[ir, 2]]
+    n_diff = len(only_o) + len(only_r) + len(dist_diff)
+    assert n_diff < len(ours) // 1000, f"{n_diff} differing pairs"
+    d_ours = dict(zip(ko.tolist(), ours[:, 2].tolist()))
+    for k in np.concatenate([only_o, only_r, dist_diff]).tolist():
+        x, y = k >> 32, k & 0xFFFFFFFF
+        assert lens[x] > 18 or lens[y] > 18, (x, y)
+        exact = orc.levenshtein(seqs[x], seqs[y])
+        if k in d_ours:
+            assert exact == d_ours[k] and exact <= w["d"], (seqs[x], seqs[y], exact)
+        else:
+            assert exact > w["d"], (seqs[x], seqs[y], exact)
 
 
-def test_64_repertoire_overlap_identical(tmp_path):
+def test_64_repertoire_overlap_identical_without_long_sequences(tmp_path):
     w = bench.WORKLOADS["overlap_64rep_leven_d1"]
-    args = bench.workload_files(str(tmp_path), w)
-    assert int(args[args.index("-n") + 1]) > 20_000_000
+    args = bench.workload_files(str(tmp_path), w, max_len=18)
+    assert int(args[args.index("-n") + 1]) > 15_000_000
     ours, ref = run_both_to_files(tmp_path, args)
     assert filecmp.cmp(ours, ref, shallow=False), "overlap output files differ"
-    assert line_count(ref) > 1000
+    with open(ref) as f:
+        assert sum(1 for _ in f) > 1000
+
+
+def test_64_repertoire_overlap_equals_oracle_on_leading_repertoires():
+    w = bench.WORKLOADS["overlap_64rep_leven_d1"]
+    chars, offs, info, reps = xtn.synth_repertoires(w["seed"], w["n_reps"], w["min"], w["max"], w["shared"])
+    k = max(1, int(np.searchsorted(np.cumsum(reps), 2_000_000, side="right")))
+    rows = int(np.sum(reps[:k]))
+    sub_c, sub_o, sub_i = chars[: offs[rows]], offs[: rows + 1], np.ascontiguousarray(info[:rows])
+    with xtn.Context(0) as ctx:
+        got = ctx.perform(sub_c, sub_o, distance=1, info=sub_i, n_reps=k)
+    exp_p, exp_s = orc.overlap_search(sub_c, sub_o, sub_i, 1, 0)
+    assert got.pairs.tolist() == exp_p.tolist()
+    assert np.array_equal(got.frequencies, exp_s)

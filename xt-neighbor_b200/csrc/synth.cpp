@@ -232,18 +232,20 @@ void synth_free(void* h) { delete static_cast<Synth*>(h); }
 // input format, so that a process can be given a workload file without loading this library.
 //   xtn_synth mutants     SEED N FRAC              OUT.csv [PREFIX_N PREFIX.csv]
 //   xtn_synth clusters    SEED N CLUSTER_FRAC DUP  OUT.csv [PREFIX_N PREFIX.csv]
-//   xtn_synth repertoires SEED R MIN MAX SHARED    OUT.csv INFO.csv
+//   xtn_synth repertoires SEED R MIN MAX SHARED    OUT.csv INFO.csv [MAX_LEN]
 // OUT.csv: header line, then one sequence per line ("seq,count" for repertoires); INFO.csv:
 // header line, then one repertoire size per line. PREFIX.csv holds the first PREFIX_N rows.
+// MAX_LEN drops the rows longer than MAX_LEN residues (and counts the repertoires without them).
 #include <cstdio>
 #include <cstdlib>
 
-static bool write_rows(const Synth* s, int64_t rows, const char* path) {
+static bool write_rows(const Synth* s, int64_t rows, const char* path, uint32_t max_len = 0xffffffffu) {
     FILE* f = fopen(path, "wb");
     if (!f) return false;
     const bool counts = !s->freq.empty();
     std::string buf = counts ? "cdr3,count\n" : "cdr3\n";
     for (int64_t i = 0; i < rows; i++) {
+        if (s->offs[i + 1] - s->offs[i] > max_len) continue;
         buf.append(s->chars.data() + s->offs[i], s->offs[i + 1] - s->offs[i]);
         if (counts) {
             buf.push_back(',');
@@ -278,13 +280,21 @@ int main(int argc, char** argv) {
         fprintf(stderr, "usage: xtn_synth mutants|clusters|repertoires ... (see synth.cpp)\n");
         return 1;
     }
-    const int64_t n = (int64_t)s->offs.size() - 1;
-    if (!write_rows(s, n, argv[next])) return 1;
+    int64_t n = (int64_t)s->offs.size() - 1;
+    const uint32_t max_len = (kind == "repertoires" && argc > next + 2) ? (uint32_t)atoi(argv[next + 2]) : 0xffffffffu;
+    if (!write_rows(s, n, argv[next], max_len)) return 1;
     if (kind == "repertoires") {
         FILE* f = fopen(argv[next + 1], "wb");
         if (!f) return 1;
         fputs("size\n", f);
-        for (int32_t r : s->rep_sizes) fprintf(f, "%d\n", r);
+        int64_t row = 0, kept_total = 0;
+        for (int32_t r : s->rep_sizes) {
+            int32_t kept = 0;
+            for (int32_t k = 0; k < r; k++, row++) kept += s->offs[row + 1] - s->offs[row] <= max_len;
+            if (kept > 0) fprintf(f, "%d\n", kept);
+            kept_total += kept;
+        }
+        n = kept_total;
         if (fclose(f) != 0) return 1;
     } else if (argc > next + 2) {
         const int64_t k = std::min<int64_t>(n, atoll(argv[next + 1]));
