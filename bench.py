@@ -553,32 +553,48 @@ def run_ours(args, w):
 
 
 def measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, plain_ms, plain_out):
+    """The plain form (the headline's search: one launch sequence per search that reads sizes
+    back between its stages, default shapes) against the batched/persistent form (shapes from
+    the autotuner, which also picks between the plain and the CUDA-graph form; the graph form is
+    the whole search captured once and replayed with every size read on the device), same
+    inputs and timing, in a second context."""
     import torch
 
+    import xtn
+
     ctx.set_profiling(False)
-    ctx.set_option("graph", 1)
-    fn = lambda: ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+    b = xtn.Context(ctx_device(ctx))
+    report = b.autotune(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"], repeats=2)
+    fn = lambda: b.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
     times, out = [], None
-    for i in range(1 + args.warmup + args.steps):  # the first search runs plain and captures
+    for i in range(1 + args.warmup + args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(ext)
+        bext = torch.cuda.ExternalStream(b.stream())
+        e0.record(bext)
         out = fn()
-        e1.record(ext)
+        e1.record(bext)
         e1.synchronize()
         if i > args.warmup:
             times.append(e0.elapsed_time(e1))
-    st = ctx.stats()
-    ctx.set_option("graph", 0)
-    assert out == plain_out, "graph form and plain form differ in output length"
+    st = b.stats()
+    b.close()
+    assert out == plain_out, "batched and plain forms differ in output length"
     g = sum(times) / len(times)
     return {"plain": {"value": n / (plain_ms / 1e3), "ms_per_step": plain_ms,
-                      "what": "one launch sequence per search, four host reads of sizes"},
-            "batched_graph": {"value": n / (g / 1e3), "ms_per_step": g, "launches_in_graph": st["n_launches"],
-                              "what": "whole search captured once in a CUDA graph, sizes read on the device, "
-                                      "grouping by persistent CTAs, one host read per search"},
+                      "what": "one launch sequence per search, four host reads of sizes, default shapes"},
+            "batched": {"value": n / (g / 1e3), "ms_per_step": g, "launches": st["n_launches"],
+                        "autotuned": report,
+                        "what": "autotuned shapes; with graph=1 the whole search captured once in a CUDA graph, "
+                                "sizes read on the device, grouping by persistent CTAs, one host read per search"},
             "batched_over_plain": plain_ms / g}
+
+
+def ctx_device(ctx):
+    import torch
+
+    return torch.cuda.current_device()
 
 
 def measure_extra(ctx, w, args, flush, ext):

@@ -209,6 +209,12 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     is redone by the plain form, which re-sizes the graph. 0 = the plain
  *                     form (default): one launch sequence per search that reads sizes back to
  *                     the host between its stages
+ *   "verify_per"      1 | 4 | 8: the verification variant - candidates each lane of a warp lists
+ *                     before the warp verifies them (default 4)
+ *   "autotune"        1 = xtn_context_nn_device takes its shape (the options the autotuner
+ *                     sets) from the context's cache for the input's class, and on a miss runs
+ *                     the autotuner on the input first (see xtn_context_autotune); 0 = the
+ *                     shape is what the options say (default)
  *   "wait_polls"      1..4194304: bound on the polls of one look-back wait in the single-pass
  *                     prefix sums (default 4194304); a wait that reaches it makes the call
  *                     return XTN_ERR_CUDA and the result is discarded
@@ -219,11 +225,14 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length
- * distribution and duplicate structure) for each bucket-engine shape - first-level and split
- * stage chunks, first-level bucket bits, then bulk-copy or plain loads in the grouping kernel -
- * taking the best of `repeats` runs after a warm-up, and leaves the fastest shape set on the
- * context. `report` (may be NULL) receives the choice and its time. No counterpart in the
- * reference, which has fixed chunk sizes (xtneighbor_streaming/src/xtn.cu:21-26). */
+ * distribution and duplicate structure) for each shape - first-level and split stage chunks and
+ * first-level bucket bits, then, on the best of those, bulk-copy or plain loads in the grouping
+ * kernel, the verification variants (verify_per 1 and 8) and the graph form - taking the best of
+ * `repeats` runs after a warm-up, and leaves the fastest shape set on the context. The choice is
+ * also remembered for the input's class (log2 of the sequence count, distance, measure, median
+ * sequence length, share of sequences longer than the 18-residue key), which option "autotune"
+ * uses. `report` (may be NULL) receives the choice, its time and the class. No counterpart in
+ * the reference, which has fixed chunk sizes (xtneighbor_streaming/src/xtn.cu:21-26). */
 int xtn_context_autotune(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
                          int32_t n_seqs, int32_t repeats, char* report, int32_t report_cap);
 

@@ -78,3 +78,30 @@ def test_graph_form_rejects_bad_lengths():
         exp_p, exp_d, _ = orc.nn_search(chars, offs, 2, 0)
         got = ctx.fetch(m)
         assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, "graph form after a rejected input")
+
+
+@pytest.mark.parametrize("per", [1, 8])
+def test_verification_variants_exact(per):
+    chars, offs = xtn.synth_clusters(seed=7, n=60_000)
+    exp_p, exp_d, _ = orc.nn_search(chars, offs, 2, 0)
+    with xtn.Context(0, verify_per=per) as ctx:
+        got = ctx.perform(chars, offs, distance=2)
+    assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, f"verify_per={per}")
+
+
+def test_autotune_cache_by_input_class():
+    """Option autotune: the first search of an input class runs the autotuner (which may pick
+    the graph form), later searches of the class reuse its choice; results stay exact."""
+    import torch
+
+    chars, offs = xtn.synth_clusters(seed=13, n=50_000)
+    exp_p, exp_d, _ = orc.nn_search(chars, offs, 2, 0)
+    dch, dof = on_device(torch, chars, offs)
+    with xtn.Context(0, autotune=1) as ctx:
+        for _ in range(3):
+            m = ctx.nn_device(dch.data_ptr(), dof.data_ptr(), 50_000, 2, 0)
+            got = ctx.fetch(m)
+            assert_same_pairs(got.pairs, got.distances, exp_p, exp_d, "autotuned")
+    with xtn.Context(0) as ctx:
+        report = ctx.autotune(dch.data_ptr(), dof.data_ptr(), 50_000, distance=2, repeats=1)
+        assert "verify_per=" in report and "graph=" in report and "median_len=" in report

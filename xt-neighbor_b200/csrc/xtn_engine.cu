@@ -324,26 +324,31 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
 // x != y, is verified; the others get distance 0 and are not kept. Most candidates are repeats
 // (a close pair shares many deletion variants), so each warp takes kVerifyPer * 32 consecutive
 // candidates, lists the ones to verify in shared memory and spreads them over its lanes.
+// The verification variant (context option verify_per, chosen by the autotuner) is the number
+// of candidates per lane a warp lists before verifying: more amortises the listing over repeats
+// of sorted candidates, fewer keeps the lanes busier when the candidates are distinct already.
 constexpr int kVerifyPer = 4;
 constexpr int kVerifyWarps = kThreads / 32;
 
-__global__ void __launch_bounds__(kThreads) k_verify(const uint64_t* __restrict__ pairs, int64_t P, int idbits,
-                                                     const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
-                                                     const int32_t* __restrict__ rows, int d, int measure,
-                                                     int8_t* __restrict__ dist, uint8_t* __restrict__ flag,
-                                                     const unsigned long long* __restrict__ P_dev) {
-    __shared__ uint64_t s_pair[kVerifyWarps][32 * kVerifyPer];
-    __shared__ uint8_t s_slot[kVerifyWarps][32 * kVerifyPer];
+template <int PER>
+__global__ void __launch_bounds__(kThreads) k_verify_t(const uint64_t* __restrict__ pairs, int64_t P, int idbits,
+                                                       const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs,
+                                                       const int32_t* __restrict__ rows, int d, int measure,
+                                                       int8_t* __restrict__ dist, uint8_t* __restrict__ flag,
+                                                       const unsigned long long* __restrict__ P_dev) {
+    static_assert(PER >= 1 && PER <= 8, "slots are 8-bit");
+    __shared__ uint64_t s_pair[kVerifyWarps][32 * PER];
+    __shared__ uint8_t s_slot[kVerifyWarps][32 * PER];
     if (P_dev) P = (int64_t)min((unsigned long long)P, *P_dev);  // graph form: grid sized for P at most
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t base = ((int64_t)blockIdx.x * kVerifyWarps + warp) * (32 * kVerifyPer);
+    const int64_t base = ((int64_t)blockIdx.x * kVerifyWarps + warp) * (32 * PER);
     if (base >= P) return;  // whole warp
     const uint64_t idmask = (1ull << idbits) - 1ull;
     const unsigned lt = (1u << lane) - 1u;
     uint64_t carry = base > 0 ? pairs[base - 1] : 0ull;  // the candidate before each row's lane 0
     uint32_t n_work = 0;
 #pragma unroll
-    for (int k = 0; k < kVerifyPer; k++) {
+    for (int k = 0; k < PER; k++) {
         const int64_t i = base + k * 32 + lane;
         const bool in = i < P;
         const uint64_t p = in ? pairs[i] : 0ull;
@@ -436,6 +441,22 @@ static int id_bits_for(int64_t n) {
     return b;
 }
 
+// Launches the verification variant `per` (1, 4 or 8) over capacity P (device count P_dev).
+static void launch_verify(int per, const uint64_t* pairs, int64_t P, int idbits, const uint8_t* chars,
+                          const uint32_t* offs, const int32_t* rows, int d, int measure, int8_t* dist, uint8_t* flag,
+                          const unsigned long long* P_dev, cudaStream_t s) {
+    if (per == 1)
+        XTN_LAUNCH("verify", k_verify_t<1><<<blocks_for(P, kThreads * 1), kThreads, 0, s>>>(
+                                 pairs, P, idbits, chars, offs, rows, d, measure, dist, flag, P_dev));
+    else if (per == 8)
+        XTN_LAUNCH("verify", k_verify_t<8><<<blocks_for(P, kThreads * 8), kThreads, 0, s>>>(
+                                 pairs, P, idbits, chars, offs, rows, d, measure, dist, flag, P_dev));
+    else
+        XTN_LAUNCH("verify", k_verify_t<kVerifyPer><<<blocks_for(P, kThreads * kVerifyPer), kThreads, 0, s>>>(
+                                 pairs, P, idbits, chars, offs, rows, d, measure, dist, flag, P_dev));
+}
+
+
 }  // namespace xtn
 
 using namespace xtn;
@@ -467,6 +488,7 @@ struct xtn_context {
     int scatter_ctas_per_sm = 0;  // 0: as many as the stage shape's shared memory allows
     int group_tma = 1;
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
+    int verify_per = kVerifyPer;  // verification variant: candidates listed per lane (1, 4, 8)
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
@@ -485,6 +507,10 @@ struct xtn_context {
     // graph form of the device-resident search (option "graph")
     int graph_mode = 0;
     void* graph = nullptr;  // GraphState (below)
+    // autotuner: shapes chosen per input class (see TuneKey), and whether device-resident
+    // searches consult (and fill) that cache by themselves
+    int autotune_auto = 0;
+    void* tune_cache = nullptr;
     // results
     DevBuf out_pairs, out_dist, out_freq;
     uint64_t* h_scalar = nullptr;  // pinned
@@ -1309,8 +1335,8 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (Pc + 1)));
     uint64_t nout = 0;
     if (Pc > 0) {
-        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure,
-                                                              P<int8_t>(c->dist), P<uint8_t>(c->flag), nullptr));
+        launch_verify(c->verify_per, pairs, (int64_t)Pc, idbits, chars, offs, rows, d, measure, P<int8_t>(c->dist),
+                      P<uint8_t>(c->flag), nullptr, s);
         XTN_CK(cudaGetLastError());
         XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)Pc)));
         XTN_CK(cudaEventRecord(c->ev[7], s));
@@ -1412,7 +1438,8 @@ __global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned in
 static int64_t graph_signature(const xtn_context* c) {
     return ((int64_t)c->stage_chunk << 40) ^ ((int64_t)c->split_chunk << 28) ^ ((int64_t)c->bucket_bits_max << 20) ^
            ((int64_t)c->group_cap << 4) ^ ((int64_t)c->group_tma << 1) ^ ((int64_t)c->key_tables << 2) ^
-           ((int64_t)c->split_slices << 16) ^ ((int64_t)c->scatter_ctas_per_sm << 48) ^ ((int64_t)c->pair_dedup << 52);
+           ((int64_t)c->split_slices << 16) ^ ((int64_t)c->scatter_ctas_per_sm << 48) ^ ((int64_t)c->pair_dedup << 52) ^
+           ((int64_t)c->verify_per << 56);
 }
 
 static void graph_release(GraphState* g) {
@@ -1510,9 +1537,8 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
                               (int64_t)(g->os_status.cap / 8), &g->os_epoch, P<unsigned int>(c->dev_err), c->sms, s,
                               "pair_sort_hist", "pair_sort_pass", ddcnt);
     g->result = pairs;
-    XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)g->Ucap, kThreads * kVerifyPer), kThreads, 0, s>>>(
-                             pairs, (int64_t)g->Ucap, idbits, g->chars, g->offs, nullptr, d, g->measure,
-                             P<int8_t>(c->dist), P<uint8_t>(c->flag), ddcnt));
+    launch_verify(c->verify_per, pairs, (int64_t)g->Ucap, idbits, g->chars, g->offs, nullptr, d, g->measure,
+                  P<int8_t>(c->dist), P<uint8_t>(c->flag), ddcnt, s);
     scan_exclusive_1p<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)g->Ucap,
                                          P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err), s,
                                          c->wait_polls, 0, ddcnt);
@@ -2117,6 +2143,186 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
 
 }  // namespace xtn
 
+namespace xtn {
+// ------------------------------------------------------------------ autotuner
+// The shape of a search - first-level and split stage chunks, first-level bucket bits, bulk-copy
+// or plain loads in the grouping kernel, the verification variant, and the plain or graph
+// form - chosen by timing on the caller's device-resident data, and remembered per input class:
+// the size (log2 n), distance, measure, the median sequence length and the share of sequences
+// longer than the 18-residue key (whose pairs take the long verification path). The reference's
+// sizes are fixed (xtneighbor_streaming/src/xtn.cu:21-26).
+struct TuneShape {
+    int stage, split, bits, tma, verify, graph;
+};
+struct TuneKey {
+    int log2n, d, measure, len_med, long_share;  // long_share in percent
+    bool operator==(const TuneKey& o) const {
+        return log2n == o.log2n && d == o.d && measure == o.measure && len_med == o.len_med &&
+               long_share == o.long_share;
+    }
+};
+struct TuneCache {
+    std::vector<std::pair<TuneKey, TuneShape>> entries;
+};
+
+constexpr int kLenBins = 34;  // lengths 0..32, then longer
+
+__global__ void k_len_hist(const uint32_t* __restrict__ offs, int n, unsigned int* __restrict__ hist) {
+    __shared__ unsigned int h[kLenBins];
+    for (int i = threadIdx.x; i < kLenBins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t L = offs[i + 1] - offs[i];
+        atomicAdd(&h[L < (uint32_t)kLenBins - 1 ? L : kLenBins - 1], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kLenBins; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+static int tune_key(xtn_context* c, const uint32_t* offs, int n, int d, int measure, TuneKey* key) {
+    XTN_TRY(ensure(c->scratch64, sizeof(unsigned int) * kLenBins));
+    XTN_CK(cudaMemsetAsync(c->scratch64.p, 0, sizeof(unsigned int) * kLenBins, c->stream));
+    XTN_LAUNCH("len_hist", k_len_hist<<<std::max(1, std::min<int>((n + kThreads - 1) / kThreads, c->sms * 4)), kThreads,
+                                        0, c->stream>>>(offs, n, P<unsigned int>(c->scratch64)));
+    unsigned int h[kLenBins];
+    XTN_CK(cudaMemcpyAsync(h, c->scratch64.p, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    int64_t acc = 0, longer = 0;
+    int med = 0;
+    for (int b = 0; b < kLenBins; b++) {
+        if (acc * 2 < n) med = b;
+        acc += h[b];
+        if (b > kKeyLen) longer += h[b];
+    }
+    key->log2n = id_bits_for(n);
+    key->d = d;
+    key->measure = measure;
+    key->len_med = med;
+    key->long_share = (int)(100 * longer / std::max(1, n));
+    return XTN_SUCCESS;
+}
+
+static void tune_apply(xtn_context* c, const TuneShape& sh) {
+    c->stage_chunk = sh.stage;
+    c->split_chunk = sh.split;
+    c->bucket_bits_max = sh.bits;
+    c->group_tma = sh.tma;
+    c->verify_per = sh.verify;
+    c->graph_mode = sh.graph;
+}
+
+static int nn_graph(xtn_context* c, const uint8_t* chars, const uint32_t* offs, int n, int d, int measure);
+
+// One search as the context's shape says (plain or graph form).
+static int tuned_search(xtn_context* c, const uint8_t* chars, const uint32_t* offs, int n, int d, int measure) {
+    if (c->graph_mode) return nn_graph(c, chars, offs, n, d, measure);
+    begin_run(c);
+    const int r = run_nn(c, chars, offs, nullptr, n, d, measure, true);
+    end_run(c);
+    return r;
+}
+
+static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, const uint32_t* offs, int n,
+                    int repeats, char* report, int report_cap) {
+    if (repeats < 1) repeats = 2;
+    const int d = args->distance, measure = args->measure;
+    TuneKey key{};
+    XTN_TRY(tune_key(c, offs, n, d, measure, &key));
+    const TuneShape saved{c->stage_chunk, c->split_chunk, c->bucket_bits_max, c->group_tma, c->verify_per, c->graph_mode};
+    const int saved_engine = c->engine;
+    c->engine = 0;
+    auto time_shape = [&](const TuneShape& sh, float* ms) -> int {
+        tune_apply(c, sh);
+        float best = 1e30f;
+        for (int r = 0; r <= repeats + sh.graph; r++) {  // warm-up first (the graph form: plain + capture too)
+            const int st = tuned_search(c, chars, offs, n, d, measure);
+            if (st != XTN_SUCCESS) return st;
+            if (r > sh.graph) best = std::min(best, (float)c->stats.ms_total);
+        }
+        *ms = best;
+        return XTN_SUCCESS;
+    };
+    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, kVerifyPer, 0};
+    float best_ms = 1e30f;
+    int tried = 0;
+    auto consider = [&](const TuneShape& sh) -> int {
+        float ms = 0;
+        const int st = time_shape(sh, &ms);
+        if (st != XTN_SUCCESS) return st;
+        tried++;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = sh;
+        }
+        return XTN_SUCCESS;
+    };
+    int st = XTN_SUCCESS;
+    // stage shapes and first-level bits
+    for (int stage : {4096, 2048})
+        for (int split : {4096, 2048})
+            for (int bits : {9, 10}) {
+                if (st != XTN_SUCCESS) break;
+                if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
+                st = consider(TuneShape{stage, split, bits, 1, kVerifyPer, 0});
+            }
+    // then, one at a time on the best so far: plain loads in grouping, the verification
+    // variants, the graph form
+    if (st == XTN_SUCCESS) {
+        TuneShape sh = best;
+        sh.tma = 0;
+        st = consider(sh);
+    }
+    for (int per : {1, 8}) {
+        if (st != XTN_SUCCESS) break;
+        TuneShape sh = best;
+        sh.verify = per;
+        st = consider(sh);
+    }
+    if (st == XTN_SUCCESS) {
+        TuneShape sh = best;
+        sh.graph = 1;
+        st = consider(sh);
+    }
+    c->engine = saved_engine;
+    if (st != XTN_SUCCESS) {
+        tune_apply(c, saved);
+        return st;
+    }
+    tune_apply(c, best);
+    if (!c->tune_cache) c->tune_cache = new TuneCache();
+    TuneCache* tc = static_cast<TuneCache*>(c->tune_cache);
+    bool stored = false;
+    for (auto& e : tc->entries)
+        if (e.first == key) {
+            e.second = best;
+            stored = true;
+        }
+    if (!stored) tc->entries.push_back({key, best});
+    if (report && report_cap > 0)
+        snprintf(report, (size_t)report_cap,
+                 "stage_chunk=%d split_chunk=%d bucket_bits_max=%d group_tma=%d verify_per=%d graph=%d: %.3f ms "
+                 "(best of %d shapes; input class log2n=%d d=%d measure=%d median_len=%d longer_than_key=%d%%)",
+                 best.stage, best.split, best.bits, best.tma, best.verify, best.graph, best_ms, tried, key.log2n,
+                 key.d, key.measure, key.len_med, key.long_share);
+    return XTN_SUCCESS;
+}
+
+// Option autotune = 1: the shape for this input's class comes from the cache, or is tuned now.
+static int autotune_lookup(xtn_context* c, const xtn_args* args, const uint8_t* chars, const uint32_t* offs, int n) {
+    TuneKey key{};
+    XTN_TRY(tune_key(c, offs, n, args->distance, args->measure, &key));
+    if (c->tune_cache)
+        for (const auto& e : static_cast<TuneCache*>(c->tune_cache)->entries)
+            if (e.first == key) {
+                tune_apply(c, e.second);
+                return XTN_SUCCESS;
+            }
+    return autotune(c, args, chars, offs, n, 2, nullptr, 0);
+}
+
+}  // namespace xtn
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -2177,6 +2383,7 @@ void xtn_context_destroy(xtn_context* c) {
                       &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
                       &c->ktab,    &c->info,     &c->lencheck, &c->pairA2, &c->ddcnt, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
     for (DevBuf* b : bufs) release(*b);
+    delete static_cast<TuneCache*>(c->tune_cache);
     if (c->graph) {
         GraphState* g = static_cast<GraphState*>(c->graph);
         graph_release(g);
@@ -2223,6 +2430,8 @@ int xtn_context_nn_device(xtn_context* c, const xtn_args* args, const char* d_se
     }
     XTN_TRY(check_args(args));
     XTN_CK(cudaSetDevice(c->device));
+    if (c->autotune_auto)
+        XTN_TRY(autotune_lookup(c, args, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n));
     int r;
     if (c->graph_mode) {
         r = nn_graph(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n, args->distance, args->measure);
@@ -2327,6 +2536,8 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "max_round_records") && v >= 0) c->max_round_records = v;
     else if (!strcmp(name, "round_overlap") && (v == 0 || v == 1)) c->round_overlap = (int)v;
     else if (!strcmp(name, "graph") && (v == 0 || v == 1)) c->graph_mode = (int)v;
+    else if (!strcmp(name, "verify_per") && (v == 1 || v == 4 || v == 8)) c->verify_per = (int)v;
+    else if (!strcmp(name, "autotune") && (v == 0 || v == 1)) c->autotune_auto = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
@@ -2343,82 +2554,7 @@ int xtn_context_autotune(xtn_context* c, const xtn_args* args, const char* d_seq
     }
     XTN_TRY(check_args(args));
     XTN_CK(cudaSetDevice(c->device));
-    if (repeats < 1) repeats = 2;
-    // the bucket engine's shapes: first-level and split stage chunks, first-level bucket bits,
-    // bulk copy or plain loads in the grouping kernel
-    struct Shape {
-        int stage, split, bits, tma;
-    };
-    std::vector<Shape> shapes;
-    for (int stage : {4096, 2048})
-        for (int split : {4096, 2048})
-            for (int bits : {9, 10}) {
-                if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
-                shapes.push_back(Shape{stage, split, bits, 1});
-            }
-    const Shape saved{c->stage_chunk, c->split_chunk, c->bucket_bits_max, c->group_tma};
-    const int saved_engine = c->engine;
-    c->engine = 0;
-    auto apply = [&](const Shape& sh) {
-        c->stage_chunk = sh.stage;
-        c->split_chunk = sh.split;
-        c->bucket_bits_max = sh.bits;
-        c->group_tma = sh.tma;
-    };
-    auto time_shape = [&](const Shape& sh, float* ms) -> int {
-        apply(sh);
-        float best = 1e30f;
-        for (int r = 0; r <= repeats; r++) {  // the first run is a warm-up
-            begin_run(c);
-            int st = run_nn(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, nullptr, n, args->distance,
-                            args->measure, true);
-            end_run(c);
-            if (st != XTN_SUCCESS) return st;
-            float t = (float)c->stats.ms_total;
-            if (r > 0) best = std::min(best, t);
-        }
-        *ms = best;
-        return XTN_SUCCESS;
-    };
-    Shape best_shape = shapes[0];
-    float best_ms = 1e30f;
-    int tried = 0;
-    for (const Shape& sh : shapes) {
-        float ms = 0;
-        int st = time_shape(sh, &ms);
-        if (st != XTN_SUCCESS) {
-            apply(saved);
-            c->engine = saved_engine;
-            return st;
-        }
-        tried++;
-        if (ms < best_ms) {
-            best_ms = ms;
-            best_shape = sh;
-        }
-    }
-    {  // the grouping kernel's load path, on the best shape
-        Shape sh = best_shape;
-        sh.tma = 0;
-        float ms = 0;
-        int st = time_shape(sh, &ms);
-        if (st != XTN_SUCCESS) {
-            apply(saved);
-            c->engine = saved_engine;
-            return st;
-        }
-        tried++;
-        if (ms < best_ms) {
-            best_ms = ms;
-            best_shape = sh;
-        }
-    }
-    apply(best_shape);
-    if (report && report_cap > 0)
-        snprintf(report, (size_t)report_cap,
-                 "stage_chunk=%d split_chunk=%d bucket_bits_max=%d group_tma=%d: %.3f ms (best of %d shapes)",
-                 best_shape.stage, best_shape.split, best_shape.bits, best_shape.tma, best_ms, tried);
-    return XTN_SUCCESS;
+    return autotune(c, args, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, n, repeats, report, report_cap);
 }
 
 int xtn_context_set_profiling(xtn_context* c, int on) {
@@ -2616,9 +2752,7 @@ static int nn_search_static(const uint8_t* chars, const uint32_t* offs, int n, i
         uint64_t* pairs = Pc > 1 ? radix_sort_u64(pairA, pairB, (int64_t)Pc, 0, 2 * idbits, pscratch, s,
                                                   "pair_sort_upsweep", "pair_sort_downsweep")
                                  : pairA;
-        XTN_LAUNCH("verify", k_verify<<<blocks_for((int64_t)Pc, kThreads * kVerifyPer), kThreads, 0, s>>>(pairs, (int64_t)Pc, idbits, chars,
-                                                                                    offs, nullptr, d, measure, dist, flag,
-                                                                                    nullptr));
+        launch_verify(kVerifyPer, pairs, (int64_t)Pc, idbits, chars, offs, nullptr, d, measure, dist, flag, nullptr, s);
         scan_exclusive<uint8_t, uint32_t>(flag, fpos, (int64_t)Pc, pscratch, s);
         XTN_TRY(read_u64(fpos + Pc, 4, s, &nout));
         if ((int64_t)nout > out_cap) {
