@@ -254,6 +254,10 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
 // bits (2 * id_bits <= 48, n <= 2^24). Slot hash: the SplitMix64 finaliser (Steele, Lea and
 // Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014). With uniq == nullptr
 // the pairs are only inserted (the rebuild of a grown table from the distinct list).
+// Partitions: a table larger than L2 makes every first insertion a DRAM access, so the table is
+// cut into 2^part_bits regions of 2^k slots each, the top part_bits bits of a pair's slot hash
+// choosing the region; one launch per region passes over all candidates and inserts those of
+// its region, so the region it probes stays in L2.
 constexpr int kDedupKeyBits = 48;
 constexpr int kDedupTagBits = 64 - kDedupKeyBits;
 constexpr uint64_t kDedupTagMask = ~((1ull << kDedupKeyBits) - 1ull);
@@ -273,9 +277,11 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
                                                          uint64_t tag, uint64_t* __restrict__ uniq,
                                                          unsigned long long* __restrict__ n_uniq,
                                                          unsigned long long* __restrict__ n_full,
-                                                         const unsigned long long* __restrict__ P_dev) {
+                                                         const unsigned long long* __restrict__ P_dev, int part_bits,
+                                                         uint32_t part) {
     // P_dev (graph form): the count is read on the device (at most P) and the grid strides
     if (P_dev) P = (int64_t)min((unsigned long long)P, *P_dev);
+    table += (size_t)part * (tmask + 1);  // this region
     const unsigned lane = threadIdx.x & 31u;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t w0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < P; w0 += stride) {
@@ -285,9 +291,10 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
         if (i < P) {
             p = pairs[i];
             const uint64_t idmask = (1ull << idbits) - 1ull;
-            if ((p >> idbits) != (p & idmask)) {
+            const uint64_t hm = mix64(p);
+            if ((p >> idbits) != (p & idmask) && (part_bits == 0 || (uint32_t)(hm >> (64 - part_bits)) == part)) {
                 const unsigned long long want = tag | p;
-                uint64_t h = mix64(p) & tmask;
+                uint64_t h = hm & tmask;
                 unsigned long long v = ld_relaxed_u64(table + h);
                 for (uint32_t probes = 0;;) {
                     if ((v & kDedupTagMask) != tag) {  // free in this search
@@ -318,6 +325,27 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
         base = __shfl_sync(0xffffffffu, base, leader);
         if (fresh) uniq[base + __popc(mask & ((1u << lane) - 1u))] = p;
     }
+}
+
+// Table regions: each at most kDedupRegionBytes (half of L2), so one pass's probes stay in L2.
+constexpr uint64_t kDedupRegionBytes = uint64_t(64) << 20;
+
+static int dedup_part_bits(uint64_t T) {
+    int pb = 0;
+    while ((T >> pb) * sizeof(uint64_t) > kDedupRegionBytes && (T >> pb) > 1024) pb++;
+    return pb;
+}
+
+// One pass per table region over the P candidates (grid-stride with `grid` blocks when P_dev
+// gives the count on the device).
+static void launch_pair_dedup(const uint64_t* pairs, int64_t P, int idbits, unsigned long long* table, uint64_t T,
+                              uint64_t tag, uint64_t* uniq, unsigned long long* n_uniq, unsigned long long* n_full,
+                              const unsigned long long* P_dev, unsigned grid, cudaStream_t s) {
+    const int pb = dedup_part_bits(T);
+    const uint64_t region = T >> pb;
+    for (uint32_t part = 0; part < (1u << pb); part++)
+        XTN_LAUNCH("pair_dedup", k_pair_dedup<<<grid, kThreads, 0, s>>>(pairs, P, idbits, table, region - 1, tag, uniq,
+                                                                        n_uniq, n_full, P_dev, pb, part));
 }
 
 // Verification of the sorted candidate pairs. Only the first of each run of equal pairs, with
@@ -1012,11 +1040,9 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
             c->dd_epoch = 1;
         }
         XTN_CK(cudaMemsetAsync(c->counter.p, 0, 16, s));
-        XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc), kThreads, 0, s>>>(
-                                     P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table),
-                                     T - 1, (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB),
-                                     P<unsigned long long>(c->counter), P<unsigned long long>(c->counter) + 1,
-                                     nullptr));
+        launch_pair_dedup(P<uint64_t>(c->pairA), (int64_t)Pc, idbits, P<unsigned long long>(c->dd_table), T,
+                          (uint64_t)c->dd_epoch << kDedupKeyBits, P<uint64_t>(c->pairB), P<unsigned long long>(c->counter),
+                          P<unsigned long long>(c->counter) + 1, nullptr, blocks_for((int64_t)Pc), s);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1158,10 +1184,9 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
     uint64_t U_before[2] = {0, 0}, Pc_r[2] = {0, 0};
     auto launch_dedup = [&](int slot) -> int {
         if (Pc_r[slot] > 0)
-            XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)Pc_r[slot]), kThreads, 0, sd>>>(
-                                         P<uint64_t>(*cand[slot]), (int64_t)Pc_r[slot], idbits,
-                                         P<unsigned long long>(c->dd_table), T - 1, tag, P<uint64_t>(c->pairB), n_uniq,
-                                         n_uniq + 1, nullptr));
+            launch_pair_dedup(P<uint64_t>(*cand[slot]), (int64_t)Pc_r[slot], idbits, P<unsigned long long>(c->dd_table),
+                              T, tag, P<uint64_t>(c->pairB), n_uniq, n_uniq + 1, nullptr,
+                              blocks_for((int64_t)Pc_r[slot]), sd);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 8, c->ddcnt.p, 16, cudaMemcpyDeviceToHost, sd));
         return XTN_SUCCESS;
@@ -1183,10 +1208,9 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
             XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, sd>>>(n_uniq, (unsigned long long)U_before[slot]));
             XTN_CK(cudaMemsetAsync(n_uniq + 1, 0, 8, sd));
             if (U_before[slot] > 0)
-                XTN_LAUNCH("pair_dedup", k_pair_dedup<<<blocks_for((int64_t)U_before[slot]), kThreads, 0, sd>>>(
-                                             P<uint64_t>(c->pairB), (int64_t)U_before[slot], idbits,
-                                             P<unsigned long long>(c->dd_table), T - 1, tag, nullptr, n_uniq,
-                                             n_uniq + 1, nullptr));
+                launch_pair_dedup(P<uint64_t>(c->pairB), (int64_t)U_before[slot], idbits,
+                                  P<unsigned long long>(c->dd_table), T, tag, nullptr, n_uniq, n_uniq + 1, nullptr,
+                                  blocks_for((int64_t)U_before[slot]), sd);
             XTN_TRY(launch_dedup(slot));
         }
     };
@@ -1526,11 +1550,9 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     unsigned long long* ddcnt = P<unsigned long long>(c->ddcnt);
     XTN_CK(cudaMemsetAsync(c->ddcnt.p, 0, 16, s));
     XTN_CK(cudaMemsetAsync(g->table.p, 0, sizeof(uint64_t) * g->T, s));
-    XTN_LAUNCH("pair_dedup", k_pair_dedup<<<(unsigned)std::min<int64_t>(blocks_for((int64_t)g->Pcap), (int64_t)c->sms * 16),
-                                            kThreads, 0, s>>>(
-                                 P<uint64_t>(c->pairA), (int64_t)g->Pcap, idbits, P<unsigned long long>(g->table), g->T - 1,
-                                 1ull << kDedupKeyBits, P<uint64_t>(c->pairB), ddcnt, ddcnt + 1,
-                                 P<unsigned long long>(c->counter)));
+    launch_pair_dedup(P<uint64_t>(c->pairA), (int64_t)g->Pcap, idbits, P<unsigned long long>(g->table), g->T,
+                      1ull << kDedupKeyBits, P<uint64_t>(c->pairB), ddcnt, ddcnt + 1, P<unsigned long long>(c->counter),
+                      (unsigned)std::min<int64_t>(blocks_for((int64_t)g->Pcap), (int64_t)c->sms * 16), s);
     uint64_t* pairs = P<uint64_t>(c->pairB);
     pairs = onesweep_sort_u64(P<uint64_t>(c->pairB), P<uint64_t>(c->pairA), (int64_t)g->Ucap, 0, 2 * idbits,
                               P<uint32_t>(c->os_scratch), P<unsigned long long>(g->os_status),
