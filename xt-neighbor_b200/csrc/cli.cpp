@@ -285,6 +285,16 @@ int parse_input(const char* path, SeqStore* seqs, std::vector<xtn_seq_info>* inf
     if (!f) return print_err("input file reading failed");
     std::vector<char> data;
     {
+        // one read of the whole file when its size is known (a regular file), else in pieces
+        size_t size = 0;
+        if (fseek(f, 0, SEEK_END) == 0) {
+            const long e = ftell(f);
+            if (e > 0) size = (size_t)e;
+            fseek(f, 0, SEEK_SET);
+        }
+        data.resize(size);
+        size_t got = size ? fread(data.data(), 1, size, f) : 0;
+        data.resize(got);
         char buf[1 << 16];
         size_t k;
         while ((k = fread(buf, 1, sizeof buf, f)) > 0) data.insert(data.end(), buf, buf + k);

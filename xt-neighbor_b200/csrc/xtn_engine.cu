@@ -1618,8 +1618,9 @@ static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, cons
     XTN_TRY(ensure(c->dist, (size_t)g->Ucap + 64));
     XTN_TRY(ensure(c->flag, (size_t)g->Ucap + 64));
     XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (g->Ucap + 1)));
-    XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * g->Ucap + 64));
-    XTN_TRY(ensure(c->out_dist, (size_t)g->Ucap + 64));
+    // the plain search's result (c->n_out entries) is still to be read by the caller
+    XTN_TRY(ensure_keep(c, c->out_pairs, sizeof(xtn_int2) * g->Ucap + 64, sizeof(xtn_int2) * (size_t)c->n_out));
+    XTN_TRY(ensure_keep(c, c->out_dist, (size_t)g->Ucap + 64, (size_t)c->n_out));
     XTN_TRY(ensure(c->os_scratch, sizeof(uint32_t) * kOsScratchWords));
     XTN_TRY(ensure_err_word(c));
     XTN_TRY(ensure(c->scan_status, sizeof(unsigned long long) * scan_1p_words((int64_t)std::max<uint64_t>(g->Ucap, n))));
