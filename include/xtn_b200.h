@@ -164,7 +164,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     2048, the first-level scatter stores records one by one)
  *   "group_cap"       2..4096: largest bucket grouped in shared memory; larger ones are split
  *                     by further hash bits, and what still does not fit is grouped by sorting
- *                     (default 4096)
+ *                     (default 4096). At 2048 or below the grouping kernel takes its small
+ *                     shape (256 threads and about 37 KB of shared memory: six CTAs per SM
+ *                     instead of three)
  *   "scatter_ctas_per_sm" 0..4: first-level tiles per SM (default 0: as many CTAs as fit)
  *   "stage_chunk"     2048 | 4096: records per shared-memory chunk of the first-level scatter
  *                     (default 4096: two CTAs per SM; 2048: four)

@@ -57,14 +57,29 @@ struct StageCfg {
 using StageLarge = StageCfg<512, 4096, 1024>;  // ~110 KB of shared memory: two CTAs per SM
 using StageSmall = StageCfg<256, 2048, 512>;   // ~55 KB: four CTAs per SM (first level, b1 <= 9)
 using SplitSmall = StageCfg<256, 2048, 1024>;  // ~60 KB: three CTAs per SM
-constexpr int kGroupThreads = 512;
-constexpr int kGroupCap = 4096;        // records a grouping CTA holds in shared memory
-constexpr int kBitmapLog = 16;         // hash bits of the "seen" / "seen twice" bitmaps
-constexpr int kBitmapBits = 1 << kBitmapLog;
-constexpr int kBitmapWords = kBitmapBits / 32;
-constexpr int kDigitBits = 11;         // hash bits of the candidates' counting sort
-constexpr int kDigits = 1 << kDigitBits;
-// Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to 2048;
+// Shape of a grouping CTA: records it holds in shared memory, threads, hash bits of the
+// "seen" / "seen twice" bitmaps, hash bits of the candidates' counting sort, and minimum CTAs per
+// SM. The large shape (~65 KB of shared memory, three CTAs per SM) holds buckets of up to 4096
+// records; the small one (~37 KB, six CTAs of 256 threads per SM) holds up to 2048, which the
+// split produces when group_cap <= 2048.
+template <int CAP, int THREADS, int BITMAP_LOG, int DIGIT_BITS, int MIN_CTAS>
+struct GroupCfg {
+    static constexpr int kCap = CAP;
+    static constexpr int kThreads = THREADS;
+    static constexpr int kBitmapLog = BITMAP_LOG;
+    static constexpr int kBitmapBits = 1 << BITMAP_LOG;
+    static constexpr int kBitmapWords = kBitmapBits / 32;
+    static constexpr int kDigitBits = DIGIT_BITS;
+    static constexpr int kDigits = 1 << DIGIT_BITS;
+    static constexpr int kMinCtas = MIN_CTAS;
+    static_assert(kDigits % THREADS == 0 && CAP < 65536, "group shape");
+};
+using GroupLarge = GroupCfg<4096, 512, 16, 11, 3>;
+using GroupSmall = GroupCfg<2048, 256, 15, 10, 6>;
+constexpr int kGroupThreads = GroupLarge::kThreads;
+constexpr int kGroupCap = GroupLarge::kCap;        // largest bucket grouped in shared memory
+constexpr int kGroupSmallCap = GroupSmall::kCap;   // group_cap at or below this: the small shape
+// Runs of >= 2 equal hashes one grouping CTA lists (a full bucket could hold up to CAP / 2;
 // buckets with more than this go to the sort-based fallback).
 constexpr int kMaxRuns = 1024;
 
@@ -646,22 +661,23 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
 // ------------------------------------------------------------------ group
 // Shared-memory layout of k_bucket_group (about 65 KB: three CTAs per SM). The two bitmaps
 // are only needed until the candidates are known; the grouping arrays reuse their space.
+template <class G>
 struct GroupSmem {
-    uint64_t rec[kGroupCap + 2];  // bucket records (+ alignment slack)
+    uint64_t rec[G::kCap + 2];  // bucket records (+ alignment slack)
     union {
         struct {
-            uint32_t seen[kBitmapWords];   // hash bit seen once
-            uint32_t twice[kBitmapWords];  // hash bit seen at least twice
+            uint32_t seen[G::kBitmapWords];   // hash bit seen once
+            uint32_t twice[G::kBitmapWords];  // hash bit seen at least twice
         } bm;
         struct {
-            uint16_t perm[kGroupCap];  // candidate record indexes grouped by digit
+            uint16_t perm[G::kCap];    // candidate record indexes grouped by digit
             uint32_t runs[kMaxRuns];   // contiguous << 31 | size << 16 | head slot, per run of >= 2
             uint32_t poff[kMaxRuns];   // first pair index of each run
         } gr;
     } u;
-    uint16_t cand[kGroupCap];  // records whose bitmap bit was hit at least twice
-    uint32_t cnt[kDigits];     // digit counts -> digit ends
-    uint32_t warp_sums[kGroupThreads / 32 + 1];
+    uint16_t cand[G::kCap];     // records whose bitmap bit was hit at least twice
+    uint32_t cnt[G::kDigits];   // digit counts -> digit ends
+    uint32_t warp_sums[G::kThreads / 32 + 1];
     uint32_t wait_failed;
     uint32_t n_cand;
     unsigned long long base;
@@ -691,7 +707,8 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 // count (the graph form).
 constexpr int kCntNext = 7;  // the persistent grouping's queue position
 
-__global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketDesc* __restrict__ descs,
+template <class G>
+__global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const BucketDesc* __restrict__ descs,
                                                                      const uint64_t* __restrict__ buf_a,
                                                                      const uint64_t* __restrict__ buf_b, int idbits,
                                                                      uint64_t* __restrict__ pairs, uint64_t cap,
@@ -702,7 +719,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
                                                                      unsigned int* __restrict__ counters,
                                                                      const unsigned int* __restrict__ n_desc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    GroupSmem& S = *reinterpret_cast<GroupSmem*>(smem_raw);
+    GroupSmem<G>& S = *reinterpret_cast<GroupSmem<G>*>(smem_raw);
     const uint32_t mbar = smem_u32(&S.mbar);
     if (use_tma && threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -740,13 +757,13 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     } else {
         const uint4* g = reinterpret_cast<const uint4*>(src16);
         uint4* dd = reinterpret_cast<uint4*>(&S.rec[0]);
-        for (uint32_t i = threadIdx.x; i < bytes / 16; i += kGroupThreads) dd[i] = __ldg(g + i);
+        for (uint32_t i = threadIdx.x; i < bytes / 16; i += G::kThreads) dd[i] = __ldg(g + i);
     }
-    for (int i = threadIdx.x; i < kBitmapWords; i += kGroupThreads) {
+    for (int i = threadIdx.x; i < G::kBitmapWords; i += G::kThreads) {
         S.u.bm.seen[i] = 0;
         S.u.bm.twice[i] = 0;
     }
-    for (int i = threadIdx.x; i < kDigits; i += kGroupThreads) S.cnt[i] = 0;
+    for (int i = threadIdx.x; i < G::kDigits; i += G::kThreads) S.cnt[i] = 0;
     if (use_tma && threadIdx.x == 0) {
         // one thread polls the barrier (sleeping between polls); the others wait at __syncthreads
         uint32_t polls = 0;
@@ -773,8 +790,8 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     const uint64_t idmask = (1ull << idbits) - 1ull;
 
     // 1. bitmap filter
-    for (uint32_t i = threadIdx.x; i < n; i += kGroupThreads) {
-        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+    for (uint32_t i = threadIdx.x; i < n; i += G::kThreads) {
+        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (G::kBitmapBits - 1);
         const uint32_t bit = 1u << (b & 31);
         if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
     }
@@ -782,11 +799,11 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     __syncthreads();
     // candidates in any order (one shared atomic per warp and round)
     const unsigned lane = threadIdx.x & 31u;
-    for (uint32_t i0 = threadIdx.x & ~31u; i0 < n; i0 += kGroupThreads) {
+    for (uint32_t i0 = threadIdx.x & ~31u; i0 < n; i0 += G::kThreads) {
         const uint32_t i = i0 + lane;
         bool hit = false;
         if (i < n) {
-            const uint32_t b = (uint32_t)(rec[i] >> idbits) & (kBitmapBits - 1);
+            const uint32_t b = (uint32_t)(rec[i] >> idbits) & (G::kBitmapBits - 1);
             hit = (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
         }
         const unsigned mask = __ballot_sync(0xffffffffu, hit);
@@ -800,10 +817,10 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     const uint32_t m = S.n_cand;
 
     // 2. counting sort of the candidates by kDigitBits hash bits above the bitmap bits
-    for (uint32_t c = threadIdx.x; c < m; c += kGroupThreads)
-        atomicAdd(&S.cnt[(uint32_t)(rec[S.cand[c]] >> (idbits + kBitmapLog)) & (kDigits - 1)], 1u);
+    for (uint32_t c = threadIdx.x; c < m; c += G::kThreads)
+        atomicAdd(&S.cnt[(uint32_t)(rec[S.cand[c]] >> (idbits + G::kBitmapLog)) & (G::kDigits - 1)], 1u);
     __syncthreads();
-    constexpr int kPer = kDigits / kGroupThreads;
+    constexpr int kPer = G::kDigits / G::kThreads;
     {
         const int d0 = threadIdx.x * kPer;
         uint32_t loc[kPer], sum = 0;
@@ -813,14 +830,14 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
             sum += S.cnt[d0 + k];
         }
         uint32_t tot;
-        const uint32_t ex = block_scan_ex<uint32_t, kGroupThreads>(sum, &tot, S.warp_sums);
+        const uint32_t ex = block_scan_ex<uint32_t, G::kThreads>(sum, &tot, S.warp_sums);
 #pragma unroll
         for (int k = 0; k < kPer; k++) S.cnt[d0 + k] = ex + loc[k];
     }
     __syncthreads();
-    for (uint32_t c = threadIdx.x; c < m; c += kGroupThreads) {
+    for (uint32_t c = threadIdx.x; c < m; c += G::kThreads) {
         const uint16_t i = S.cand[c];
-        const uint32_t p = atomicAdd(&S.cnt[(uint32_t)(rec[i] >> (idbits + kBitmapLog)) & (kDigits - 1)], 1u);
+        const uint32_t p = atomicAdd(&S.cnt[(uint32_t)(rec[i] >> (idbits + G::kBitmapLog)) & (G::kDigits - 1)], 1u);
         S.u.gr.perm[p] = i;
     }
     __syncthreads();
@@ -829,7 +846,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     // 3. runs
     auto scan_pos = [&](uint32_t i, uint32_t& size, uint32_t& contiguous) -> bool {
         const uint64_t kv = rec[S.u.gr.perm[i]] >> idbits;
-        const uint32_t dg = (uint32_t)(kv >> kBitmapLog) & (kDigits - 1);
+        const uint32_t dg = (uint32_t)(kv >> G::kBitmapLog) & (G::kDigits - 1);
         const uint32_t a = dg == 0 ? 0u : S.cnt[dg - 1], b = S.cnt[dg];
         if (b - a < 2) return false;
         for (uint32_t y = a; y < i; y++)
@@ -843,24 +860,24 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     // each slot's run word (contiguous << 15 | size for a run head, 0 otherwise) is kept in
     // `cand`, which the counting sort no longer needs, for the second pass
     uint32_t my_runs = 0, my_pairs = 0;
-    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {
+    for (uint32_t i = threadIdx.x; i < m; i += G::kThreads) {
         uint32_t sz, ct;
         uint16_t word = 0;
         if (scan_pos(i, sz, ct)) {
             my_runs++;
             my_pairs += sz * (sz - 1) / 2;
-            word = (uint16_t)((ct << 15) | sz);  // size <= kGroupCap < 2^15
+            word = (uint16_t)((ct << 15) | sz);  // size <= G::kCap < 2^15
         }
         S.cand[i] = word;
     }
     uint32_t nr, total;
-    uint32_t run_off = block_scan_ex<uint32_t, kGroupThreads>(my_runs, &nr, S.warp_sums);
-    uint32_t pair_off = block_scan_ex<uint32_t, kGroupThreads>(my_pairs, &total, S.warp_sums);
+    uint32_t run_off = block_scan_ex<uint32_t, G::kThreads>(my_runs, &nr, S.warp_sums);
+    uint32_t pair_off = block_scan_ex<uint32_t, G::kThreads>(my_pairs, &total, S.warp_sums);
     if (nr > (uint32_t)kMaxRuns) {  // too many runs to list: the bucket is regrouped by sorting
         if (threadIdx.x == 0) bounded_append(overflow, overflow_cap, counters, kCntFallback, bd);
         continue;
     }
-    for (uint32_t i = threadIdx.x; i < m; i += kGroupThreads) {  // the same slots as above
+    for (uint32_t i = threadIdx.x; i < m; i += G::kThreads) {  // the same slots as above
         const uint32_t word = S.cand[i];
         if (word) {
             const uint32_t sz = word & 0x7fffu, ct = word >> 15;
@@ -875,7 +892,7 @@ __global__ void __launch_bounds__(kGroupThreads, 3) k_bucket_group(const BucketD
     const uint64_t base = S.base;
 
     // 4. pair t of the bucket -> run (binary search over the offsets) -> (i, j) inside the run
-    for (uint32_t t = threadIdx.x; t < total; t += kGroupThreads) {
+    for (uint32_t t = threadIdx.x; t < total; t += G::kThreads) {
         uint32_t lo = 0, hi = nr - 1;
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;

@@ -796,8 +796,30 @@ static int bucket_attrs(xtn_context* c) {
                                 (int)sizeof(StageSmem<SplitSmall>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<SplitSmall, kSplitSlices>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<SplitSmall>)));
-    XTN_CK(cudaFuncSetAttribute(k_bucket_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_group<GroupLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(GroupSmem<GroupLarge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_group<GroupSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(GroupSmem<GroupSmall>)));
     c->attrs_set = true;
+    return XTN_SUCCESS;
+}
+
+// The grouping kernel in the shape group_cap asks for: one CTA per descriptor (ndesc of them),
+// or persistent CTAs (MIN_CTAS per SM) reading the descriptor count on the device.
+static int launch_group(xtn_context* c, uint32_t ndesc, bool persistent, int idbits, uint64_t* pairs, uint64_t cap,
+                        uint32_t desc_cap, cudaStream_t s) {
+#define XTN_GROUP(G)                                                                                              \
+    XTN_LAUNCH("bucket_group",                                                                                   \
+               k_bucket_group<G><<<persistent ? (unsigned)c->sms * G::kMinCtas : ndesc, G::kThreads,             \
+                                   sizeof(GroupSmem<G>), s>>>(                                                   \
+                   P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits, pairs, cap,     \
+                   P<unsigned long long>(c->counter), P<unsigned int>(c->counter) + 2, c->group_tma,           \
+                   P<BucketDesc>(c->bfall), desc_cap, P<unsigned int>(c->bcnt),                                 \
+                   persistent ? P<unsigned int>(c->bcnt) + kCntDesc : nullptr))
+    if (c->group_cap <= (uint32_t)kGroupSmallCap) XTN_GROUP(GroupSmall);
+    else XTN_GROUP(GroupLarge);
+#undef XTN_GROUP
+    XTN_CK(cudaGetLastError());
     return XTN_SUCCESS;
 }
 
@@ -818,6 +840,11 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     const int bits_cap = tables ? c->bucket_bits_max : std::max(c->bucket_bits_max, kDirectBucketBitsMax);
     int b1 = 1;
     while (b1 < bits_cap && (V >> b1) > 7000) b1++;
+    // enough first-level buckets that the split (at most 2^kMaxSplitBits ways) can bring each to
+    // the grouping capacity (the small grouping shape at 10M sequences needs 1024 of them)
+    const int fan_bits = tables ? (small ? 9 : 10) : kDirectBucketBitsMax;
+    const uint64_t target = std::max<uint64_t>(1, (uint64_t)c->group_cap * 7 / 8);
+    while (b1 < fan_bits && ((V >> b1) >> kMaxSplitBits) > target) b1++;
     const int nb = 1 << b1;
     const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
                                               : (small ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
@@ -970,11 +997,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
             XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->bcnt) + kCntFallback / 2,
                                                                ((unsigned long long)nfall_split << 32) | cnt[2]));
         if (ndesc > 0)
-            XTN_LAUNCH("bucket_group", k_bucket_group<<<ndesc, kGroupThreads, sizeof(GroupSmem), s>>>(
-                                           P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
-                                           P<uint64_t>(out), cap, P<unsigned long long>(c->counter),
-                                           P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
-                                           (uint32_t)desc_cap, P<unsigned int>(c->bcnt), nullptr));
+            XTN_TRY(launch_group(c, ndesc, false, idbits, P<uint64_t>(out), cap, (uint32_t)desc_cap, s));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
@@ -1541,11 +1564,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     }
     XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
     XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
-    XTN_LAUNCH("bucket_group", k_bucket_group<<<(unsigned)c->sms * 3, kGroupThreads, sizeof(GroupSmem), s>>>(
-                                   P<BucketDesc>(c->bdesc), P<uint64_t>(c->recA), P<uint64_t>(c->recB), idbits,
-                                   P<uint64_t>(c->pairA), g->Pcap, P<unsigned long long>(c->counter),
-                                   P<unsigned int>(c->counter) + 2, c->group_tma, P<BucketDesc>(c->bfall),
-                                   (uint32_t)desc_cap, P<unsigned int>(c->bcnt), P<unsigned int>(c->bcnt) + kCntDesc));
+    XTN_TRY(launch_group(c, 0, true, idbits, P<uint64_t>(c->pairA), g->Pcap, (uint32_t)desc_cap, s));
     // candidate pairs -> distinct pairs (the table is cleared every replay: a fixed epoch)
     unsigned long long* ddcnt = P<unsigned long long>(c->ddcnt);
     XTN_CK(cudaMemsetAsync(c->ddcnt.p, 0, 16, s));
