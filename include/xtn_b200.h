@@ -159,9 +159,11 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  * a value out of range):
  *   "engine"          0 = hash-bucket grouping in shared memory (default),
  *                     1 = full radix sort of the variant records (the plain comparison form)
- *   "bucket_bits_max" 1..14: upper bound on log2(number of first-level buckets) (default 9;
- *                     above the stage shape's fan-out, 10 for stage_chunk 4096 and 9 for
- *                     2048, the first-level scatter stores records one by one)
+ *   "bucket_bits_max" 1..14: upper bound on log2(number of first-level buckets) (default 10;
+ *                     the search takes 512 buckets, or 1024 when they would exceed 1.5M
+ *                     records). With the key tables (d <= 2) the stage shape's fan-out also
+ *                     bounds it (10 for stage_chunk 4096, 9 for 2048); the direct scatter
+ *                     (d > 2, key_tables = 0) takes up to 14
  *   "group_cap"       2..4096: largest bucket grouped in shared memory; larger ones are split
  *                     by further hash bits, and what still does not fit is grouped by sorting
  *                     (default 4096). At 2048 or below the grouping kernel takes its small
@@ -212,7 +214,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     form (default): one launch sequence per search that reads sizes back to
  *                     the host between its stages
  *   "verify_per"      1 | 4 | 8: the verification variant - candidates each lane of a warp lists
- *                     before the warp verifies them (default 4)
+ *                     before the warp verifies them (default 1: the candidates are distinct
+ *                     after the hash set, so listing more per lane only lengthens the warps;
+ *                     4 or 8 amortise the listing when sorted candidates repeat)
  *   "autotune"        1 = xtn_context_nn_device takes its shape (the options the autotuner
  *                     sets) from the context's cache for the input's class, and on a miss runs
  *                     the autotuner on the input first (see xtn_context_autotune); 0 = the
@@ -229,7 +233,7 @@ int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length
  * distribution and duplicate structure) for each shape - first-level and split stage chunks and
  * first-level bucket bits, then, on the best of those, bulk-copy or plain loads in the grouping
- * kernel, the verification variants (verify_per 1 and 8) and the graph form - taking the best of
+ * kernel, the verification variants (verify_per 4 and 8) and the graph form - taking the best of
  * `repeats` runs after a warm-up, and leaves the fastest shape set on the context. The choice is
  * also remembered for the input's class (log2 of the sequence count, distance, measure, median
  * sequence length, share of sequences longer than the 18-residue key), which option "autotune"

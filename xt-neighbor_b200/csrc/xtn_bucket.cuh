@@ -40,7 +40,7 @@ constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp
 // First-level fan-out: a staged chunk of 2048..4096 records leaves runs of 4..8 records
 // (32..64 bytes) per bucket; consecutive chunks of one CTA extend the same runs, so their
 // boundary sectors complete in L2.
-constexpr int kMaxFirstLevelBits = 9;  // default bound; the large stage shape takes up to 10
+constexpr int kMaxFirstLevelBits = 10;  // default bound on the first-level bits (the large stage shape's fan-out)
 constexpr int kMaxSplitBits = 10;
 constexpr int kSplitSlices = 8;        // CTAs (one thread-block cluster) per split bucket
 

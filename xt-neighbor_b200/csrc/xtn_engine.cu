@@ -327,8 +327,11 @@ __global__ void __launch_bounds__(kThreads) k_pair_dedup(const uint64_t* __restr
     }
 }
 
-// Table regions: each at most kDedupRegionBytes (half of L2), so one pass's probes stay in L2.
-constexpr uint64_t kDedupRegionBytes = uint64_t(64) << 20;
+// Table regions: each at most kDedupRegionBytes. Regions of 64 MiB (a quarter of the 10M
+// workload's 256 MiB table, so that each pass's probes stay in L2) were measured slower on B200
+// (2.97 ms against 1.75 ms for 56M candidates: four passes over the candidates cost more than
+// the L2 hits save), so tables up to 1 GiB take one pass.
+constexpr uint64_t kDedupRegionBytes = uint64_t(1) << 30;
 
 static int dedup_part_bits(uint64_t T) {
     int pb = 0;
@@ -516,7 +519,7 @@ struct xtn_context {
     int scatter_ctas_per_sm = 0;  // 0: as many as the stage shape's shared memory allows
     int group_tma = 1;
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
-    int verify_per = kVerifyPer;  // verification variant: candidates listed per lane (1, 4, 8)
+    int verify_per = 1;     // verification variant: candidates listed per lane (1, 4, 8)
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
@@ -828,6 +831,7 @@ static int launch_group(xtn_context* c, uint32_t ndesc, bool persistent, int idb
 // the buckets of very large variant counts (10M sequences at d = 3: ~6e9) small enough for the
 // split to bring them to shared-memory size.
 constexpr int kDirectBucketBitsMax = 14;
+constexpr uint64_t kFirstLevelRecords = 1500000;
 
 // The first-level plan: count pass over every variant (per-tile histograms of the top b1 hash
 // bits), per-tile offsets inside each bucket, bucket starts (c->bstart, nb + 1 entries) and, for
@@ -835,16 +839,23 @@ constexpr int kDirectBucketBitsMax = 14;
 // The first-level shape for n sequences and V variant records (no device work).
 static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
     const bool small = c->stage_chunk == 2048;
-    const int stage_fan = small ? StageSmall::kFan : StageLarge::kFan;
     const bool tables = d <= 2 && c->key_tables;
-    const int bits_cap = tables ? c->bucket_bits_max : std::max(c->bucket_bits_max, kDirectBucketBitsMax);
-    int b1 = 1;
-    while (b1 < bits_cap && (V >> b1) > 7000) b1++;
-    // enough first-level buckets that the split (at most 2^kMaxSplitBits ways) can bring each to
-    // the grouping capacity (the small grouping shape at 10M sequences needs 1024 of them)
+    // the staged scatter's fan-out bounds the first-level bits; the direct scatter (d > 2, or
+    // per-key hashing) takes up to 2^14 buckets
     const int fan_bits = tables ? (small ? 9 : 10) : kDirectBucketBitsMax;
+    const int lim = tables ? std::min(c->bucket_bits_max, fan_bits) : std::max(c->bucket_bits_max, kDirectBucketBitsMax);
+    int b1 = 1;
+    // buckets of about 7000 records or more (up to 512 of them with the key tables)
+    while (b1 < (tables ? std::min(lim, 9) : lim) && (V >> b1) > 7000) b1++;
+    // first-level buckets of more than kFirstLevelRecords records make the split re-read its
+    // slices from DRAM (a cluster's bucket no longer stays in L2) and write short runs: at 10M
+    // sequences 1024 buckets instead of 512 cut the split from 10.5 to 7.5 ms for 1.7 ms more
+    // scatter; at 1M, 512 stay faster
+    while (b1 < lim && (V >> b1) > kFirstLevelRecords) b1++;
+    // enough buckets that the split (at most 2^kMaxSplitBits ways) can bring each to the
+    // grouping capacity (the small grouping shape at 10M sequences needs 1024 of them)
     const uint64_t target = std::max<uint64_t>(1, (uint64_t)c->group_cap * 7 / 8);
-    while (b1 < fan_bits && ((V >> b1) >> kMaxSplitBits) > target) b1++;
+    while (b1 < lim && ((V >> b1) >> kMaxSplitBits) > target) b1++;
     const int nb = 1 << b1;
     const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
                                               : (small ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
@@ -856,7 +867,7 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     bp->ntiles = ntiles;
     bp->tile = (n + ntiles - 1) / ntiles;
     bp->small = small;
-    bp->staged = tables && nb <= stage_fan;
+    bp->staged = tables && b1 <= fan_bits;
     bp->tseq = nullptr;
 }
 
@@ -2285,7 +2296,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
         *ms = best;
         return XTN_SUCCESS;
     };
-    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, kVerifyPer, 0};
+    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, 1, 0};
     float best_ms = 1e30f;
     int tried = 0;
     auto consider = [&](const TuneShape& sh) -> int {
@@ -2306,7 +2317,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
             for (int bits : {9, 10}) {
                 if (st != XTN_SUCCESS) break;
                 if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
-                st = consider(TuneShape{stage, split, bits, 1, kVerifyPer, 0});
+                st = consider(TuneShape{stage, split, bits, 1, 1, 0});
             }
     // then, one at a time on the best so far: plain loads in grouping, the verification
     // variants, the graph form
@@ -2315,7 +2326,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
         sh.tma = 0;
         st = consider(sh);
     }
-    for (int per : {1, 8}) {
+    for (int per : {4, 8}) {
         if (st != XTN_SUCCESS) break;
         TuneShape sh = best;
         sh.verify = per;
