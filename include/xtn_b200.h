@@ -170,8 +170,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     shape (256 threads and about 37 KB of shared memory: six CTAs per SM
  *                     instead of three)
  *   "scatter_ctas_per_sm" 0..4: first-level tiles per SM (default 0: as many CTAs as fit)
- *   "stage_chunk"     2048 | 4096: records per shared-memory chunk of the first-level scatter
- *                     (default 4096: two CTAs per SM; 2048: four)
+ *   "stage_chunk"     2048 | 4096 | 8192: records per shared-memory chunk of the first-level
+ *                     scatter (default 4096: two CTAs of 512 threads per SM; 2048: four of 256;
+ *                     8192: one of 1024, longer runs per bucket)
  *   "split_chunk"     2048 | 4096: the same for the split of large buckets (default 4096)
  *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
  *                     CTAs take slices of the bucket and merge their histograms through

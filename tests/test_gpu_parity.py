@@ -27,9 +27,10 @@ ENGINES = {
     # every variant key hashed directly (the d > 2 and no-allocation form) instead of from
     # per-sequence tables; direct first-level scatter
     "bucket_key_hash": {"key_tables": 0},
-    # the small grouping shape (buckets of up to 2048 records, 256 threads, six CTAs per SM)
-    # and the verification variant that lists one candidate per lane
-    "bucket_small_group": {"group_cap": 2048, "verify_per": 1},
+    # the small grouping shape (buckets of up to 2048 records, 256 threads, six CTAs per SM),
+    # the 8192-record first-level stage shape and the verification variant that lists four
+    # candidates per lane
+    "bucket_small_group": {"group_cap": 2048, "stage_chunk": 8192, "verify_per": 4},
 }
 
 

@@ -56,6 +56,9 @@ struct StageCfg {
 };
 using StageLarge = StageCfg<512, 4096, 1024>;  // ~110 KB of shared memory: two CTAs per SM
 using StageSmall = StageCfg<256, 2048, 512>;   // ~55 KB: four CTAs per SM (first level, b1 <= 9)
+// ~210 KB: one CTA of 1024 threads per SM (first level only): with 1024 first-level buckets a
+// chunk of 8192 records leaves runs of about eight records (64 bytes) per bucket instead of four
+using StageHuge = StageCfg<1024, 8192, 1024>;
 using SplitSmall = StageCfg<256, 2048, 1024>;  // ~60 KB: three CTAs per SM
 // Shape of a grouping CTA: records it holds in shared memory, threads, hash bits of the
 // "seen" / "seen twice" bitmaps, hash bits of the candidates' counting sort, and minimum CTAs per
@@ -74,8 +77,12 @@ struct GroupCfg {
     static constexpr int kMinCtas = MIN_CTAS;
     static_assert(kDigits % THREADS == 0 && CAP < 65536, "group shape");
 };
-using GroupLarge = GroupCfg<4096, 512, 16, 11, 3>;
-using GroupSmall = GroupCfg<2048, 256, 15, 10, 6>;
+// The candidates (records that pass the bitmap filter: the members of runs and a few percent of
+// the singletons) number a few hundred in a typical bucket, so one digit per thread (512 / 256
+// digits) keeps the digit zeroing and scan at one item per thread; a digit then holds about one
+// candidate.
+using GroupLarge = GroupCfg<4096, 512, 16, 9, 3>;
+using GroupSmall = GroupCfg<2048, 256, 15, 8, 6>;
 constexpr int kGroupThreads = GroupLarge::kThreads;
 constexpr int kGroupCap = GroupLarge::kCap;        // largest bucket grouped in shared memory
 constexpr int kGroupSmallCap = GroupSmall::kCap;   // group_cap at or below this: the small shape
@@ -678,6 +685,7 @@ struct GroupSmem {
     uint16_t cand[G::kCap];     // records whose bitmap bit was hit at least twice
     uint32_t cnt[G::kDigits];   // digit counts -> digit ends
     uint32_t warp_sums[G::kThreads / 32 + 1];
+    unsigned long long warp_sums64[G::kThreads / 32 + 1];
     uint32_t wait_failed;
     uint32_t n_cand;
     unsigned long long base;
@@ -870,9 +878,12 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
         }
         S.cand[i] = word;
     }
-    uint32_t nr, total;
-    uint32_t run_off = block_scan_ex<uint32_t, G::kThreads>(my_runs, &nr, S.warp_sums);
-    uint32_t pair_off = block_scan_ex<uint32_t, G::kThreads>(my_pairs, &total, S.warp_sums);
+    // runs (high half) and pairs (low half: a bucket has fewer than 2^32 pairs) in one scan
+    unsigned long long tot64;
+    const unsigned long long off64 = block_scan_ex<unsigned long long, G::kThreads>(
+        ((unsigned long long)my_runs << 32) | my_pairs, &tot64, S.warp_sums64);
+    uint32_t run_off = (uint32_t)(off64 >> 32), pair_off = (uint32_t)off64;
+    const uint32_t nr = (uint32_t)(tot64 >> 32), total = (uint32_t)tot64;
     if (nr > (uint32_t)kMaxRuns) {  // too many runs to list: the bucket is regrouped by sorting
         if (threadIdx.x == 0) bounded_append(overflow, overflow_cap, counters, kCntFallback, bd);
         continue;

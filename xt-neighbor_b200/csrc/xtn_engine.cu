@@ -522,7 +522,7 @@ struct xtn_context {
     int verify_per = 1;     // verification variant: candidates listed per lane (1, 4, 8)
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
-    int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096)
+    int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
     int split_chunk = 4096;  // the same for the split (2048 | 4096)
     int split_slices = kSplitSlices;  // CTAs (one cluster) per split bucket: 1 | kSplitSlices
     uint32_t group_cap = kGroupCap;
@@ -791,6 +791,8 @@ static int bucket_attrs(xtn_context* c) {
                                 (int)sizeof(ScatterSmem<StageLarge>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(ScatterSmem<StageSmall>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_scatter_staged<StageHuge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<StageHuge>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(StageSmem<StageLarge>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_split_staged<StageLarge, kSplitSlices>,
@@ -858,8 +860,9 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     while (b1 < lim && ((V >> b1) >> kMaxSplitBits) > target) b1++;
     const int nb = 1 << b1;
     const int per_sm = c->scatter_ctas_per_sm ? c->scatter_ctas_per_sm  // count/scatter tiles per SM
-                                              : (small ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
-                                                       : ctas_per_sm_for<ScatterSmem<StageLarge>>());
+                       : small                  ? ctas_per_sm_for<ScatterSmem<StageSmall>>()
+                       : c->stage_chunk == 8192 ? ctas_per_sm_for<ScatterSmem<StageHuge>>()
+                                                : ctas_per_sm_for<ScatterSmem<StageLarge>>();
     const int64_t wave = (int64_t)c->sms * per_sm;
     const int ntiles = (int)(wave * std::max<int64_t>(1, ((int64_t)n + wave * 4096 - 1) / (wave * 4096)));
     bp->b1 = b1;
@@ -912,6 +915,21 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
     return XTN_SUCCESS;
 }
 
+// The staged first-level scatter in the context's stage shape (stage_chunk 2048, 4096 or 8192).
+static void launch_scatter_staged(xtn_context* c, const BucketPlan& bp, int n, int d, int idbits, uint32_t b_lo,
+                                  uint32_t b_n, uint64_t base, const unsigned int* abort, cudaStream_t s) {
+#define XTN_SCATTER(CFG)                                                                                          \
+    XTN_LAUNCH("bucket_scatter",                                                                                 \
+               k_bucket_scatter_staged<CFG><<<bp.ntiles, CFG::kThreads, sizeof(ScatterSmem<CFG>), s>>>(           \
+                   P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),    \
+                   P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, bp.b1, idbits, P<uint32_t>(c->boffs),         \
+                   P<uint64_t>(c->bstart), b_lo, b_n, base, P<uint64_t>(c->recA), abort))
+    if (bp.small) XTN_SCATTER(StageSmall);
+    else if (c->stage_chunk == 8192) XTN_SCATTER(StageHuge);
+    else XTN_SCATTER(StageLarge);
+#undef XTN_SCATTER
+}
+
 // One round: the records of first-level buckets [b_lo, b_lo + b_n), which hold Vr records at
 // global positions [base, base + Vr), are written to recA (positions minus base), oversized
 // buckets split into recB, and every bucket grouped; the candidate pairs are written to `out`
@@ -925,18 +943,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_TRY(ensure(c->recB, sizeof(uint64_t) * Vr + 64));
     const uint64_t* bstart = P<uint64_t>(c->bstart);
     if (bp.staged) {
-        if (bp.small)
-            XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageSmall><<<bp.ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
-                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           b_lo, b_n, base, P<uint64_t>(c->recA), nullptr));
-        else
-            XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageLarge><<<bp.ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
-                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           b_lo, b_n, base, P<uint64_t>(c->recA), nullptr));
+        launch_scatter_staged(c, bp, n, d, idbits, b_lo, b_n, base, nullptr, s);
     } else {
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, bp.tile, d, b1, idbits,
@@ -1533,18 +1540,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     const int nb = bp.nb;
     const uint64_t* bstart = P<uint64_t>(c->bstart);
     if (bp.staged) {
-        if (bp.small)
-            XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageSmall><<<bp.ntiles, StageSmall::kThreads, sizeof(ScatterSmem<StageSmall>), s>>>(
-                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, bp.b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           0u, (uint32_t)nb, 0ull, P<uint64_t>(c->recA), abort));
-        else
-            XTN_LAUNCH("bucket_scatter",
-                       k_bucket_scatter_staged<StageLarge><<<bp.ntiles, StageLarge::kThreads, sizeof(ScatterSmem<StageLarge>), s>>>(
-                           P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab), P<uint64_t>(c->voff),
-                           P<uint64_t>(c->toff), bp.tseq, n, bp.tile, d, bp.b1, idbits, P<uint32_t>(c->boffs), bstart,
-                           0u, (uint32_t)nb, 0ull, P<uint64_t>(c->recA), abort));
+        launch_scatter_staged(c, bp, n, d, idbits, 0u, (uint32_t)nb, 0ull, abort, s);
     } else {
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
                                          P<u128>(c->keys), P<uint8_t>(c->klen), n, bp.tile, d, bp.b1, idbits,
@@ -2581,7 +2577,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "onesweep") && (v == 0 || v == 1)) c->onesweep = (int)v;
     else if (!strcmp(name, "pair_dedup") && v >= 0 && v <= 2) c->pair_dedup = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
-    else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096)) c->stage_chunk = (int)v;
+    else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096 || v == 8192)) c->stage_chunk = (int)v;
     else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
     else if (!strcmp(name, "split_slices") && (v == 1 || v == kSplitSlices)) c->split_slices = (int)v;
     else if (!strcmp(name, "wait_polls") && v >= 1 && v <= (int64_t)kScanPollLimit) c->wait_polls = (uint32_t)v;
