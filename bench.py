@@ -533,8 +533,9 @@ def run_ours(args, w):
     # the plain form (above: one launch sequence per search, sizes read back between stages)
     # against the batched/persistent form (the search captured once into a CUDA graph and
     # replayed, every size read on the device), same inputs, same timing
-    if not overlap and not args.no_forms:
-        line["forms"] = measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, ms_step, n_out)
+    if not args.no_forms:
+        line["forms"] = measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, ms_step, n_out,
+                                      (d_info, len(reps)) if overlap else None)
     extras = {}
     for name in ([] if args.no_extra else EXTRA_WORKLOADS.get(args.workload, [])):
         extras[name] = measure_extra(ctx, WORKLOADS[name], args, flush, ext)
@@ -552,20 +553,28 @@ def run_ours(args, w):
     return line
 
 
-def measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, plain_ms, plain_out):
+def measure_forms(ctx, w, n, d_chars, d_offs, args, flush, ext, plain_ms, plain_out, overlap=None):
     """The plain form (the headline's search: one launch sequence per search that reads sizes
     back between its stages, default shapes) against the batched/persistent form (shapes from
     the autotuner, which also picks between the plain and the CUDA-graph form; the graph form is
     the whole search captured once and replayed with every size read on the device), same
-    inputs and timing, in a second context."""
+    inputs and timing, in a second context. Overlap mode (overlap = (device info, repertoires)):
+    the graph form of the whole overlap sequence, default shapes."""
     import torch
 
     import xtn
 
     ctx.set_profiling(False)
-    b = xtn.Context(ctx_device(ctx))
-    report = b.autotune(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"], repeats=2)
-    fn = lambda: b.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+    if overlap:
+        b = xtn.Context(ctx_device(ctx), graph=1)
+        report = "graph=1 (overlap mode: string merge, diagonal, search, cross term and matrix in one graph)"
+        d_info, R = overlap
+        fn = lambda: b.overlap_device(d_chars.data_ptr(), d_offs.data_ptr(), n, d_info.data_ptr(), R, w["d"],
+                                      w["measure"])
+    else:
+        b = xtn.Context(ctx_device(ctx))
+        report = b.autotune(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"], repeats=2)
+        fn = lambda: b.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
     times, out = [], None
     for i in range(1 + args.warmup + args.steps):
         flush.zero_()

@@ -139,6 +139,22 @@ int xtn_context_fetch(xtn_context* ctx, xtn_int2* pairs, int8_t* distances, uint
 /* Device pointers of the last result (valid until the next run on the context). */
 int xtn_context_result_device(xtn_context* ctx, const xtn_int2** d_pairs, const int8_t** d_distances, int64_t* n_out);
 
+/* Shard exchange (multi-GPU search, options "shard_count" / "shard_index"). The reference runs
+ * on one GPU and has no counterpart; these two calls are what a rank adds around its shard's
+ * search.
+ * xtn_context_result_keys writes the last nearest-neighbour result (sorted by (x, y)) to d_keys
+ * (device memory, at least n_out entries) as one 64-bit key per pair,
+ *   x << (b + 8) | y << 8 | (uint8_t)distance,   b = the smallest b >= 1 with 2^b >= n_seqs,
+ * and range_starts[k] (host, n_ranges + 1 entries) = the first key whose x >= ceil(k n / K),
+ * K = n_ranges, range_starts[K] = n_out: keys [range_starts[k], range_starts[k+1]) belong to
+ * rank k's id range. xtn_context_merge_keys takes the keys a rank received (device memory, any
+ * order, duplicates allowed), sorts them, drops repeats and leaves the pairs as the context's
+ * result (xtn_context_fetch, *n_out entries): the ranks' results in rank order are the whole
+ * search's output. */
+int xtn_context_result_keys(xtn_context* ctx, int32_t n_seqs, uint64_t* d_keys, int64_t capacity, int32_t n_ranges,
+                            int64_t* range_starts);
+int xtn_context_merge_keys(xtn_context* ctx, int32_t n_seqs, const uint64_t* d_keys, int64_t count, int64_t* n_out);
+
 /* The CUDA stream the context launches on (as a cudaStream_t cast to void*). */
 void* xtn_context_stream(xtn_context* ctx);
 
@@ -177,6 +193,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
  *                     CTAs take slices of the bucket and merge their histograms through
  *                     distributed shared memory)
+ *   "group_persistent" 1 = when there are many buckets to group (more than 8 per SM), the
+ *                     grouping kernel runs as persistent CTAs that take bucket descriptors from
+ *                     a queue on the device (default), 0 = one CTA per bucket
  *   "group_tma"       1 = load each bucket into shared memory with one TMA bulk copy
  *                     (default), 0 = with plain 16-byte loads from every thread
  *   "key_tables"      1 = for d <= 2, hash variants from per-sequence tables (default),
@@ -211,9 +230,25 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     search on that input replays it with one synchronisation at the end.
  *                     Capacities come from the plain search that precedes the capture; a
  *                     replay that exceeds one (or meets a bucket too large for shared memory)
- *                     is redone by the plain form, which re-sizes the graph. 0 = the plain
- *                     form (default): one launch sequence per search that reads sizes back to
- *                     the host between its stages
+ *                     is redone by the plain form, which re-sizes the graph. The same holds
+ *                     for xtn_context_overlap_device: the string merge, diagonal term, the
+ *                     search over the unique strings, cross term and matrix compaction form one
+ *                     graph (per input and repertoire count); a replay whose unique-string
+ *                     count differs from the capture's is redone by the plain form. A graph is
+ *                     also re-captured when a search through another entry point has
+ *                     reallocated the context's buffers. 0 = the plain form (default): one
+ *                     launch sequence per search that reads sizes back to the host between
+ *                     its stages
+ *   "shard_count"     1..1024 (default 1) and
+ *   "shard_index"     0..shard_count-1 (default 0): the nearest-neighbour search covers only
+ *                     shard shard_index of shard_count - the first-level hash buckets whose
+ *                     first record lies in [k V / K, (k + 1) V / K) of the V variant records,
+ *                     so every group of equal variants lies in exactly one shard - and returns
+ *                     that shard's verified pairs (sorted, unique within the shard). One rank
+ *                     per GPU runs one shard on the same (replicated) input; the ranks then
+ *                     exchange their pairs by owner (xtn_context_result_keys) and each merges
+ *                     what it receives (xtn_context_merge_keys). Bucket engine only; the
+ *                     overlap mode and the graph form run unsharded
  *   "verify_per"      1 | 4 | 8: the verification variant - candidates each lane of a warp lists
  *                     before the warp verifies them (default 1: the candidates are distinct
  *                     after the hash set, so listing more per lane only lengthens the warps;

@@ -520,6 +520,8 @@ struct xtn_context {
     int group_tma = 1;
     int key_tables = 1;     // d <= 2 variant hashes from per-sequence tables
     int verify_per = 1;     // verification variant: candidates listed per lane (1, 4, 8)
+    int group_persistent = 1;  // grouping by persistent CTAs on a descriptor queue (large grids)
+    int shard_count = 1, shard_index = 0;  // this search covers shard shard_index of shard_count
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
@@ -538,6 +540,7 @@ struct xtn_context {
     // graph form of the device-resident search (option "graph")
     int graph_mode = 0;
     void* graph = nullptr;  // GraphState (below)
+    void* ograph = nullptr; // OverlapGraph (below)
     // autotuner: shapes chosen per input class (see TuneKey), and whether device-resident
     // searches consult (and fill) that cache by themselves
     int autotune_auto = 0;
@@ -821,6 +824,7 @@ static int launch_group(xtn_context* c, uint32_t ndesc, bool persistent, int idb
                    P<unsigned long long>(c->counter), P<unsigned int>(c->counter) + 2, c->group_tma,           \
                    P<BucketDesc>(c->bfall), desc_cap, P<unsigned int>(c->bcnt),                                 \
                    persistent ? P<unsigned int>(c->bcnt) + kCntDesc : nullptr))
+    if (persistent) XTN_CK(cudaMemsetAsync(P<unsigned int>(c->bcnt) + kCntNext, 0, sizeof(unsigned int), s));
     if (c->group_cap <= (uint32_t)kGroupSmallCap) XTN_GROUP(GroupSmall);
     else XTN_GROUP(GroupLarge);
 #undef XTN_GROUP
@@ -1015,7 +1019,8 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
             XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->bcnt) + kCntFallback / 2,
                                                                ((unsigned long long)nfall_split << 32) | cnt[2]));
         if (ndesc > 0)
-            XTN_TRY(launch_group(c, ndesc, false, idbits, P<uint64_t>(out), cap, (uint32_t)desc_cap, s));
+            XTN_TRY(launch_group(c, ndesc, c->group_persistent != 0 && ndesc > (uint32_t)c->sms * 8, idbits,
+                                 P<uint64_t>(out), cap, (uint32_t)desc_cap, s));
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->counter.p, 16, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaMemcpyAsync(c->h_scalar + 2, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
@@ -1108,6 +1113,8 @@ static int dedup_pairs(xtn_context* c, uint64_t Pc, int idbits, uint64_t* U) {
 // lower-bound rounds over the min-id space (S/src/xtn.cu:383-470, cal_lowerbounds
 // S/src/xtn.cu:179-184,218-230), which bound the candidate pairs held in host RAM; here the
 // bound is on device memory, and the records are what grows with the input.
+constexpr int kMaxShards = 1024;
+
 struct Round {
     uint32_t b_lo, b_n;  // first-level buckets [b_lo, b_lo + b_n)
     uint64_t base, size; // their records: global positions [base, base + size)
@@ -1156,20 +1163,35 @@ static uint64_t round_record_limit(xtn_context* c, int n, int d, uint64_t V) {
 }
 
 // Contiguous bucket ranges of at most `limit` records each (bucket starts read from the device).
+// Sharding (options shard_count, shard_index): shard k of K covers the first-level buckets whose
+// first record lies in [k V / K, (k + 1) V / K), so the shards hold about equal numbers of
+// records and every group of equal hashes lies in exactly one shard.
+static void shard_buckets(const std::vector<uint64_t>& bs, int nb, int k, int K, uint32_t* lo, uint32_t* hi) {
+    const uint64_t V = bs[nb];
+    auto bound = [&](int j) -> uint32_t {
+        if (j >= K) return (uint32_t)nb;
+        const uint64_t at = (uint64_t)((unsigned __int128)V * (unsigned)j / (unsigned)K);
+        return (uint32_t)(std::lower_bound(bs.begin(), bs.begin() + nb, at) - bs.begin());
+    };
+    *lo = bound(k);
+    *hi = std::max(*lo, bound(k + 1));
+}
+
 static int plan_rounds(xtn_context* c, const BucketPlan& bp, uint64_t limit, std::vector<Round>* rounds) {
     std::vector<uint64_t> bs(bp.nb + 1);
     XTN_CK(cudaMemcpyAsync(bs.data(), c->bstart.p, sizeof(uint64_t) * (bp.nb + 1), cudaMemcpyDeviceToHost, c->stream));
     XTN_CK(cudaStreamSynchronize(c->stream));
     rounds->clear();
-    uint32_t lo = 0;
-    while (lo < (uint32_t)bp.nb) {
+    uint32_t lo = 0, end = (uint32_t)bp.nb;
+    if (c->shard_count > 1) shard_buckets(bs, bp.nb, c->shard_index, c->shard_count, &lo, &end);
+    while (lo < end) {
         if (bs[lo + 1] - bs[lo] > limit) {
             set_err("the memory budget cannot hold one first-level bucket (" + std::to_string(bs[lo + 1] - bs[lo]) +
                     " variant records, at most " + std::to_string(limit) + " per round)");
             return XTN_ERR_NOMEM;
         }
         uint32_t hi = lo + 1;
-        while (hi < (uint32_t)bp.nb && bs[hi + 1] - bs[lo] <= limit) hi++;
+        while (hi < end && bs[hi + 1] - bs[lo] <= limit) hi++;
         rounds->push_back(Round{lo, hi - lo, bs[lo], bs[hi] - bs[lo]});
         lo = hi;
     }
@@ -1204,6 +1226,10 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
     cudaStream_t s = c->stream;
     uint64_t Ptot = 0;
     *distinct = c->pair_dedup && 2 * idbits <= kDedupKeyBits;
+    if (rounds.empty()) {  // a shard without buckets
+        *Ptotal = *U_out = 0;
+        return XTN_SUCCESS;
+    }
     if (!*distinct) {
         for (const Round& r : rounds) {
             uint64_t pc = 0;
@@ -1330,6 +1356,11 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         return XTN_ERR_CUDA;
     }
     st.n_variants = (int64_t)V;
+    if (c->shard_count > 1 && (c->engine != 0 || c->shard_index >= c->shard_count)) {
+        set_err(c->engine != 0 ? "sharding needs the bucket engine (engine 0)"
+                               : "shard_index must be below shard_count");
+        return XTN_ERR_ARG;
+    }
     if (c->engine == 1 && V >= (uint64_t)UINT32_MAX) {
         set_err("too many deletion variants for the sort engine's one round (" + std::to_string(V) + ")");
         return XTN_ERR_LIMIT;
@@ -1345,7 +1376,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         BucketPlan bp;
         XTN_TRY(bucket_prepare(c, n, d, V, &bp));
         const uint64_t limit = round_record_limit(c, n, d, V);
-        if (V <= limit) {
+        if (V <= limit && c->shard_count <= 1) {
             XTN_TRY(candidates_bucketed(c, bp, n, d, idbits, V, &Pc));
         } else {
             std::vector<Round> rounds;
@@ -1455,6 +1486,8 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
 struct GraphState {
     const uint8_t* chars = nullptr;
     const uint32_t* offs = nullptr;
+    const int32_t* rows = nullptr;            // sequence i is row rows[i] (overlap: one row per unique string)
+    const unsigned int* pre_abort = nullptr;  // an abort word set by stages captured before the search
     int n = 0, d = 0, measure = 0;
     int64_t sig = 0;                 // options the capture depends on
     uint64_t Vcap = 0, Pcap = 0, Ucap = 0, T = 0;
@@ -1465,6 +1498,7 @@ struct GraphState {
     int64_t launches = 0;
     DevBuf status, table, os_status;
     uint32_t os_epoch = 0;
+    std::vector<const void*> bufs;   // the context's buffers at capture (a reallocation invalidates it)
 };
 
 // Status block of one replay (device words, copied to the pinned host scalars 16..31).
@@ -1473,10 +1507,11 @@ enum {
     GS_FULL, GS_LOOKBACK_ERR, GS_OUT, GS_NDESC, GS_WORDS
 };
 
-// Sets the abort word when the variant records exceed their capacity or a length is invalid.
+// Sets the abort word when the variant records exceed their capacity, a length is invalid or an
+// earlier stage aborted.
 __global__ void k_graph_guard(const uint64_t* __restrict__ V, uint64_t Vcap, const unsigned int* __restrict__ lenbad,
-                              unsigned int* __restrict__ abort) {
-    *abort = (*V > Vcap || *lenbad != 0xffffffffu) ? 1u : 0u;
+                              const unsigned int* __restrict__ pre, unsigned int* __restrict__ abort) {
+    *abort = (*V > Vcap || *lenbad != 0xffffffffu || (pre && *pre)) ? 1u : 0u;
 }
 
 __global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned int* __restrict__ abort,
@@ -1523,14 +1558,14 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     const bool tables = d <= 2 && c->key_tables;
     unsigned int* abort = P<unsigned int>(c->lencheck) + 1;
     XTN_CK(cudaMemsetAsync(c->lencheck.p, 0xff, 4, s));
-    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, s>>>(g->offs, nullptr, n,
+    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, s>>>(g->offs, g->rows, n,
                                                                                     P<unsigned int>(c->lencheck)));
     XTN_LAUNCH("pack", k_pack<<<blocks_for(n, kPackThreads), kPackThreads, 0, s>>>(
-                           g->chars, g->offs, nullptr, n, d, P<u128>(c->keys), P<uint8_t>(c->klen), P<uint32_t>(c->vcnt),
+                           g->chars, g->offs, g->rows, n, d, P<u128>(c->keys), P<uint8_t>(c->klen), P<uint32_t>(c->vcnt),
                            P<uint64_t>(c->runinfo), tables ? P<uint64_t>(c->ktab) : nullptr));
     XTN_TRY((scan_1p<uint32_t, uint64_t>(c, P<uint32_t>(c->vcnt), P<uint64_t>(c->voff), n)));
     XTN_LAUNCH("graph_guard", k_graph_guard<<<1, 1, 0, s>>>(P<uint64_t>(c->voff) + n, g->Vcap,
-                                                            P<unsigned int>(c->lencheck), abort));
+                                                            P<unsigned int>(c->lencheck), g->pre_abort, abort));
     BucketPlan bp;
     XTN_TRY(bucket_prepare(c, n, d, g->Vcap, &bp));
     if (bp.b1 != g->b1) {
@@ -1585,7 +1620,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
                               (int64_t)(g->os_status.cap / 8), &g->os_epoch, P<unsigned int>(c->dev_err), c->sms, s,
                               "pair_sort_hist", "pair_sort_pass", ddcnt);
     g->result = pairs;
-    launch_verify(c->verify_per, pairs, (int64_t)g->Ucap, idbits, g->chars, g->offs, nullptr, d, g->measure,
+    launch_verify(c->verify_per, pairs, (int64_t)g->Ucap, idbits, g->chars, g->offs, g->rows, d, g->measure,
                   P<int8_t>(c->dist), P<uint8_t>(c->flag), ddcnt, s);
     scan_exclusive_1p<uint8_t, uint32_t>(P<uint8_t>(c->flag), P<uint32_t>(c->fpos), (int64_t)g->Ucap,
                                          P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err), s,
@@ -1602,14 +1637,17 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     return XTN_SUCCESS;
 }
 
-// Capacities from the plain search just run on this input, buffers reserved, graph captured.
-static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, const uint32_t* offs, int n, int d,
-                       int measure) {
-    graph_release(g);
+// Capacities from the plain search just run on this input (its statistics), every buffer the
+// capture uses reserved. XTN_ERR_LIMIT: the input stays in the plain form.
+static int graph_reserve(xtn_context* c, GraphState* g, const uint8_t* chars, const uint32_t* offs, const int32_t* rows,
+                         int n, int d, int measure) {
     const xtn_stats& st = c->stats;
-    if (c->engine != 0 || st.n_rounds != 1 || !c->pair_dedup || 2 * id_bits_for(n) > kDedupKeyBits) return XTN_ERR_LIMIT;
+    if (c->engine != 0 || st.n_rounds != 1 || c->shard_count > 1 || !c->pair_dedup || 2 * id_bits_for(n) > kDedupKeyBits)
+        return XTN_ERR_LIMIT;
     g->chars = chars;
     g->offs = offs;
+    g->rows = rows;
+    g->pre_abort = nullptr;
     g->n = n;
     g->d = d;
     g->measure = measure;
@@ -1654,13 +1692,19 @@ static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, cons
     XTN_TRY(ensure(g->table, sizeof(uint64_t) * g->T));
     XTN_TRY(ensure(g->os_status, sizeof(unsigned long long) * (size_t)onesweep_status_words((int64_t)g->Ucap)));
     XTN_TRY(bucket_attrs(c));
+    return XTN_SUCCESS;
+}
+
+// Captures what enqueue() launches on the context's stream (launches counted, no per-launch
+// events).
+template <class F>
+static int capture(xtn_context* c, F&& enqueue, cudaGraph_t* out, int64_t* launches) {
     XTN_CK(cudaStreamSynchronize(c->stream));
-    // capture (launches counted, no per-launch events)
     KernelProfiler counting;
     KernelProfiler* saved = current_profiler();
     current_profiler() = &counting;
     XTN_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int r = graph_enqueue(c, g);
+    int r = enqueue();
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     current_profiler() = saved;
@@ -1670,24 +1714,51 @@ static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, cons
         if (r == XTN_SUCCESS) set_err(std::string("graph capture failed: ") + cudaGetErrorString(e));
         return r != XTN_SUCCESS ? r : XTN_ERR_CUDA;
     }
-    g->graph = graph;
-    g->launches = counting.launches;
-    XTN_CK(cudaGraphInstantiate(&g->exec, graph, 0));
+    *out = graph;
+    *launches = counting.launches;
     return XTN_SUCCESS;
 }
 
-// One search by the graph form; *redo is set when the plain form has to run instead.
-static int graph_replay(xtn_context* c, GraphState* g, bool* redo) {
+// Every device buffer of the context: a graph holds their addresses, so it is replayed only while
+// none of them has been reallocated (by a search of another input, or by another form).
+static std::vector<const void*> context_buffer_ptrs(const xtn_context* c);
+
+// Capacities from the plain search just run on this input, buffers reserved, graph captured.
+static int graph_build(xtn_context* c, GraphState* g, const uint8_t* chars, const uint32_t* offs, int n, int d,
+                       int measure) {
+    graph_release(g);
+    XTN_TRY(graph_reserve(c, g, chars, offs, nullptr, n, d, measure));
+    cudaGraph_t graph = nullptr;
+    XTN_TRY(capture(c, [&] { return graph_enqueue(c, g); }, &graph, &g->launches));
+    g->graph = graph;
+    XTN_CK(cudaGraphInstantiate(&g->exec, graph, 0));
+    g->bufs = context_buffer_ptrs(c);
+    return XTN_SUCCESS;
+}
+
+// One replay of a captured form, timed with events; the statistics are reset (ms_total set).
+static int graph_launch(xtn_context* c, cudaGraphExec_t exec) {
     cudaStream_t s = c->stream;
     xtn_stats& st = c->stats;
     memset(&st, 0, sizeof st);
+    XTN_CK(cudaEventRecord(c->ev[0], s));
+    XTN_CK(cudaGraphLaunch(exec, s));
+    XTN_CK(cudaEventRecord(c->ev[8], s));
+    XTN_CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[8]);
+    st.ms_total = ms;
+    return XTN_SUCCESS;
+}
+
+// The search's status block of a replay (host scalars 16..28) into the statistics and the result
+// count; *redo is set when the plain form has to run instead.
+static int graph_check(xtn_context* c, GraphState* g, bool* redo) {
+    cudaStream_t s = c->stream;
+    xtn_stats& st = c->stats;
     st.n_seqs = g->n;
     st.n_rounds = 1;
     st.id_bits = id_bits_for(g->n);
-    XTN_CK(cudaEventRecord(c->ev[0], s));
-    XTN_CK(cudaGraphLaunch(g->exec, s));
-    XTN_CK(cudaEventRecord(c->ev[8], s));
-    XTN_CK(cudaStreamSynchronize(s));
     const uint64_t* h = c->h_scalar + 16;
     *redo = false;
     if ((uint32_t)h[GS_LENBAD] != 0xffffffffu) return length_check_result(c, (uint32_t)h[GS_LENBAD]);
@@ -1711,12 +1782,15 @@ static int graph_replay(xtn_context* c, GraphState* g, bool* redo) {
     st.n_unique = (int64_t)h[GS_UNIQUE];
     st.n_out = (int64_t)h[GS_OUT];
     st.n_launches = g->launches;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev[0], c->ev[8]);
-    st.ms_total = ms;
     c->n_out = st.n_out;
     c->overlap_result = false;
     return XTN_SUCCESS;
+}
+
+// One search by the graph form; *redo is set when the plain form has to run instead.
+static int graph_replay(xtn_context* c, GraphState* g, bool* redo) {
+    XTN_TRY(graph_launch(c, g->exec));
+    return graph_check(c, g, redo);
 }
 
 // The device-resident search in the graph form (option "graph" = 1).
@@ -1724,7 +1798,7 @@ static int nn_graph(xtn_context* c, const uint8_t* chars, const uint32_t* offs, 
     if (!c->graph) c->graph = new GraphState();
     GraphState* g = static_cast<GraphState*>(c->graph);
     const bool same = g->exec && g->chars == chars && g->offs == offs && g->n == n && g->d == d &&
-                      g->measure == measure && g->sig == graph_signature(c);
+                      g->measure == measure && g->sig == graph_signature(c) && g->bufs == context_buffer_ptrs(c);
     if (same) {
         bool redo = false;
         XTN_TRY(graph_replay(c, g, &redo));
@@ -1841,10 +1915,15 @@ static int deliver(xtn_context* c, xtn_callback cb, void* user) {
 //   5. the R x R matrix of sums (u64, wrapping like the reference's size_t) is emitted in
 //      (x, y) order for every entry that received a contribution.
 
+// Kernels of the overlap form take an abort word (nullptr in the plain form): the graph form
+// sets it when the lengths or repertoire ids are invalid, or the unique-string count differs from
+// the one the graph was captured for, and every kernel that would index by them then does nothing.
+__device__ __forceinline__ bool aborted(const unsigned int* abort) { return abort && *abort; }
+
 __global__ void k_row_hash(const uint8_t* __restrict__ chars, const uint32_t* __restrict__ offs, int n, int idbits,
-                           uint64_t* __restrict__ recs) {
+                           uint64_t* __restrict__ recs, const unsigned int* __restrict__ abort) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || aborted(abort)) return;
     uint32_t s = offs[i];
     int L = (int)(offs[i + 1] - s);
     uint64_t h = 0x84222325cbf29ce4ULL ^ (uint64_t)L;
@@ -1867,9 +1946,9 @@ __device__ __forceinline__ int cmp_rows(const uint8_t* chars, const uint32_t* of
 // A run of equal hashes that holds different strings (a hash collision) is re-ordered by
 // (string, row) so that equal strings are contiguous again with rows ascending.
 __global__ void k_run_fix(uint64_t* __restrict__ recs, int n, int idbits, const uint8_t* __restrict__ chars,
-                          const uint32_t* __restrict__ offs) {
+                          const uint32_t* __restrict__ offs, const unsigned int* __restrict__ abort) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || aborted(abort)) return;
     const uint64_t idmask = (1ull << idbits) - 1ull;
     uint64_t k = recs[i] >> idbits;
     if (i > 0 && (recs[i - 1] >> idbits) == k) return;
@@ -1894,9 +1973,14 @@ __global__ void k_run_fix(uint64_t* __restrict__ recs, int n, int idbits, const 
 }
 
 __global__ void k_uniq_flags(const uint64_t* __restrict__ recs, int n, int idbits, const uint8_t* __restrict__ chars,
-                             const uint32_t* __restrict__ offs, uint8_t* __restrict__ head) {
+                             const uint32_t* __restrict__ offs, uint8_t* __restrict__ head,
+                             const unsigned int* __restrict__ abort) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (aborted(abort)) {
+        head[i] = 0;
+        return;
+    }
     const uint64_t idmask = (1ull << idbits) - 1ull;
     bool h = i == 0 || (recs[i] >> idbits) != (recs[i - 1] >> idbits) ||
              cmp_rows(chars, offs, (uint32_t)(recs[i - 1] & idmask), (uint32_t)(recs[i] & idmask)) != 0;
@@ -1905,9 +1989,10 @@ __global__ void k_uniq_flags(const uint64_t* __restrict__ recs, int n, int idbit
 
 __global__ void k_uniq_build(const uint64_t* __restrict__ recs, const uint8_t* __restrict__ head,
                              const uint32_t* __restrict__ uidx, int n, int idbits, int32_t* __restrict__ rep_row,
-                             uint32_t* __restrict__ occ_start, uint32_t* __restrict__ srow) {
+                             uint32_t* __restrict__ occ_start, uint32_t* __restrict__ srow,
+                             const unsigned int* __restrict__ abort) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || aborted(abort)) return;
     uint32_t row = (uint32_t)(recs[i] & ((1ull << idbits) - 1ull));
     srow[i] = row;
     if (head[i]) {
@@ -1923,15 +2008,17 @@ __global__ void k_uniq_build(const uint64_t* __restrict__ recs, const uint8_t* _
 // after an exclusive scan row_uid[row] is the row-order number of a first occurrence, and
 // k_uniq_row_order fills row_rep (row-order number -> row, ascending) and row_map (row-order
 // number -> hash-order number, which indexes the occurrence lists).
-__global__ void k_uniq_row_heads(const int32_t* __restrict__ rep_row, int U, uint8_t* __restrict__ row_head) {
+__global__ void k_uniq_row_heads(const int32_t* __restrict__ rep_row, int U, uint8_t* __restrict__ row_head,
+                                 const unsigned int* __restrict__ abort) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u < U) row_head[rep_row[u]] = 1;
+    if (u < U && !aborted(abort)) row_head[rep_row[u]] = 1;
 }
 
 __global__ void k_uniq_row_order(const int32_t* __restrict__ rep_row, int U, const uint32_t* __restrict__ row_uid,
-                                 int32_t* __restrict__ row_rep, uint32_t* __restrict__ row_map) {
+                                 int32_t* __restrict__ row_rep, uint32_t* __restrict__ row_map,
+                                 const unsigned int* __restrict__ abort) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= U) return;
+    if (u >= U || aborted(abort)) return;
     const int32_t row = rep_row[u];
     const uint32_t v = row_uid[row];
     row_rep[v] = row;
@@ -1947,8 +2034,10 @@ constexpr int kSmemReps = 96;
 
 __global__ void k_diag(const uint32_t* __restrict__ occ_start, const uint32_t* __restrict__ srow, int U,
                        const int32_t* __restrict__ freq, const int32_t* __restrict__ rep, int R,
-                       unsigned long long* __restrict__ M, uint8_t* __restrict__ present) {
+                       unsigned long long* __restrict__ M, uint8_t* __restrict__ present,
+                       const unsigned int* __restrict__ abort) {
     extern __shared__ unsigned long long s_m[];
+    if (aborted(abort)) return;
     const bool local = R <= kSmemReps;
     uint8_t* s_p = reinterpret_cast<uint8_t*>(s_m + (local ? R * R : 0));
     if (local) {
@@ -1988,13 +2077,16 @@ __global__ void k_diag(const uint32_t* __restrict__ occ_start, const uint32_t* _
     }
 }
 
-// Cross term; with R <= kSmemReps the block accumulates into shared memory first.
-
+// Cross term; with R <= kSmemReps the block accumulates into shared memory first. The graph
+// form passes the verified-pair count on the device (np_dev) instead of np.
 __global__ void k_cross(const xtn_int2* __restrict__ pairs, int64_t np, const uint32_t* __restrict__ occ_start,
                         const uint32_t* __restrict__ srow, const int32_t* __restrict__ freq,
                         const int32_t* __restrict__ rep, int R, unsigned long long* __restrict__ M,
-                        uint8_t* __restrict__ present, const uint32_t* __restrict__ row_map) {
+                        uint8_t* __restrict__ present, const uint32_t* __restrict__ row_map,
+                        const uint64_t* __restrict__ np_dev, const unsigned int* __restrict__ abort) {
     extern __shared__ unsigned long long s_m[];
+    if (aborted(abort)) return;
+    if (np_dev) np = (int64_t)*np_dev;
     const bool local = R <= kSmemReps;
     uint8_t* s_p = reinterpret_cast<uint8_t*>(s_m + (local ? R * R : 0));
     if (local) {
@@ -2061,6 +2153,31 @@ namespace xtn {
 
 constexpr int kMaxRepertoires = 8192;
 
+static std::vector<DevBuf*> context_buffers(xtn_context* c) {
+    std::vector<DevBuf*> v = {
+        &c->chars,   &c->offs,      &c->keys,      &c->klen,     &c->vcnt,       &c->voff,     &c->recA,
+        &c->recB,    &c->gstart,    &c->gsize,     &c->gcnt,     &c->goff,       &c->pairA,    &c->pairB,
+        &c->dist,    &c->flag,      &c->fpos,      &c->scratch64, &c->scratch32, &c->counter,  &c->out_pairs,
+        &c->out_dist, &c->out_freq, &c->bcounts,   &c->boffs,    &c->btotals,    &c->bstart,   &c->bdesc,
+        &c->bjobs,   &c->bfall,     &c->bcnt,      &c->fbA,      &c->fbB,        &c->runinfo,  &c->tcnt,
+        &c->toff,    &c->ktab,      &c->info,      &c->lencheck, &c->pairA2,     &c->ddcnt,    &c->tseq,
+        &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
+    if (c->overlap_bufs) {
+        xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
+        for (DevBuf* b : {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
+                          &ob->occ_start, &ob->srow, &ob->M, &ob->present, &ob->mpos, &ob->scratch, &ob->row_head,
+                          &ob->row_uid, &ob->row_rep, &ob->row_map})
+            v.push_back(b);
+    }
+    return v;
+}
+
+static std::vector<const void*> context_buffer_ptrs(const xtn_context* c) {
+    std::vector<const void*> v;
+    for (const DevBuf* b : context_buffers(const_cast<xtn_context*>(c))) v.push_back(b->p);
+    return v;
+}
+
 // De-interleaves the per-row info into frequency and repertoire arrays; *bad_row receives the
 // smallest row whose repertoire id is outside [0, R) (it starts at INT_MAX).
 __global__ void k_split_info(const xtn_seq_info* __restrict__ info, int n, int R, int32_t* __restrict__ freq,
@@ -2073,19 +2190,123 @@ __global__ void k_split_info(const xtn_seq_info* __restrict__ info, int n, int R
     if (v.repertoire < 0 || v.repertoire >= R) atomicMin(bad_row, i);
 }
 
+// The overlap form's buffers: everything indexed by a unique string is sized for n + 1 entries
+// (the unique count is at most n), so that no stage has to wait for that count to size them.
+static int ov_reserve(xtn_context* c, xtn_overlap_bufs& b, int n, int R) {
+    const size_t RR = (size_t)R * R;
+    XTN_TRY(ensure(b.freq, sizeof(int32_t) * n));
+    XTN_TRY(ensure(b.rep, sizeof(int32_t) * n));
+    XTN_TRY(ensure(c->counter, 64));
+    XTN_TRY(ensure(b.recA, sizeof(uint64_t) * n));
+    XTN_TRY(ensure(b.recB, sizeof(uint64_t) * n));
+    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
+    XTN_TRY(ensure(b.head, (size_t)n));
+    XTN_TRY(ensure(b.uidx, sizeof(uint32_t) * (n + 1)));
+    XTN_TRY(ensure(b.scratch, sizeof(uint32_t) * std::max(scan_scratch_elems(n), scan_scratch_elems((int64_t)RR))));
+    XTN_TRY(ensure(b.rep_row, sizeof(int32_t) * (n + 1)));
+    XTN_TRY(ensure(b.occ_start, sizeof(uint32_t) * (n + 1)));
+    XTN_TRY(ensure(b.srow, sizeof(uint32_t) * n));
+    XTN_TRY(ensure(b.row_head, (size_t)n));
+    XTN_TRY(ensure(b.row_uid, sizeof(uint32_t) * (n + 1)));
+    XTN_TRY(ensure(b.row_rep, sizeof(int32_t) * (n + 1)));
+    XTN_TRY(ensure(b.row_map, sizeof(uint32_t) * (n + 1)));
+    XTN_TRY(ensure(b.M, sizeof(unsigned long long) * RR));
+    XTN_TRY(ensure(b.present, RR));
+    XTN_TRY(ensure(b.mpos, sizeof(uint32_t) * (RR + 1)));
+    XTN_TRY(ensure(c->scan_status, sizeof(unsigned long long) * scan_1p_words(n)));
+    XTN_TRY(ensure_err_word(c));
+    const size_t msmem = R <= kSmemReps ? RR * (sizeof(unsigned long long) + 1) : 0;
+    if (msmem > 48 * 1024) {
+        XTN_CK(cudaFuncSetAttribute(k_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+        XTN_CK(cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+    }
+    return XTN_SUCCESS;
+}
+
+static size_t ov_matrix_smem(int R) {
+    return R <= kSmemReps ? (size_t)R * R * (sizeof(unsigned long long) + 1) : 0;
+}
+
+// 1. identical strings merged: row hashes sorted, hash collisions re-ordered by string, first
+// occurrences flagged and numbered (uidx[n] = U), occurrence lists (occ_start, srow) and one
+// representative row per unique string (rep_row, hash order).
+static void ov_unique(xtn_context* c, xtn_overlap_bufs& b, const uint8_t* chars, const uint32_t* offs, int n,
+                      const unsigned int* abort) {
+    cudaStream_t s = c->stream;
+    const int idbits = id_bits_for(n);
+    XTN_LAUNCH("row_hash", k_row_hash<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, n, idbits, P<uint64_t>(b.recA),
+                                                                          abort));
+    uint64_t* recs = radix_sort_u64(P<uint64_t>(b.recA), P<uint64_t>(b.recB), n, idbits, 64, P<uint32_t>(c->scratch32),
+                                    s, "row_sort_upsweep", "row_sort_downsweep");
+    XTN_LAUNCH("run_fix", k_run_fix<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs, abort));
+    XTN_LAUNCH("uniq_flags", k_uniq_flags<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs,
+                                                                              P<uint8_t>(b.head), abort));
+    scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, P<uint32_t>(b.scratch), s);
+    XTN_LAUNCH("uniq_build", k_uniq_build<<<blocks_for(n), kThreads, 0, s>>>(
+                                 recs, P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, idbits, P<int32_t>(b.rep_row),
+                                 P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), abort));
+}
+
+// The unique strings renumbered in row order (row_rep: row-order number -> row, row_map:
+// row-order number -> hash-order number), then the diagonal term into the cleared matrix.
+static int ov_rows_diag(xtn_context* c, xtn_overlap_bufs& b, int n, uint32_t U, int R, const unsigned int* abort) {
+    cudaStream_t s = c->stream;
+    const size_t RR = (size_t)R * R;
+    XTN_CK(cudaMemsetAsync(b.row_head.p, 0, (size_t)n, s));
+    XTN_LAUNCH("uniq_row_heads", k_uniq_row_heads<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
+                                     P<int32_t>(b.rep_row), (int)U, P<uint8_t>(b.row_head), abort));
+    scan_exclusive_1p<uint8_t, uint32_t>(P<uint8_t>(b.row_head), P<uint32_t>(b.row_uid), n,
+                                         P<unsigned long long>(c->scan_status), P<unsigned int>(c->dev_err), s,
+                                         c->wait_polls, 0);
+    XTN_LAUNCH("uniq_row_order", k_uniq_row_order<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
+                                     P<int32_t>(b.rep_row), (int)U, P<uint32_t>(b.row_uid), P<int32_t>(b.row_rep),
+                                     P<uint32_t>(b.row_map), abort));
+    XTN_CK(cudaMemsetAsync(b.M.p, 0, sizeof(unsigned long long) * RR, s));
+    XTN_CK(cudaMemsetAsync(b.present.p, 0, RR, s));
+    const unsigned dblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(blocks_for((int64_t)U), c->sms * 4));
+    XTN_LAUNCH("diag", k_diag<<<dblocks, kThreads, ov_matrix_smem(R), s>>>(
+                           P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), (int)U, P<int32_t>(b.freq), P<int32_t>(b.rep),
+                           R, P<unsigned long long>(b.M), P<uint8_t>(b.present), abort));
+    return XTN_SUCCESS;
+}
+
+// 4. cross term over the verified unique pairs (np on the host, or *np_dev on the device).
+static void ov_cross(xtn_context* c, xtn_overlap_bufs& b, int64_t np, const uint64_t* np_dev, int R,
+                     const unsigned int* abort) {
+    const int64_t blocks = np_dev ? (int64_t)c->sms * 4 : std::min<int64_t>((np + kThreads - 1) / kThreads, (int64_t)c->sms * 4);
+    XTN_LAUNCH("cross", k_cross<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, ov_matrix_smem(R), c->stream>>>(
+                            P<xtn_int2>(c->out_pairs), np, P<uint32_t>(b.occ_start), P<uint32_t>(b.srow),
+                            P<int32_t>(b.freq), P<int32_t>(b.rep), R, P<unsigned long long>(b.M),
+                            P<uint8_t>(b.present), P<uint32_t>(b.row_map), np_dev, abort));
+}
+
+// 5. matrix -> entries in (x, y) order (positions scanned from the presence flags; the count is
+// mpos[R * R]).
+static void ov_matrix(xtn_context* c, xtn_overlap_bufs& b, int R, bool scan) {
+    const size_t RR = (size_t)R * R;
+    if (scan)
+        scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.present), P<uint32_t>(b.mpos), (int64_t)RR,
+                                          P<uint32_t>(b.scratch), c->stream);
+    else
+        XTN_LAUNCH("matrix_compact", k_matrix_compact<<<blocks_for((int64_t)RR), kThreads, 0, c->stream>>>(
+                                         P<unsigned long long>(b.M), P<uint8_t>(b.present), P<uint32_t>(b.mpos), R,
+                                         P<xtn_int2>(c->out_pairs), P<uint64_t>(c->out_freq)));
+}
+
 // Overlap mode on device-resident inputs (d_info: one xtn_seq_info per row, row order).
 int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* d_info, int n, int d,
                 int measure, int R, bool validate) {
+    if (c->shard_count > 1) {
+        set_err("sharding covers the nearest-neighbour mode only");
+        return XTN_ERR_ARG;
+    }
     if (R > kMaxRepertoires) {
         set_err("overlap mode supports at most " + std::to_string(kMaxRepertoires) + " repertoires");
         return XTN_ERR_LIMIT;
     }
     cudaStream_t s = c->stream;
     xtn_overlap_bufs& b = *reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
-    const int idbits = id_bits_for(n);
-    XTN_TRY(ensure(b.freq, sizeof(int32_t) * n));
-    XTN_TRY(ensure(b.rep, sizeof(int32_t) * n));
-    XTN_TRY(ensure(c->counter, 64));
+    XTN_TRY(ov_reserve(c, b, n, R));
     const int int_max = 0x7fffffff;
     XTN_CK(cudaMemcpyAsync(c->counter.p, &int_max, sizeof(int), cudaMemcpyHostToDevice, s));
     if (validate) XTN_TRY(launch_length_check(c, offs, nullptr, n));
@@ -2102,57 +2323,12 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     }
 
     // 1. merge identical strings
-    XTN_TRY(ensure(b.recA, sizeof(uint64_t) * n));
-    XTN_TRY(ensure(b.recB, sizeof(uint64_t) * n));
-    XTN_LAUNCH("row_hash", k_row_hash<<<blocks_for(n), kThreads, 0, s>>>(chars, offs, n, idbits, P<uint64_t>(b.recA)));
+    ov_unique(c, b, chars, offs, n, nullptr);
     XTN_CK(cudaGetLastError());
-    uint64_t* recs = nullptr;
-    XTN_TRY(ensure(c->scratch32, sizeof(uint32_t) * radix_scratch_elems(n)));
-    recs = radix_sort_u64(P<uint64_t>(b.recA), P<uint64_t>(b.recB), n, idbits, 64, P<uint32_t>(c->scratch32), s,
-                          "row_sort_upsweep", "row_sort_downsweep");
-    XTN_LAUNCH("run_fix", k_run_fix<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs));
-    XTN_TRY(ensure(b.head, (size_t)n));
-    XTN_TRY(ensure(b.uidx, sizeof(uint32_t) * (n + 1)));
-    XTN_LAUNCH("uniq_flags", k_uniq_flags<<<blocks_for(n), kThreads, 0, s>>>(recs, n, idbits, chars, offs, P<uint8_t>(b.head)));
-    XTN_TRY(ensure(b.scratch, sizeof(uint32_t) * scan_scratch_elems(n)));
-    scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, P<uint32_t>(b.scratch), s);
     uint64_t U = 0;
     XTN_TRY(read_scalar(c, P<uint32_t>(b.uidx) + n, 4, &U));
-    XTN_TRY(ensure(b.rep_row, sizeof(int32_t) * U));
-    XTN_TRY(ensure(b.occ_start, sizeof(uint32_t) * (U + 1)));
-    XTN_TRY(ensure(b.srow, sizeof(uint32_t) * n));
-    XTN_LAUNCH("uniq_build", k_uniq_build<<<blocks_for(n), kThreads, 0, s>>>(recs, P<uint8_t>(b.head), P<uint32_t>(b.uidx), n, idbits,
-                                                    P<int32_t>(b.rep_row), P<uint32_t>(b.occ_start), P<uint32_t>(b.srow)));
-    XTN_CK(cudaGetLastError());
-    // row-order numbering of the unique strings
-    XTN_TRY(ensure(b.row_head, (size_t)n));
-    XTN_TRY(ensure(b.row_uid, sizeof(uint32_t) * (n + 1)));
-    XTN_TRY(ensure(b.row_rep, sizeof(int32_t) * (U + 1)));
-    XTN_TRY(ensure(b.row_map, sizeof(uint32_t) * (U + 1)));
-    XTN_CK(cudaMemsetAsync(b.row_head.p, 0, (size_t)n, s));
-    XTN_LAUNCH("uniq_row_heads", k_uniq_row_heads<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
-                                     P<int32_t>(b.rep_row), (int)U, P<uint8_t>(b.row_head)));
-    XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(b.row_head), P<uint32_t>(b.row_uid), n)));
-    XTN_LAUNCH("uniq_row_order", k_uniq_row_order<<<blocks_for((int64_t)U), kThreads, 0, s>>>(
-                                     P<int32_t>(b.rep_row), (int)U, P<uint32_t>(b.row_uid), P<int32_t>(b.row_rep),
-                                     P<uint32_t>(b.row_map)));
-    XTN_CK(cudaGetLastError());
-
-    // 2. diagonal term
-    size_t RR = (size_t)R * R;
-    XTN_TRY(ensure(b.M, sizeof(unsigned long long) * RR));
-    XTN_TRY(ensure(b.present, RR));
-    XTN_CK(cudaMemsetAsync(b.M.p, 0, sizeof(unsigned long long) * RR, s));
-    XTN_CK(cudaMemsetAsync(b.present.p, 0, RR, s));
-    const size_t msmem = R <= kSmemReps ? RR * (sizeof(unsigned long long) + 1) : 0;
-    if (msmem > 48 * 1024) {
-        XTN_CK(cudaFuncSetAttribute(k_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
-        XTN_CK(cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
-    }
-    const unsigned dblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(blocks_for((int64_t)U), c->sms * 4));
-    XTN_LAUNCH("diag", k_diag<<<dblocks, kThreads, msmem, s>>>(P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), (int)U,
-                                                       P<int32_t>(b.freq), P<int32_t>(b.rep), R,
-                                                       P<unsigned long long>(b.M), P<uint8_t>(b.present)));
+    // 2. row-order numbering, diagonal term
+    XTN_TRY(ov_rows_diag(c, b, n, (uint32_t)U, R, nullptr));
     XTN_CK(cudaGetLastError());
 
     // 3. neighbours among the unique strings
@@ -2160,26 +2336,17 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     const int64_t nverified = c->n_out;
 
     // 4. cross term
-    if (nverified > 0) {
-        const size_t smem = msmem;
-        int64_t blocks = std::min<int64_t>((nverified + kThreads - 1) / kThreads, (int64_t)c->sms * 4);
-        XTN_LAUNCH("cross", k_cross<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, smem, s>>>(
-            P<xtn_int2>(c->out_pairs), nverified, P<uint32_t>(b.occ_start), P<uint32_t>(b.srow), P<int32_t>(b.freq),
-            P<int32_t>(b.rep), R, P<unsigned long long>(b.M), P<uint8_t>(b.present), P<uint32_t>(b.row_map)));
-        XTN_CK(cudaGetLastError());
-    }
+    if (nverified > 0) ov_cross(c, b, nverified, nullptr, R, nullptr);
+    XTN_CK(cudaGetLastError());
 
     // 5. matrix -> sorted entries
-    XTN_TRY(ensure(b.mpos, sizeof(uint32_t) * (RR + 1)));
-    XTN_TRY(ensure(b.scratch, sizeof(uint32_t) * scan_scratch_elems((int64_t)RR)));
-    scan_exclusive<uint8_t, uint32_t>(P<uint8_t>(b.present), P<uint32_t>(b.mpos), (int64_t)RR, P<uint32_t>(b.scratch), s);
+    const size_t RR = (size_t)R * R;
+    ov_matrix(c, b, R, true);
     uint64_t nent = 0;
     XTN_TRY(read_scalar(c, P<uint32_t>(b.mpos) + RR, 4, &nent));
     XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * nent));
     XTN_TRY(ensure(c->out_freq, sizeof(uint64_t) * nent));
-    XTN_LAUNCH("matrix_compact", k_matrix_compact<<<blocks_for((int64_t)RR), kThreads, 0, s>>>(P<unsigned long long>(b.M), P<uint8_t>(b.present),
-                                                                 P<uint32_t>(b.mpos), R, P<xtn_int2>(c->out_pairs),
-                                                                 P<uint64_t>(c->out_freq)));
+    ov_matrix(c, b, R, false);
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaStreamSynchronize(s));
     c->n_out = (int64_t)nent;
@@ -2187,6 +2354,177 @@ int run_overlap(xtn_context* c, const uint8_t* chars, const uint32_t* offs, cons
     c->stats.n_verified_pairs = nverified;
     c->stats.n_out = (int64_t)nent;
     c->stats.n_seqs = (int64_t)U;
+    return XTN_SUCCESS;
+}
+
+// ------------------------------------------------------------------ overlap graph form
+// The overlap mode on device-resident inputs as one captured launch sequence (option "graph"):
+// the length and repertoire checks, the merge of identical strings, the row-order numbering and
+// the diagonal term, the whole neighbour search over the unique strings as the search's graph
+// form enqueues it (persistent grouping, device-side sizes), the cross term over the verified
+// count on the device and the matrix compaction, with one status block read per replay. The
+// unique-string count and the search's capacities come from the plain run that precedes the
+// capture; a replay whose unique count differs, or whose search outgrows a capacity, is redone
+// by the plain form, which re-captures.
+struct OverlapGraph {
+    const uint8_t* chars = nullptr;
+    const uint32_t* offs = nullptr;
+    const xtn_seq_info* info = nullptr;
+    int n = 0, d = 0, measure = 0, R = 0;
+    int64_t sig = 0;
+    uint32_t U = 0;
+    GraphState nn;  // capacities and device tables of the search over the unique strings
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+    std::vector<const void*> bufs;  // the context's buffers at capture (a reallocation invalidates it)
+    DevBuf ost;  // u32 [0] first bad repertoire row, [1] first bad length, [2] abort word
+};
+
+// Overlap status words, copied to the pinned host scalars 29..31.
+enum { OS_BAD, OS_UNIQUE, OS_ENTRIES, OS_WORDS };
+
+__global__ void k_overlap_guard(const unsigned int* __restrict__ ost, unsigned int* __restrict__ abort) {
+    abort[0] = (ost[0] != 0x7fffffffu || ost[1] != 0xffffffffu) ? 1u : 0u;
+}
+
+__global__ void k_overlap_unique_guard(const uint32_t* __restrict__ U_dev, uint32_t U, unsigned int* __restrict__ abort) {
+    if (*U_dev != U) abort[0] = 1u;
+}
+
+__global__ void k_overlap_status(const unsigned int* __restrict__ ost, const uint32_t* __restrict__ U_dev,
+                                 const uint32_t* __restrict__ nent, uint64_t* __restrict__ st) {
+    st[OS_BAD] = (uint64_t)ost[0] | ((uint64_t)ost[1] << 32);
+    st[OS_UNIQUE] = *U_dev;
+    st[OS_ENTRIES] = *nent;
+}
+
+static void overlap_graph_release(OverlapGraph* og) {
+    if (og->exec) cudaGraphExecDestroy(og->exec);
+    if (og->graph) cudaGraphDestroy(og->graph);
+    og->exec = nullptr;
+    og->graph = nullptr;
+}
+
+static int overlap_graph_enqueue(xtn_context* c, OverlapGraph* og) {
+    cudaStream_t s = c->stream;
+    xtn_overlap_bufs& b = *reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
+    const int n = og->n, R = og->R;
+    unsigned int* ost = P<unsigned int>(og->ost);
+    unsigned int* abort = ost + 2;
+    XTN_LAUNCH("set_status", k_set_u64<<<1, 1, 0, s>>>(reinterpret_cast<unsigned long long*>(ost),
+                                                       0xffffffff7fffffffull));
+    XTN_LAUNCH("check_lengths", k_check_lengths<<<blocks_for(n), kThreads, 0, s>>>(og->offs, nullptr, n, ost + 1));
+    XTN_LAUNCH("split_info", k_split_info<<<blocks_for(n), kThreads, 0, s>>>(og->info, n, R, P<int32_t>(b.freq),
+                                                                              P<int32_t>(b.rep), reinterpret_cast<int*>(ost)));
+    XTN_LAUNCH("overlap_guard", k_overlap_guard<<<1, 1, 0, s>>>(ost, abort));
+    ov_unique(c, b, og->chars, og->offs, n, abort);
+    XTN_LAUNCH("overlap_guard", k_overlap_unique_guard<<<1, 1, 0, s>>>(P<uint32_t>(b.uidx) + n, og->U, abort));
+    // rows the search reads when an abort leaves them unset
+    XTN_CK(cudaMemsetAsync(b.row_rep.p, 0, sizeof(int32_t) * (og->U + 1), s));
+    XTN_TRY(ov_rows_diag(c, b, n, og->U, R, abort));
+    og->nn.rows = P<int32_t>(b.row_rep);
+    og->nn.pre_abort = abort;
+    XTN_TRY(graph_enqueue(c, &og->nn));
+    ov_cross(c, b, 0, P<uint64_t>(og->nn.status) + GS_OUT, R, abort);
+    ov_matrix(c, b, R, true);
+    ov_matrix(c, b, R, false);
+    XTN_LAUNCH("overlap_status", k_overlap_status<<<1, 1, 0, s>>>(ost, P<uint32_t>(b.uidx) + n,
+                                                                   P<uint32_t>(b.mpos) + (size_t)R * R,
+                                                                   P<uint64_t>(og->ost) + 2));
+    XTN_CK(cudaMemcpyAsync(c->h_scalar + 29, P<uint64_t>(og->ost) + 2, sizeof(uint64_t) * OS_WORDS,
+                           cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaGetLastError());
+    return XTN_SUCCESS;
+}
+
+// Capacities from the plain overlap run just made on this input, buffers reserved, graph captured.
+static int overlap_graph_build(xtn_context* c, OverlapGraph* og, const uint8_t* chars, const uint32_t* offs,
+                               const xtn_seq_info* info, int n, int d, int measure, int R) {
+    overlap_graph_release(og);
+    xtn_overlap_bufs& b = *reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
+    const uint32_t U = (uint32_t)c->stats.n_seqs;
+    const size_t RR = (size_t)R * R;
+    if (RR > ((size_t)1 << 24)) return XTN_ERR_LIMIT;  // matrix output capacity: at most 2^24 entries
+    og->chars = chars;
+    og->offs = offs;
+    og->info = info;
+    og->n = n;
+    og->d = d;
+    og->measure = measure;
+    og->R = R;
+    og->U = U;
+    og->sig = graph_signature(c);
+    XTN_TRY(graph_reserve(c, &og->nn, chars, offs, P<int32_t>(b.row_rep), (int)U, d, measure));
+    XTN_TRY(ov_reserve(c, b, n, R));
+    // the matrix entries of the plain run are still to be read by the caller
+    XTN_TRY(ensure_keep(c, c->out_pairs, std::max<size_t>(c->out_pairs.cap, sizeof(xtn_int2) * RR + 64),
+                        sizeof(xtn_int2) * (size_t)c->n_out));
+    XTN_TRY(ensure_keep(c, c->out_freq, sizeof(uint64_t) * RR + 64, sizeof(uint64_t) * (size_t)c->n_out));
+    XTN_TRY(ensure(og->ost, 64));
+    XTN_CK(cudaStreamSynchronize(c->stream));
+    cudaGraph_t graph = nullptr;
+    XTN_TRY(capture(c, [&] { return overlap_graph_enqueue(c, og); }, &graph, &og->launches));
+    og->graph = graph;
+    XTN_CK(cudaGraphInstantiate(&og->exec, graph, 0));
+    og->bufs = context_buffer_ptrs(c);
+    return XTN_SUCCESS;
+}
+
+static int overlap_graph_replay(xtn_context* c, OverlapGraph* og, bool* redo) {
+    *redo = false;
+    XTN_TRY(graph_launch(c, og->exec));
+    xtn_stats& st = c->stats;
+    const uint64_t* h = c->h_scalar + 29;
+    const uint32_t lenbad = (uint32_t)(h[OS_BAD] >> 32);
+    const int bad = (int)(uint32_t)h[OS_BAD];
+    if (lenbad != 0xffffffffu) return length_check_result(c, lenbad);
+    if (bad != 0x7fffffff) {
+        set_err("repertoire id out of range at row " + std::to_string(bad));
+        return XTN_ERR_ARG;
+    }
+    if (h[OS_UNIQUE] != og->U) {
+        *redo = true;
+        return XTN_SUCCESS;
+    }
+    const float ms = st.ms_total;
+    XTN_TRY(graph_check(c, &og->nn, redo));
+    if (*redo) return XTN_SUCCESS;
+    st.ms_total = ms;
+    st.n_launches = og->launches;
+    st.n_verified_pairs = st.n_out;
+    st.n_out = (int64_t)h[OS_ENTRIES];
+    st.n_seqs = (int64_t)og->U;
+    c->n_out = st.n_out;
+    c->overlap_result = true;
+    return XTN_SUCCESS;
+}
+
+// The device-resident overlap mode in the graph form (option "graph" = 1).
+static int overlap_graph(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const xtn_seq_info* info, int n,
+                         int d, int measure, int R) {
+    if (!c->ograph) c->ograph = new OverlapGraph();
+    OverlapGraph* og = static_cast<OverlapGraph*>(c->ograph);
+    const bool same = og->exec && og->chars == chars && og->offs == offs && og->info == info && og->n == n &&
+                      og->d == d && og->measure == measure && og->R == R && og->sig == graph_signature(c) &&
+                      og->bufs == context_buffer_ptrs(c);
+    if (same) {
+        bool redo = false;
+        XTN_TRY(overlap_graph_replay(c, og, &redo));
+        if (!redo) return XTN_SUCCESS;
+    }
+    begin_run(c);
+    int r = run_overlap(c, chars, offs, info, n, d, measure, R, true);
+    end_run(c);
+    if (r != XTN_SUCCESS) return r;
+    const xtn_stats keep = c->stats;
+    const int64_t keep_out = c->n_out;
+    const int b = overlap_graph_build(c, og, chars, offs, info, n, d, measure, R);
+    if (b != XTN_SUCCESS && b != XTN_ERR_LIMIT) return b;
+    if (b == XTN_ERR_LIMIT) overlap_graph_release(og);  // this input stays in the plain form
+    c->stats = keep;
+    c->n_out = keep_out;
+    c->overlap_result = true;
     return XTN_SUCCESS;
 }
 
@@ -2424,15 +2762,6 @@ void xtn_context_destroy(xtn_context* c) {
     if (current_profiler() == &c->prof) current_profiler() = nullptr;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->chars,   &c->offs,     &c->keys,      &c->klen,      &c->vcnt,     &c->voff,
-                      &c->recA,    &c->recB,     &c->gstart,    &c->gsize,     &c->gcnt,     &c->goff,
-                      &c->pairA,   &c->pairB,    &c->dist,      &c->flag,      &c->fpos,     &c->scratch64,
-                      &c->scratch32, &c->counter, &c->out_pairs, &c->out_dist, &c->out_freq, &c->bcounts,
-                      &c->boffs,   &c->btotals,  &c->bstart,    &c->bdesc,     &c->bjobs,    &c->bfall,
-                      &c->bcnt,    &c->fbA,      &c->fbB,       &c->runinfo,   &c->tcnt,     &c->toff,
-                      &c->ktab,    &c->info,     &c->lencheck, &c->pairA2, &c->ddcnt, &c->tseq,      &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
-    for (DevBuf* b : bufs) release(*b);
-    delete static_cast<TuneCache*>(c->tune_cache);
     if (c->graph) {
         GraphState* g = static_cast<GraphState*>(c->graph);
         graph_release(g);
@@ -2441,14 +2770,18 @@ void xtn_context_destroy(xtn_context* c) {
         release(g->os_status);
         delete g;
     }
-    if (c->overlap_bufs) {
-        xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
-        DevBuf* obufs[] = {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
-                           &ob->occ_start, &ob->srow, &ob->M, &ob->present, &ob->mpos, &ob->scratch,
-                           &ob->row_head, &ob->row_uid, &ob->row_rep, &ob->row_map};
-        for (DevBuf* b : obufs) release(*b);
-        delete ob;
+    if (c->ograph) {
+        OverlapGraph* og = static_cast<OverlapGraph*>(c->ograph);
+        overlap_graph_release(og);
+        release(og->nn.status);
+        release(og->nn.table);
+        release(og->nn.os_status);
+        release(og->ost);
+        delete og;
     }
+    for (DevBuf* b : context_buffers(c)) release(*b);
+    delete static_cast<TuneCache*>(c->tune_cache);
+    delete reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : c->ev_round)
@@ -2506,10 +2839,16 @@ int xtn_context_overlap_device(xtn_context* c, const xtn_args* args, const char*
         return XTN_ERR_ARG;
     }
     XTN_CK(cudaSetDevice(c->device));
-    begin_run(c);
-    int r = run_overlap(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, d_info, n, args->distance, args->measure,
-                        args->info_len, true);
-    end_run(c);
+    int r;
+    if (c->graph_mode) {
+        r = overlap_graph(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, d_info, n, args->distance,
+                          args->measure, args->info_len);
+    } else {
+        begin_run(c);
+        r = run_overlap(c, reinterpret_cast<const uint8_t*>(d_seqs), d_offsets, d_info, n, args->distance,
+                        args->measure, args->info_len, true);
+        end_run(c);
+    }
     if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
     return r;
 }
@@ -2587,6 +2926,9 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "graph") && (v == 0 || v == 1)) c->graph_mode = (int)v;
     else if (!strcmp(name, "verify_per") && (v == 1 || v == 4 || v == 8)) c->verify_per = (int)v;
     else if (!strcmp(name, "autotune") && (v == 0 || v == 1)) c->autotune_auto = (int)v;
+    else if (!strcmp(name, "group_persistent") && (v == 0 || v == 1)) c->group_persistent = (int)v;
+    else if (!strcmp(name, "shard_count") && v >= 1 && v <= kMaxShards) c->shard_count = (int)v;
+    else if (!strcmp(name, "shard_index") && v >= 0 && v < kMaxShards) c->shard_index = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
         set_err(std::string("unknown option or value out of range: ") + name);
@@ -2646,6 +2988,145 @@ int xtn_context_result_device(xtn_context* c, const xtn_int2** d_pairs, const in
     if (!c) return XTN_ERR_ARG;
     if (d_pairs) *d_pairs = P<xtn_int2>(c->out_pairs);
     if (d_dist) *d_dist = P<int8_t>(c->out_dist);
+    if (n_out) *n_out = c->n_out;
+    return XTN_SUCCESS;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ shard exchange
+// A sharded search (options shard_count / shard_index) leaves on each rank the verified pairs
+// of its first-level buckets, sorted by (x, y); a pair whose sequences share variants in the
+// buckets of several shards is found by each of them. The exchange gives every rank the pairs
+// whose x lies in its id range, [ceil(k n / K), ceil((k + 1) n / K)) for rank k of K, as one
+// 64-bit key per pair, x << (b + 8) | y << 8 | distance with b = id bits of n: the sorted
+// output splits into contiguous runs per owner, and the owner's merge (sort, unique) restores
+// the reference's sorted, duplicate-free order over its range, so that the ranks' outputs in
+// rank order are the whole search's output.
+namespace xtn {
+
+__global__ void k_result_keys(const xtn_int2* __restrict__ pairs, const int8_t* __restrict__ dist, int64_t m, int b,
+                              uint64_t* __restrict__ keys) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const xtn_int2 p = pairs[i];
+    keys[i] = ((uint64_t)(uint32_t)p.x << (b + 8)) | ((uint64_t)(uint32_t)p.y << 8) | (uint64_t)(uint8_t)dist[i];
+}
+
+// starts[k] = first index of the sorted pairs whose x >= ceil(k n / K) (starts[K] = m).
+__global__ void k_range_starts(const xtn_int2* __restrict__ pairs, int64_t m, int64_t n, int K,
+                               int64_t* __restrict__ starts) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > K) return;
+    if (k == K) {
+        starts[k] = m;
+        return;
+    }
+    const int64_t x0 = ((int64_t)k * n + K - 1) / K;
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)pairs[mid].x < x0) lo = mid + 1;
+        else hi = mid;
+    }
+    starts[k] = lo;
+}
+
+__global__ void k_key_heads(const uint64_t* __restrict__ keys, int64_t m, uint8_t* __restrict__ head) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_key_compact(const uint64_t* __restrict__ keys, int64_t m, int b, const uint8_t* __restrict__ head,
+                              const uint32_t* __restrict__ pos, xtn_int2* __restrict__ out, int8_t* __restrict__ dist) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !head[i]) return;
+    const uint64_t k = keys[i];
+    const uint32_t o = pos[i];
+    const uint64_t idmask = (1ull << b) - 1ull;
+    out[o] = xtn_int2{(int32_t)(k >> (b + 8)), (int32_t)((k >> 8) & idmask)};
+    dist[o] = (int8_t)(uint8_t)(k & 0xffu);
+}
+
+static int key_bits_for(xtn_context* c, int32_t n_seqs, int* b) {
+    *b = id_bits_for(n_seqs);
+    if (2 * *b + 8 > 64) {
+        set_err("too many sequences for 64-bit pair keys");
+        return XTN_ERR_LIMIT;
+    }
+    return XTN_SUCCESS;
+}
+
+}  // namespace xtn
+
+extern "C" {
+
+int xtn_context_result_keys(xtn_context* c, int32_t n_seqs, uint64_t* d_keys, int64_t capacity, int32_t n_ranges,
+                            int64_t* range_starts) {
+    if (!c || n_seqs < 1 || n_ranges < 1 || n_ranges > kMaxShards || !range_starts || (c->n_out > 0 && !d_keys)) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    if (c->overlap_result) {
+        set_err("the last result is an overlap matrix, not pairs");
+        return XTN_ERR_ARG;
+    }
+    if (capacity < c->n_out) {
+        set_err("the key buffer holds fewer entries than the result");
+        return XTN_ERR_ARG;
+    }
+    int b = 0;
+    XTN_TRY(key_bits_for(c, n_seqs, &b));
+    XTN_CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const int64_t m = c->n_out;
+    if (m > 0)
+        XTN_LAUNCH("result_keys", k_result_keys<<<blocks_for(m), kThreads, 0, s>>>(
+                                      P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist), m, b, d_keys));
+    XTN_TRY(ensure(c->scratch64, sizeof(int64_t) * (n_ranges + 1)));
+    XTN_LAUNCH("range_starts", k_range_starts<<<blocks_for(n_ranges + 1), kThreads, 0, s>>>(
+                                   P<xtn_int2>(c->out_pairs), m, n_seqs, n_ranges, P<int64_t>(c->scratch64)));
+    XTN_CK(cudaGetLastError());
+    XTN_CK(cudaMemcpyAsync(range_starts, c->scratch64.p, sizeof(int64_t) * (n_ranges + 1), cudaMemcpyDeviceToHost, s));
+    XTN_CK(cudaStreamSynchronize(s));
+    return XTN_SUCCESS;
+}
+
+int xtn_context_merge_keys(xtn_context* c, int32_t n_seqs, const uint64_t* d_keys, int64_t count, int64_t* n_out) {
+    if (!c || n_seqs < 1 || count < 0 || (count > 0 && !d_keys) || count >= (int64_t)UINT32_MAX) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    int b = 0;
+    XTN_TRY(key_bits_for(c, n_seqs, &b));
+    XTN_CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    memset(&c->stats, 0, sizeof c->stats);
+    c->overlap_result = false;
+    c->n_out = 0;
+    if (count > 0) {
+        XTN_TRY(ensure(c->pairA, sizeof(uint64_t) * count + 64));
+        XTN_TRY(ensure(c->pairB, sizeof(uint64_t) * count + 64));
+        XTN_CK(cudaMemcpyAsync(c->pairB.p, d_keys, sizeof(uint64_t) * count, cudaMemcpyDeviceToDevice, s));
+        uint64_t* keys = P<uint64_t>(c->pairB);
+        if (count > 1)
+            XTN_TRY(sort_u64(c, c->pairB, c->pairA, count, 0, 2 * b + 8, &keys, XTN_SORT_NAMES("shard_key_sort")));
+        XTN_TRY(ensure(c->flag, (size_t)count));
+        XTN_TRY(ensure(c->fpos, sizeof(uint32_t) * (count + 1)));
+        XTN_LAUNCH("key_heads", k_key_heads<<<blocks_for(count), kThreads, 0, s>>>(keys, count, P<uint8_t>(c->flag)));
+        XTN_TRY((scan_1p<uint8_t, uint32_t>(c, P<uint8_t>(c->flag), P<uint32_t>(c->fpos), count)));
+        XTN_TRY(ensure(c->out_pairs, sizeof(xtn_int2) * count));
+        XTN_TRY(ensure(c->out_dist, (size_t)count));
+        XTN_LAUNCH("key_compact", k_key_compact<<<blocks_for(count), kThreads, 0, s>>>(
+                                      keys, count, b, P<uint8_t>(c->flag), P<uint32_t>(c->fpos),
+                                      P<xtn_int2>(c->out_pairs), P<int8_t>(c->out_dist)));
+        XTN_CK(cudaGetLastError());
+        uint64_t u = 0;
+        XTN_TRY(read_scalar(c, P<uint32_t>(c->fpos) + count, 4, &u));
+        c->n_out = (int64_t)u;
+    }
+    c->stats.n_out = c->n_out;
+    c->stats.n_seqs = n_seqs;
     if (n_out) *n_out = c->n_out;
     return XTN_SUCCESS;
 }

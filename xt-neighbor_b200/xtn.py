@@ -43,6 +43,8 @@ SYMBOLS = (
     "xtn_index_serve",
     "xtn_context_fetch",
     "xtn_context_result_device",
+    "xtn_context_result_keys",
+    "xtn_context_merge_keys",
     "xtn_context_stream",
     "xtn_context_stats",
     "xtn_context_set_option",
@@ -189,6 +191,9 @@ def load():
     lib.xtn_index_serve.argtypes = [P, ctypes.POINTER(Request), ctypes.c_int32, ctypes.POINTER(ServeOptions),
                                     ctypes.POINTER(RequestResult), REQUEST_CALLBACK, P]
     lib.xtn_context_result_device.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_context_result_keys.argtypes = [P, ctypes.c_int32, P, ctypes.c_int64, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_context_merge_keys.argtypes = [P, ctypes.c_int32, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_stream.argtypes = [P]
     lib.xtn_context_stream.restype = P
     lib.xtn_context_stats.argtypes = [P, ctypes.POINTER(Stats)]
@@ -362,6 +367,20 @@ class Context:
     def stream(self) -> int:
         return self.lib.xtn_context_stream(self.h) or 0
 
+    def result_keys(self, n: int, d_keys: int, capacity: int, n_ranges: int) -> list:
+        """Writes the last result as 64-bit pair keys to d_keys (xtn_context_result_keys) and
+        returns the n_ranges + 1 range starts by owner rank."""
+        starts = (ctypes.c_int64 * (n_ranges + 1))()
+        _check(self.lib.xtn_context_result_keys(self.h, n, ctypes.c_void_p(d_keys), capacity, n_ranges, starts))
+        return list(starts)
+
+    def merge_keys(self, n: int, d_keys: int, count: int) -> int:
+        """Sorts and de-duplicates received pair keys into the context's result
+        (xtn_context_merge_keys); returns its length."""
+        nout = ctypes.c_int64()
+        _check(self.lib.xtn_context_merge_keys(self.h, n, ctypes.c_void_p(d_keys), count, ctypes.byref(nout)))
+        return nout.value
+
     def set_profiling(self, on: bool, only: str = None):
         """Brackets kernel launches with CUDA events; `only` restricts that to one kernel name."""
         _check(self.lib.xtn_context_set_profiling(self.h, 1 if on else 0))
@@ -430,6 +449,46 @@ def synth_clusters(seed: int, n: int, cluster_frac: float = 0.20, dup_frac: floa
     """n generator sequences with mutant clusters and exact duplicates, shuffled."""
     chars, offs, _, _ = _take(_load_synth().synth_nn(seed, n, 1, cluster_frac, dup_frac))
     return chars, offs
+
+
+def exchange_keys(keys, starts, group=None):
+    """All-to-all of pair keys by owner rank (torch.distributed, NCCL for CUDA tensors, gloo on
+    CPU): keys[starts[k]:starts[k+1]] go to rank k; returns what this rank receives (the
+    sources' runs in rank order). Sizes are exchanged first, so every rank takes the same two
+    collective steps."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    send = [int(starts[k + 1] - starts[k]) for k in range(world)]
+    sizes = torch.tensor(send, dtype=torch.int64, device=keys.device)
+    got = torch.empty(world, dtype=torch.int64, device=keys.device)
+    dist.all_to_all_single(got, sizes, group=group)
+    recv = [int(v) for v in got.tolist()]
+    out = torch.empty(sum(recv), dtype=torch.int64, device=keys.device)
+    dist.all_to_all_single(out, keys[: starts[world]].contiguous(), recv, send, group=group)
+    return out
+
+
+def nn_sharded(ctx, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN, group=None) -> int:
+    """One rank's part of a nearest-neighbour search sharded over the ranks of `group` (one GPU
+    each, the same input on every rank): the search over this rank's share of the first-level
+    hash buckets (context options shard_count / shard_index), the exchange of the verified pairs
+    by owner (pairs whose x lies in this rank's id range come here), and the merge. Returns the
+    number of pairs left as the context's result: this rank's id range of the whole output, in
+    order, so that the ranks' results in rank order are the unsharded search's output."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    ctx.set_option("shard_count", world)
+    ctx.set_option("shard_index", rank)
+    m = ctx.nn_device(d_chars, d_offsets, n, distance, measure)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    keys = torch.empty(max(m, 1), dtype=torch.int64, device=dev)
+    starts = ctx.result_keys(n, keys.data_ptr(), keys.numel(), world)
+    got = exchange_keys(keys, starts, group)
+    return ctx.merge_keys(n, got.data_ptr(), got.numel())
 
 
 def synth_repertoires(seed: int, n_reps: int, min_size: float, max_size: float, shared: float = 0.05):
