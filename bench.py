@@ -821,6 +821,135 @@ def run_reference(args, w):
     }
 
 
+def run_sharded(args, w):
+    """The nearest-neighbour search sharded by first-level hash buckets (options shard_count /
+    shard_index, xtn.nn_sharded): under torchrun every rank (one GPU each) searches its share of
+    the buckets of the same input, the verified pairs are exchanged by owner over NCCL and
+    merged; one step is the whole search over all ranks (strong scaling), timed on the device
+    from the search's start to the merge's end, slowest rank. On one process, --shards K runs
+    the K shards one after another on the one GPU and exchanges on the device with the same
+    splits (per-shard and merge times reported): what each rank of a K-GPU run would compute,
+    without the collective."""
+    import datetime
+
+    import numpy as np
+    import torch
+
+    import xtn
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    K = world if world > 1 else args.shards
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    chars, offs, info, _ = gen_workload(w)
+    if info is not None:
+        raise SystemExit("sharding covers the nearest-neighbour workloads only")
+    n = len(offs) - 1
+    opts = {k: int(v) for k, v in (o.split("=", 1) for o in args.opt)}
+    ctx = xtn.Context(local, **opts)
+    d_chars = torch.from_numpy(chars).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int32)).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ext = torch.cuda.ExternalStream(ctx.stream())
+    torch.cuda.synchronize()
+    unsharded = ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+
+    def one_rank():
+        return xtn.nn_sharded(ctx, d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+
+    def emulated():
+        shard_ms, sent = [], []
+        ctx.set_option("shard_count", K)
+        for k in range(K):
+            ctx.set_option("shard_index", k)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            m = ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+            keys = torch.empty(max(m, 1), dtype=torch.int64, device="cuda")
+            starts = ctx.result_keys(n, keys.data_ptr(), keys.numel(), K)
+            e1.record(ext)
+            e1.synchronize()
+            shard_ms.append(e0.elapsed_time(e1))
+            sent.append((keys, starts))
+        merge_ms, total = [], 0
+        for dst in range(K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            got = torch.cat([keys[st[dst]: st[dst + 1]] for keys, st in sent])
+            total += ctx.merge_keys(n, got.data_ptr(), got.numel())
+            e1.record(ext)
+            e1.synchronize()
+            merge_ms.append(e0.elapsed_time(e1))
+        return total, shard_ms, merge_ms
+
+    times, out, detail = [], 0, None
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        if world > 1:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            out = one_rank()
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+        else:
+            out, shard_ms, merge_ms = emulated()
+            ms = sum(shard_ms) + sum(merge_ms)
+            if i >= args.warmup:
+                detail = (detail or [np.zeros(K), np.zeros(K)])
+                detail[0] += np.array(shard_ms) / args.steps
+                detail[1] += np.array(merge_ms) / args.steps
+        if i >= args.warmup:
+            times.append(ms)
+    ms_step = reduce_max([sum(times) / len(times)], pg, "cuda")[0]
+    if pg:
+        import torch.distributed as dist
+
+        t = torch.tensor([out], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        out = int(t.item())
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC,
+        "value": n / (ms_step / 1e3),
+        "unit": "seqs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded CDR3 generator)",
+        "config": {"workload": args.workload, "n_seqs": n, "distance": w["d"],
+                   "measure": "hamming" if w["measure"] else "leven", "mode": "nn",
+                   "parallelism": f"shards x{K}" + ("" if world > 1 else " run in sequence on one GPU"),
+                   "l2": "flushed between steps (256 MiB write)"},
+        "output_entries": out,
+        "output_matches_unsharded": out == unsharded,
+    }
+    if detail is not None:
+        line["shards_one_gpu"] = {
+            "shard_ms": [round(float(x), 3) for x in detail[0]],
+            "merge_ms": [round(float(x), 3) for x in detail[1]],
+            "what": "each shard's search + key packing, then each owner's merge of the keys it receives, "
+                    "one after another on one GPU (the collective between them is not run)"}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -839,6 +968,9 @@ def main():
                     help="pick the bucket-engine shape by timing on the workload first (xtn_context_autotune)")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
                     help="context option (xtn_context_set_option), repeatable")
+    ap.add_argument("--shards", type=int, default=0,
+                    help="sharded search: under torchrun one shard per rank (any value > 0); on one process, "
+                         "this many shards run in sequence on the one GPU")
     args = ap.parse_args()
     if args.workload in SERVE_WORKLOADS:
         if args.impl == "reference":
@@ -847,7 +979,12 @@ def main():
             line = run_serve(args, SERVE_WORKLOADS[args.workload])
     else:
         w = WORKLOADS[args.workload]
-        line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
+        if args.impl == "reference":
+            line = run_reference(args, w)
+        elif args.shards > 0:
+            line = run_sharded(args, w)
+        else:
+            line = run_ours(args, w)
     if line is not None:
         print(json.dumps(line), flush=True)
 

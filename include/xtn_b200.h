@@ -193,6 +193,14 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
  *                     CTAs take slices of the bucket and merge their histograms through
  *                     distributed shared memory)
+ *   "flat_gen"        1 = a search that keeps every record at once (one round, not sharded,
+ *                     d <= 2, key tables, stage_chunk 4096) builds the first level in two
+ *                     passes (default): every variant record generated in sequence order,
+ *                     stored straight from the generating threads, with the per-tile bucket
+ *                     histograms (in place of the count pass), then moved into its first-level
+ *                     bucket by a streaming staged partition of 8192-record chunks; 0 = the
+ *                     one-pass scatter that generates and partitions each chunk of 4096 (always
+ *                     used in rounds and shards)
  *   "group_persistent" 1 = when there are many buckets to group (more than 8 per SM), the
  *                     grouping kernel runs as persistent CTAs that take bucket descriptors from
  *                     a queue on the device (default), 0 = one CTA per bucket
@@ -267,8 +275,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
 int xtn_context_set_option(xtn_context* ctx, const char* name, int64_t value);
 
 /* Autotuner: times the search on these device-resident inputs (the caller's data, so its length
- * distribution and duplicate structure) for each shape - first-level and split stage chunks and
- * first-level bucket bits, then, on the best of those, bulk-copy or plain loads in the grouping
+ * distribution and duplicate structure) for each shape - the first-level form (two passes or
+ * the one-pass scatter), first-level and split stage chunks and first-level bucket bits, then,
+ * on the best of those, bulk-copy or plain loads in the grouping
  * kernel, the verification variants (verify_per 4 and 8) and the graph form - taking the best of
  * `repeats` runs after a warm-up, and leaves the fastest shape set on the context. The choice is
  * also remembered for the input's class (log2 of the sequence count, distance, measure, median

@@ -31,6 +31,9 @@ ENGINES = {
     # the 8192-record first-level stage shape and the verification variant that lists four
     # candidates per lane
     "bucket_small_group": {"group_cap": 2048, "stage_chunk": 8192, "verify_per": 4},
+    # the one-pass first-level scatter (generation and partition per chunk) in place of the
+    # default two passes (every record generated in sequence order, then partitioned)
+    "bucket_one_pass": {"flat_gen": 0},
 }
 
 

@@ -175,6 +175,14 @@ __global__ void k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles
     totals[b] = run;
 }
 
+// Counter words shared by the plan, split and grouping kernels (unsigned int counters[16]).
+constexpr int kCntDesc = 0;      // descriptors listed for grouping
+constexpr int kCntJobs = 1;      // split jobs
+constexpr int kCntSub = 2;       // sub-buckets the split jobs produce
+constexpr int kCntFallback = 3;  // buckets grouped by sorting instead
+constexpr int kCntWaitFail = 5;  // split and partition CTAs whose chunk copy did not complete in time
+constexpr int kCntDropped = 6;   // appends refused because a list was full (must stay 0)
+
 // ------------------------------------------------------------------ staged partition
 template <class C>
 struct StageSmem {
@@ -199,9 +207,24 @@ constexpr int stage_ctas_per_sm() {
 // Staged partition of a split chunk: the chunk's records are r[0..m), the bucket of r[p] is
 // r[p] >> shift; each bucket's records are appended at gcur[bucket] as contiguous runs written by
 // consecutive threads. after_rank() runs once every thread is done reading r.
+// `strip` > 0 (first level from records in sequence order): a record x = hash field | id
+// carries its bucket in its top `strip` bits. They are dropped on the way out and the field
+// shifted up by `strip`, as the one-pass scatter's records are; the `strip` bits that opens
+// above the id take a multiplicative hash of the whole field, so that the low field bits, which
+// the grouping's bitmap filter indexes, vary within a bucket (equal fields still give equal
+// records; the field keeps 64 - idbits - strip bits of the hash, against 64 - idbits for the
+// one-pass scatter, so a bucket sees a few more hash collisions, which verification removes).
+__device__ __forceinline__ uint64_t strip_bucket(uint64_t x, int strip, int idbits) {
+    const uint64_t idmask = (1ull << idbits) - 1ull;
+    const uint64_t f = x & ~idmask;
+    const uint64_t mix = (f * 0x9E3779B97F4A7C15ull) >> (64 - strip);
+    return (f << strip) | (mix << idbits) | (x & idmask);
+}
+
 template <class C, class Hook>
 __device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r, int shift,
-                                                uint64_t* __restrict__ dst, Hook&& after_rank) {
+                                                uint64_t* __restrict__ dst, Hook&& after_rank, int strip = 0,
+                                                int idbits = 0) {
     constexpr int kStageThreads = C::kThreads, kFanPer = C::kFanPer;
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
     __syncthreads();
@@ -235,7 +258,8 @@ __device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_
     after_rank();
     for (uint32_t q = threadIdx.x; q < m; q += kStageThreads) {
         const uint16_t b = S.sbkt[q];
-        dst[S.gcur[b] + (q - S.lstart[b])] = S.sorted[q];
+        const uint64_t x = S.sorted[q];
+        dst[S.gcur[b] + (q - S.lstart[b])] = strip ? strip_bucket(x, strip, idbits) : x;
     }
     __syncthreads();
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
@@ -306,6 +330,67 @@ constexpr int ctas_per_sm_for() {
     return (int)((228u * 1024u) / (sizeof(SM) + 1024u));
 }
 
+// Chunks of a tile of sequences [t0, t1) for the staged first-level kernels: chunk k holds the
+// sequences whose first variant lies in [k * span, (k + 1) * span) from voff[r0], with
+// span = CHUNK - 172 (a key has at most 172 variants at d <= 2), so that no chunk overflows and
+// none is empty. Fills cstart[0..nch] (at most kScatterChunksPerRound chunks per call, from r0);
+// returns nch. The caller synchronises before reading cstart.
+template <int T, int CHUNK>
+__device__ __forceinline__ int chunk_starts(const uint64_t* __restrict__ voff, int r0, int t1, uint32_t* cstart) {
+    constexpr uint64_t kSpan = (uint64_t)(CHUNK - kMaxVariantsD2);
+    const uint64_t base = voff[r0];
+    const uint64_t last = (voff[t1 - 1] - base) / kSpan;
+    const int nch = last + 1 < (uint64_t)kScatterChunksPerRound ? (int)(last + 1) : kScatterChunksPerRound;
+    for (int s = r0 + threadIdx.x; s < t1; s += T) {
+        const uint64_t k = (voff[s] - base) / kSpan;
+        if (k > (uint64_t)nch) break;
+        if (s == r0 || (voff[s - 1] - base) / kSpan != k) cstart[k] = (uint32_t)s;
+    }
+    if (threadIdx.x == 0 && (uint64_t)nch == last + 1) cstart[nch] = (uint32_t)t1;
+    return nch;
+}
+
+// The variant hashes of the chunk of sequences [s0, s1) (d <= 2, from the key tables): the
+// chunk's generation tasks are spread over the CTA's T threads and put(pos, hash, seq) is
+// called once per variant, pos = its slot in the chunk (voff[seq] - voff[s0] + the variant's
+// index). At d = 2 the tasks are k_task_counts' balanced halves of run pairs and task_seq maps a
+// task to its sequence; at d = 1 (task_seq null) a task is a whole sequence: its table row is
+// loaded into registers at once and the key and single deletions are emitted by an unrolled
+// loop.
+template <int T, class Put>
+__device__ __forceinline__ void chunk_hashes(const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo,
+                                             const uint64_t* __restrict__ tab, const uint64_t* __restrict__ voff,
+                                             const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq,
+                                             int s0, int s1, int d, Put&& put) {
+    const uint64_t vbase = voff[s0];
+    const uint64_t tb = task_seq ? toff[s0] : (uint64_t)s0;
+    const uint32_t nt = (uint32_t)((task_seq ? toff[s1] : (uint64_t)s1) - tb);
+    for (uint32_t tau = threadIdx.x; tau < nt; tau += T) {
+        const uint64_t g = tb + tau;
+        const int i = task_seq ? (int)task_seq[g] : (int)g;
+        const int t = task_seq ? (int)(g - toff[i]) : 0;
+        const uint32_t vb = (uint32_t)(voff[i] - vbase);
+        auto emit = [&](int v, uint64_t h) { put(vb + (uint32_t)v, h, i); };
+        const uint64_t* row = tab + (size_t)i * kTabLen;
+        if (d >= 2) {
+            for_each_task_hash(row, klen[i], runinfo[i], d, t, emit);
+        } else {
+            // the key, then the single deletion of each run: r G[p] + r^-1 P_L
+            uint64_t G[kKeyLen];
+#pragma unroll
+            for (int q = 0; q < kKeyLen; q++) G[q] = row[kTabG + q];
+            const uint64_t PL = row[kTabKey];
+            const uint32_t rs = (uint32_t)runinfo[i];
+            emit(0, hash_fin(PL));
+            const uint64_t single = kPolyRI * PL;
+            int v = 1;
+#pragma unroll
+            for (int q = 0; q < kKeyLen; q++)
+                if ((rs >> q) & 1u) emit(v++, hash_fin(kPolyR * G[q] + single));
+        }
+    }
+}
+
 // First-level scatter for d <= 2. The CTA's tile of sequences is cut into chunks of at most
 // C::kChunk variants by a rule every thread can apply alone: chunk k holds the sequences whose
 // first variant lies in [k * span, (k + 1) * span) from the tile's first variant, with
@@ -333,7 +418,6 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     const unsigned int* __restrict__ abort) {
     constexpr int T = C::kThreads, kFanPer = C::kFanPer;
     if (abort && *abort) return;  // graph form: the records would not fit their buffer
-    constexpr uint64_t kSpan = (uint64_t)(C::kChunk - kMaxVariantsD2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem<C>& S = *reinterpret_cast<ScatterSmem<C>*>(smem_raw);
     const int nb = 1 << b1;
@@ -348,56 +432,20 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
     for (int r0 = t0; r0 < t1;) {
         // chunk starts of this round (at most kScatterChunksPerRound chunks)
-        const uint64_t base = voff[r0];
-        const uint64_t last = (voff[t1 - 1] - base) / kSpan;
-        const int nch = last + 1 < (uint64_t)kScatterChunksPerRound ? (int)(last + 1) : kScatterChunksPerRound;
-        for (int s = r0 + threadIdx.x; s < t1; s += T) {
-            const uint64_t k = (voff[s] - base) / kSpan;
-            if (k > (uint64_t)nch) break;
-            if (s == r0 || (voff[s - 1] - base) / kSpan != k) S.cstart[k] = (uint32_t)s;
-        }
-        if (threadIdx.x == 0 && (uint64_t)nch == last + 1) S.cstart[nch] = (uint32_t)t1;
+        const int nch = chunk_starts<T, C::kChunk>(voff, r0, t1, S.cstart);
         __syncthreads();
         for (int c = 0; c < nch; c++) {
             const int s0 = (int)S.cstart[c], s1 = (int)S.cstart[c + 1];
-            const uint64_t vbase = voff[s0];
-            const uint64_t tb = task_seq ? toff[s0] : (uint64_t)s0;
-            const uint32_t m = (uint32_t)(voff[s1] - vbase);
-            const uint32_t nt = (uint32_t)((task_seq ? toff[s1] : (uint64_t)s1) - tb);
-            for (uint32_t tau = threadIdx.x; tau < nt; tau += T) {
-                const uint64_t g = tb + tau;
-                const int i = task_seq ? (int)task_seq[g] : (int)g;
-                const int t = task_seq ? (int)(g - toff[i]) : 0;
-                const uint32_t vb = (uint32_t)(voff[i] - vbase);
-                const uint64_t id = (uint64_t)i;
-                auto put = [&](int v, uint64_t h) {
-                    const uint32_t b = (uint32_t)(h >> shift);
-                    const uint32_t pos = vb + (uint32_t)v;
-                    if (b - b_lo >= b_n) {  // another round's bucket
-                        S.br[pos] = 0xffffffffu;
-                        return;
-                    }
-                    S.br[pos] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
-                    S.rec[pos] = ((h << b1) & hi_mask) | id;
-                };
-                const uint64_t* row = tab + (size_t)i * kTabLen;
-                if (d >= 2) {
-                    for_each_task_hash(row, klen[i], runinfo[i], d, t, put);
-                } else {
-                    // the key, then the single deletion of each run: r G[p] + r^-1 P_L
-                    uint64_t G[kKeyLen];
-#pragma unroll
-                    for (int q = 0; q < kKeyLen; q++) G[q] = row[kTabG + q];
-                    const uint64_t PL = row[kTabKey];
-                    const uint32_t rs = (uint32_t)runinfo[i];
-                    put(0, hash_fin(PL));
-                    const uint64_t single = kPolyRI * PL;
-                    int v = 1;
-#pragma unroll
-                    for (int q = 0; q < kKeyLen; q++)
-                        if ((rs >> q) & 1u) put(v++, hash_fin(kPolyR * G[q] + single));
+            const uint32_t m = (uint32_t)(voff[s1] - voff[s0]);
+            chunk_hashes<T>(klen, runinfo, tab, voff, toff, task_seq, s0, s1, d, [&](uint32_t pos, uint64_t h, int i) {
+                const uint32_t b = (uint32_t)(h >> shift);
+                if (b - b_lo >= b_n) {  // another round's bucket
+                    S.br[pos] = 0xffffffffu;
+                    return;
                 }
-            }
+                S.br[pos] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
+                S.rec[pos] = ((h << b1) & hi_mask) | (uint64_t)i;
+            });
             __syncthreads();
             {
                 uint32_t tot, loc[kFanPer], sum = 0;
@@ -436,6 +484,116 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
     }
 }
 
+// ------------------------------------------------------------------ generate, then partition
+// The first level in two passes (searches that keep every record at once, d <= 2 with key
+// tables): k_bucket_gen writes every variant record in sequence order, (hash & ~idmask) | id,
+// and the per-tile histogram of the top b1 hash bits (the count pass's output, so that pass is
+// not run); k_bucket_partition then moves each tile's records, read back by bulk copies, through
+// the staged partition into their first-level buckets. Generation has no chunks, ranking or
+// barriers, and the partition is a streaming pass with known offsets; the one-pass scatter
+// interleaves both inside each chunk of 4096 records.
+//
+// k_bucket_gen: the tile's generation tasks are spread over the CTA at once and every variant
+// is stored straight to its slot; a lane's consecutive variants fill whole sectors, which L2
+// merges before they reach DRAM (two CTAs of 512 threads per SM at 64 registers; a bound of
+// three CTAs measured slower: 6.46 against 5.55 ms at 10M). abort (graph form, may be null): the
+// records would not fit.
+template <int THREADS, int MIN_CTAS>
+__global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
+    const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
+    const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
+    int tile, int d, int b1, int idbits, uint64_t* __restrict__ flat, uint32_t* __restrict__ counts,
+    const unsigned int* __restrict__ abort) {
+    extern __shared__ uint32_t s_hist[];
+    if (abort && *abort) return;
+    const int nb = 1 << b1;
+    for (int b = threadIdx.x; b < nb; b += THREADS) s_hist[b] = 0;
+    __syncthreads();
+    const int t0 = min(n, blockIdx.x * tile);
+    const int t1 = min(n, t0 + tile);
+    const int shift = 64 - b1;
+    const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
+    if (t0 < t1) {
+        uint64_t* out = flat + voff[t0];
+        chunk_hashes<THREADS>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d, [&](uint32_t pos, uint64_t h, int i) {
+            atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
+            out[pos] = (h & hi_mask) | (uint64_t)i;
+        });
+    }
+    __syncthreads();
+    uint32_t* dst = counts + (size_t)blockIdx.x * nb;
+    for (int b = threadIdx.x; b < nb; b += THREADS) dst[b] = s_hist[b];
+}
+
+// k_bucket_partition: tile t's records, flat[voff[t * tile] .. voff[min(n, (t + 1) * tile)]),
+// through the staged partition into their first-level buckets in `recs`: bucket b's records of
+// tile t start at bstart[b] + offsets[t][b]; the top b1 bits are dropped on the way
+// (strip_bucket). Chunk c reaches shared memory by one bulk copy, issued as soon as chunk c - 1
+// is ranked; counters[kCntWaitFail] counts CTAs whose bounded wait for a copy ran out. The
+// 8192-record stage shape (one CTA of 1024 threads per SM) leaves runs of about eight records
+// per bucket and chunk at 1024 first-level buckets.
+template <class C>
+__global__ void __launch_bounds__(C::kThreads) k_bucket_partition(
+    const uint64_t* __restrict__ flat, const uint64_t* __restrict__ voff, int n, int tile, int b1, int idbits,
+    const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs,
+    unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
+    constexpr int T = C::kThreads;
+    if (abort && *abort) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
+    const int nb = 1 << b1;
+    const int t0 = min(n, blockIdx.x * tile);  // (tiles past the last sequence are empty)
+    const int t1 = min(n, t0 + tile);
+    const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
+    for (int b = threadIdx.x; b < nb; b += T) S.gcur[b] = (uint32_t)bstart[b] + off[b];
+    const uint64_t r0 = voff[t0];
+    const uint32_t size = (uint32_t)(voff[t1] - r0);
+    const uint64_t* src = flat + r0;
+    const uint32_t mbar = smem_u32(&S.mbar);
+    auto issue = [&](uint32_t c0) {
+        const uint32_t m = min((uint32_t)C::kChunk, size - c0);
+        const uint64_t* a = src + c0;
+        const uint32_t lead = (uint32_t)(((uintptr_t)a & 15u) >> 3);
+        bulk_load(smem_u32(&S.rec[0]), a - lead, ((lead + m) * 8u + 15u) & ~15u, mbar);
+    };
+    if (threadIdx.x == 0) {
+        S.wait_failed = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (size > 0) issue(0);
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    for (uint32_t c0 = 0; c0 < size; c0 += C::kChunk, parity ^= 1u) {
+        const uint32_t m = min((uint32_t)C::kChunk, size - c0);
+        const uint32_t lead = (uint32_t)(((uintptr_t)(src + c0) & 15u) >> 3);
+        if (threadIdx.x == 0) {
+            uint32_t polls = 0;
+            while (!mbar_try_wait(mbar, parity)) {
+                if (++polls > kWaitLimit) {
+                    S.wait_failed = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __syncthreads();
+        if (S.wait_failed) {
+            // one more bounded wait for the copy to land before the shared memory is released
+            if (threadIdx.x == 0) {
+                uint32_t polls = 0;
+                while (!mbar_try_wait(mbar, parity) && ++polls < kWaitLimit) __nanosleep(64);
+                atomicAdd(&counters[kCntWaitFail], 1u);
+            }
+            __syncthreads();
+            return;
+        }
+        split_partition(S, nb, m, S.rec + lead, 64 - b1, recs, [&] {
+            if (threadIdx.x == 0 && c0 + C::kChunk < size) issue(c0 + C::kChunk);
+        }, b1, idbits);
+    }
+}
+
 // First-level scatter for any d: one thread per sequence, smem cursors, direct stores. Rounds
 // as in k_bucket_scatter_staged: buckets [b_lo, b_lo + b_n) only, positions minus `round_base`.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* __restrict__ keys,
@@ -467,13 +625,6 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const u128* _
     }
 }
 
-// Counter words shared by the plan, split and grouping kernels (unsigned int counters[16]).
-constexpr int kCntDesc = 0;      // descriptors listed for grouping
-constexpr int kCntJobs = 1;      // split jobs
-constexpr int kCntSub = 2;       // sub-buckets the split jobs produce
-constexpr int kCntFallback = 3;  // buckets grouped by sorting instead
-constexpr int kCntWaitFail = 5;  // split CTAs whose chunk copy did not complete in time
-constexpr int kCntDropped = 6;   // appends refused because a list was full (must stay 0)
 
 // Appends v to list[0..cap) at counters[which]; an append past the capacity is counted in
 // counters[kCntDropped] instead (the host then reports an error: the capacities are bounds

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstdlib>
 #include <cmath>
@@ -522,6 +523,7 @@ struct xtn_context {
     int verify_per = 1;     // verification variant: candidates listed per lane (1, 4, 8)
     int group_persistent = 1;  // grouping by persistent CTAs on a descriptor queue (large grids)
     int shard_count = 1, shard_index = 0;  // this search covers shard shard_index of shard_count
+    int flat_gen = 1;       // one-round first level: generate in sequence order, then partition
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
@@ -781,6 +783,7 @@ static int candidates_sorted(xtn_context* c, int n, int d, int idbits, uint64_t 
 struct BucketPlan {
     int b1 = 1, nb = 2, ntiles = 1, tile = 1;
     bool small = false, staged = false;
+    bool flat = false;  // generate in sequence order (recB), then partition (k_bucket_gen / k_bucket_partition)
     const uint32_t* tseq = nullptr;
 };
 
@@ -808,6 +811,8 @@ static int bucket_attrs(xtn_context* c) {
                                 (int)sizeof(GroupSmem<GroupLarge>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_group<GroupSmall>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(GroupSmem<GroupSmall>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_partition<StageHuge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(StageSmem<StageHuge>)));
     c->attrs_set = true;
     return XTN_SUCCESS;
 }
@@ -893,20 +898,19 @@ static int bucket_reserve(xtn_context* c, const BucketPlan& bp, int n, int d, ui
     return XTN_SUCCESS;
 }
 
-static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
+// one_round: the search keeps every record at once (no rounds, no shards), which the
+// generate-then-partition first level (option flat_gen) needs: it holds all V records twice.
+// abort (graph form, may be null): the generation does nothing when it is set.
+static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp, bool one_round = false,
+                          const unsigned int* abort = nullptr) {
     cudaStream_t s = c->stream;
     bucket_shape(c, n, d, V, bp);
     const int b1 = bp->b1, nb = bp->nb, ntiles = bp->ntiles, tile = bp->tile;
     const bool tables = d <= 2 && c->key_tables;
     const size_t hist_smem = sizeof(uint32_t) * nb;
+    bp->flat = one_round && c->flat_gen && tables && bp->staged && !bp->small && c->stage_chunk == 4096;
     XTN_TRY(bucket_reserve(c, *bp, n, d, V));
     XTN_TRY(bucket_attrs(c));
-    XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
-                                   P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
-                                   tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1, P<uint32_t>(c->bcounts)));
-    XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
-                                     P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
-    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
     if (bp->staged && d >= 2) {
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
                                                                                    P<uint32_t>(c->tcnt)));
@@ -915,8 +919,33 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
                                                                              P<uint32_t>(c->tseq)));
         bp->tseq = P<uint32_t>(c->tseq);
     }
+    if (bp->flat) {
+        // every record in sequence order into recB, with the per-tile histograms
+        XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
+        XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
+        XTN_LAUNCH("bucket_gen", (k_bucket_gen<kBucketThreads, 2><<<ntiles, kBucketThreads, hist_smem, s>>>(
+                                     P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
+                                     P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp->tseq, n, tile, d, b1,
+                                     id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), abort)));
+    } else {
+        XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
+                                       P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
+                                       tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1, P<uint32_t>(c->bcounts)));
+    }
+    XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
+                                     P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
+    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
     XTN_CK(cudaGetLastError());
     return XTN_SUCCESS;
+}
+
+// The first-level partition of the records k_bucket_gen wrote in sequence order (recB -> recA).
+static void launch_partition(xtn_context* c, const BucketPlan& bp, int n, int idbits, const unsigned int* abort,
+                             cudaStream_t s) {
+    XTN_LAUNCH("bucket_partition",
+               k_bucket_partition<StageHuge><<<bp.ntiles, StageHuge::kThreads, sizeof(StageSmem<StageHuge>), s>>>(
+                   P<uint64_t>(c->recB), P<uint64_t>(c->voff), n, bp.tile, bp.b1, idbits, P<uint32_t>(c->boffs),
+                   P<uint64_t>(c->bstart), P<uint64_t>(c->recA), P<unsigned int>(c->bcnt), abort));
 }
 
 // The staged first-level scatter in the context's stage shape (stage_chunk 2048, 4096 or 8192).
@@ -946,7 +975,11 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * Vr + 64));
     XTN_TRY(ensure(c->recB, sizeof(uint64_t) * Vr + 64));
     const uint64_t* bstart = P<uint64_t>(c->bstart);
-    if (bp.staged) {
+    XTN_TRY(ensure(c->bcnt, 64));
+    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
+    if (bp.flat) {
+        launch_partition(c, bp, n, idbits, nullptr, s);
+    } else if (bp.staged) {
         launch_scatter_staged(c, bp, n, d, idbits, b_lo, b_n, base, nullptr, s);
     } else {
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
@@ -962,8 +995,6 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * b_n));
-    XTN_TRY(ensure(c->bcnt, 64));
-    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(b_n), kThreads, 0, s>>>(
                                   bstart + b_lo, (int)b_n, base, c->group_cap, P<BucketDesc>(c->bdesc),
                                   (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), nullptr));
@@ -992,7 +1023,8 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
         XTN_CK(cudaStreamSynchronize(s));
         memcpy(cnt, c->h_scalar, 32);
         if (cnt[kCntWaitFail] != 0) {
-            set_err("bucket split: " + std::to_string(cnt[kCntWaitFail]) + " chunk copies did not complete in time");
+            set_err("bucket partition or split: " + std::to_string(cnt[kCntWaitFail]) +
+                    " chunk copies did not complete in time");
             return XTN_ERR_CUDA;
         }
         if (cnt[kCntDropped] != 0) {
@@ -1374,9 +1406,10 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         XTN_TRY(candidates_sorted(c, n, d, idbits, V, &Pc));
     } else {
         BucketPlan bp;
-        XTN_TRY(bucket_prepare(c, n, d, V, &bp));
         const uint64_t limit = round_record_limit(c, n, d, V);
-        if (V <= limit && c->shard_count <= 1) {
+        const bool one_round = V <= limit && c->shard_count <= 1;
+        XTN_TRY(bucket_prepare(c, n, d, V, &bp, one_round));
+        if (one_round) {
             XTN_TRY(candidates_bucketed(c, bp, n, d, idbits, V, &Pc));
         } else {
             std::vector<Round> rounds;
@@ -1483,13 +1516,15 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
 // that outgrows a capacity, meets a bucket too large for shared memory or a hash set too full,
 // is redone by the plain form, which also re-sizes the graph. The plain form
 // (run_nn) waits for the device four times per search to size its buffers and grids.
+using GraphSig = std::array<int64_t, 11>;
+
 struct GraphState {
     const uint8_t* chars = nullptr;
     const uint32_t* offs = nullptr;
     const int32_t* rows = nullptr;            // sequence i is row rows[i] (overlap: one row per unique string)
     const unsigned int* pre_abort = nullptr;  // an abort word set by stages captured before the search
     int n = 0, d = 0, measure = 0;
-    int64_t sig = 0;                 // options the capture depends on
+    GraphSig sig{};                  // options the capture depends on
     uint64_t Vcap = 0, Pcap = 0, Ucap = 0, T = 0;
     int b1 = 0;
     cudaGraph_t graph = nullptr;
@@ -1535,11 +1570,11 @@ __global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned in
     st[GS_NDESC] = bcnt[kCntDesc];
 }
 
-static int64_t graph_signature(const xtn_context* c) {
-    return ((int64_t)c->stage_chunk << 40) ^ ((int64_t)c->split_chunk << 28) ^ ((int64_t)c->bucket_bits_max << 20) ^
-           ((int64_t)c->group_cap << 4) ^ ((int64_t)c->group_tma << 1) ^ ((int64_t)c->key_tables << 2) ^
-           ((int64_t)c->split_slices << 16) ^ ((int64_t)c->scatter_ctas_per_sm << 48) ^ ((int64_t)c->pair_dedup << 52) ^
-           ((int64_t)c->verify_per << 56);
+// The options a capture depends on.
+static GraphSig graph_signature(const xtn_context* c) {
+    return GraphSig{c->stage_chunk,  c->split_chunk,  c->bucket_bits_max,     (int64_t)c->group_cap,
+                    c->group_tma,    c->key_tables,   c->split_slices,        c->scatter_ctas_per_sm,
+                    c->pair_dedup,   c->verify_per,   c->flat_gen};
 }
 
 static void graph_release(GraphState* g) {
@@ -1567,14 +1602,17 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     XTN_LAUNCH("graph_guard", k_graph_guard<<<1, 1, 0, s>>>(P<uint64_t>(c->voff) + n, g->Vcap,
                                                             P<unsigned int>(c->lencheck), g->pre_abort, abort));
     BucketPlan bp;
-    XTN_TRY(bucket_prepare(c, n, d, g->Vcap, &bp));
+    XTN_TRY(bucket_prepare(c, n, d, g->Vcap, &bp, true, abort));
     if (bp.b1 != g->b1) {
         set_err("graph capture: first-level bucket bits changed");
         return XTN_ERR_CUDA;
     }
     const int nb = bp.nb;
     const uint64_t* bstart = P<uint64_t>(c->bstart);
-    if (bp.staged) {
+    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
+    if (bp.flat) {
+        launch_partition(c, bp, n, idbits, abort, s);
+    } else if (bp.staged) {
         launch_scatter_staged(c, bp, n, d, idbits, 0u, (uint32_t)nb, 0ull, abort, s);
     } else {
         XTN_LAUNCH("bucket_scatter", k_bucket_scatter<<<bp.ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
@@ -1583,7 +1621,6 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
                                          abort));
     }
     const size_t desc_cap = (size_t)nb * 3 + 4 * g->Vcap / c->group_cap + 2048;
-    XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
                                   bstart, nb, 0ull, c->group_cap, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
@@ -2371,7 +2408,7 @@ struct OverlapGraph {
     const uint32_t* offs = nullptr;
     const xtn_seq_info* info = nullptr;
     int n = 0, d = 0, measure = 0, R = 0;
-    int64_t sig = 0;
+    GraphSig sig{};
     uint32_t U = 0;
     GraphState nn;  // capacities and device tables of the search over the unique strings
     cudaGraph_t graph = nullptr;
@@ -2539,7 +2576,7 @@ namespace xtn {
 // longer than the 18-residue key (whose pairs take the long verification path). The reference's
 // sizes are fixed (xtneighbor_streaming/src/xtn.cu:21-26).
 struct TuneShape {
-    int stage, split, bits, tma, verify, graph;
+    int stage, split, bits, tma, verify, graph, flat;
 };
 struct TuneKey {
     int log2n, d, measure, len_med, long_share;  // long_share in percent
@@ -2597,6 +2634,7 @@ static void tune_apply(xtn_context* c, const TuneShape& sh) {
     c->group_tma = sh.tma;
     c->verify_per = sh.verify;
     c->graph_mode = sh.graph;
+    c->flat_gen = sh.flat;
 }
 
 static int nn_graph(xtn_context* c, const uint8_t* chars, const uint32_t* offs, int n, int d, int measure);
@@ -2616,7 +2654,8 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
     const int d = args->distance, measure = args->measure;
     TuneKey key{};
     XTN_TRY(tune_key(c, offs, n, d, measure, &key));
-    const TuneShape saved{c->stage_chunk, c->split_chunk, c->bucket_bits_max, c->group_tma, c->verify_per, c->graph_mode};
+    const TuneShape saved{c->stage_chunk, c->split_chunk, c->bucket_bits_max, c->group_tma,
+                          c->verify_per,  c->graph_mode,  c->flat_gen};
     const int saved_engine = c->engine;
     c->engine = 0;
     auto time_shape = [&](const TuneShape& sh, float* ms) -> int {
@@ -2630,7 +2669,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
         *ms = best;
         return XTN_SUCCESS;
     };
-    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, 1, 0};
+    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, 1, 0, 1};
     float best_ms = 1e30f;
     int tried = 0;
     auto consider = [&](const TuneShape& sh) -> int {
@@ -2645,14 +2684,17 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
         return XTN_SUCCESS;
     };
     int st = XTN_SUCCESS;
-    // stage shapes and first-level bits
-    for (int stage : {4096, 2048})
-        for (int split : {4096, 2048})
-            for (int bits : {9, 10}) {
-                if (st != XTN_SUCCESS) break;
-                if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
-                st = consider(TuneShape{stage, split, bits, 1, 1, 0});
-            }
+    // first level (generate-then-partition, or the one-pass scatter in two stage shapes), split
+    // stage shape and first-level bits
+    for (int flat : {1, 0})
+        for (int stage : {4096, 2048})
+            for (int split : {4096, 2048})
+                for (int bits : {9, 10}) {
+                    if (st != XTN_SUCCESS) break;
+                    if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
+                    if (flat && stage != 4096) continue;         // the two-pass first level has one shape
+                    st = consider(TuneShape{stage, split, bits, 1, 1, 0, flat});
+                }
     // then, one at a time on the best so far: plain loads in grouping, the verification
     // variants, the graph form
     if (st == XTN_SUCCESS) {
@@ -2688,9 +2730,9 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
     if (!stored) tc->entries.push_back({key, best});
     if (report && report_cap > 0)
         snprintf(report, (size_t)report_cap,
-                 "stage_chunk=%d split_chunk=%d bucket_bits_max=%d group_tma=%d verify_per=%d graph=%d: %.3f ms "
-                 "(best of %d shapes; input class log2n=%d d=%d measure=%d median_len=%d longer_than_key=%d%%)",
-                 best.stage, best.split, best.bits, best.tma, best.verify, best.graph, best_ms, tried, key.log2n,
+                 "flat_gen=%d stage_chunk=%d split_chunk=%d bucket_bits_max=%d group_tma=%d verify_per=%d graph=%d: "
+                 "%.3f ms (best of %d shapes; input class log2n=%d d=%d measure=%d median_len=%d longer_than_key=%d%%)",
+                 best.flat, best.stage, best.split, best.bits, best.tma, best.verify, best.graph, best_ms, tried, key.log2n,
                  key.d, key.measure, key.len_med, key.long_share);
     return XTN_SUCCESS;
 }
@@ -2928,6 +2970,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "autotune") && (v == 0 || v == 1)) c->autotune_auto = (int)v;
     else if (!strcmp(name, "group_persistent") && (v == 0 || v == 1)) c->group_persistent = (int)v;
     else if (!strcmp(name, "shard_count") && v >= 1 && v <= kMaxShards) c->shard_count = (int)v;
+    else if (!strcmp(name, "flat_gen") && (v == 0 || v == 1)) c->flat_gen = (int)v;
     else if (!strcmp(name, "shard_index") && v >= 0 && v < kMaxShards) c->shard_index = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
