@@ -183,6 +183,12 @@ def algorithmic_bytes(kernel: str, st: dict, n: int, n_chars: int) -> float | No
         # each 8-byte record written once; per sequence its 19-word key table (152 B), run info,
         # variant and task offsets (8 B each) and key length (1 B) read once
         return 8.0 * V + 177.0 * n
+    if kernel == "bucket_gen":
+        # two-pass first level, generation: each 8-byte record written once; per sequence the
+        # same 177 bytes read as the one-pass scatter
+        return 8.0 * V + 177.0 * n
+    if kernel == "bucket_partition":
+        return 16.0 * V  # each record read once and written once
     if kernel == "bucket_group":
         return 8.0 * V + 8.0 * Pc  # each record read once; candidate pairs written
     if kernel == "bucket_split":
@@ -504,7 +510,7 @@ def run_ours(args, w):
         "pairs_per_s": None if overlap else world * n_out / (ms_step / 1e3),
         "verified_pairs": stats["n_verified_pairs"] if overlap else n_out,
         "output_entries": n_out,
-        "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_out")},
+        "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_unique", "n_out")},
         "e2e": {
             "value": replica_throughput(n, world, e2e_ms),
             "unit": "seqs/s",

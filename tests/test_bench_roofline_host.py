@@ -17,6 +17,8 @@ def test_algorithmic_bytes():
     V, P, U = ST["n_variants"], ST["n_candidates"], ST["n_unique"]
     assert bench.algorithmic_bytes("bucket_scatter", ST, n, nch) == 8.0 * V + 177.0 * n
     assert bench.algorithmic_bytes("bucket_split", ST, n, nch) == 16.0 * V
+    assert bench.algorithmic_bytes("bucket_gen", ST, n, nch) == 8.0 * V + 177.0 * n
+    assert bench.algorithmic_bytes("bucket_partition", ST, n, nch) == 16.0 * V
     assert bench.algorithmic_bytes("bucket_group", ST, n, nch) == 8.0 * V + 8.0 * P
     assert bench.algorithmic_bytes("pair_dedup", ST, n, nch) == 8.0 * P + 16.0 * U
     # 40-bit pair keys: five 8-bit passes over the distinct pairs

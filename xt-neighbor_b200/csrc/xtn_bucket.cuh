@@ -81,6 +81,8 @@ struct GroupCfg {
 // 9.90 ms, as more candidates share a digit.)
 using GroupLarge = GroupCfg<4096, 512, 16, 11, 3>;
 using GroupSmall = GroupCfg<2048, 256, 15, 10, 6>;
+// (Half the bitmap and digits at the large cap, 2^15 bits and 1024 digits, measured slower:
+// 9.32 against 8.99 ms at 10M, 0.80 against 0.70 ms at 1M.)
 constexpr int kGroupThreads = GroupLarge::kThreads;
 constexpr int kGroupCap = GroupLarge::kCap;        // largest bucket grouped in shared memory
 constexpr int kGroupSmallCap = GroupSmall::kCap;   // group_cap at or below this: the small shape
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
     int tile, int d, int b1, int idbits, uint64_t* __restrict__ flat, uint32_t* __restrict__ counts,
-    const unsigned int* __restrict__ abort) {
+    const unsigned int* __restrict__ abort, int per_seq) {
     extern __shared__ uint32_t s_hist[];
     if (abort && *abort) return;
     const int nb = 1 << b1;
@@ -513,12 +515,21 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
-    if (t0 < t1) {
+    if (t0 < t1 && !per_seq) {
         uint64_t* out = flat + voff[t0];
         chunk_hashes<THREADS>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d, [&](uint32_t pos, uint64_t h, int i) {
             atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
             out[pos] = (h & hi_mask) | (uint64_t)i;
         });
+    } else if (per_seq) {
+        // one thread per sequence, its variants in seq_items order
+        for (int i = t0 + threadIdx.x; i < t1; i += THREADS) {
+            uint64_t* out = flat + voff[i];
+            for_each_seq_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d, [&](int v, uint64_t h) {
+                atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
+                out[v] = (h & hi_mask) | (uint64_t)i;
+            });
+        }
     }
     __syncthreads();
     uint32_t* dst = counts + (size_t)blockIdx.x * nb;
@@ -840,6 +851,10 @@ struct GroupSmem {
     unsigned long long base;
     unsigned long long mbar;
 };
+// (the bitmaps and digit counts are cleared with 16-byte stores)
+static_assert(offsetof(GroupSmem<GroupLarge>, u) % 16 == 0 && offsetof(GroupSmem<GroupLarge>, cnt) % 16 == 0 &&
+                  offsetof(GroupSmem<GroupSmall>, u) % 16 == 0 && offsetof(GroupSmem<GroupSmall>, cnt) % 16 == 0,
+              "grouping shared-memory layout");
 
 __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits) {
     return a < b ? ((a << idbits) | b) : ((b << idbits) | a);
@@ -916,11 +931,13 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
         uint4* dd = reinterpret_cast<uint4*>(&S.rec[0]);
         for (uint32_t i = threadIdx.x; i < bytes / 16; i += G::kThreads) dd[i] = __ldg(g + i);
     }
-    for (int i = threadIdx.x; i < G::kBitmapWords; i += G::kThreads) {
-        S.u.bm.seen[i] = 0;
-        S.u.bm.twice[i] = 0;
+    {
+        // both bitmaps and the digit counts cleared with 16-byte stores
+        uint4* bm = reinterpret_cast<uint4*>(S.u.bm.seen);
+        for (int i = threadIdx.x; i < G::kBitmapWords / 2; i += G::kThreads) bm[i] = make_uint4(0, 0, 0, 0);
+        uint4* cn = reinterpret_cast<uint4*>(S.cnt);
+        for (int i = threadIdx.x; i < G::kDigits / 4; i += G::kThreads) cn[i] = make_uint4(0, 0, 0, 0);
     }
-    for (int i = threadIdx.x; i < G::kDigits; i += G::kThreads) S.cnt[i] = 0;
     if (use_tma && threadIdx.x == 0) {
         // one thread polls the barrier (sleeping between polls); the others wait at __syncthreads
         uint32_t polls = 0;
@@ -946,21 +963,32 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
     const uint64_t* rec = S.rec + lead;
     const uint64_t idmask = (1ull << idbits) - 1ull;
 
-    // 1. bitmap filter
-    for (uint32_t i = threadIdx.x; i < n; i += G::kThreads) {
-        const uint32_t b = (uint32_t)(rec[i] >> idbits) & (G::kBitmapBits - 1);
-        const uint32_t bit = 1u << (b & 31);
-        if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
+    // 1. bitmap filter; each thread keeps its records' bitmap positions for the second pass
+    constexpr int kPerThread = G::kCap / G::kThreads;
+    uint32_t pos[kPerThread];
+#pragma unroll
+    for (int k = 0; k < kPerThread; k++) {
+        const uint32_t i = threadIdx.x + (uint32_t)k * G::kThreads;
+        pos[k] = 0;
+        if (i < n) {
+            const uint32_t b = (uint32_t)(rec[i] >> idbits) & (G::kBitmapBits - 1);
+            const uint32_t bit = 1u << (b & 31);
+            if (atomicOr(&S.u.bm.seen[b >> 5], bit) & bit) atomicOr(&S.u.bm.twice[b >> 5], bit);
+            pos[k] = b;
+        }
     }
     if (threadIdx.x == 0) S.n_cand = 0;  // (read as the descriptor index before the first barrier)
     __syncthreads();
     // candidates in any order (one shared atomic per warp and round)
     const unsigned lane = threadIdx.x & 31u;
-    for (uint32_t i0 = threadIdx.x & ~31u; i0 < n; i0 += G::kThreads) {
+#pragma unroll
+    for (int k = 0; k < kPerThread; k++) {
+        const uint32_t i0 = (threadIdx.x & ~31u) + (uint32_t)k * G::kThreads;
+        if (i0 >= n) break;
         const uint32_t i = i0 + lane;
         bool hit = false;
         if (i < n) {
-            const uint32_t b = (uint32_t)(rec[i] >> idbits) & (G::kBitmapBits - 1);
+            const uint32_t b = pos[k];
             hit = (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
         }
         const unsigned mask = __ballot_sync(0xffffffffu, hit);
