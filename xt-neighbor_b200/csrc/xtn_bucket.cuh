@@ -498,14 +498,14 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
 // k_bucket_gen: the tile's generation tasks are spread over the CTA at once and every variant
 // is stored straight to its slot; a lane's consecutive variants fill whole sectors, which L2
 // merges before they reach DRAM (two CTAs of 512 threads per SM at 64 registers; a bound of
-// three CTAs measured slower: 6.46 against 5.55 ms at 10M). abort (graph form, may be null): the
-// records would not fit.
+// three CTAs measured slower: 6.46 against 5.55 ms at 10M, and one thread per sequence instead
+// of the balanced tasks 12.7 ms). abort (graph form, may be null): the records would not fit.
 template <int THREADS, int MIN_CTAS>
 __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
     int tile, int d, int b1, int idbits, uint64_t* __restrict__ flat, uint32_t* __restrict__ counts,
-    const unsigned int* __restrict__ abort, int per_seq) {
+    const unsigned int* __restrict__ abort) {
     extern __shared__ uint32_t s_hist[];
     if (abort && *abort) return;
     const int nb = 1 << b1;
@@ -515,21 +515,12 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
-    if (t0 < t1 && !per_seq) {
+    if (t0 < t1) {
         uint64_t* out = flat + voff[t0];
         chunk_hashes<THREADS>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d, [&](uint32_t pos, uint64_t h, int i) {
             atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
             out[pos] = (h & hi_mask) | (uint64_t)i;
         });
-    } else if (per_seq) {
-        // one thread per sequence, its variants in seq_items order
-        for (int i = t0 + threadIdx.x; i < t1; i += THREADS) {
-            uint64_t* out = flat + voff[i];
-            for_each_seq_hash(tab + (size_t)i * kTabLen, klen[i], runinfo[i], d, [&](int v, uint64_t h) {
-                atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
-                out[v] = (h & hi_mask) | (uint64_t)i;
-            });
-        }
     }
     __syncthreads();
     uint32_t* dst = counts + (size_t)blockIdx.x * nb;

@@ -926,8 +926,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
         XTN_LAUNCH("bucket_gen", (k_bucket_gen<kBucketThreads, 2><<<ntiles, kBucketThreads, hist_smem, s>>>(
                                      P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
                                      P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp->tseq, n, tile, d, b1,
-                                     id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), abort,
-                                     c->flat_gen == 2 ? 1 : 0)));
+                                     id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), abort)));
     } else {
         XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                        P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
@@ -2971,7 +2970,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "autotune") && (v == 0 || v == 1)) c->autotune_auto = (int)v;
     else if (!strcmp(name, "group_persistent") && (v == 0 || v == 1)) c->group_persistent = (int)v;
     else if (!strcmp(name, "shard_count") && v >= 1 && v <= kMaxShards) c->shard_count = (int)v;
-    else if (!strcmp(name, "flat_gen") && v >= 0 && v <= 2) c->flat_gen = (int)v;
+    else if (!strcmp(name, "flat_gen") && (v == 0 || v == 1)) c->flat_gen = (int)v;
     else if (!strcmp(name, "shard_index") && v >= 0 && v < kMaxShards) c->shard_index = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
