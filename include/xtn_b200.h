@@ -396,8 +396,7 @@ int xtn_index_serve(xtn_index* index, const xtn_request* requests, int32_t n_req
  *     oversized result, *n_out holds the needed size.
  *   - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) on the current
  *     device, and returns after the stream has drained.
- *   - The first call on a device resolves the array's device address, so make that call before
- *     any stream capture.
+ *   - The first call on a device also resolves the array's device address.
  *   - Every call reuses the same array (the call resets what must start at zero), so calls that
  *     overlap on the GPU, from any thread or stream, race. */
 int xtn_nn_search_static(const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets, int32_t n_seqs,

@@ -304,10 +304,22 @@ __global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint3
 
 // Task -> sequence map of the staged scatter: the k_task_counts tasks of sequence i occupy
 // task_seq[toff[i] .. toff[i+1]).
-__global__ void k_task_seq(const uint64_t* __restrict__ toff, int n, uint32_t* __restrict__ task_seq) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (uint64_t g = toff[i], e = toff[i + 1]; g < e; g++) task_seq[g] = (uint32_t)i;
+// The CTA's sequences write their task ids into shared memory (at most kKeyLen tasks each), then
+// the CTA stores its contiguous task range with consecutive threads on consecutive words.
+constexpr int kTaskSeqThreads = 256;
+
+__global__ void __launch_bounds__(kTaskSeqThreads) k_task_seq(const uint64_t* __restrict__ toff, int n,
+                                                              uint32_t* __restrict__ task_seq) {
+    __shared__ uint32_t s_ids[kTaskSeqThreads * kKeyLen];
+    const int i0 = blockIdx.x * kTaskSeqThreads;
+    const int i = i0 + threadIdx.x;
+    const int i1 = min(n, i0 + kTaskSeqThreads);
+    const uint64_t base = toff[i0];
+    if (i < n)
+        for (uint64_t g = toff[i], e = toff[i + 1]; g < e; g++) s_ids[g - base] = (uint32_t)i;
+    __syncthreads();
+    const uint32_t cnt = (uint32_t)(toff[i1] - base);
+    for (uint32_t k = threadIdx.x; k < cnt; k += kTaskSeqThreads) task_seq[base + k] = s_ids[k];
 }
 
 constexpr int kMaxVariantsD2 = 1 + kKeyLen + kKeyLen * (kKeyLen - 1) / 2;  // 172: all runs of length 1
