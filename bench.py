@@ -510,7 +510,7 @@ def run_ours(args, w):
         "pairs_per_s": None if overlap else world * n_out / (ms_step / 1e3),
         "verified_pairs": stats["n_verified_pairs"] if overlap else n_out,
         "output_entries": n_out,
-        "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_candidates", "n_unique", "n_out")},
+        "counts": {k: stats[k] for k in ("n_variants", "n_groups", "n_fallback", "n_candidates", "n_unique", "n_out")},
         "e2e": {
             "value": replica_throughput(n, world, e2e_ms),
             "unit": "seqs/s",

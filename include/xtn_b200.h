@@ -190,6 +190,10 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     scatter (default 4096: two CTAs of 512 threads per SM; 2048: four of 256;
  *                     8192: one of 1024, longer runs per bucket)
  *   "split_chunk"     2048 | 4096: the same for the split of large buckets (default 4096)
+ *   "split_fill"      25..95 (default 87): a first-level bucket larger than group_cap is split
+ *                     into ceil(size / (group_cap * split_fill / 100)) sub-buckets (at most
+ *                     1024) by ranges of the records' top hash bits, so the sub-buckets hold about
+ *                     that share of the grouping capacity
  *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
  *                     CTAs take slices of the bucket and merge their histograms through
  *                     distributed shared memory)

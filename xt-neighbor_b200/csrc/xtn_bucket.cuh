@@ -42,7 +42,10 @@ constexpr int kPrivFan = 64;           // split fan-outs up to this use per-warp
 // boundary sectors complete in L2.
 constexpr int kMaxFirstLevelBits = 10;  // default bound on the first-level bits (the large stage shape's fan-out)
 constexpr int kMaxSplitBits = 10;
-constexpr int kSplitSlices = 8;        // CTAs (one thread-block cluster) per split bucket
+constexpr int kMaxSplitFan = 1 << kMaxSplitBits;  // sub-buckets of one split job, at most
+// CTAs (one thread-block cluster) per split bucket (16, the non-portable cluster size, measured
+// slower at 10M: 8.24 against 7.40 ms)
+constexpr int kSplitSlices = 8;
 
 // Shape of a staged partition: threads per CTA, records per chunk, largest fan-out.
 template <int THREADS, int CHUNK, int FAN>
@@ -97,12 +100,18 @@ struct BucketDesc {
     uint32_t src;     // 0: records in buffer A, 1: in buffer B
 };
 
-// Split job: bucket `start,size` (buffer A) is divided into 2^bits sub-buckets (buffer B).
+// Split job: bucket `start,size` (buffer A) is divided into `nsub` sub-buckets (buffer B) by
+// ranges of the records' top hash bits (split_sub).
 struct SplitJob {
     uint64_t start;
     uint32_t size;
-    uint32_t bits;
+    uint32_t nsub;
 };
+
+// Sub-bucket of record x among nsub: the top 32 hash bits scaled to [0, nsub), so that any
+// count of near-equal sub-buckets can be made (not only powers of two); equal records land in
+// the same one.
+__device__ __forceinline__ uint32_t split_sub(uint64_t x, uint32_t nsub) { return __umulhi((uint32_t)(x >> 32), nsub); }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -223,14 +232,14 @@ __device__ __forceinline__ uint64_t strip_bucket(uint64_t x, int strip, int idbi
     return (f << strip) | (mix << idbits) | (x & idmask);
 }
 
-template <class C, class Hook>
-__device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r, int shift,
+template <class C, class Bkt, class Hook>
+__device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r, Bkt&& bkt,
                                                 uint64_t* __restrict__ dst, Hook&& after_rank, int strip = 0,
                                                 int idbits = 0) {
     constexpr int kStageThreads = C::kThreads, kFanPer = C::kFanPer;
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.cnt[b] = 0;
     __syncthreads();
-    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[(uint32_t)(r[p] >> shift)], 1u);
+    for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) atomicAdd(&S.cnt[bkt(r[p])], 1u);
     __syncthreads();
     {
         uint32_t tot, loc[kFanPer], sum = 0;
@@ -251,7 +260,7 @@ __device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < m; p += kStageThreads) {
         const uint64_t x = r[p];
-        const uint32_t b = (uint32_t)(x >> shift);
+        const uint32_t b = bkt(x);
         const uint32_t q = atomicAdd(&S.cnt[b], 1u);
         S.sorted[q] = x;
         S.sbkt[q] = (uint16_t)b;
@@ -602,7 +611,8 @@ __global__ void __launch_bounds__(C::kThreads) k_bucket_partition(
             __syncthreads();
             return;
         }
-        split_partition(S, nb, m, S.rec + lead, 64 - b1, recs, [&] {
+        const int shift = 64 - b1;
+        split_partition(S, nb, m, S.rec + lead, [shift](uint64_t x) { return (uint32_t)(x >> shift); }, recs, [&] {
             if (threadIdx.x == 0 && c0 + C::kChunk < size) issue(c0 + C::kChunk);
         }, b1, idbits);
     }
@@ -657,8 +667,9 @@ __device__ __forceinline__ void bounded_append(T* __restrict__ list, uint32_t ca
 // abort (graph form, may be null): when set, nothing is listed, so the split and grouping that
 // follow have no work.
 __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint64_t base, uint32_t group_cap,
-                              BucketDesc* __restrict__ desc, uint32_t desc_cap, SplitJob* __restrict__ jobs,
-                              unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
+                              uint32_t split_fill, BucketDesc* __restrict__ desc, uint32_t desc_cap,
+                              SplitJob* __restrict__ jobs, unsigned int* __restrict__ counters,
+                              const unsigned int* __restrict__ abort) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb || (abort && *abort)) return;
     uint64_t s = bstart[b] - base, e = bstart[b + 1] - base;
@@ -667,12 +678,13 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint6
     if (size <= group_cap) {
         bounded_append(desc, desc_cap, counters, kCntDesc, BucketDesc{s, size, 0});
     } else {
-        // sub-buckets aim at 7/8 of the shared-memory capacity (hash buckets are near-uniform)
-        const uint32_t target = group_cap * 7 / 8;
-        uint32_t bits = 1;
-        while (bits < kMaxSplitBits && ((uint64_t)size >> bits) > (uint64_t)(target > 1 ? target : 1)) bits++;
-        bounded_append(jobs, (uint32_t)nb, counters, kCntJobs, SplitJob{s, size, bits});
-        atomicAdd(&counters[kCntSub], 1u << bits);
+        // sub-buckets of about split_fill % of the shared-memory capacity (hash buckets are
+        // near-uniform, so the largest stays below the capacity)
+        const uint64_t target = max(1u, (uint32_t)((uint64_t)group_cap * split_fill / 100));
+        const uint64_t want = (size + target - 1) / target;
+        const uint32_t nsub = want < 2 ? 2u : want > (uint64_t)kMaxSplitFan ? (uint32_t)kMaxSplitFan : (uint32_t)want;
+        bounded_append(jobs, (uint32_t)nb, counters, kCntJobs, SplitJob{s, size, nsub});
+        atomicAdd(&counters[kCntSub], nsub);
     }
 }
 
@@ -702,9 +714,8 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
     const int rank = (int)cluster.block_rank();
     if (blockIdx.x / kSlices >= min(counters[kCntJobs], (unsigned)(gridDim.x / kSlices))) return;  // no such job
     const SplitJob job = jobs[blockIdx.x / kSlices];
-    const int nsub = 1 << job.bits;
-    const int shift = 64 - (int)job.bits;
-    const bool priv = nsub <= kPrivFan;
+    const uint32_t nsub = job.nsub;
+    const bool priv = nsub <= (uint32_t)kPrivFan;
     const uint32_t s_lo = (uint32_t)((uint64_t)job.size * rank / kSlices);
     const uint32_t s_hi = (uint32_t)((uint64_t)job.size * (rank + 1) / kSlices);
     const uint32_t size = s_hi - s_lo;
@@ -729,13 +740,13 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
     // 1. slice histogram into S.lstart (per-warp copies in `sorted`, unused until the first
     //    chunk, for small fan-outs)
     uint32_t* hist = priv ? reinterpret_cast<uint32_t*>(S.sorted) + (threadIdx.x >> 5) * kPrivFan : S.lstart;
-    for (int i = threadIdx.x; i < (priv ? kPrivFan * (kStageThreads / 32) : nsub); i += kStageThreads)
+    for (int i = threadIdx.x; i < (priv ? kPrivFan * (kStageThreads / 32) : (int)nsub); i += kStageThreads)
         (priv ? reinterpret_cast<uint32_t*>(S.sorted) : S.lstart)[i] = 0;
     __syncthreads();
     {
         // 16-byte loads, four in flight per thread (the slice is 8-byte aligned: peel one)
         const uint32_t lead = size > 0 ? (uint32_t)(((uintptr_t)src & 15u) >> 3) : 0u;
-        if (lead && threadIdx.x == 0) atomicAdd(&hist[src[0] >> shift], 1u);
+        if (lead && threadIdx.x == 0) atomicAdd(&hist[split_sub(src[0], nsub)], 1u);
         const uint32_t nv = (size - lead) >> 1;
         const uint4* v = reinterpret_cast<const uint4*>(src + lead);
         uint32_t i = threadIdx.x;
@@ -744,20 +755,20 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
                                 __ldg(v + i + 3 * kStageThreads)};
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                atomicAdd(&hist[(((uint64_t)w[k].y << 32) | w[k].x) >> shift], 1u);
-                atomicAdd(&hist[(((uint64_t)w[k].w << 32) | w[k].z) >> shift], 1u);
+                atomicAdd(&hist[__umulhi(w[k].y, nsub)], 1u);  // (the top 32 bits of each record)
+                atomicAdd(&hist[__umulhi(w[k].w, nsub)], 1u);
             }
         }
         for (; i < nv; i += kStageThreads) {
             const uint4 a = __ldg(v + i);
-            atomicAdd(&hist[(((uint64_t)a.y << 32) | a.x) >> shift], 1u);
-            atomicAdd(&hist[(((uint64_t)a.w << 32) | a.z) >> shift], 1u);
+            atomicAdd(&hist[__umulhi(a.y, nsub)], 1u);
+            atomicAdd(&hist[__umulhi(a.w, nsub)], 1u);
         }
-        if (threadIdx.x == 0 && ((size - lead) & 1u)) atomicAdd(&hist[src[size - 1] >> shift], 1u);
+        if (threadIdx.x == 0 && ((size - lead) & 1u)) atomicAdd(&hist[split_sub(src[size - 1], nsub)], 1u);
     }
     __syncthreads();
     if (priv) {
-        for (int b = threadIdx.x; b < nsub; b += kStageThreads) {
+        for (int b = threadIdx.x; b < (int)nsub; b += kStageThreads) {
             uint32_t t = 0;
             for (int w = 0; w < kStageThreads / 32; w++) t += reinterpret_cast<uint32_t*>(S.sorted)[w * kPrivFan + b];
             S.lstart[b] = t;
@@ -771,7 +782,7 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
 #pragma unroll
         for (int k = 0; k < kFanPer; k++) {
             tot_b[k] = mine_b[k] = 0;
-            if (b0 + k < nsub)
+            if (b0 + k < (int)nsub)
                 for (int r = 0; r < kSlices; r++) {
                     const uint32_t c = cluster.map_shared_rank(S.lstart, r)[b0 + k];
                     tot_b[k] += c;
@@ -785,7 +796,7 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
 #pragma unroll
         for (int k = 0; k < kFanPer; k++) {
             const int b = b0 + k;
-            if (b >= nsub) continue;
+            if (b >= (int)nsub) continue;
             const uint32_t st = ex + loc[k];
             S.gcur[b] = (uint32_t)job.start + st + mine_b[k];
             if (rank == 0 && tot_b[k] >= 2) {
@@ -822,7 +833,7 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
             __syncthreads();
             return;
         }
-        split_partition(S, nsub, m, S.rec + lead, shift, out, [&] {
+        split_partition(S, (int)nsub, m, S.rec + lead, [nsub](uint64_t x) { return split_sub(x, nsub); }, out, [&] {
             if (threadIdx.x == 0 && c0 + kStageChunk < size) issue(c0 + kStageChunk);
         });
     }

@@ -524,6 +524,7 @@ struct xtn_context {
     int group_persistent = 1;  // grouping by persistent CTAs on a descriptor queue (large grids)
     int shard_count = 1, shard_index = 0;  // this search covers shard shard_index of shard_count
     int flat_gen = 1;       // one-round first level: generate in sequence order, then partition
+    int split_fill = 87;    // split sub-buckets sized at this percentage of group_cap
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
@@ -939,6 +940,27 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
     return XTN_SUCCESS;
 }
 
+// The split of the plan's jobs (recA -> recB): one CTA per bucket, or a cluster of
+// split_slices CTAs per bucket, launched for every one of the b_n buckets without waiting for
+// the plan: those past the plan's job count exit at once.
+static void launch_split(xtn_context* c, uint32_t b_n, size_t desc_cap, cudaStream_t s) {
+    const int sl = c->split_slices;
+    const unsigned grid = b_n * (unsigned)sl;
+#define XTN_SPLIT(CFG, SL)                                                                                         \
+    XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
+                                   P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
+                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,        \
+                                   P<unsigned int>(c->bcnt)))
+    if (c->split_chunk == 2048) {
+        if (sl == kSplitSlices) XTN_SPLIT(SplitSmall, kSplitSlices);
+        else XTN_SPLIT(SplitSmall, 1);
+    } else {
+        if (sl == kSplitSlices) XTN_SPLIT(StageLarge, kSplitSlices);
+        else XTN_SPLIT(StageLarge, 1);
+    }
+#undef XTN_SPLIT
+}
+
 // The first-level partition of the records k_bucket_gen wrote in sequence order (recB -> recA).
 static void launch_partition(xtn_context* c, const BucketPlan& bp, int n, int idbits, const unsigned int* abort,
                              cudaStream_t s) {
@@ -996,28 +1018,12 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * b_n));
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(b_n), kThreads, 0, s>>>(
-                                  bstart + b_lo, (int)b_n, base, c->group_cap, P<BucketDesc>(c->bdesc),
+                                  bstart + b_lo, (int)b_n, base, c->group_cap, (uint32_t)c->split_fill, P<BucketDesc>(c->bdesc),
                                   (uint32_t)desc_cap, P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), nullptr));
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
-        // one CTA per bucket, or a cluster of kSplitSlices CTAs per bucket, launched for every
-        // bucket without waiting for the plan: those past the plan's job count exit at once
-        const bool sliced = c->split_slices > 1;
-        const unsigned grid = (unsigned)b_n * (sliced ? kSplitSlices : 1);
-#define XTN_SPLIT(CFG, SL)                                                                                         \
-    XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
-                                   P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
-                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,        \
-                                   P<unsigned int>(c->bcnt)))
-        if (c->split_chunk == 2048) {
-            if (sliced) XTN_SPLIT(SplitSmall, kSplitSlices);
-            else XTN_SPLIT(SplitSmall, 1);
-        } else {
-            if (sliced) XTN_SPLIT(StageLarge, kSplitSlices);
-            else XTN_SPLIT(StageLarge, 1);
-        }
-#undef XTN_SPLIT
+        launch_split(c, b_n, desc_cap, s);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1516,7 +1522,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
 // that outgrows a capacity, meets a bucket too large for shared memory or a hash set too full,
 // is redone by the plain form, which also re-sizes the graph. The plain form
 // (run_nn) waits for the device four times per search to size its buffers and grids.
-using GraphSig = std::array<int64_t, 11>;
+using GraphSig = std::array<int64_t, 12>;
 
 struct GraphState {
     const uint8_t* chars = nullptr;
@@ -1574,7 +1580,7 @@ __global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned in
 static GraphSig graph_signature(const xtn_context* c) {
     return GraphSig{c->stage_chunk,  c->split_chunk,  c->bucket_bits_max,     (int64_t)c->group_cap,
                     c->group_tma,    c->key_tables,   c->split_slices,        c->scatter_ctas_per_sm,
-                    c->pair_dedup,   c->verify_per,   c->flat_gen};
+                    c->pair_dedup,   c->verify_per,   c->flat_gen,            c->split_fill};
 }
 
 static void graph_release(GraphState* g) {
@@ -1622,25 +1628,9 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     }
     const size_t desc_cap = (size_t)nb * 3 + 4 * g->Vcap / c->group_cap + 2048;
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
-                                  bstart, nb, 0ull, c->group_cap, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
+                                  bstart, nb, 0ull, c->group_cap, (uint32_t)c->split_fill, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
-    {
-        const bool sliced = c->split_slices > 1;
-        const unsigned grid = (unsigned)nb * (sliced ? kSplitSlices : 1);
-#define XTN_SPLIT(CFG, SL)                                                                                         \
-    XTN_LAUNCH("bucket_split", k_bucket_split_staged<CFG, SL><<<grid, CFG::kThreads, sizeof(StageSmem<CFG>), s>>>( \
-                                   P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap, \
-                                   P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,        \
-                                   P<unsigned int>(c->bcnt)))
-        if (c->split_chunk == 2048) {
-            if (sliced) XTN_SPLIT(SplitSmall, kSplitSlices);
-            else XTN_SPLIT(SplitSmall, 1);
-        } else {
-            if (sliced) XTN_SPLIT(StageLarge, kSplitSlices);
-            else XTN_SPLIT(StageLarge, 1);
-        }
-#undef XTN_SPLIT
-    }
+    launch_split(c, (uint32_t)nb, desc_cap, s);
     XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
     XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
     XTN_TRY(launch_group(c, 0, true, idbits, P<uint64_t>(c->pairA), g->Pcap, (uint32_t)desc_cap, s));
@@ -2971,6 +2961,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "group_persistent") && (v == 0 || v == 1)) c->group_persistent = (int)v;
     else if (!strcmp(name, "shard_count") && v >= 1 && v <= kMaxShards) c->shard_count = (int)v;
     else if (!strcmp(name, "flat_gen") && (v == 0 || v == 1)) c->flat_gen = (int)v;
+    else if (!strcmp(name, "split_fill") && v >= 25 && v <= 95) c->split_fill = (int)v;
     else if (!strcmp(name, "shard_index") && v >= 0 && v < kMaxShards) c->shard_index = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
