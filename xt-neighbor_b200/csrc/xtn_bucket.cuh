@@ -15,7 +15,8 @@
 //                              a coalesced run, so L2 receives whole sectors instead of
 //                              read-modify-writing partial ones
 //   plan     k_bucket_plan     buckets that fit in shared memory go straight to grouping;
-//                              larger ones are split by their next hash bits
+//                              larger ones are split by ranges of their next hash bits into
+//                              sub-buckets of about split_fill % of the grouping capacity
 //   split    k_bucket_split_staged
 //                              per oversized bucket, the same staged partition into
 //                              sub-buckets (chunks arrive by bulk copy)
@@ -690,7 +691,7 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint6
 
 // Split of the oversized first-level buckets. Each job (bucket) is handled by a cluster of
 // kSlices CTAs, each taking a contiguous slice of the bucket's records:
-//   1. each CTA histograms its slice by the records' top `bits` bits (the next hash bits);
+//   1. each CTA histograms its slice by sub-bucket (split_sub: ranges of the top hash bits);
 //   2. after a cluster barrier, each CTA reads every slice's histogram from its peers' shared
 //      memory (distributed shared memory, plain loads) and derives the sub-bucket totals, their
 //      starts and its own offset inside each sub-bucket; rank 0 lists the sub-buckets (those

@@ -716,6 +716,20 @@ static int ensure_keep(xtn_context* c, DevBuf& b, size_t bytes, size_t used) {
     return XTN_SUCCESS;
 }
 
+// Records of the fallback buckets desc[0..gridDim.x) copied one after another into `out`
+// (bucket k at off[k]); one CTA per bucket.
+__global__ void k_fallback_gather(const BucketDesc* __restrict__ desc, const uint64_t* __restrict__ off,
+                                  const uint64_t* __restrict__ recA, const uint64_t* __restrict__ recB,
+                                  uint64_t* __restrict__ out) {
+    const BucketDesc f = desc[blockIdx.x];
+    const uint64_t* src = (f.src ? recB : recA) + f.start;
+    uint64_t* dst = out + off[blockIdx.x];
+    for (uint32_t i = threadIdx.x; i < f.size; i += blockDim.x) dst[i] = src[i];
+}
+
+// Records gathered per batch of fallback buckets (more when one bucket alone is larger).
+constexpr uint64_t kFallbackBatchRecords = uint64_t(1) << 26;
+
 // Candidate pairs of a record array sorted by hash: runs of equal hash, every id pair of every
 // run appended to `out` at index `base`. *count receives the number appended.
 static int group_sorted(xtn_context* c, const uint64_t* recs, int64_t V, int idbits, DevBuf& out, uint64_t base,
@@ -844,14 +858,18 @@ static int launch_group(xtn_context* c, uint32_t ndesc, bool persistent, int idb
 // split to bring them to shared-memory size.
 constexpr int kDirectBucketBitsMax = 14;
 constexpr uint64_t kFirstLevelRecords = 1500000;
+constexpr uint64_t kFirstLevelRecordsFlat = 2500000;
 
 // The first-level plan: count pass over every variant (per-tile histograms of the top b1 hash
 // bits), per-tile offsets inside each bucket, bucket starts (c->bstart, nb + 1 entries) and, for
 // the staged scatter at d = 2, the balanced task map.
 // The first-level shape for n sequences and V variant records (no device work).
-static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp) {
+// one_round: every record is kept at once, so the two-pass first level (option flat_gen) can
+// run; bp->flat says whether it does.
+static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp, bool one_round) {
     const bool small = c->stage_chunk == 2048;
     const bool tables = d <= 2 && c->key_tables;
+    const bool flat = one_round && c->flat_gen && tables && c->stage_chunk == 4096;
     // the staged scatter's fan-out bounds the first-level bits; the direct scatter (d > 2, or
     // per-key hashing) takes up to 2^14 buckets
     const int fan_bits = tables ? (small ? 9 : 10) : kDirectBucketBitsMax;
@@ -862,8 +880,10 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     // first-level buckets of more than kFirstLevelRecords records make the split re-read its
     // slices from DRAM (a cluster's bucket no longer stays in L2) and write short runs: at 10M
     // sequences 1024 buckets instead of 512 cut the split from 10.5 to 7.5 ms for 1.7 ms more
-    // scatter; at 1M, 512 stay faster
-    while (b1 < lim && (V >> b1) > kFirstLevelRecords) b1++;
+    // one-pass scatter; at 1M, 512 stay faster. The two-pass first level's partition gains more
+    // from the longer runs of 512 buckets (10M: partition 5.09 against 6.78 ms, split 7.94
+    // against 6.66 ms), so it keeps buckets of up to kFirstLevelRecordsFlat records.
+    while (b1 < lim && (V >> b1) > (flat ? kFirstLevelRecordsFlat : kFirstLevelRecords)) b1++;
     // enough buckets that the split (at most 2^kMaxSplitBits ways) can bring each to the
     // grouping capacity (the small grouping shape at 10M sequences needs 1024 of them)
     const uint64_t target = std::max<uint64_t>(1, (uint64_t)c->group_cap * 7 / 8);
@@ -881,6 +901,7 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     bp->tile = (n + ntiles - 1) / ntiles;
     bp->small = small;
     bp->staged = tables && b1 <= fan_bits;
+    bp->flat = flat && bp->staged;
     bp->tseq = nullptr;
 }
 
@@ -905,11 +926,10 @@ static int bucket_reserve(xtn_context* c, const BucketPlan& bp, int n, int d, ui
 static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp, bool one_round = false,
                           const unsigned int* abort = nullptr) {
     cudaStream_t s = c->stream;
-    bucket_shape(c, n, d, V, bp);
+    bucket_shape(c, n, d, V, bp, one_round);
     const int b1 = bp->b1, nb = bp->nb, ntiles = bp->ntiles, tile = bp->tile;
     const bool tables = d <= 2 && c->key_tables;
     const size_t hist_smem = sizeof(uint32_t) * nb;
-    bp->flat = one_round && c->flat_gen && tables && bp->staged && !bp->small && c->stage_chunk == 4096;
     XTN_TRY(bucket_reserve(c, *bp, n, d, V));
     XTN_TRY(bucket_attrs(c));
     if (bp->staged && d >= 2) {
@@ -1012,7 +1032,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_CK(cudaGetLastError());
     XTN_CK(cudaEventRecord(c->ev[2], s));
 
-    // plan: buckets that fit go to grouping, the rest are split by the next hash bits
+    // plan: buckets that fit go to grouping, the rest are split by ranges of the next hash bits
     const size_t desc_cap = (size_t)b_n * 3 + 4 * Vr / c->group_cap + 2048;
     XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
@@ -1079,20 +1099,41 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     c->stats.n_groups += ndesc;
     XTN_CK(cudaEventRecord(c->ev[4], s));
 
-    // buckets too large for shared memory: sorted and grouped in global memory
+    // buckets too large for shared memory: gathered in batches (one kernel per batch), sorted
+    // and grouped in global memory. Equal hashes lie in one bucket, so a batch of several
+    // buckets groups exactly as the buckets one by one would (records of different first-level
+    // buckets whose remaining hash fields agree add candidates that verification removes).
     if (nfall > 0) {
         std::vector<BucketDesc> fl(nfall);
         XTN_CK(cudaMemcpy(fl.data(), c->bfall.p, sizeof(BucketDesc) * nfall, cudaMemcpyDeviceToHost));
-        for (const BucketDesc& f : fl) {
-            XTN_TRY(ensure(c->fbA, sizeof(uint64_t) * f.size + 64));
-            XTN_TRY(ensure(c->fbB, sizeof(uint64_t) * f.size + 64));
-            const uint64_t* srcbuf = f.src ? P<uint64_t>(c->recB) : P<uint64_t>(c->recA);
-            XTN_CK(cudaMemcpyAsync(c->fbA.p, srcbuf + f.start, sizeof(uint64_t) * f.size, cudaMemcpyDeviceToDevice, s));
+        uint64_t largest = 0;
+        for (const BucketDesc& f : fl) largest = std::max<uint64_t>(largest, f.size);
+        const uint64_t batch_cap = std::max<uint64_t>(largest, kFallbackBatchRecords);
+        XTN_TRY(ensure(c->fbA, sizeof(uint64_t) * batch_cap + 64));
+        XTN_TRY(ensure(c->fbB, sizeof(uint64_t) * batch_cap + 64));
+        std::vector<uint64_t> offs;
+        for (size_t b0 = 0; b0 < fl.size();) {
+            size_t b1 = b0;
+            uint64_t recs = 0;
+            offs.clear();
+            while (b1 < fl.size() && (b1 == b0 || recs + fl[b1].size <= batch_cap)) {
+                offs.push_back(recs);
+                recs += fl[b1].size;
+                b1++;
+            }
+            offs.push_back(recs);
+            XTN_TRY(ensure(c->scratch64, sizeof(uint64_t) * offs.size()));
+            XTN_CK(cudaMemcpyAsync(c->scratch64.p, offs.data(), sizeof(uint64_t) * offs.size(), cudaMemcpyHostToDevice, s));
+            XTN_LAUNCH("fallback_gather", k_fallback_gather<<<(unsigned)(b1 - b0), kThreads, 0, s>>>(
+                                              P<BucketDesc>(c->bfall) + b0, P<uint64_t>(c->scratch64),
+                                              P<uint64_t>(c->recA), P<uint64_t>(c->recB), P<uint64_t>(c->fbA)));
             uint64_t* sorted = nullptr;
-            XTN_TRY(sort_u64(c, c->fbA, c->fbB, f.size, idbits, 64, &sorted, XTN_SORT_NAMES("fallback_sort")));
+            XTN_TRY(sort_u64(c, c->fbA, c->fbB, (int64_t)recs, idbits, 64, &sorted, XTN_SORT_NAMES("fallback_sort")));
             uint64_t more = 0;
-            XTN_TRY(group_sorted(c, sorted, f.size, idbits, out, total, &more));
+            XTN_TRY(group_sorted(c, sorted, (int64_t)recs, idbits, out, total, &more));
             total += more;
+            XTN_CK(cudaStreamSynchronize(s));  // offs (host) is refilled for the next batch
+            b0 = b1;
         }
     }
     c->stats.n_fallback += nfall;
@@ -1690,7 +1731,7 @@ static int graph_reserve(xtn_context* c, GraphState* g, const uint8_t* chars, co
     // the first-level shape the capacity implies, and every buffer reserved (the capture must
     // not allocate)
     BucketPlan bp;
-    bucket_shape(c, n, d, g->Vcap, &bp);
+    bucket_shape(c, n, d, g->Vcap, &bp, true);
     g->b1 = bp.b1;
     XTN_TRY(bucket_reserve(c, bp, n, d, g->Vcap));
     const int nb = bp.nb;
