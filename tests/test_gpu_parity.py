@@ -34,6 +34,9 @@ ENGINES = {
     # the one-pass first-level scatter (generation and partition per chunk) in place of the
     # default two passes (every record generated in sequence order, then partitioned)
     "bucket_one_pass": {"flat_gen": 0},
+    # the two-pass split (slice histograms merged in a cluster, exact sub-bucket placement) in
+    # place of the default one-pass split into fixed slots of the grouping capacity
+    "bucket_two_pass_split": {"split_slotted": 0},
 }
 
 

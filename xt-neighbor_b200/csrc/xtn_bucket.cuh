@@ -107,6 +107,8 @@ struct SplitJob {
     uint64_t start;
     uint32_t size;
     uint32_t nsub;
+    uint32_t sub0;   // the job's first sub-bucket among all jobs' (slotted split)
+    uint32_t pad;
 };
 
 // Sub-bucket of record x among nsub: the top 32 hash bits scaled to [0, nsub), so that any
@@ -684,8 +686,8 @@ __global__ void k_bucket_plan(const uint64_t* __restrict__ bstart, int nb, uint6
         const uint64_t target = max(1u, (uint32_t)((uint64_t)group_cap * split_fill / 100));
         const uint64_t want = (size + target - 1) / target;
         const uint32_t nsub = want < 2 ? 2u : want > (uint64_t)kMaxSplitFan ? (uint32_t)kMaxSplitFan : (uint32_t)want;
-        bounded_append(jobs, (uint32_t)nb, counters, kCntJobs, SplitJob{s, size, nsub});
-        atomicAdd(&counters[kCntSub], nsub);
+        const uint32_t sub0 = atomicAdd(&counters[kCntSub], nsub);
+        bounded_append(jobs, (uint32_t)nb, counters, kCntJobs, SplitJob{s, size, nsub, sub0, 0});
     }
 }
 
@@ -837,6 +839,137 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
         split_partition(S, (int)nsub, m, S.rec + lead, [nsub](uint64_t x) { return split_sub(x, nsub); }, out, [&] {
             if (threadIdx.x == 0 && c0 + kStageChunk < size) issue(c0 + kStageChunk);
         });
+    }
+}
+
+// ------------------------------------------------------------------ slotted split
+// The split in one pass over the records: every sub-bucket gets a slot of `slot` records (the
+// grouping capacity) in buffer B at (job.sub0 + sub) * slot, and each chunk of a slice, after
+// its staged ranking, reserves its runs with one global atomic per sub-bucket on that
+// sub-bucket's cursor and writes them there. No histogram pass, no cluster: kSlices CTAs take
+// slices of a job independently. Records past a slot's end are not written but counted, so a
+// cursor above `slot` marks a sub-bucket too large for shared memory; k_split_slot_descs then
+// lists the job's whole first-level bucket for the sort-based fallback instead (the other
+// sub-buckets' pairs it also finds again are removed with the other repeats).
+template <class C, int kSlices>
+__global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
+    k_bucket_split_slotted(const SplitJob* __restrict__ jobs, const uint64_t* __restrict__ in,
+                           uint64_t* __restrict__ out, uint32_t slot, unsigned int* __restrict__ cursors,
+                           unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
+    constexpr int T = C::kThreads, kChunk = C::kChunk, kFanPer = C::kFanPer;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
+    if (abort && *abort) return;
+    if (blockIdx.x / kSlices >= min(counters[kCntJobs], (unsigned)(gridDim.x / kSlices))) return;  // no such job
+    const SplitJob job = jobs[blockIdx.x / kSlices];
+    const int rank = (int)(blockIdx.x % kSlices);
+    const uint32_t nsub = job.nsub;
+    const uint32_t s_lo = (uint32_t)((uint64_t)job.size * rank / kSlices);
+    const uint32_t s_hi = (uint32_t)((uint64_t)job.size * (rank + 1) / kSlices);
+    const uint32_t size = s_hi - s_lo;
+    const uint64_t* src = in + job.start + s_lo;
+    uint64_t* dst = out + (uint64_t)job.sub0 * slot;
+    unsigned int* cur = cursors + job.sub0;
+    const uint32_t mbar = smem_u32(&S.mbar);
+    auto issue = [&](uint32_t c0) {
+        const uint32_t m = min((uint32_t)kChunk, size - c0);
+        const uint64_t* a = src + c0;
+        const uint32_t lead = (uint32_t)(((uintptr_t)a & 15u) >> 3);
+        bulk_load(smem_u32(&S.rec[0]), a - lead, ((lead + m) * 8u + 15u) & ~15u, mbar);
+    };
+    if (threadIdx.x == 0) {
+        S.wait_failed = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (size > 0) issue(0);
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    for (uint32_t c0 = 0; c0 < size; c0 += kChunk, parity ^= 1u) {
+        const uint32_t m = min((uint32_t)kChunk, size - c0);
+        const uint32_t lead = (uint32_t)(((uintptr_t)(src + c0) & 15u) >> 3);
+        if (threadIdx.x == 0) {
+            uint32_t polls = 0;
+            while (!mbar_try_wait(mbar, parity)) {
+                if (++polls > kWaitLimit) {
+                    S.wait_failed = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __syncthreads();
+        if (S.wait_failed) {
+            if (threadIdx.x == 0) {
+                uint32_t polls = 0;
+                while (!mbar_try_wait(mbar, parity) && ++polls < kWaitLimit) __nanosleep(64);
+                atomicAdd(&counters[kCntWaitFail], 1u);
+            }
+            __syncthreads();
+            return;
+        }
+        const uint64_t* r = S.rec + lead;
+        for (uint32_t b = threadIdx.x; b < nsub; b += T) S.cnt[b] = 0;
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p < m; p += T) atomicAdd(&S.cnt[split_sub(r[p], nsub)], 1u);
+        __syncthreads();
+        {
+            uint32_t tot, loc[kFanPer], cnt[kFanPer], sum = 0;
+            const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+            for (int k = 0; k < kFanPer; k++) {
+                loc[k] = sum;
+                cnt[k] = (b0 + k < (int)nsub) ? S.cnt[b0 + k] : 0u;
+                sum += cnt[k];
+            }
+            const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
+#pragma unroll
+            for (int k = 0; k < kFanPer; k++)
+                if (cnt[k]) {
+                    S.lstart[b0 + k] = ex + loc[k];
+                    S.cnt[b0 + k] = ex + loc[k];
+                    S.gcur[b0 + k] = atomicAdd(&cur[b0 + k], cnt[k]);  // this chunk's runs in the slot
+                }
+        }
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p < m; p += T) {
+            const uint64_t x = r[p];
+            const uint32_t b = split_sub(x, nsub);
+            const uint32_t q = atomicAdd(&S.cnt[b], 1u);
+            S.sorted[q] = x;
+            S.sbkt[q] = (uint16_t)b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && c0 + kChunk < size) issue(c0 + kChunk);
+        for (uint32_t q = threadIdx.x; q < m; q += T) {
+            const uint16_t b = S.sbkt[q];
+            const uint32_t pos = S.gcur[b] + (q - S.lstart[b]);
+            if (pos < slot) dst[(uint64_t)b * slot + pos] = S.sorted[q];
+        }
+        __syncthreads();
+    }
+}
+
+// Descriptors of the slotted split, one CTA per job: the sub-buckets of two or more records
+// (slot positions, buffer B), or, when any sub-bucket outgrew its slot, the job's whole
+// first-level bucket (buffer A) for the sort-based fallback.
+__global__ void k_split_slot_descs(const SplitJob* __restrict__ jobs, const unsigned int* __restrict__ cursors,
+                                   uint32_t slot, BucketDesc* __restrict__ desc, BucketDesc* __restrict__ fallback,
+                                   uint32_t desc_cap, unsigned int* __restrict__ counters,
+                                   const unsigned int* __restrict__ abort) {
+    if (abort && *abort) return;
+    if (blockIdx.x >= counters[kCntJobs]) return;
+    const SplitJob job = jobs[blockIdx.x];
+    const unsigned int* cur = cursors + job.sub0;
+    int over = 0;
+    for (uint32_t b = threadIdx.x; b < job.nsub; b += blockDim.x) over |= cur[b] > slot;
+    if (__syncthreads_or(over)) {
+        if (threadIdx.x == 0) bounded_append(fallback, desc_cap, counters, kCntFallback, BucketDesc{job.start, job.size, 0});
+        return;
+    }
+    for (uint32_t b = threadIdx.x; b < job.nsub; b += blockDim.x) {
+        const uint32_t c = cur[b];
+        if (c >= 2) bounded_append(desc, desc_cap, counters, kCntDesc, BucketDesc{(uint64_t)(job.sub0 + b) * slot, c, 1});
     }
 }
 

@@ -525,6 +525,7 @@ struct xtn_context {
     int shard_count = 1, shard_index = 0;  // this search covers shard shard_index of shard_count
     int flat_gen = 1;       // one-round first level: generate in sequence order, then partition
     int split_fill = 87;    // split sub-buckets sized at this percentage of group_cap
+    int split_slotted = 1;  // one-round searches split in one pass into fixed slots
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
@@ -540,6 +541,7 @@ struct xtn_context {
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_round[2] = {};
     DevBuf pairA2, ddcnt;
+    DevBuf scur;             // sub-bucket cursors of the slotted split
     // graph form of the device-resident search (option "graph")
     int graph_mode = 0;
     void* graph = nullptr;  // GraphState (below)
@@ -799,6 +801,9 @@ struct BucketPlan {
     int b1 = 1, nb = 2, ntiles = 1, tile = 1;
     bool small = false, staged = false;
     bool flat = false;  // generate in sequence order (recB), then partition (k_bucket_gen / k_bucket_partition)
+    bool slotted = false;  // one-pass split into fixed slots (k_bucket_split_slotted)
+    uint64_t sub_bound = 0;  // slotted: sub-buckets of all jobs, at most
+    uint64_t recb = 0;       // records buffer B must hold
     const uint32_t* tseq = nullptr;
 };
 
@@ -828,6 +833,8 @@ static int bucket_attrs(xtn_context* c) {
                                 (int)sizeof(GroupSmem<GroupSmall>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_partition<StageHuge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(StageSmem<StageHuge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_slotted<StageLarge, kSplitSlices>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageLarge>)));
     c->attrs_set = true;
     return XTN_SUCCESS;
 }
@@ -902,11 +909,18 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     bp->small = small;
     bp->staged = tables && b1 <= fan_bits;
     bp->flat = flat && bp->staged;
+    // the slotted split (one round only: buffer B then holds a slot of group_cap records per
+    // sub-bucket, about 1 / split_fill of the records plus one slot per first-level bucket)
+    bp->slotted = one_round && c->split_slotted;
+    const uint64_t sub_target = std::max<uint64_t>(1, (uint64_t)c->group_cap * c->split_fill / 100);
+    bp->sub_bound = V / sub_target + (uint64_t)nb + 1;
+    bp->recb = bp->slotted ? std::max<uint64_t>(V, bp->sub_bound * c->group_cap) : V;
     bp->tseq = nullptr;
 }
 
 // Reserves the buffers bucket_prepare uses for this shape.
 static int bucket_reserve(xtn_context* c, const BucketPlan& bp, int n, int d, uint64_t V) {
+    if (bp.slotted) XTN_TRY(ensure(c->scur, sizeof(uint32_t) * bp.sub_bound));
     XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)bp.ntiles * bp.nb));
     XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)bp.ntiles * bp.nb));
     XTN_TRY(ensure(c->btotals, sizeof(uint32_t) * (bp.nb + 1)));
@@ -943,7 +957,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
     if (bp->flat) {
         // every record in sequence order into recB, with the per-tile histograms
         XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
-        XTN_TRY(ensure(c->recB, sizeof(uint64_t) * V + 64));
+        XTN_TRY(ensure(c->recB, sizeof(uint64_t) * bp->recb + 64));
         XTN_LAUNCH("bucket_gen", (k_bucket_gen<kBucketThreads, 2><<<ntiles, kBucketThreads, hist_smem, s>>>(
                                      P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
                                      P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp->tseq, n, tile, d, b1,
@@ -962,8 +976,23 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
 
 // The split of the plan's jobs (recA -> recB): one CTA per bucket, or a cluster of
 // split_slices CTAs per bucket, launched for every one of the b_n buckets without waiting for
-// the plan: those past the plan's job count exit at once.
-static void launch_split(xtn_context* c, uint32_t b_n, size_t desc_cap, cudaStream_t s) {
+// the plan: those past the plan's job count exit at once. The slotted split (bp.slotted) takes
+// kSplitSlices independent CTAs per job and lists its sub-buckets afterwards.
+static void launch_split(xtn_context* c, const BucketPlan& bp, uint32_t b_n, size_t desc_cap,
+                         const unsigned int* abort, cudaStream_t s) {
+    if (bp.slotted) {
+        cudaMemsetAsync(c->scur.p, 0, sizeof(uint32_t) * bp.sub_bound, s);
+        XTN_LAUNCH("bucket_split",
+                   (k_bucket_split_slotted<StageLarge, kSplitSlices><<<b_n * kSplitSlices, StageLarge::kThreads,
+                                                                      sizeof(StageSmem<StageLarge>), s>>>(
+                       P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                       P<unsigned int>(c->scur), P<unsigned int>(c->bcnt), abort)));
+        XTN_LAUNCH("split_descs", k_split_slot_descs<<<b_n, 256, 0, s>>>(
+                                      P<SplitJob>(c->bjobs), P<unsigned int>(c->scur), c->group_cap,
+                                      P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,
+                                      P<unsigned int>(c->bcnt), abort));
+        return;
+    }
     const int sl = c->split_slices;
     const unsigned grid = b_n * (unsigned)sl;
 #define XTN_SPLIT(CFG, SL)                                                                                         \
@@ -1015,7 +1044,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     cudaStream_t s = c->stream;
     const int b1 = bp.b1, nb = bp.nb;
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * Vr + 64));
-    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * Vr + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * (bp.slotted ? bp.recb : Vr) + 64));
     const uint64_t* bstart = P<uint64_t>(c->bstart);
     XTN_TRY(ensure(c->bcnt, 64));
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
@@ -1043,7 +1072,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
-        launch_split(c, b_n, desc_cap, s);
+        launch_split(c, bp, b_n, desc_cap, nullptr, s);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1223,7 +1252,9 @@ static size_t held_bytes(const xtn_context* c) {
 static uint64_t round_record_limit(xtn_context* c, int n, int d, uint64_t V) {
     const double cpr = c->last_pc_per_rec > 0 ? c->last_pc_per_rec : 0.06;
     const double share = std::min(1.0, 1.25 * c->dd_share);
-    const double per_rec = 16.0 + 20.0 * cpr;
+    // (the slotted split's buffer B holds about 1 / split_fill of the records plus a slot per
+    // first-level bucket: up to 1.75x the records)
+    const double per_rec = (c->split_slotted ? 22.0 : 16.0) + 20.0 * cpr;
     const double fixed = (d <= 2 && c->key_tables ? 273.0 : 41.0) * (double)n;
     const double pairs = 48.0 * share * cpr * (double)V;
     double budget = (double)c->memory_budget;
@@ -1563,7 +1594,7 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
 // that outgrows a capacity, meets a bucket too large for shared memory or a hash set too full,
 // is redone by the plain form, which also re-sizes the graph. The plain form
 // (run_nn) waits for the device four times per search to size its buffers and grids.
-using GraphSig = std::array<int64_t, 12>;
+using GraphSig = std::array<int64_t, 13>;
 
 struct GraphState {
     const uint8_t* chars = nullptr;
@@ -1621,7 +1652,8 @@ __global__ void k_graph_status(const uint64_t* __restrict__ V, const unsigned in
 static GraphSig graph_signature(const xtn_context* c) {
     return GraphSig{c->stage_chunk,  c->split_chunk,  c->bucket_bits_max,     (int64_t)c->group_cap,
                     c->group_tma,    c->key_tables,   c->split_slices,        c->scatter_ctas_per_sm,
-                    c->pair_dedup,   c->verify_per,   c->flat_gen,            c->split_fill};
+                    c->pair_dedup,   c->verify_per,   c->flat_gen,            c->split_fill,
+                    c->split_slotted};
 }
 
 static void graph_release(GraphState* g) {
@@ -1671,7 +1703,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
                                   bstart, nb, 0ull, c->group_cap, (uint32_t)c->split_fill, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
-    launch_split(c, (uint32_t)nb, desc_cap, s);
+    launch_split(c, bp, (uint32_t)nb, desc_cap, abort, s);
     XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
     XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
     XTN_TRY(launch_group(c, 0, true, idbits, P<uint64_t>(c->pairA), g->Pcap, (uint32_t)desc_cap, s));
@@ -1738,7 +1770,7 @@ static int graph_reserve(xtn_context* c, GraphState* g, const uint8_t* chars, co
     const size_t desc_cap = (size_t)nb * 3 + 4 * g->Vcap / c->group_cap + 2048;
     XTN_TRY(ensure(c->lencheck, 16));
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * g->Vcap + 64));
-    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * g->Vcap + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * bp.recb + 64));
     XTN_TRY(ensure(c->bdesc, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bfall, sizeof(BucketDesc) * desc_cap));
     XTN_TRY(ensure(c->bjobs, sizeof(SplitJob) * nb));
@@ -2229,7 +2261,7 @@ static std::vector<DevBuf*> context_buffers(xtn_context* c) {
         &c->out_dist, &c->out_freq, &c->bcounts,   &c->boffs,    &c->btotals,    &c->bstart,   &c->bdesc,
         &c->bjobs,   &c->bfall,     &c->bcnt,      &c->fbA,      &c->fbB,        &c->runinfo,  &c->tcnt,
         &c->toff,    &c->ktab,      &c->info,      &c->lencheck, &c->pairA2,     &c->ddcnt,    &c->tseq,
-        &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status};
+        &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status, &c->scur};
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
         for (DevBuf* b : {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
@@ -3003,6 +3035,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "shard_count") && v >= 1 && v <= kMaxShards) c->shard_count = (int)v;
     else if (!strcmp(name, "flat_gen") && (v == 0 || v == 1)) c->flat_gen = (int)v;
     else if (!strcmp(name, "split_fill") && v >= 25 && v <= 95) c->split_fill = (int)v;
+    else if (!strcmp(name, "split_slotted") && (v == 0 || v == 1)) c->split_slotted = (int)v;
     else if (!strcmp(name, "shard_index") && v >= 0 && v < kMaxShards) c->shard_index = (int)v;
     else if (!strcmp(name, "wait_fault_test") && (v == 0 || v == 1)) c->wait_fault_test = (int)v;
     else {
