@@ -996,6 +996,7 @@ struct GroupSmem {
     unsigned long long warp_sums64[G::kThreads / 32 + 1];
     uint32_t wait_failed;
     uint32_t n_cand;
+    uint32_t next_di;   // persistent CTAs: the descriptor taken ahead (its records prefetched to L2)
     unsigned long long base;
     unsigned long long mbar;
 };
@@ -1024,7 +1025,8 @@ __device__ __forceinline__ uint64_t pack_pair(uint64_t a, uint64_t b, int idbits
 // With n_desc null, CTA i groups descriptor i (the grid has one CTA per descriptor). Otherwise
 // the CTAs are persistent: they take descriptors from a queue (counters[kCntNext]) until the
 // device-side count *n_desc (at most overflow_cap) is reached, so the grid needs no host-side
-// count (the graph form).
+// count (the graph form); each takes its next descriptor one bucket ahead and prefetches that
+// bucket's records to L2 while it works on the current one.
 constexpr int kCntNext = 7;  // the persistent grouping's queue position
 
 template <class G>
@@ -1049,7 +1051,9 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
     uint32_t phase = 0;
     for (uint32_t iter = 0;; iter++, phase ^= 1u) {
     __syncthreads();  // the previous descriptor is done with the shared memory
-    if (threadIdx.x == 0) S.n_cand = n_desc ? atomicAdd(&counters[kCntNext], 1u) : (iter == 0 ? blockIdx.x : count);
+    if (threadIdx.x == 0)
+        S.n_cand = n_desc ? (iter == 0 ? atomicAdd(&counters[kCntNext], 1u) : S.next_di)
+                          : (iter == 0 ? blockIdx.x : count);
     __syncthreads();
     const uint32_t di = S.n_cand;
     if (di >= count) return;
@@ -1078,6 +1082,19 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
         const uint4* g = reinterpret_cast<const uint4*>(src16);
         uint4* dd = reinterpret_cast<uint4*>(&S.rec[0]);
         for (uint32_t i = threadIdx.x; i < bytes / 16; i += G::kThreads) dd[i] = __ldg(g + i);
+    }
+    if (n_desc && threadIdx.x == 0) {
+        // persistent CTAs take their next descriptor now and start its records towards L2, so
+        // that its copy, one bucket later, does not wait on DRAM
+        const uint32_t nd = atomicAdd(&counters[kCntNext], 1u);
+        S.next_di = nd;
+        if (nd < count) {
+            const BucketDesc nbd = descs[nd];
+            const uint64_t* nsrc = (nbd.src ? buf_b : buf_a) + nbd.start;
+            const uint32_t nlead = (uint32_t)(((uintptr_t)nsrc & 15u) >> 3);
+            const uint32_t nbytes = ((nlead + nbd.size) * 8u + 15u) & ~15u;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(nsrc - nlead), "r"(nbytes) : "memory");
+        }
     }
     {
         // both bitmaps and the digit counts cleared with 16-byte stores
@@ -1125,29 +1142,40 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
             pos[k] = b;
         }
     }
-    if (threadIdx.x == 0) S.n_cand = 0;  // (read as the descriptor index before the first barrier)
     __syncthreads();
-    // candidates in any order (one shared atomic per warp and round)
-    const unsigned lane = threadIdx.x & 31u;
+    // candidates in any order: each warp keeps its ballots in registers and counts its hits, the
+    // warps' counts are summed in order, then each warp writes its candidates at its offset (no
+    // shared counter for all warps to contend on)
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned masks[kPerThread];
+    uint32_t mine = 0;
 #pragma unroll
     for (int k = 0; k < kPerThread; k++) {
-        const uint32_t i0 = (threadIdx.x & ~31u) + (uint32_t)k * G::kThreads;
-        if (i0 >= n) break;
-        const uint32_t i = i0 + lane;
+        const uint32_t i = threadIdx.x + (uint32_t)k * G::kThreads;
         bool hit = false;
         if (i < n) {
             const uint32_t b = pos[k];
             hit = (S.u.bm.twice[b >> 5] >> (b & 31)) & 1u;
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, hit);
-        if (mask == 0u) continue;
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&S.n_cand, (uint32_t)__popc(mask));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (hit) S.cand[base + __popc(mask & ((1u << lane) - 1u))] = (uint16_t)i;
+        masks[k] = __ballot_sync(0xffffffffu, hit);
+        mine += __popc(masks[k]);
+    }
+    if (lane == 0) S.warp_sums[warp] = mine;
+    __syncthreads();
+    uint32_t cbase = 0, m = 0;
+#pragma unroll
+    for (int w = 0; w < G::kThreads / 32; w++) {
+        const uint32_t v = S.warp_sums[w];
+        cbase += w < (int)warp ? v : 0u;
+        m += v;
+    }
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < kPerThread; k++) {
+        if ((masks[k] >> lane) & 1u) S.cand[cbase + __popc(masks[k] & lt)] = (uint16_t)(threadIdx.x + k * G::kThreads);
+        cbase += __popc(masks[k]);
     }
     __syncthreads();  // the bitmaps are dead from here on
-    const uint32_t m = S.n_cand;
 
     // 2. counting sort of the candidates by kDigitBits hash bits above the bitmap bits
     for (uint32_t c = threadIdx.x; c < m; c += G::kThreads)
@@ -1184,8 +1212,15 @@ __global__ void __launch_bounds__(G::kThreads, G::kMinCtas) k_bucket_group(const
         if (b - a < 2) return false;
         for (uint32_t y = a; y < i; y++)
             if ((rec[S.u.gr.perm[y]] >> idbits) == kv) return false;
-        uint32_t sz = 1;
-        for (uint32_t y = i + 1; y < b; y++) sz += (rec[S.u.gr.perm[y]] >> idbits) == kv;
+        // (four independent loads per step: a long run's head does not wait on one chain)
+        uint32_t sz = 1, y = i + 1;
+        for (; y + 4 <= b; y += 4) {
+            const uint32_t p0 = S.u.gr.perm[y], p1 = S.u.gr.perm[y + 1], p2 = S.u.gr.perm[y + 2],
+                           p3 = S.u.gr.perm[y + 3];
+            sz += ((rec[p0] >> idbits) == kv) + ((rec[p1] >> idbits) == kv) + ((rec[p2] >> idbits) == kv) +
+                  ((rec[p3] >> idbits) == kv);
+        }
+        for (; y < b; y++) sz += (rec[S.u.gr.perm[y]] >> idbits) == kv;
         size = sz;
         contiguous = (sz == b - a) ? 1u : 0u;
         return sz >= 2;
