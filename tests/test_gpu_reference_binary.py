@@ -60,8 +60,24 @@ def test_nn_output_identical(tmp_path, kind, n, d, measure):
     assert oracle_nn_text(chars, offs, d, 1 if measure == "hamming" else 0) == ref
 
 
+def parse_triples(text):
+    out = {}
+    for line in text.decode().splitlines():
+        x, y, v = line.split()
+        out[(int(x), int(y))] = int(v)
+    return out
+
+
 def test_long_sequences_identical(tmp_path):
-    """Lengths 19..100: verification on the full strings beyond the 18-residue key."""
+    """Lengths 19..100: verification on the full strings beyond the 18-residue key.
+
+    This build must equal the CPU oracle exactly. The reference binary is not deterministic on
+    such pairs: its Levenshtein (xtneighbor_streaming/src/kernel.cu:263-278) allocates
+    max(len1, len2) bytes with device-side new, writes one past the end when the first string is
+    the longer, and frees the column before it reads the result, so a result can come out as
+    whatever another thread wrote there meanwhile (a negative distance, say). Most runs give
+    identical files; otherwise every differing pair must be decided by the exact distance in
+    this build's favour, and the differences must stay a small share of the output."""
     rng = np.random.default_rng(4)
     seqs = []
     for _ in range(1500):
@@ -75,7 +91,19 @@ def test_long_sequences_identical(tmp_path):
     f = tmp_path / "in.csv"
     write_nn_csv(f, chars, offs)
     ours, ref = run_both(tmp_path, ["-i", str(f), "-n", str(len(seqs)), "-d", "2"])
-    assert ours == ref and len(ref) > 0
+    assert len(ref) > 0
+    assert ours == oracle_nn_text(chars, offs, 2, 0)
+    if ours == ref:
+        return
+    o, r = parse_triples(ours), parse_triples(ref)
+    diff = [k for k in set(o) | set(r) if o.get(k) != r.get(k)]
+    assert len(diff) <= max(1, len(o) // 100), f"{len(diff)} differing pairs"
+    for x, y in diff:
+        exact = orc.levenshtein(seqs[x], seqs[y])
+        if (x, y) in o:
+            assert exact == o[(x, y)] <= 2, (seqs[x], seqs[y], exact, r.get((x, y)))
+        else:
+            assert exact > 2, (seqs[x], seqs[y], exact, r[(x, y)])
 
 
 def test_overlap_output_identical(tmp_path):
