@@ -523,8 +523,9 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
 // k_bucket_gen: the tile's generation tasks are spread over the CTA at once and every variant
 // is stored straight to its slot; a lane's consecutive variants fill whole sectors, which L2
 // merges before they reach DRAM (two CTAs of 512 threads per SM at 64 registers; a bound of
-// three CTAs measured slower: 6.46 against 5.55 ms at 10M, and one thread per sequence instead
-// of the balanced tasks 12.7 ms). abort (graph form, may be null): the records would not fit.
+// three CTAs measured slower: 6.46 against 5.55 ms at 10M, one thread per sequence instead of
+// the balanced tasks 12.7 ms, and whole run-pair tasks instead of halves 7.2 ms). abort (graph
+// form, may be null): the records would not fit.
 template <int THREADS, int MIN_CTAS>
 __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
@@ -542,7 +543,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
     if (t0 < t1) {
         uint64_t* out = flat + voff[t0];
-        chunk_hashes<THREADS, true>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d,
+        chunk_hashes<THREADS, false>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d,
                                     [&](uint32_t pos, uint64_t h, int i) {
                                         atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
                                         out[pos] = (h & hi_mask) | (uint64_t)i;
