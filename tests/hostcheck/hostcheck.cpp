@@ -73,27 +73,6 @@ int hc_task_variants_ok(const char* s, int L, int d) {
     return ok ? 1 : 0;
 }
 
-// 1 when the two-pass generation's whole run-pair tasks (for_each_task_hash<true>, t <
-// ceil(R/2)) produce every flat variant index exactly once, each with its key_hash; d <= 2.
-int hc_whole_task_hashes_ok(const char* s, int L, int d) {
-    u128 key = pack(s, L);
-    int Lk = L < kKeyLen ? L : kKeyLen;
-    const int n = variant_count(key, Lk, d);
-    const uint64_t info = key_run_info(key, Lk);
-    uint64_t tab[kTabLen];
-    key_table(key, [&](int slot, uint64_t x) { tab[slot] = x; });
-    const int R = popc32((uint32_t)info), T = (R + 1) / 2;
-    int seen[1024] = {0};
-    bool ok = n <= 1024;
-    for (int t = 0; t < T && ok; t++)
-        for_each_task_hash<true>(tab, Lk, info, d, t, [&](int v, uint64_t h) {
-            if (v < 0 || v >= n || h != key_hash(variant_at(key, info, v))) ok = false;
-            else seen[v]++;
-        });
-    for (int v = 0; v < n && ok; v++) ok = seen[v] == 1;
-    return ok ? 1 : 0;
-}
-
 // 1 when the key-table hashes equal key_hash of the variant keys: per task with the flat
 // index (for_each_task_hash), and as a whole multiset (for_each_hash); d <= 2.
 int hc_table_hash_ok(const char* s, int L, int d) {

@@ -84,15 +84,6 @@ def test_task_partition_of_variants(hc):
             assert hc.hc_task_variants_ok(s.encode(), len(s), d) == 1, (s, d)
 
 
-def test_whole_run_pair_tasks_cover_variants(hc):
-    """The two-pass generation's tasks (whole run pairs) cover every flat variant index exactly
-    once, each with the variant's key hash."""
-    rng = np.random.default_rng(31)
-    for s in rand_seqs(rng, 1500, 1, 26) + ["A" * 30, "AAC" * 8, "ACACAC", "A", "AC"]:
-        for d in (1, 2):
-            assert hc.hc_whole_task_hashes_ok(s.encode(), len(s), d) == 1, (s, d)
-
-
 def test_table_hashes_equal_variant_hashes(hc):
     """The key-table hashes of the d <= 2 kernels equal key_hash of each variant key."""
     rng = np.random.default_rng(29)

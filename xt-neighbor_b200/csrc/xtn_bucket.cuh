@@ -305,14 +305,13 @@ __device__ __forceinline__ void bulk_load(uint32_t dst_smem, const void* src, ui
                  : "memory");
 }
 
-// Tasks per sequence at d = 2: 2 * ceil(runs / 2) balanced tasks for the one-pass scatter, or
-// ceil(runs / 2) whole run pairs (whole = 1) for the two-pass generation (task_items). (At
-// d = 1 each sequence is one task and needs no map.)
-__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, int whole, uint32_t* __restrict__ tcnt) {
+// Tasks per sequence for the first-level generation at d = 2: 2 * ceil(runs / 2) balanced
+// tasks (task_items). (At d = 1 each sequence is one task and needs no map.)
+__global__ void k_task_counts(const uint64_t* __restrict__ runinfo, int n, uint32_t* __restrict__ tcnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t R = (uint32_t)popc32((uint32_t)runinfo[i]);
-    tcnt[i] = (whole ? 1u : 2u) * ((R + 1u) >> 1);
+    tcnt[i] = 2u * ((R + 1u) >> 1);
 }
 
 // Task -> sequence map of the staged scatter: the k_task_counts tasks of sequence i occupy
@@ -384,7 +383,7 @@ __device__ __forceinline__ int chunk_starts(const uint64_t* __restrict__ voff, i
 // task to its sequence; at d = 1 (task_seq null) a task is a whole sequence: its table row is
 // loaded into registers at once and the key and single deletions are emitted by an unrolled
 // loop.
-template <int T, bool WHOLE = false, class Put>
+template <int T, class Put>
 __device__ __forceinline__ void chunk_hashes(const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo,
                                              const uint64_t* __restrict__ tab, const uint64_t* __restrict__ voff,
                                              const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq,
@@ -400,7 +399,7 @@ __device__ __forceinline__ void chunk_hashes(const uint8_t* __restrict__ klen, c
         auto emit = [&](int v, uint64_t h) { put(vb + (uint32_t)v, h, i); };
         const uint64_t* row = tab + (size_t)i * kTabLen;
         if (d >= 2) {
-            for_each_task_hash<WHOLE>(row, klen[i], runinfo[i], d, t, emit);
+            for_each_task_hash(row, klen[i], runinfo[i], d, t, emit);
         } else {
             // the key, then the single deletion of each run: r G[p] + r^-1 P_L
             uint64_t G[kKeyLen];
@@ -543,7 +542,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
     if (t0 < t1) {
         uint64_t* out = flat + voff[t0];
-        chunk_hashes<THREADS, false>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d,
+        chunk_hashes<THREADS>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d,
                                     [&](uint32_t pos, uint64_t h, int i) {
                                         atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
                                         out[pos] = (h & hi_mask) | (uint64_t)i;

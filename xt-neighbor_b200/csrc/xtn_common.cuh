@@ -295,17 +295,16 @@ XTN_HD uint32_t pair_positions(uint32_t rs, uint32_t longr, uint32_t lmask, int 
 // Task t (0 <= t < 2*ceil(R/2)) of a key's d <= 2 variants, for parallel generation with even
 // work: tasks 2j and 2j+1 share the items of runs j and R-1-j (the single deletion of each run
 // and its pairs; about R+1 items together), split into two halves; task 0 also emits the key.
-// With WHOLE, task t (0 <= t < ceil(R/2)) takes both halves of runs t and R-1-t: half the
-// tasks, so the per-task setup is spread over twice the items. Item indices v are
-// variant_at's flat order.
-template <bool WHOLE = false, class E>
+// (Whole run pairs per task, half as many tasks, measured slower in the generation kernel.)
+// Item indices v are variant_at's flat order.
+template <class E>
 XTN_HD void task_items(int L, uint64_t info, int d, int t, E& e) {
     const uint32_t rs = (uint32_t)info, longr = (uint32_t)(info >> 32);
     const uint32_t lmask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
     const int R = popc32(rs);
     const bool two = d >= 2 && L >= 2;
     if (t == 0) e.key(0);
-    const int jA = WHOLE ? t : (t >> 1), jB = R - 1 - jA;
+    const int jA = t >> 1, jB = R - 1 - jA;
     // items of one run: the single deletion, then its pairs in ascending q
     int wA, wB = 0;
     uint32_t allowA = 0, allowB = 0;
@@ -317,7 +316,7 @@ XTN_HD void task_items(int L, uint64_t info, int d, int t, E& e) {
         wB = 1 + popc32(allowB);
     }
     const int total = wA + wB, half = total >> 1;
-    const int i0 = WHOLE ? 0 : ((t & 1) ? half : 0), i1 = WHOLE ? total : ((t & 1) ? total : half);
+    const int i0 = (t & 1) ? half : 0, i1 = (t & 1) ? total : half;
     auto run_items = [&](int j, int p, uint32_t allow, int a, int b) {  // local items [a, b)
         if (a >= b) return;
         e.run(p);
@@ -393,10 +392,10 @@ XTN_HD void for_each_task_variant(u128 key, int L, uint64_t info, int d, int t, 
 }
 
 // Task t's variants as hashes: f(v, hash).
-template <bool WHOLE = false, class F>
+template <class F>
 XTN_HD void for_each_task_hash(const uint64_t* tab, int L, uint64_t info, int d, int t, F&& f) {
     TableHashEmitter<F> e(tab, f);
-    task_items<WHOLE>(L, info, d, t, e);
+    task_items(L, info, d, t, e);
 }
 
 // All of a key's d <= 2 variants as hashes with the call count v = 0, 1, ...: f(v, hash).

@@ -948,7 +948,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
     XTN_TRY(bucket_attrs(c));
     if (bp->staged && d >= 2) {
         XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
-                                                                                   0, P<uint32_t>(c->tcnt)));
+                                                                                   P<uint32_t>(c->tcnt)));
         XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
         XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n, kTaskSeqThreads), kTaskSeqThreads, 0, s>>>(P<uint64_t>(c->toff), n,
                                                                              P<uint32_t>(c->tseq)));
