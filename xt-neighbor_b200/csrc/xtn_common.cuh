@@ -296,7 +296,7 @@ XTN_HD uint32_t pair_positions(uint32_t rs, uint32_t longr, uint32_t lmask, int 
 // work: tasks 2j and 2j+1 share the items of runs j and R-1-j (the single deletion of each run
 // and its pairs; about R+1 items together), split into two halves; task 0 also emits the key.
 // (Whole run pairs per task, half as many tasks, and quarters, twice as many, both measured
-// slower in the generation kernel: 7.2 and 0.99 ms against 5.6 ms at 10M and 0.60 ms at 1M.)
+// slower in the generation kernel at 10M: 7.2 and 9.2 ms against 5.6 ms.)
 // Item indices v are variant_at's flat order.
 template <class E>
 XTN_HD void task_items(int L, uint64_t info, int d, int t, E& e) {
