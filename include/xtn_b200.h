@@ -194,12 +194,12 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     into ceil(size / (group_cap * split_fill / 100)) sub-buckets (at most
  *                     1024) by ranges of the records' top hash bits, so the sub-buckets hold about
  *                     that share of the grouping capacity
- *   "split_slotted"   1 = a search that keeps every record at once splits in one pass: each
- *                     sub-bucket gets a fixed slot of group_cap records and every chunk reserves
- *                     its runs there with one atomic per sub-bucket (no histogram pass); a
- *                     first-level bucket whose sub-bucket outgrows its slot goes whole to the
- *                     sort-based fallback (default); 0 = the two-pass split (a histogram pass
- *                     merged across a cluster, then exact placement), always used in rounds
+ *   "split_slotted"   1 = the split runs in one pass: each sub-bucket gets a fixed slot of
+ *                     group_cap records and every chunk reserves its runs there with one atomic
+ *                     per sub-bucket (no histogram pass); a first-level bucket whose sub-bucket
+ *                     outgrows its slot goes whole to the sort-based fallback (default);
+ *                     0 = the two-pass split (a histogram pass merged across a cluster, then
+ *                     exact placement)
  *   "split_slices"    1 | 8: CTAs per split bucket (default 8: one thread-block cluster whose
  *                     CTAs take slices of the bucket and merge their histograms through
  *                     distributed shared memory)

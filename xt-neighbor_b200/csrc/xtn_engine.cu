@@ -871,6 +871,16 @@ constexpr uint64_t kFirstLevelRecordsFlat = 2500000;
 // bits), per-tile offsets inside each bucket, bucket starts (c->bstart, nb + 1 entries) and, for
 // the staged scatter at d = 2, the balanced task map.
 // The first-level shape for n sequences and V variant records (no device work).
+// Sub-buckets at most and records of buffer B for the split of V records in b_n first-level
+// buckets: with the slotted split, ceil(size / target) sub-buckets per split bucket and a slot of
+// group_cap records each.
+static void slot_sizes(const xtn_context* c, const BucketPlan& bp, uint64_t V, uint32_t b_n, uint64_t* sub_bound,
+                       uint64_t* recb) {
+    const uint64_t sub_target = std::max<uint64_t>(1, (uint64_t)c->group_cap * c->split_fill / 100);
+    *sub_bound = V / sub_target + (uint64_t)b_n + 1;
+    *recb = bp.slotted ? std::max<uint64_t>(V, *sub_bound * c->group_cap) : V;
+}
+
 // one_round: every record is kept at once, so the two-pass first level (option flat_gen) can
 // run; bp->flat says whether it does.
 static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketPlan* bp, bool one_round) {
@@ -909,12 +919,10 @@ static void bucket_shape(const xtn_context* c, int n, int d, uint64_t V, BucketP
     bp->small = small;
     bp->staged = tables && b1 <= fan_bits;
     bp->flat = flat && bp->staged;
-    // the slotted split (one round only: buffer B then holds a slot of group_cap records per
-    // sub-bucket, about 1 / split_fill of the records plus one slot per first-level bucket)
-    bp->slotted = one_round && c->split_slotted;
-    const uint64_t sub_target = std::max<uint64_t>(1, (uint64_t)c->group_cap * c->split_fill / 100);
-    bp->sub_bound = V / sub_target + (uint64_t)nb + 1;
-    bp->recb = bp->slotted ? std::max<uint64_t>(V, bp->sub_bound * c->group_cap) : V;
+    // the slotted split: buffer B then holds a slot of group_cap records per sub-bucket, about
+    // 1 / split_fill of the records plus one slot per first-level bucket (sized per round)
+    bp->slotted = c->split_slotted != 0;
+    slot_sizes(c, *bp, V, (uint32_t)nb, &bp->sub_bound, &bp->recb);
     bp->tseq = nullptr;
 }
 
@@ -978,10 +986,10 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
 // split_slices CTAs per bucket, launched for every one of the b_n buckets without waiting for
 // the plan: those past the plan's job count exit at once. The slotted split (bp.slotted) takes
 // kSplitSlices independent CTAs per job and lists its sub-buckets afterwards.
-static void launch_split(xtn_context* c, const BucketPlan& bp, uint32_t b_n, size_t desc_cap,
+static void launch_split(xtn_context* c, const BucketPlan& bp, uint32_t b_n, uint64_t sub_bound, size_t desc_cap,
                          const unsigned int* abort, cudaStream_t s) {
     if (bp.slotted) {
-        cudaMemsetAsync(c->scur.p, 0, sizeof(uint32_t) * bp.sub_bound, s);
+        cudaMemsetAsync(c->scur.p, 0, sizeof(uint32_t) * sub_bound, s);
         XTN_LAUNCH("bucket_split",
                    (k_bucket_split_slotted<StageLarge, kSplitSlices><<<b_n * kSplitSlices, StageLarge::kThreads,
                                                                       sizeof(StageSmem<StageLarge>), s>>>(
@@ -1043,8 +1051,11 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
                         uint64_t base, uint64_t Vr, DevBuf& out, uint64_t at, uint64_t* Pc) {
     cudaStream_t s = c->stream;
     const int b1 = bp.b1, nb = bp.nb;
+    uint64_t sub_bound = 0, recb = 0;
+    slot_sizes(c, bp, Vr, b_n, &sub_bound, &recb);
     XTN_TRY(ensure(c->recA, sizeof(uint64_t) * Vr + 64));
-    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * (bp.slotted ? bp.recb : Vr) + 64));
+    XTN_TRY(ensure(c->recB, sizeof(uint64_t) * recb + 64));
+    if (bp.slotted) XTN_TRY(ensure(c->scur, sizeof(uint32_t) * sub_bound));
     const uint64_t* bstart = P<uint64_t>(c->bstart);
     XTN_TRY(ensure(c->bcnt, 64));
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
@@ -1072,7 +1083,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
-        launch_split(c, bp, b_n, desc_cap, nullptr, s);
+        launch_split(c, bp, b_n, sub_bound, desc_cap, nullptr, s);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1703,7 +1714,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
                                   bstart, nb, 0ull, c->group_cap, (uint32_t)c->split_fill, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
-    launch_split(c, bp, (uint32_t)nb, desc_cap, abort, s);
+    launch_split(c, bp, (uint32_t)nb, bp.sub_bound, desc_cap, abort, s);
     XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
     XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
     XTN_TRY(launch_group(c, 0, true, idbits, P<uint64_t>(c->pairA), g->Pcap, (uint32_t)desc_cap, s));
