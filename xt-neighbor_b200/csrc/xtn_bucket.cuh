@@ -3,30 +3,36 @@
 // The sort-based engine orders all V variant records by hash with a multi-pass radix sort
 // (about 24 bytes of HBM traffic per record per 8-bit digit). Grouping only needs equal
 // hashes to meet, not a global order, so this engine moves each 8-byte record through HBM a
-// fixed small number of times:
-//   count    k_bucket_count    per tile of sequences: histogram of the top b1 hash bits
-//                              (variants generated and hashed, not stored)
+// fixed small number of times. First level, when the search keeps every record at once:
+//   gen      k_bucket_gen      every variant hashed from the key tables by balanced tasks
+//                              and stored in sequence order, (hash & ~idmask) | id, with the
+//                              per-tile histogram of the top b1 hash bits
 //   offsets  k_bucket_colscan  per bucket: exclusive prefix over tiles, bucket totals
-//   scatter  k_bucket_scatter_staged
-//                              the variants again (hashed from the key tables by balanced
-//                              tasks), up to 4096 at a time in shared memory, ranked within
-//                              their bucket as they are made, reordered by bucket and
-//                              written out as contiguous runs: every global store is part of
-//                              a coalesced run, so L2 receives whole sectors instead of
-//                              read-modify-writing partial ones
+//   partition k_bucket_partition
+//                              each tile's records, read back by bulk copies, through a staged
+//                              partition into their first-level buckets (every global store
+//                              part of a coalesced run, so L2 receives whole sectors)
+// First level in rounds and shards (records of a bucket range only), or at d > 2:
+//   count    k_bucket_count    per tile: histogram of the top b1 hash bits (not stored)
+//   scatter  k_bucket_scatter_staged / k_bucket_scatter
+//                              the variants again, up to 4096 at a time in shared memory,
+//                              ranked within their bucket as they are made and written out as
+//                              contiguous runs (or stored directly at d > 2)
+// Then:
 //   plan     k_bucket_plan     buckets that fit in shared memory go straight to grouping;
 //                              larger ones are split by ranges of their next hash bits into
 //                              sub-buckets of about split_fill % of the grouping capacity
-//   split    k_bucket_split_staged
-//                              per oversized bucket, the same staged partition into
-//                              sub-buckets (chunks arrive by bulk copy)
-//   group    k_bucket_group    one CTA per (sub-)bucket: TMA bulk copy into shared memory,
-//                              a bitmap filter that drops records without a partner, a
-//                              counting sort of the rest, runs of equal hashes, then every id
-//                              pair of every run, spread evenly over the CTA's threads and
-//                              written with coalesced stores
+//   split    k_bucket_split_slotted (+ k_split_slot_descs), or k_bucket_split_staged
+//                              per oversized bucket, the staged partition into sub-buckets:
+//                              in one pass into fixed slots with a cursor per sub-bucket, or in
+//                              two (histograms merged across a cluster, exact placement)
+//   group    k_bucket_group    one CTA per (sub-)bucket (persistent CTAs on a queue): TMA bulk
+//                              copy into shared memory, a bitmap filter that drops records
+//                              without a partner, a counting sort of the rest, runs of equal
+//                              hashes, then every id pair of every run, spread evenly over the
+//                              CTA's threads and written with coalesced stores
 // Buckets that still exceed shared memory after the split (one variant shared by very many
-// sequences) are grouped by the sort-based path instead.
+// sequences) are grouped by the sort-based path instead, in batches.
 #pragma once
 #include <cstdint>
 

@@ -2,17 +2,21 @@
 // C ABI declared in include/xtn_b200.h.
 //
 // Pipeline for nearest-neighbour mode (reference stages in S/src/xtn.cu:311-473):
-//   pack     k_pack          first 18 residues -> 128-bit key, variant count per sequence
+//   check    k_check_lengths every sequence 1..500 residues (device-resident inputs)
+//   pack     k_pack          first 18 residues -> 128-bit key, run masks, variant count and
+//                            the 19-word key table of the polynomial variant hash
 //   scan                     variant offsets
-//   gen      k_gen           one 64-bit record per deletion variant: hash bits | sequence id
-//   sort     radix_sort_u64  records by their hash bits (equal variants become adjacent)
-//   group    k_find_groups   runs of >= 2 equal hashes
-//   emit     k_emit          every id pair of every run, packed (min << b) | max
-//   sort     radix_sort_u64  candidate pairs
-//   verify   k_verify        unique pairs, x != y, Levenshtein (Myers) / Hamming on the full
-//                            strings, keep dist <= d (S/src/kernel.cu:359-392)
+//   group    bucket engine   (xtn_bucket.cuh) first-level buckets, split, grouping in shared
+//                            memory: every id pair of every run of equal variant hashes,
+//                            packed (min << b) | max; or the sort engine (engine = 1): k_gen,
+//                            radix_sort_u64, k_find_groups, k_emit
+//   dedup    k_pair_dedup    hash set of candidate pairs in HBM; the distinct ones listed
+//   sort     onesweep_sort_u64 / radix_sort_u64  distinct pairs in (x, y) order
+//   verify   k_verify_t      x != y, Levenshtein (Myers) / Hamming on the full strings, keep
+//                            dist <= d (S/src/kernel.cu:359-392)
 //   compact  k_compact       sorted (x, y, dist) output
-// Everything stays in device memory; the host reads four scalars to size buffers.
+// Everything stays in device memory; the plain form reads a few scalars back to size buffers,
+// the graph form none. Larger inputs run in rounds over ranges of first-level buckets.
 #include <cuda_runtime.h>
 
 #include <algorithm>
