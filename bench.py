@@ -831,7 +831,8 @@ def run_sharded(args, w):
     """The nearest-neighbour search sharded by first-level hash buckets (options shard_count /
     shard_index, xtn.nn_sharded): under torchrun every rank (one GPU each) searches its share of
     the buckets of the same input, the verified pairs are exchanged by owner over NCCL and
-    merged; one step is the whole search over all ranks (strong scaling), timed on the device
+    merged; with --shard-by sequences (xtn.nn_sharded_exchange) every rank generates its own
+    sequences' records and sends them to the bucket owners first; one step is the whole search over all ranks (strong scaling), timed on the device
     from the search's start to the merge's end, slowest rank. On one process, --shards K runs
     the K shards one after another on the one GPU and exchanges on the device with the same
     splits (per-shard and merge times reported): what each rank of a K-GPU run would compute,
@@ -865,8 +866,61 @@ def run_sharded(args, w):
     torch.cuda.synchronize()
     unsharded = ctx.nn_device(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
 
+    by_seq = args.shard_by == "sequences"
+
     def one_rank():
-        return xtn.nn_sharded(ctx, d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+        search = xtn.nn_sharded_exchange if by_seq else xtn.nn_sharded
+        return search(ctx, d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"])
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        r = fn()
+        e1.record(ext)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    def emulated_exchange():
+        """Sequence sharding: every rank's generate, then every owner's search over the pieces
+        the ranks send it, then every owner's merge, in sequence on the one GPU. A rank's records
+        are copied out of the context before the next rank's generate reuses its buffer; that copy
+        and the gathering of an owner's pieces stand in for the all-to-all and are not timed."""
+        gen_ms, sent_recs, counts = [], [], []
+        for r in range(K):
+            (cnt, ptr, nrec), ms = timed(lambda: ctx.shard_generate(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"],
+                                                                    w["measure"], r, K))
+            gen_ms.append(ms)
+            counts.append(cnt.astype(np.int64))
+            sent_recs.append(torch.as_tensor(xtn._DeviceWords(ptr, nrec), device="cuda").clone() if nrec else None)
+        bounds = xtn.owner_ranges(sum(counts), K)
+        cums = [np.concatenate([[0], np.cumsum(c)]) for c in counts]
+        search_ms, sent_keys, remote = [], [], 0
+        for k in range(K):
+            lo, hi = bounds[k], bounds[k + 1]
+            parts = [sent_recs[r][int(cums[r][lo]): int(cums[r][hi])] for r in range(K)
+                     if sent_recs[r] is not None and cums[r][hi] > cums[r][lo]]
+            remote += sum(int(cums[r][hi] - cums[r][lo]) for r in range(K) if r != k)
+            got = torch.cat(parts) if parts else torch.zeros(1, dtype=torch.int64, device="cuda")
+            pcs = np.stack([c[lo:hi] for c in counts]).astype(np.uint64)
+            torch.cuda.synchronize()
+
+            def search():
+                m = ctx.shard_search(d_chars.data_ptr(), d_offs.data_ptr(), n, w["d"], w["measure"], got.data_ptr(), pcs)
+                keys = torch.empty(max(m, 1), dtype=torch.int64, device="cuda")
+                return keys, ctx.result_keys(n, keys.data_ptr(), keys.numel(), K)
+
+            kst, ms = timed(search)
+            search_ms.append(ms)
+            sent_keys.append(kst)
+            del got
+        del sent_recs
+        merge_ms, total = [], 0
+        for dst in range(K):
+            got = torch.cat([keys[st[dst]: st[dst + 1]] for keys, st in sent_keys])
+            u, ms = timed(lambda: ctx.merge_keys(n, got.data_ptr(), got.numel()))
+            total += u
+            merge_ms.append(ms)
+        return total, gen_ms, search_ms, merge_ms, remote * 8
 
     def emulated():
         shard_ms, sent = [], []
@@ -906,6 +960,15 @@ def run_sharded(args, w):
             e1.record()
             e1.synchronize()
             ms = e0.elapsed_time(e1)
+        elif by_seq:
+            out, gen_ms, search_ms, merge_ms, sent_bytes = emulated_exchange()
+            ms = sum(gen_ms) + sum(search_ms) + sum(merge_ms)
+            if i >= args.warmup:
+                detail = (detail or [np.zeros(K), np.zeros(K), np.zeros(K), 0])
+                detail[0] += np.array(gen_ms) / args.steps
+                detail[1] += np.array(search_ms) / args.steps
+                detail[2] += np.array(merge_ms) / args.steps
+                detail[3] = sent_bytes
         else:
             out, shard_ms, merge_ms = emulated()
             ms = sum(shard_ms) + sum(merge_ms)
@@ -942,12 +1005,21 @@ def run_sharded(args, w):
         "data": "synthetic (seeded CDR3 generator)",
         "config": {"workload": args.workload, "n_seqs": n, "distance": w["d"],
                    "measure": "hamming" if w["measure"] else "leven", "mode": "nn",
-                   "parallelism": f"shards x{K}" + ("" if world > 1 else " run in sequence on one GPU"),
+                   "parallelism": f"shards x{K} by {args.shard_by}" + ("" if world > 1 else " run in sequence on one GPU"),
                    "l2": "flushed between steps (256 MiB write)"},
         "output_entries": out,
         "output_matches_unsharded": out == unsharded,
     }
-    if detail is not None:
+    if detail is not None and by_seq:
+        line["shards_one_gpu"] = {
+            "generate_ms": [round(float(x), 3) for x in detail[0]],
+            "search_ms": [round(float(x), 3) for x in detail[1]],
+            "merge_ms": [round(float(x), 3) for x in detail[2]],
+            "records_sent_to_other_ranks_bytes": int(detail[3]),
+            "what": "each rank's generate of its own sequences' records, each owner's search over the "
+                    "records sent to it + key packing, then each owner's merge, one after another on one "
+                    "GPU (the two all-to-alls between them are not run)"}
+    elif detail is not None:
         line["shards_one_gpu"] = {
             "shard_ms": [round(float(x), 3) for x in detail[0]],
             "merge_ms": [round(float(x), 3) for x in detail[1]],
@@ -977,6 +1049,10 @@ def main():
     ap.add_argument("--shards", type=int, default=0,
                     help="sharded search: under torchrun one shard per rank (any value > 0); on one process, "
                          "this many shards run in sequence on the one GPU")
+    ap.add_argument("--shard-by", choices=["buckets", "sequences"], default="buckets",
+                    help="sharding: every rank generates all variants and keeps its first-level buckets "
+                         "(buckets), or generates its own sequences' variants and sends records to the "
+                         "bucket owners (sequences)")
     args = ap.parse_args()
     if args.workload in SERVE_WORKLOADS:
         if args.impl == "reference":

@@ -155,6 +155,29 @@ int xtn_context_result_keys(xtn_context* ctx, int32_t n_seqs, uint64_t* d_keys, 
                             int64_t* range_starts);
 int xtn_context_merge_keys(xtn_context* ctx, int32_t n_seqs, const uint64_t* d_keys, int64_t count, int64_t* n_out);
 
+/* Sharded search with a record exchange (the reference has no counterpart): every rank holds
+ * the whole input and generates only the deletion variants of its own sequences
+ * [rank n / K, (rank + 1) n / K).
+ * xtn_shard_generate (rank `rank` of n_ranks): checks the lengths, packs all sequences (every
+ * rank derives the same first-level shape from the whole search), generates and partitions its
+ * own sequences' variant records into the search's first-level buckets. *n_buckets receives the
+ * bucket count, bucket_counts[0..min(cap, n_buckets)) the records per bucket, *d_records /
+ * *n_records the partitioned records in device memory (held by the context, valid until its
+ * next call; bucket b's records follow bucket b - 1's). Needs distance <= 2 and the default
+ * options key_tables = 1 and stage_chunk = 4096.
+ * xtn_shard_search: d_records holds the n_pieces pieces a rank received for the b_n buckets it
+ * owns (a contiguous range of the search's buckets), one after another; piece p holds
+ * piece_counts[p * b_n + k] records of the rank's k-th bucket, in bucket order. The pieces are
+ * gathered into contiguous buckets, split, grouped, de-duplicated, sorted and verified; the
+ * verified pairs become the context's result (*n_out of them), to be exchanged by owner with
+ * xtn_context_result_keys / xtn_context_merge_keys. */
+int xtn_shard_generate(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                       int32_t n_seqs, int32_t rank, int32_t n_ranks, uint64_t* bucket_counts, int32_t cap,
+                       int32_t* n_buckets, const uint64_t** d_records, int64_t* n_records);
+int xtn_shard_search(xtn_context* ctx, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                     int32_t n_seqs, const uint64_t* d_records, const uint64_t* piece_counts, int32_t n_pieces,
+                     int32_t b_n, int64_t* n_out);
+
 /* The CUDA stream the context launches on (as a cudaStream_t cast to void*). */
 void* xtn_context_stream(xtn_context* ctx);
 

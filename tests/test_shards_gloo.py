@@ -91,3 +91,17 @@ def test_three_rank_exchange_restores_the_output():
         x = res[r] >> (13 + 8)
         lo, hi = -(-r * 5000 // WORLD), -(-(r + 1) * 5000 // WORLD)
         assert len(x) == 0 or (x.min() >= lo and x.max() < hi)
+
+
+def test_owner_ranges_cover_the_buckets_in_order():
+    sys.path.insert(0, os.path.join(ROOT, "xt-neighbor_b200"))
+    import xtn
+
+    rng = np.random.default_rng(7)
+    for K in (1, 2, 3, 8):
+        counts = rng.integers(0, 1000, 512)
+        b = xtn.owner_ranges(counts, K)
+        assert b[0] == 0 and b[-1] == 512 and all(x <= y for x, y in zip(b, b[1:])) and len(b) == K + 1
+        starts = np.concatenate([[0], np.cumsum(counts)])
+        for k in range(1, K):  # rank k starts at the bucket holding record k V / K
+            assert starts[b[k]] >= starts[-1] * k // K and (b[k] == 0 or starts[b[k] - 1] < starts[-1] * k // K)

@@ -530,24 +530,25 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
 // merges before they reach DRAM (two CTAs of 512 threads per SM at 64 registers; a bound of
 // three CTAs measured slower: 6.46 against 5.55 ms at 10M, one thread per sequence instead of
 // the balanced tasks 12.7 ms, and whole run-pair tasks instead of halves 7.2 ms). abort (graph
-// form, may be null): the records would not fit.
+// form, may be null): the records would not fit. The tiles cover sequences [seq0, n), whose
+// records start at record rec0 = voff[seq0] (a shard of a search: flat holds only those).
 template <int THREADS, int MIN_CTAS>
 __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
     const uint8_t* __restrict__ klen, const uint64_t* __restrict__ runinfo, const uint64_t* __restrict__ tab,
     const uint64_t* __restrict__ voff, const uint64_t* __restrict__ toff, const uint32_t* __restrict__ task_seq, int n,
     int tile, int d, int b1, int idbits, uint64_t* __restrict__ flat, uint32_t* __restrict__ counts,
-    const unsigned int* __restrict__ abort) {
+    const unsigned int* __restrict__ abort, int seq0, uint64_t rec0) {
     extern __shared__ uint32_t s_hist[];
     if (abort && *abort) return;
     const int nb = 1 << b1;
     for (int b = threadIdx.x; b < nb; b += THREADS) s_hist[b] = 0;
     __syncthreads();
-    const int t0 = min(n, blockIdx.x * tile);
+    const int t0 = (int)min((int64_t)n, (int64_t)seq0 + (int64_t)blockIdx.x * tile);
     const int t1 = min(n, t0 + tile);
     const int shift = 64 - b1;
     const uint64_t hi_mask = ~((1ull << idbits) - 1ull);
     if (t0 < t1) {
-        uint64_t* out = flat + voff[t0];
+        uint64_t* out = flat + (voff[t0] - rec0);
         chunk_hashes<THREADS>(klen, runinfo, tab, voff, toff, task_seq, t0, t1, d,
                                     [&](uint32_t pos, uint64_t h, int i) {
                                         atomicAdd(&s_hist[(uint32_t)(h >> shift)], 1u);
@@ -560,6 +561,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) k_bucket_gen(
 }
 
 // k_bucket_partition: tile t's records, flat[voff[t * tile] .. voff[min(n, (t + 1) * tile)]),
+// (tiles from sequence seq0 on, flat starting at record rec0 = voff[seq0], as k_bucket_gen)
 // through the staged partition into their first-level buckets in `recs`: bucket b's records of
 // tile t start at bstart[b] + offsets[t][b]; the top b1 bits are dropped on the way
 // (strip_bucket). Chunk c reaches shared memory by one bulk copy, issued as soon as chunk c - 1
@@ -570,19 +572,20 @@ template <class C>
 __global__ void __launch_bounds__(C::kThreads) k_bucket_partition(
     const uint64_t* __restrict__ flat, const uint64_t* __restrict__ voff, int n, int tile, int b1, int idbits,
     const uint32_t* __restrict__ offsets, const uint64_t* __restrict__ bstart, uint64_t* __restrict__ recs,
-    unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
+    unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort, int seq0, uint64_t rec0) {
     constexpr int T = C::kThreads;
     if (abort && *abort) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
     const int nb = 1 << b1;
-    const int t0 = min(n, blockIdx.x * tile);  // (tiles past the last sequence are empty)
+    // (tiles past the last sequence are empty)
+    const int t0 = (int)min((int64_t)n, (int64_t)seq0 + (int64_t)blockIdx.x * tile);
     const int t1 = min(n, t0 + tile);
     const uint32_t* off = offsets + (size_t)blockIdx.x * nb;
     for (int b = threadIdx.x; b < nb; b += T) S.gcur[b] = (uint32_t)bstart[b] + off[b];
     const uint64_t r0 = voff[t0];
     const uint32_t size = (uint32_t)(voff[t1] - r0);
-    const uint64_t* src = flat + r0;
+    const uint64_t* src = flat + (r0 - rec0);
     const uint32_t mbar = smem_u32(&S.mbar);
     auto issue = [&](uint32_t c0) {
         const uint32_t m = min((uint32_t)C::kChunk, size - c0);
@@ -848,6 +851,20 @@ __global__ void __cluster_dims__(kSlices, 1, 1) __launch_bounds__(C::kThreads, s
             if (threadIdx.x == 0 && c0 + kStageChunk < size) issue(c0 + kStageChunk);
         });
     }
+}
+
+// ------------------------------------------------------------------ shard exchange
+// A run of records copied from `src` to `dst` (received pieces gathered into contiguous
+// first-level buckets).
+struct GatherRun {
+    uint64_t src, dst;
+    uint64_t size;
+};
+
+__global__ void k_gather_runs(const GatherRun* __restrict__ runs, const uint64_t* __restrict__ src,
+                              uint64_t* __restrict__ dst) {
+    const GatherRun r = runs[blockIdx.x];
+    for (uint64_t i = threadIdx.x; i < r.size; i += blockDim.x) dst[r.dst + i] = src[r.src + i];
 }
 
 // ------------------------------------------------------------------ slotted split

@@ -546,6 +546,7 @@ struct xtn_context {
     cudaEvent_t ev_round[2] = {};
     DevBuf pairA2, ddcnt;
     DevBuf scur;             // sub-bucket cursors of the slotted split
+    DevBuf gruns;            // shard exchange: runs gathered into contiguous first-level buckets
     // graph form of the device-resident search (option "graph")
     int graph_mode = 0;
     void* graph = nullptr;  // GraphState (below)
@@ -946,6 +947,19 @@ static int bucket_reserve(xtn_context* c, const BucketPlan& bp, int n, int d, ui
     return XTN_SUCCESS;
 }
 
+// The generation tasks of the n sequences at d = 2 (counts, offsets toff, task -> sequence map);
+// the buffers come from bucket_reserve.
+static int build_task_map(xtn_context* c, int n, BucketPlan* bp) {
+    cudaStream_t s = c->stream;
+    XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
+                                                                               P<uint32_t>(c->tcnt)));
+    XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
+    XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n, kTaskSeqThreads), kTaskSeqThreads, 0, s>>>(
+                               P<uint64_t>(c->toff), n, P<uint32_t>(c->tseq)));
+    bp->tseq = P<uint32_t>(c->tseq);
+    return XTN_SUCCESS;
+}
+
 // one_round: the search keeps every record at once (no rounds, no shards), which the
 // generate-then-partition first level (option flat_gen) needs: it holds all V records twice.
 // abort (graph form, may be null): the generation does nothing when it is set.
@@ -958,14 +972,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
     const size_t hist_smem = sizeof(uint32_t) * nb;
     XTN_TRY(bucket_reserve(c, *bp, n, d, V));
     XTN_TRY(bucket_attrs(c));
-    if (bp->staged && d >= 2) {
-        XTN_LAUNCH("task_counts", k_task_counts<<<blocks_for(n), kThreads, 0, s>>>(P<uint64_t>(c->runinfo), n,
-                                                                                   P<uint32_t>(c->tcnt)));
-        XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->tcnt), P<uint64_t>(c->toff), n));
-        XTN_LAUNCH("task_seq", k_task_seq<<<blocks_for(n, kTaskSeqThreads), kTaskSeqThreads, 0, s>>>(P<uint64_t>(c->toff), n,
-                                                                             P<uint32_t>(c->tseq)));
-        bp->tseq = P<uint32_t>(c->tseq);
-    }
+    if (bp->staged && d >= 2) XTN_TRY(build_task_map(c, n, bp));
     if (bp->flat) {
         // every record in sequence order into recB, with the per-tile histograms
         XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
@@ -973,7 +980,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
         XTN_LAUNCH("bucket_gen", (k_bucket_gen<kBucketThreads, 2><<<ntiles, kBucketThreads, hist_smem, s>>>(
                                      P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
                                      P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp->tseq, n, tile, d, b1,
-                                     id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), abort)));
+                                     id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), abort, 0, 0ull)));
     } else {
         XTN_LAUNCH("bucket_count", k_bucket_count<<<ntiles, kBucketThreads, hist_smem, s>>>(
                                        P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
@@ -1028,7 +1035,7 @@ static void launch_partition(xtn_context* c, const BucketPlan& bp, int n, int id
     XTN_LAUNCH("bucket_partition",
                k_bucket_partition<StageHuge><<<bp.ntiles, StageHuge::kThreads, sizeof(StageSmem<StageHuge>), s>>>(
                    P<uint64_t>(c->recB), P<uint64_t>(c->voff), n, bp.tile, bp.b1, idbits, P<uint32_t>(c->boffs),
-                   P<uint64_t>(c->bstart), P<uint64_t>(c->recA), P<unsigned int>(c->bcnt), abort));
+                   P<uint64_t>(c->bstart), P<uint64_t>(c->recA), P<unsigned int>(c->bcnt), abort, 0, 0ull));
 }
 
 // The staged first-level scatter in the context's stage shape (stage_chunk 2048, 4096 or 8192).
@@ -1052,7 +1059,8 @@ static void launch_scatter_staged(xtn_context* c, const BucketPlan& bp, int n, i
 // from index `at` (grown, keeping entries [0, at), when they do not fit). *Pc receives the
 // number of candidates of the round.
 static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int idbits, uint32_t b_lo, uint32_t b_n,
-                        uint64_t base, uint64_t Vr, DevBuf& out, uint64_t at, uint64_t* Pc) {
+                        uint64_t base, uint64_t Vr, DevBuf& out, uint64_t at, uint64_t* Pc,
+                        bool first_level_done = false) {
     cudaStream_t s = c->stream;
     const int b1 = bp.b1, nb = bp.nb;
     uint64_t sub_bound = 0, recb = 0;
@@ -1063,7 +1071,9 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     const uint64_t* bstart = P<uint64_t>(c->bstart);
     XTN_TRY(ensure(c->bcnt, 64));
     XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
-    if (bp.flat) {
+    if (first_level_done) {
+        // (recA and bstart hold the round's first-level buckets already: the shard exchange)
+    } else if (bp.flat) {
         launch_partition(c, bp, n, idbits, nullptr, s);
     } else if (bp.staged) {
         launch_scatter_staged(c, bp, n, d, idbits, b_lo, b_n, base, nullptr, s);
@@ -1441,6 +1451,13 @@ static int candidates_rounds(xtn_context* c, const BucketPlan& bp, int n, int d,
 // The nearest-neighbour pipeline on device-resident input. rows (optional) maps search index
 // -> CSR row. On success the result is in c->out_pairs / c->out_dist, c->n_out entries; the
 // verified pair list in sorted (x, y) order of search indexes.
+static int nn_tail(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n, int d,
+                   int measure, uint64_t Pc, bool distinct);
+static int pack_and_count(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n,
+                          int d, bool validate, uint64_t* V_out);
+static int nn_after_count(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n,
+                          int d, int measure, uint64_t V);
+
 static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n, int d,
                   int measure, bool validate) {
     xtn_stats& st = c->stats;
@@ -1451,6 +1468,25 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     st.id_bits = idbits;
     cudaStream_t s = c->stream;
     XTN_CK(cudaEventRecord(c->ev[0], s));
+    uint64_t V = 0;
+    XTN_TRY(pack_and_count(c, chars, offs, rows, n, d, validate, &V));
+    st.n_variants = (int64_t)V;
+    if (c->shard_count > 1 && (c->engine != 0 || c->shard_index >= c->shard_count)) {
+        set_err(c->engine != 0 ? "sharding needs the bucket engine (engine 0)"
+                               : "shard_index must be below shard_count");
+        return XTN_ERR_ARG;
+    }
+    if (c->engine == 1 && V >= (uint64_t)UINT32_MAX) {
+        set_err("too many deletion variants for the sort engine's one round (" + std::to_string(V) + ")");
+        return XTN_ERR_LIMIT;
+    }
+    return nn_after_count(c, chars, offs, rows, n, d, measure, V);
+}
+
+// Length check (validate), pack and variant offsets of a search; *V receives the variant count.
+static int pack_and_count(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n,
+                          int d, bool validate, uint64_t* V_out) {
+    cudaStream_t s = c->stream;
     if (validate) XTN_TRY(launch_length_check(c, offs, rows, n));
 
     // pack + variant counts
@@ -1480,16 +1516,16 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
                 " look-back waits (radix sort or scan) did not complete in time");
         return XTN_ERR_CUDA;
     }
-    st.n_variants = (int64_t)V;
-    if (c->shard_count > 1 && (c->engine != 0 || c->shard_index >= c->shard_count)) {
-        set_err(c->engine != 0 ? "sharding needs the bucket engine (engine 0)"
-                               : "shard_index must be below shard_count");
-        return XTN_ERR_ARG;
-    }
-    if (c->engine == 1 && V >= (uint64_t)UINT32_MAX) {
-        set_err("too many deletion variants for the sort engine's one round (" + std::to_string(V) + ")");
-        return XTN_ERR_LIMIT;
-    }
+    *V_out = V;
+    return XTN_SUCCESS;
+}
+
+// The search from its variant offsets on: candidate pairs (bucket or sort engine, in rounds
+// when needed), then nn_tail.
+static int nn_after_count(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n,
+                          int d, int measure, uint64_t V) {
+    xtn_stats& st = c->stats;
+    const int idbits = id_bits_for(n);
 
     // candidate pairs: every (min id, max id) of every group of equal variant hashes
     uint64_t Pc = 0;
@@ -1521,6 +1557,18 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
         c->last_pc_per_rec = V ? (double)Pc / (double)V : 0.0;
         st.n_candidates = (int64_t)Pc;
     }
+    return nn_tail(c, chars, offs, rows, n, d, measure, Pc, distinct);
+}
+
+// The end of a nearest-neighbour search once its candidate pairs are known: Pc candidates in
+// c->pairA (distinct = false), or Pc distinct pairs in c->pairB (distinct = true, rounds); the
+// candidates are de-duplicated (hash set), sorted, verified and compacted into the context's
+// result. The statistics' stage times run from event 0, recorded by the caller.
+static int nn_tail(xtn_context* c, const uint8_t* chars, const uint32_t* offs, const int32_t* rows, int n, int d,
+                   int measure, uint64_t Pc, bool distinct) {
+    xtn_stats& st = c->stats;
+    cudaStream_t s = c->stream;
+    const int idbits = id_bits_for(n);
     if (Pc >= (uint64_t)UINT32_MAX) {
         set_err("too many " + std::string(distinct ? "distinct" : "candidate") + " pairs (" + std::to_string(Pc) + ")");
         return XTN_ERR_LIMIT;
@@ -1591,7 +1639,12 @@ static int run_nn(xtn_context* c, const uint8_t* chars, const uint32_t* offs, co
     // unique candidates = number of distinct pairs; counted from the verify flags' input side
     float ms = 0;
     for (int k = 0; k < S_COUNT; k++) {
-        cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+        // a stage that a search form skips leaves its event unrecorded: its time reads as 0,
+        // and the query's error is cleared so that no later cudaGetLastError reports it
+        if (cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]) != cudaSuccess) {
+            ms = 0;
+            (void)cudaGetLastError();
+        }
         st.ms_stage[k] = ms;
     }
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[S_COUNT]);
@@ -2276,7 +2329,7 @@ static std::vector<DevBuf*> context_buffers(xtn_context* c) {
         &c->out_dist, &c->out_freq, &c->bcounts,   &c->boffs,    &c->btotals,    &c->bstart,   &c->bdesc,
         &c->bjobs,   &c->bfall,     &c->bcnt,      &c->fbA,      &c->fbB,        &c->runinfo,  &c->tcnt,
         &c->toff,    &c->ktab,      &c->info,      &c->lencheck, &c->pairA2,     &c->ddcnt,    &c->tseq,
-        &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status, &c->scur};
+        &c->os_scratch, &c->os_status, &c->dev_err, &c->dd_table, &c->scan_status, &c->scur, &c->gruns};
     if (c->overlap_bufs) {
         xtn_overlap_bufs* ob = reinterpret_cast<xtn_overlap_bufs*>(c->overlap_bufs);
         for (DevBuf* b : {&ob->freq, &ob->rep, &ob->recA, &ob->recB, &ob->head, &ob->uidx, &ob->rep_row,
@@ -3252,6 +3305,200 @@ int xtn_context_merge_keys(xtn_context* c, int32_t n_seqs, const uint64_t* d_key
     c->stats.n_seqs = n_seqs;
     if (n_out) *n_out = c->n_out;
     return XTN_SUCCESS;
+}
+
+// ------------------------------------------------------------------ sharded search with exchange
+// One search over K ranks, each holding the whole input (for verification) and generating the
+// variants of its own sequences [rank n / K, (rank + 1) n / K) only. xtn_shard_generate:
+// length check, pack and variant offsets of all sequences (the first-level shape depends on
+// the whole search, so every rank derives the same one), then the two-pass first level over the
+// rank's own sequences: their records, partitioned into the search's first-level buckets, in
+// the context's record buffer A, and the per-bucket counts on the host. The ranks then sum the
+// counts, give each rank a contiguous range of buckets, and send each owner its buckets'
+// records (xtn.nn_sharded_exchange: two all-to-alls). xtn_shard_search gathers what a rank
+// received into contiguous buckets and runs the rest of the search on them (plan, split,
+// grouping, pair dedup, sort, verification); the exchange of verified pairs by owner follows.
+extern "C" int xtn_shard_generate(xtn_context* c, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                                  int32_t n, int32_t rank, int32_t n_ranks, uint64_t* bucket_counts, int32_t cap,
+                                  int32_t* n_buckets, const uint64_t** d_records, int64_t* n_records) {
+    if (!c || !d_seqs || !d_offsets || n < 1 || n_ranks < 1 || n_ranks > kMaxShards || rank < 0 || rank >= n_ranks ||
+        !n_buckets || !d_records || !n_records || (cap > 0 && !bucket_counts)) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    const int d = args->distance;
+    if (d > 2 || !c->key_tables || c->stage_chunk != 4096) {
+        set_err("the sharded exchange needs distance <= 2, the key tables and stage_chunk 4096");
+        return XTN_ERR_ARG;
+    }
+    XTN_CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    begin_run(c);
+    const uint8_t* chars = reinterpret_cast<const uint8_t*>(d_seqs);
+    xtn_stats& st = c->stats;
+    memset(&st, 0, sizeof st);
+    st.n_seqs = n;
+    st.id_bits = id_bits_for(n);
+    uint64_t V = 0;
+    int r = pack_and_count(c, chars, d_offsets, nullptr, n, d, true, &V);
+    if (r != XTN_SUCCESS) {
+        end_run(c);
+        return r;
+    }
+    st.n_variants = (int64_t)V;
+    BucketPlan bp;
+    bucket_shape(c, n, d, V, &bp, true);
+    const int nb = bp.nb, b1 = bp.b1;
+    // this rank's sequences and their tiles (the partition and the histograms use the same)
+    const int s0 = (int)((int64_t)n * rank / n_ranks), s1 = (int)((int64_t)n * (rank + 1) / n_ranks);
+    const int nr = s1 - s0;
+    const int64_t wave = (int64_t)c->sms * ctas_per_sm_for<ScatterSmem<StageLarge>>();
+    const int ntiles = nr > 0 ? (int)(wave * std::max<int64_t>(1, ((int64_t)nr + wave * 4096 - 1) / (wave * 4096))) : 0;
+    const int tile = ntiles > 0 ? (nr + ntiles - 1) / ntiles : 1;
+    uint64_t rec0 = 0, rec1 = 0;
+    r = read_scalar(c, P<uint64_t>(c->voff) + s0, 8, &rec0);
+    if (r == XTN_SUCCESS) r = read_scalar(c, P<uint64_t>(c->voff) + s1, 8, &rec1);
+    const uint64_t Vr = rec1 - rec0;
+    if (r == XTN_SUCCESS && Vr >= (uint64_t)UINT32_MAX - (uint64_t(1) << 20)) {
+        set_err("too many records for one rank (" + std::to_string(Vr) + "): use more ranks");
+        r = XTN_ERR_LIMIT;
+    }
+    auto run = [&]() -> int {
+        XTN_TRY(bucket_reserve(c, bp, n, d, V));
+        XTN_TRY(ensure(c->bcounts, sizeof(uint32_t) * (size_t)std::max(1, ntiles) * nb));
+        XTN_TRY(ensure(c->boffs, sizeof(uint32_t) * (size_t)std::max(1, ntiles) * nb));
+        XTN_TRY(bucket_attrs(c));
+        if (d >= 2) XTN_TRY(build_task_map(c, n, &bp));
+        XTN_TRY(ensure(c->recA, sizeof(uint64_t) * Vr + 64));
+        XTN_TRY(ensure(c->recB, sizeof(uint64_t) * Vr + 64));
+        XTN_TRY(ensure(c->bcnt, 64));
+        XTN_CK(cudaMemsetAsync(c->bcnt.p, 0, 64, s));
+        if (ntiles > 0) {
+            XTN_LAUNCH("bucket_gen", (k_bucket_gen<kBucketThreads, 2><<<ntiles, kBucketThreads, sizeof(uint32_t) * nb, s>>>(
+                                         P<uint8_t>(c->klen), P<uint64_t>(c->runinfo), P<uint64_t>(c->ktab),
+                                         P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp.tseq, s1, tile, d, b1,
+                                         id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), nullptr, s0,
+                                         rec0)));
+            XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
+                                             P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs),
+                                             P<uint32_t>(c->btotals)));
+            XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
+            XTN_LAUNCH("bucket_partition",
+                       k_bucket_partition<StageHuge><<<ntiles, StageHuge::kThreads, sizeof(StageSmem<StageHuge>), s>>>(
+                           P<uint64_t>(c->recB), P<uint64_t>(c->voff), s1, tile, b1, id_bits_for(n),
+                           P<uint32_t>(c->boffs), P<uint64_t>(c->bstart), P<uint64_t>(c->recA),
+                           P<unsigned int>(c->bcnt), nullptr, s0, rec0));
+        } else {
+            XTN_CK(cudaMemsetAsync(c->btotals.p, 0, sizeof(uint32_t) * nb, s));
+        }
+        XTN_CK(cudaGetLastError());
+        std::vector<uint32_t> tot(nb);
+        XTN_CK(cudaMemcpyAsync(tot.data(), c->btotals.p, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
+        XTN_CK(cudaStreamSynchronize(s));
+        uint32_t cnt[8];
+        memcpy(cnt, c->h_scalar, 32);
+        if (cnt[kCntWaitFail] != 0) {
+            set_err("bucket partition: " + std::to_string(cnt[kCntWaitFail]) + " chunk copies did not complete in time");
+            return XTN_ERR_CUDA;
+        }
+        for (int k = 0; k < nb && k < cap; k++) bucket_counts[k] = tot[k];
+        return XTN_SUCCESS;
+    };
+    if (r == XTN_SUCCESS) r = run();
+    end_run(c);
+    if (r != XTN_SUCCESS) return r;
+    *n_buckets = nb;
+    *d_records = P<uint64_t>(c->recA);
+    *n_records = (int64_t)Vr;
+    return XTN_SUCCESS;
+}
+
+extern "C" int xtn_shard_search(xtn_context* c, const xtn_args* args, const char* d_seqs, const uint32_t* d_offsets,
+                                int32_t n, const uint64_t* d_records, const uint64_t* piece_counts, int32_t n_pieces,
+                                int32_t b_n, int64_t* n_out) {
+    if (!c || !d_seqs || !d_offsets || n < 1 || n_pieces < 1 || b_n < 0 || (b_n > 0 && !piece_counts)) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    XTN_TRY(check_args(args));
+    XTN_CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const uint8_t* chars = reinterpret_cast<const uint8_t*>(d_seqs);
+    const int d = args->distance, idbits = id_bits_for(n);
+    // the buckets' totals and starts, and one gather run per (bucket, piece)
+    std::vector<uint64_t> bstart((size_t)b_n + 1, 0), piece_base((size_t)n_pieces + 1, 0);
+    for (int p = 0; p < n_pieces; p++) {
+        uint64_t t = 0;
+        for (int k = 0; k < b_n; k++) t += piece_counts[(size_t)p * b_n + k];
+        piece_base[p + 1] = piece_base[p] + t;
+    }
+    for (int k = 0; k < b_n; k++) {
+        uint64_t t = 0;
+        for (int p = 0; p < n_pieces; p++) t += piece_counts[(size_t)p * b_n + k];
+        bstart[k + 1] = bstart[k] + t;
+    }
+    const uint64_t V = bstart[b_n];
+    if (V > 0 && !d_records) {
+        set_err("invalid arguments");
+        return XTN_ERR_ARG;
+    }
+    if (V >= (uint64_t)UINT32_MAX - (uint64_t(1) << 20)) {
+        set_err("too many records for one rank's buckets (" + std::to_string(V) + ")");
+        return XTN_ERR_LIMIT;
+    }
+    std::vector<GatherRun> runs;
+    {
+        std::vector<uint64_t> in_piece(n_pieces, 0);
+        for (int k = 0; k < b_n; k++) {
+            uint64_t dst = bstart[k];
+            for (int p = 0; p < n_pieces; p++) {
+                const uint64_t m = piece_counts[(size_t)p * b_n + k];
+                if (m) runs.push_back(GatherRun{piece_base[p] + in_piece[p], dst, m});
+                in_piece[p] += m;
+                dst += m;
+            }
+        }
+    }
+    begin_run(c);
+    xtn_stats& st = c->stats;
+    memset(&st, 0, sizeof st);
+    st.n_seqs = n;
+    st.n_rounds = 1;
+    st.id_bits = idbits;
+    st.n_variants = (int64_t)V;
+    auto run = [&]() -> int {
+        XTN_CK(cudaEventRecord(c->ev[0], s));
+        XTN_TRY(ensure(c->recA, sizeof(uint64_t) * V + 64));
+        XTN_TRY(ensure(c->bstart, sizeof(uint64_t) * (b_n + 1)));
+        XTN_TRY(ensure(c->gruns, sizeof(GatherRun) * std::max<size_t>(1, runs.size())));
+        XTN_CK(cudaMemcpyAsync(c->bstart.p, bstart.data(), sizeof(uint64_t) * (b_n + 1), cudaMemcpyHostToDevice, s));
+        if (!runs.empty()) {
+            XTN_CK(cudaMemcpyAsync(c->gruns.p, runs.data(), sizeof(GatherRun) * runs.size(), cudaMemcpyHostToDevice, s));
+            XTN_LAUNCH("gather_runs", k_gather_runs<<<(unsigned)runs.size(), 256, 0, s>>>(P<GatherRun>(c->gruns), d_records,
+                                                                                         P<uint64_t>(c->recA)));
+        }
+        XTN_CK(cudaEventRecord(c->ev[1], s));
+        XTN_TRY(bucket_attrs(c));
+        BucketPlan bp;
+        bp.nb = b_n;
+        bp.slotted = c->split_slotted != 0;
+        uint64_t Pc = 0;
+        XTN_TRY(ensure(c->counter, 64));
+        if (b_n > 0) {
+            XTN_TRY(bucket_round(c, bp, n, d, idbits, 0, (uint32_t)b_n, 0, V, c->pairA, 0, &Pc, true));
+        } else {  // a rank that owns no bucket: the bucket stages take no time
+            for (int k = 2; k <= 4; k++) XTN_CK(cudaEventRecord(c->ev[k], s));
+        }
+        c->last_pc_per_rec = V ? (double)Pc / (double)V : 0.0;
+        st.n_candidates = (int64_t)Pc;
+        return nn_tail(c, chars, d_offsets, nullptr, n, d, args->measure, Pc, false);
+    };
+    const int r = run();
+    end_run(c);
+    if (r == XTN_SUCCESS && n_out) *n_out = c->n_out;
+    return r;
 }
 
 static std::mutex g_default_mu;

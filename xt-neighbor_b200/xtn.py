@@ -45,6 +45,8 @@ SYMBOLS = (
     "xtn_context_result_device",
     "xtn_context_result_keys",
     "xtn_context_merge_keys",
+    "xtn_shard_generate",
+    "xtn_shard_search",
     "xtn_context_stream",
     "xtn_context_stats",
     "xtn_context_set_option",
@@ -194,6 +196,11 @@ def load():
     lib.xtn_context_result_keys.argtypes = [P, ctypes.c_int32, P, ctypes.c_int64, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_merge_keys.argtypes = [P, ctypes.c_int32, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_shard_generate.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(P),
+                                       ctypes.POINTER(ctypes.c_int64)]
+    lib.xtn_shard_search.argtypes = [P, ctypes.POINTER(Args), P, P, ctypes.c_int32, P, P, ctypes.c_int32,
+                                     ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
     lib.xtn_context_stream.argtypes = [P]
     lib.xtn_context_stream.restype = P
     lib.xtn_context_stats.argtypes = [P, ctypes.POINTER(Stats)]
@@ -374,6 +381,34 @@ class Context:
         _check(self.lib.xtn_context_result_keys(self.h, n, ctypes.c_void_p(d_keys), capacity, n_ranges, starts))
         return list(starts)
 
+    def shard_generate(self, d_chars: int, d_offsets: int, n: int, distance: int, measure: int, rank: int,
+                       n_ranks: int):
+        """xtn_shard_generate: this rank's variant records in the search's first-level buckets.
+        Returns (per-bucket counts as uint64 array, device pointer of the records, record count)."""
+        args = Args(distance, measure, 0, 0)
+        cap = 1 << 15
+        counts = np.zeros(cap, np.uint64)
+        nb = ctypes.c_int32()
+        ptr = ctypes.c_void_p()
+        nrec = ctypes.c_int64()
+        _check(self.lib.xtn_shard_generate(self.h, ctypes.byref(args), ctypes.c_void_p(d_chars),
+                                           ctypes.c_void_p(d_offsets), n, rank, n_ranks,
+                                           counts.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(nb),
+                                           ctypes.byref(ptr), ctypes.byref(nrec)))
+        return counts[: nb.value].copy(), ptr.value or 0, nrec.value
+
+    def shard_search(self, d_chars: int, d_offsets: int, n: int, distance: int, measure: int, d_records: int,
+                     piece_counts) -> int:
+        """xtn_shard_search over the pieces a rank received (piece_counts: n_pieces x b_n)."""
+        args = Args(distance, measure, 0, 0)
+        pc = np.ascontiguousarray(piece_counts, dtype=np.uint64)
+        nout = ctypes.c_int64()
+        _check(self.lib.xtn_shard_search(self.h, ctypes.byref(args), ctypes.c_void_p(d_chars),
+                                         ctypes.c_void_p(d_offsets), n, ctypes.c_void_p(d_records),
+                                         pc.ctypes.data_as(ctypes.c_void_p), pc.shape[0], pc.shape[1],
+                                         ctypes.byref(nout)))
+        return nout.value
+
     def merge_keys(self, n: int, d_keys: int, count: int) -> int:
         """Sorts and de-duplicates received pair keys into the context's result
         (xtn_context_merge_keys); returns its length."""
@@ -468,6 +503,63 @@ def exchange_keys(keys, starts, group=None):
     out = torch.empty(sum(recv), dtype=torch.int64, device=keys.device)
     dist.all_to_all_single(out, keys[: starts[world]].contiguous(), recv, send, group=group)
     return out
+
+
+class _DeviceWords:
+    """A view of n int64 words of device memory for torch.as_tensor (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False), "version": 3}
+
+
+def owner_ranges(counts, n_ranks: int):
+    """First-level buckets of each rank: rank k owns [bounds[k], bounds[k + 1]), contiguous
+    ranges that start at the bucket holding record k V / K of the V records (the same rule as
+    the shard_count option's)."""
+    counts = np.asarray(counts, dtype=np.int64)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    total = int(starts[-1])
+    nb = len(counts)
+    bounds = [0]
+    for k in range(1, n_ranks):
+        b = int(np.searchsorted(starts[:nb], total * k // n_ranks, side="left"))
+        bounds.append(max(bounds[-1], b))
+    bounds.append(nb)
+    return bounds
+
+
+def nn_sharded_exchange(ctx, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN,
+                        group=None) -> int:
+    """One rank's part of a search sharded by sequences (xtn_shard_generate / xtn_shard_search):
+    every rank generates its own sequences' variant records in the first-level buckets; the
+    bucket counts are summed over the ranks, each rank gets a contiguous range of buckets, and
+    two all-to-alls send it its buckets' per-source counts and records; the rank then searches
+    its buckets, and the verified pairs are exchanged by owner and merged as in nn_sharded.
+    Returns the number of pairs left as the context's result (this rank's id range)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    counts, ptr, nrec = ctx.shard_generate(d_chars, d_offsets, n, distance, measure, rank, world)
+    local = torch.from_numpy(counts.astype(np.int64)).to(dev)
+    total = local.clone()
+    dist.all_reduce(total, group=group)
+    bounds = owner_ranges(total.cpu().numpy(), world)
+    cum = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+    # records: keys [cum[bounds[k]], cum[bounds[k+1]]) go to rank k
+    recs = torch.as_tensor(_DeviceWords(ptr, nrec), device=dev) if nrec > 0 else torch.zeros(1, dtype=torch.int64,
+                                                                                             device=dev)
+    got = exchange_keys(recs, [int(cum[b]) for b in bounds], group)
+    # per-bucket counts of the sent pieces: counts[bounds[k]:bounds[k+1]] go to rank k
+    got_counts = exchange_keys(local, bounds, group)
+    b_n = bounds[rank + 1] - bounds[rank]
+    piece_counts = got_counts.cpu().numpy().astype(np.uint64).reshape(world, b_n)
+    m = ctx.shard_search(d_chars, d_offsets, n, distance, measure, got.data_ptr(), piece_counts)
+    keys = torch.empty(max(m, 1), dtype=torch.int64, device=dev)
+    starts = ctx.result_keys(n, keys.data_ptr(), keys.numel(), world)
+    merged = exchange_keys(keys, starts, group)
+    return ctx.merge_keys(n, merged.data_ptr(), merged.numel())
 
 
 def nn_sharded(ctx, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN, group=None) -> int:
