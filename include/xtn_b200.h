@@ -250,6 +250,9 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *                     candidates and for n <= 2^24), 0 = every candidate is sorted,
  *                     2 = as 1 with the table always sized from the previous search's share
  *                     of distinct pairs (the sizing used above 256 MiB of table)
+ *   "dedup_slots_log2" 0 = size the one-round hash set as "pair_dedup" says (default);
+ *                     16..30 = its first table has 2^this slots (a table found too full is
+ *                     still regrown)
  *   "memory_budget"   bytes of device memory a search may hold (default 0: 80% of the free
  *                     device memory plus what the context holds, read only when one round
  *                     would need more than half of the device). A search whose variant
