@@ -182,17 +182,34 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const u128* __r
 }
 
 // counts/offsets are tile-major [tile][bucket]; offsets become the exclusive prefix over tiles.
-__global__ void k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles, int nb, uint32_t* __restrict__ offsets,
-                                 uint32_t* __restrict__ totals) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+// Per bucket, the exclusive prefix of its tile counts and its total. A block takes 32 buckets
+// (one per lane, so that every row read is one 128-byte line) and its warps split the tiles:
+// each warp sums its share, then writes its prefixes from the warps before it. (One thread per
+// bucket over all tiles, two blocks at 512 buckets, took 0.2 ms at 10M sequences.)
+constexpr int kColscanWarps = 32;
+
+__global__ void __launch_bounds__(kColscanWarps * 32) k_bucket_colscan(const uint32_t* __restrict__ counts, int ntiles,
+                                                                      int nb, uint32_t* __restrict__ offsets,
+                                                                      uint32_t* __restrict__ totals) {
+    __shared__ uint32_t s_part[kColscanWarps][33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int b = blockIdx.x * 32 + lane;
+    const int per = (ntiles + kColscanWarps - 1) / kColscanWarps;
+    const int t0 = min(ntiles, w * per), t1 = min(ntiles, t0 + per);
+    uint32_t sum = 0;
+    if (b < nb)
+        for (int t = t0; t < t1; t++) sum += counts[(size_t)t * nb + b];
+    s_part[w][lane] = sum;
+    __syncthreads();
     uint32_t run = 0;
-    for (int t = 0; t < ntiles; t++) {
-        uint32_t c = counts[(size_t)t * nb + b];
+    for (int k = 0; k < w; k++) run += s_part[k][lane];
+    if (b >= nb) return;
+    for (int t = t0; t < t1; t++) {
+        const uint32_t c = counts[(size_t)t * nb + b];
         offsets[(size_t)t * nb + b] = run;
         run += c;
     }
-    totals[b] = run;
+    if (w == kColscanWarps - 1) totals[b] = run;
 }
 
 // Counter words shared by the plan, split and grouping kernels (unsigned int counters[16]).
@@ -283,6 +300,70 @@ __device__ __forceinline__ void split_partition(StageSmem<C>& S, int nb, uint32_
     }
     __syncthreads();
     for (int b = threadIdx.x; b < nb; b += kStageThreads) S.gcur[b] += S.cnt[b] - S.lstart[b];
+    __syncthreads();
+}
+
+// The staged partition with one shared-memory atomic per record: the counting atomic returns the
+// record's rank within its bucket, kept in a register (bucket << 16 | rank; a chunk holds at most
+// 2^16 records and a stage at most 2^16 buckets) until the scan has placed the buckets, so that
+// no second ranking pass reads the chunk again. KEEP: the records stay in registers as well, the
+// chunk buffer is free once every thread has read it, and after_read() (the next chunk's bulk
+// copy) runs before the scan instead of after the ranking. (k_bucket_partition: 4.90 against
+// 5.10 ms at 10M.)
+template <class C, bool KEEP, class Bkt, class Hook>
+__device__ __forceinline__ void split_partition_ranked(StageSmem<C>& S, int nb, uint32_t m, const uint64_t* r,
+                                                       Bkt&& bkt, uint64_t* __restrict__ dst, Hook&& after_read,
+                                                       int strip, int idbits) {
+    constexpr int T = C::kThreads, kFanPer = C::kFanPer, kPer = C::kPer;
+    static_assert(C::kChunk <= 65536 && C::kFan <= 65536, "rank word");
+    for (int b = threadIdx.x; b < nb; b += T) S.cnt[b] = 0;
+    __syncthreads();
+    uint32_t rk[kPer];
+    uint64_t xs[KEEP ? kPer : 1];
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const uint32_t p = threadIdx.x + (uint32_t)k * T;
+        rk[k] = ~0u;
+        if (p < m) {
+            const uint64_t x = r[p];
+            if (KEEP) xs[k] = x;
+            const uint32_t b = bkt(x);
+            rk[k] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
+        }
+    }
+    __syncthreads();
+    if (KEEP) after_read();
+    {
+        uint32_t tot, loc[kFanPer], sum = 0;
+        const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++) {
+            loc[k] = sum;
+            sum += (b0 + k < nb) ? S.cnt[b0 + k] : 0u;
+        }
+        const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
+#pragma unroll
+        for (int k = 0; k < kFanPer; k++)
+            if (b0 + k < nb) S.lstart[b0 + k] = ex + loc[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        if (rk[k] == ~0u) continue;
+        const uint32_t b = rk[k] >> 16;
+        const uint32_t q = S.lstart[b] + (rk[k] & 0xffffu);
+        S.sorted[q] = KEEP ? xs[k] : r[threadIdx.x + (uint32_t)k * T];
+        S.sbkt[q] = (uint16_t)b;
+    }
+    __syncthreads();
+    if (!KEEP) after_read();
+    for (uint32_t q = threadIdx.x; q < m; q += T) {
+        const uint16_t b = S.sbkt[q];
+        const uint64_t x = S.sorted[q];
+        dst[S.gcur[b] + (q - S.lstart[b])] = strip ? strip_bucket(x, strip, idbits) : x;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += T) S.gcur[b] += S.cnt[b];
     __syncthreads();
 }
 
@@ -529,7 +610,11 @@ __global__ void __launch_bounds__(C::kThreads, ctas_per_sm_for<ScatterSmem<C>>()
 // is stored straight to its slot; a lane's consecutive variants fill whole sectors, which L2
 // merges before they reach DRAM (two CTAs of 512 threads per SM at 64 registers; a bound of
 // three CTAs measured slower: 6.46 against 5.55 ms at 10M, one thread per sequence instead of
-// the balanced tasks 12.7 ms, and whole run-pair tasks instead of halves 7.2 ms). abort (graph
+// the balanced tasks 12.7 ms, and whole run-pair tasks instead of halves 7.2 ms. Ordering the
+// tasks by item count within groups of 32 sequences, so that a warp's loops have equal length
+// (95% instead of 83% of its issue slots busy), measured slower too: 7.1 ms, as a warp's lanes
+// then read 32 sequences' table rows and write into 32 sequences' records per instruction
+// instead of two or three; 14.2 ms within groups of 256). abort (graph
 // form, may be null): the records would not fit. The tiles cover sequences [seq0, n), whose
 // records start at record rec0 = voff[seq0] (a shard of a search: flat holds only those).
 template <int THREADS, int MIN_CTAS>
@@ -626,9 +711,10 @@ __global__ void __launch_bounds__(C::kThreads) k_bucket_partition(
             return;
         }
         const int shift = 64 - b1;
-        split_partition(S, nb, m, S.rec + lead, [shift](uint64_t x) { return (uint32_t)(x >> shift); }, recs, [&] {
-            if (threadIdx.x == 0 && c0 + C::kChunk < size) issue(c0 + C::kChunk);
-        }, b1, idbits);
+        split_partition_ranked<C, true>(S, nb, m, S.rec + lead, [shift](uint64_t x) { return (uint32_t)(x >> shift); },
+                                        recs, [&] {
+                                            if (threadIdx.x == 0 && c0 + C::kChunk < size) issue(c0 + C::kChunk);
+                                        }, b1, idbits);
     }
 }
 
@@ -957,6 +1043,8 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
                 }
         }
         __syncthreads();
+        // (the ranks kept in registers from the counting pass, as split_partition_ranked does,
+        // measured slower here: 5.53 against 5.44 ms at 10M)
         for (uint32_t p = threadIdx.x; p < m; p += T) {
             const uint64_t x = r[p];
             const uint32_t b = split_sub(x, nsub);

@@ -1033,7 +1033,7 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
                                        P<u128>(c->keys), P<uint8_t>(c->klen), P<uint64_t>(c->runinfo),
                                        tables ? P<uint64_t>(c->ktab) : nullptr, n, tile, d, b1, P<uint32_t>(c->bcounts)));
     }
-    XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
+    XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<(nb + 31) / 32, kColscanWarps * 32, 0, s>>>(
                                      P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs), P<uint32_t>(c->btotals)));
     XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
     XTN_CK(cudaGetLastError());
@@ -3429,7 +3429,7 @@ extern "C" int xtn_shard_generate(xtn_context* c, const xtn_args* args, const ch
                                          P<uint64_t>(c->voff), P<uint64_t>(c->toff), bp.tseq, s1, tile, d, b1,
                                          id_bits_for(n), P<uint64_t>(c->recB), P<uint32_t>(c->bcounts), nullptr, s0,
                                          rec0)));
-            XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<blocks_for(nb), kThreads, 0, s>>>(
+            XTN_LAUNCH("bucket_colscan", k_bucket_colscan<<<(nb + 31) / 32, kColscanWarps * 32, 0, s>>>(
                                              P<uint32_t>(c->bcounts), ntiles, nb, P<uint32_t>(c->boffs),
                                              P<uint32_t>(c->btotals)));
             XTN_TRY(scan_u32_to_u64(c, P<uint32_t>(c->btotals), P<uint64_t>(c->bstart), nb));
