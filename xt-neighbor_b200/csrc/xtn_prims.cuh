@@ -458,6 +458,11 @@ inline uint64_t* radix_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int lo
 // bits 32-61 epoch (a per-pass tag: words of earlier passes read as unset, so the array is
 // never cleared between passes), bits 0-31 the count.
 constexpr int kOsMaxPasses = 8;
+// A pass's tile: 16 keys per thread (4096 per CTA, three CTAs per SM); 8 keys per thread and
+// five CTAs per SM took 0.076 ms per pass for the 10M search's 5.2M distinct pairs.
+constexpr int kOsItems = 16;
+constexpr int kOsTile = kSortThreads * kOsItems;
+inline int64_t os_tiles(int64_t n) { return (n + kOsTile - 1) / kOsTile; }
 constexpr uint32_t kOsPollLimit = 1u << 22;
 constexpr uint32_t kOsMaxEpoch = (1u << 30) - 1u;
 constexpr unsigned long long kOsFlagCount = 1ull << 62;
@@ -503,13 +508,13 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep_hist(const uint64_t* 
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep_pass(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
                                                                 int64_t n, int shift, const uint32_t* __restrict__ dstart,
                                                                 unsigned long long* __restrict__ status, uint32_t epoch,
                                                                 unsigned int* __restrict__ ticket,
                                                                 unsigned int* __restrict__ err,
                                                                 const unsigned long long* __restrict__ n_dev) {
-    __shared__ uint64_t s_keys[kSortTile];
+    __shared__ uint64_t s_keys[kOsTile];
     __shared__ uint32_t s_cnt[kSortWarps][kRadix + 1];
     __shared__ uint32_t s_start[kRadix];
     __shared__ uint32_t s_base[kRadix];
@@ -523,7 +528,7 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
     for (int i = threadIdx.x; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&s_cnt[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
-    const int64_t tile_base = (int64_t)tile * kSortTile;
+    const int64_t tile_base = (int64_t)tile * kOsTile;
     // graph form: the grid covers n keys at most and the count is read on the device; tiles past
     // it leave before publishing (no later tile is real, so none waits for them)
     if (n_dev) {
@@ -531,13 +536,13 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
         if (tile_base >= n) return;
     }
     const int64_t valid64 = n - tile_base;
-    const int valid = valid64 > kSortTile ? kSortTile : (int)valid64;
+    const int valid = valid64 > kOsTile ? kOsTile : (int)valid64;
     const unsigned lt = (1u << lane) - 1u;
-    uint64_t key[kSortItems];
-    uint32_t rank[kSortItems];
+    uint64_t key[kOsItems];
+    uint32_t rank[kOsItems];
 #pragma unroll
-    for (int k = 0; k < kSortItems; k++) {
-        const int pos = warp * (32 * kSortItems) + k * 32 + lane;  // warp-contiguous tile order
+    for (int k = 0; k < kOsItems; k++) {
+        const int pos = warp * (32 * kOsItems) + k * 32 + lane;  // warp-contiguous tile order
         const bool ok = pos < valid;
         const uint64_t kv = ok ? in[tile_base + pos] : 0ull;
         const unsigned dg = ok ? (unsigned)((kv >> shift) & (kRadix - 1)) : (unsigned)kRadix;
@@ -601,8 +606,8 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
     s_base[d] = dstart[d] + excl - start;  // global index of local slot i of digit d: s_base[d] + i
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kSortItems; k++) {
-        const int pos = warp * (32 * kSortItems) + k * 32 + lane;
+    for (int k = 0; k < kOsItems; k++) {
+        const int pos = warp * (32 * kOsItems) + k * 32 + lane;
         if (pos < valid) {
             const unsigned dg = (unsigned)((key[k] >> shift) & (kRadix - 1));
             s_keys[s_start[dg] + s_cnt[warp][dg] + rank[k]] = key[k];
@@ -619,7 +624,7 @@ __global__ void __launch_bounds__(kSortThreads, 5) k_onesweep_pass(const uint64_
 }
 
 // Status words a single-sweep sort of n keys uses.
-inline int64_t onesweep_status_words(int64_t n) { return radix_tiles(n) * kRadix; }
+inline int64_t onesweep_status_words(int64_t n) { return os_tiles(n) * kRadix; }
 
 // Same contract as radix_sort_u64, for n < 2^32 and at most kOsMaxPasses passes. `scratch`
 // holds kOsScratchWords u32; `status` onesweep_status_words(n) words, all of whose epochs are
@@ -634,7 +639,7 @@ inline uint64_t* onesweep_sort_u64(uint64_t* keys, uint64_t* alt, int64_t n, int
                                    const unsigned long long* n_dev = nullptr) {
     if ((!n_dev && n <= 1) || hi_bit <= lo_bit) return keys;
     const int passes = (hi_bit - lo_bit + kRadixBits - 1) / kRadixBits;
-    const int64_t ntiles = radix_tiles(n);
+    const int64_t ntiles = os_tiles(n);
     uint32_t* dstart = scratch;
     uint32_t* counts = scratch + kOsStartWords;
     unsigned int* tickets = counts + kOsMaxPasses * kRadix;
