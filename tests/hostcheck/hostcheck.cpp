@@ -115,6 +115,10 @@ int hc_lev_myers(const char* a, int la, const char* b, int lb) {
     return lev_myers64((const uint8_t*)a, la, (const uint8_t*)b, lb);
 }
 
+int hc_lev_myers32(const char* a, int la, const char* b, int lb) {
+    return lev_myers<uint32_t>((const uint8_t*)a, la, (const uint8_t*)b, lb);
+}
+
 int hc_lev_dp(const char* a, int la, const char* b, int lb, int cap) {
     int col[kMaxInputLength + 2];
     return lev_dp((const uint8_t*)a, la, (const uint8_t*)b, lb, col, cap);

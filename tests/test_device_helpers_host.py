@@ -124,6 +124,8 @@ def test_levenshtein_myers_and_dp(hc):
         ref = orc.levenshtein(a, b)
         if len(a) <= 64:
             assert hc.hc_lev_myers(a.encode(), len(a), b.encode(), len(b)) == ref, (a, b)
+        if len(a) <= 32:  # the 32-bit word form, patterns of up to 32 residues
+            assert hc.hc_lev_myers32(a.encode(), len(a), b.encode(), len(b)) == ref, (a, b)
         assert hc.hc_lev_dp(a.encode(), len(a), b.encode(), len(b), 1000) == ref
         got = hc.hc_lev_dp(a.encode(), len(a), b.encode(), len(b), 2)
         assert (got == ref) if ref <= 2 else got > 2

@@ -449,43 +449,48 @@ inline uint64_t pow2_at_least(uint64_t x) {
 
 // ------------------------------------------------------------------ distances
 // Levenshtein distance by Myers' bit-vector algorithm in Hyyro's global form
-// (G. Myers, J. ACM 46(3) 1999; H. Hyyro, 2001). `a` is the pattern (1 <= m <= 64).
-XTN_HD int lev_myers64(const uint8_t* a, int m, const uint8_t* b, int n) {
-    uint64_t p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0;  // bit-sliced residue codes of a
+// (G. Myers, J. ACM 46(3) 1999; H. Hyyro, 2001). `a` is the pattern (1 <= m <= bits of W); W is
+// uint32_t for patterns of up to 32 residues (one instruction per word operation instead of two)
+// or uint64_t up to 64.
+template <class W>
+XTN_HD int lev_myers(const uint8_t* a, int m, const uint8_t* b, int n) {
+    constexpr int kBits = 8 * (int)sizeof(W);
+    W p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0;  // bit-sliced residue codes of a
     for (int i = 0; i < m; i++) {
         unsigned c = (unsigned)code_of(a[i]);
-        uint64_t bit = 1ull << i;
+        const W bit = (W)1 << i;
         if (c & 1u) p0 |= bit;
         if (c & 2u) p1 |= bit;
         if (c & 4u) p2 |= bit;
         if (c & 8u) p3 |= bit;
         if (c & 16u) p4 |= bit;
     }
-    const uint64_t mask = m == 64 ? ~0ull : ((1ull << m) - 1);
-    const uint64_t high = 1ull << (m - 1);
-    uint64_t pv = mask, mv = 0;
+    const W mask = m == kBits ? ~(W)0 : (W)(((W)1 << m) - 1);
+    const W high = (W)1 << (m - 1);
+    W pv = mask, mv = 0;
     int score = m;
     for (int j = 0; j < n; j++) {
         unsigned c = (unsigned)code_of(b[j]);
-        uint64_t eq = mask;
-        eq &= (c & 1u) ? p0 : ~p0;
-        eq &= (c & 2u) ? p1 : ~p1;
-        eq &= (c & 4u) ? p2 : ~p2;
-        eq &= (c & 8u) ? p3 : ~p3;
-        eq &= (c & 16u) ? p4 : ~p4;
-        uint64_t xv = eq | mv;
-        uint64_t xh = (((eq & pv) + pv) ^ pv) | eq;
-        uint64_t ph = mv | ~(xh | pv);
-        uint64_t mh = pv & xh;
+        W eq = mask;
+        eq &= (c & 1u) ? p0 : (W)~p0;
+        eq &= (c & 2u) ? p1 : (W)~p1;
+        eq &= (c & 4u) ? p2 : (W)~p2;
+        eq &= (c & 8u) ? p3 : (W)~p3;
+        eq &= (c & 16u) ? p4 : (W)~p4;
+        const W xv = eq | mv;
+        const W xh = (W)((W)((W)(eq & pv) + pv) ^ pv) | eq;
+        W ph = (W)(mv | (W)~(W)(xh | pv));
+        W mh = pv & xh;
         if (ph & high) score++;
         else if (mh & high) score--;
-        ph = (ph << 1) | 1ull;
-        mh = mh << 1;
-        pv = mh | ~(xv | ph);
+        ph = (W)((W)(ph << 1) | (W)1);
+        mh = (W)(mh << 1);
+        pv = (W)(mh | (W)~(W)(xv | ph));
         mv = ph & xv;
     }
     return score;
 }
+XTN_HD int lev_myers64(const uint8_t* a, int m, const uint8_t* b, int n) { return lev_myers<uint64_t>(a, m, b, n); }
 
 // Exact Levenshtein with the column held in `col` (>= m+1 ints), stopping early once every
 // cell of a column exceeds `cap` (the result is then some value > cap).

@@ -239,7 +239,9 @@ __device__ int pair_distance(const uint8_t* a, int la, const uint8_t* b, int lb,
         return diff;
     }
     int dv;
-    if (la <= 64 && la <= lb) dv = lev_myers64(a, la, b, lb);
+    if (la <= 32 && la <= lb) dv = lev_myers<uint32_t>(a, la, b, lb);
+    else if (lb <= 32 && lb <= la) dv = lev_myers<uint32_t>(b, lb, a, la);
+    else if (la <= 64 && la <= lb) dv = lev_myers64(a, la, b, lb);
     else if (lb <= 64) dv = lev_myers64(b, lb, a, la);
     else {
         int col[kMaxInputLength + 1];
