@@ -212,7 +212,11 @@ int xtn_context_profile_only(xtn_context* ctx, const char* name);
  *   "stage_chunk"     2048 | 4096 | 8192: records per shared-memory chunk of the first-level
  *                     scatter (default 4096: two CTAs of 512 threads per SM; 2048: four of 256;
  *                     8192: one of 1024, longer runs per bucket)
- *   "split_chunk"     2048 | 4096: the same for the split of large buckets (default 4096)
+ *   "split_chunk"     2048 | 4096: the same for the split of large buckets; 8192: the one-pass
+ *                     split (split_slotted) on 8192-record chunks, one CTA of 1024 threads per
+ *                     SM (the two-pass split then takes 4096); 0 (default): 8192 for the
+ *                     one-pass split when the first-level buckets average 2^20 records or
+ *                     more, else 4096
  *   "split_fill"      25..95 (default 87): a first-level bucket larger than group_cap is split
  *                     into ceil(size / (group_cap * split_fill / 100)) sub-buckets (at most
  *                     1024) by ranges of the records' top hash bits, so the sub-buckets hold about

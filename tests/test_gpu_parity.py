@@ -37,6 +37,8 @@ ENGINES = {
     # the two-pass split (slice histograms merged in a cluster, exact sub-bucket placement) in
     # place of the default one-pass split into fixed slots of the grouping capacity
     "bucket_two_pass_split": {"split_slotted": 0},
+    # the one-pass split on the 8192-record stage (records and ranks kept in registers)
+    "bucket_split_8192": {"split_chunk": 8192},
 }
 
 

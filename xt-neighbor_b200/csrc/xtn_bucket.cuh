@@ -968,6 +968,9 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
                            uint64_t* __restrict__ out, uint32_t slot, unsigned int* __restrict__ cursors,
                            unsigned int* __restrict__ counters, const unsigned int* __restrict__ abort) {
     constexpr int T = C::kThreads, kChunk = C::kChunk, kFanPer = C::kFanPer;
+    // the 8192-record stage (one CTA of 1024 threads per SM, 64 registers a thread) keeps a
+    // chunk's records in registers; the 4096-record one (two CTAs per SM) reads them twice
+    constexpr bool kKeep = C::kChunk >= 8192;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StageSmem<C>& S = *reinterpret_cast<StageSmem<C>*>(smem_raw);
     if (abort && *abort) return;
@@ -1022,6 +1025,59 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
         const uint64_t* r = S.rec + lead;
         for (uint32_t b = threadIdx.x; b < nsub; b += T) S.cnt[b] = 0;
         __syncthreads();
+        if constexpr (kKeep) {
+            // records and their ranks stay in registers (split_partition_ranked): one shared
+            // atomic per record, and the next chunk's copy starts once the chunk is read
+            uint32_t rk[C::kPer];
+            uint64_t xs[C::kPer];
+#pragma unroll
+            for (int k = 0; k < C::kPer; k++) {
+                const uint32_t p = threadIdx.x + (uint32_t)k * T;
+                rk[k] = ~0u;
+                xs[k] = 0;
+                if (p < m) {
+                    xs[k] = r[p];
+                    const uint32_t b = split_sub(xs[k], nsub);
+                    rk[k] = (b << 16) | atomicAdd(&S.cnt[b], 1u);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0 && c0 + kChunk < size) issue(c0 + kChunk);
+            {
+                uint32_t tot, loc[kFanPer], cnt[kFanPer], sum = 0;
+                const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++) {
+                    loc[k] = sum;
+                    cnt[k] = (b0 + k < (int)nsub) ? S.cnt[b0 + k] : 0u;
+                    sum += cnt[k];
+                }
+                const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++)
+                    if (cnt[k]) {
+                        S.lstart[b0 + k] = ex + loc[k];
+                        S.gcur[b0 + k] = atomicAdd(&cur[b0 + k], cnt[k]);  // this chunk's runs in the slot
+                    }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < C::kPer; k++) {
+                if (rk[k] == ~0u) continue;
+                const uint32_t b = rk[k] >> 16;
+                const uint32_t q = S.lstart[b] + (rk[k] & 0xffffu);
+                S.sorted[q] = xs[k];
+                S.sbkt[q] = (uint16_t)b;
+            }
+            __syncthreads();
+            for (uint32_t q = threadIdx.x; q < m; q += T) {
+                const uint16_t b = S.sbkt[q];
+                const uint32_t pos = S.gcur[b] + (q - S.lstart[b]);
+                if (pos < slot) dst[(uint64_t)b * slot + pos] = S.sorted[q];
+            }
+            __syncthreads();
+            continue;
+        }
         for (uint32_t p = threadIdx.x; p < m; p += T) atomicAdd(&S.cnt[split_sub(r[p], nsub)], 1u);
         __syncthreads();
         {

@@ -582,7 +582,7 @@ struct xtn_context {
     uint32_t wait_polls = kScanPollLimit;  // bound on a single-pass scan's look-back polls
     int wait_fault_test = 0;  // 1: the next variant-offset scan withholds tile 0's status word
     int stage_chunk = 4096;  // records per staged chunk of the first-level scatter (2048 | 4096 | 8192)
-    int split_chunk = 4096;  // the same for the split (2048 | 4096)
+    int split_chunk = 0;     // the same for the split (2048 | 4096 | 8192; 0: by bucket size)
     int split_slices = kSplitSlices;  // CTAs (one cluster) per split bucket: 1 | kSplitSlices
     uint32_t group_cap = kGroupCap;
     double last_pc_per_rec = 0;  // candidates per variant record of the previous run (buffer sizing)
@@ -889,6 +889,8 @@ static int bucket_attrs(xtn_context* c) {
                                 (int)sizeof(StageSmem<StageHuge>)));
     XTN_CK(cudaFuncSetAttribute(k_bucket_split_slotted<StageLarge, kSplitSlices>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageLarge>)));
+    XTN_CK(cudaFuncSetAttribute(k_bucket_split_slotted<StageHuge, kSplitSlices>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageSmem<StageHuge>)));
     c->attrs_set = true;
     return XTN_SUCCESS;
 }
@@ -1046,15 +1048,27 @@ static int bucket_prepare(xtn_context* c, int n, int d, uint64_t V, BucketPlan* 
 // split_slices CTAs per bucket, launched for every one of the b_n buckets without waiting for
 // the plan: those past the plan's job count exit at once. The slotted split (bp.slotted) takes
 // kSplitSlices independent CTAs per job and lists its sub-buckets afterwards.
+// recs: the records of the b_n first-level buckets (a capacity in the graph form). The one-pass
+// split takes the 8192-record stage when the buckets average 2^20 records or more (split_chunk 0)
+// or when split_chunk is 8192: at 10M sequences (2.1M-record buckets) it took 5.27 against 5.44
+// ms, at 1M (214k-record buckets, slices of 27k records) 0.57 against 0.49 ms.
 static void launch_split(xtn_context* c, const BucketPlan& bp, uint32_t b_n, uint64_t sub_bound, size_t desc_cap,
-                         const unsigned int* abort, cudaStream_t s) {
+                         uint64_t recs, const unsigned int* abort, cudaStream_t s) {
     if (bp.slotted) {
         cudaMemsetAsync(c->scur.p, 0, sizeof(uint32_t) * sub_bound, s);
-        XTN_LAUNCH("bucket_split",
-                   (k_bucket_split_slotted<StageLarge, kSplitSlices><<<b_n * kSplitSlices, StageLarge::kThreads,
-                                                                      sizeof(StageSmem<StageLarge>), s>>>(
-                       P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
-                       P<unsigned int>(c->scur), P<unsigned int>(c->bcnt), abort)));
+        const bool huge = c->split_chunk == 8192 || (c->split_chunk == 0 && b_n > 0 && recs / b_n >= (uint64_t(1) << 20));
+        if (huge)
+            XTN_LAUNCH("bucket_split",
+                       (k_bucket_split_slotted<StageHuge, kSplitSlices><<<b_n * kSplitSlices, StageHuge::kThreads,
+                                                                         sizeof(StageSmem<StageHuge>), s>>>(
+                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                           P<unsigned int>(c->scur), P<unsigned int>(c->bcnt), abort)));
+        else
+            XTN_LAUNCH("bucket_split",
+                       (k_bucket_split_slotted<StageLarge, kSplitSlices><<<b_n * kSplitSlices, StageLarge::kThreads,
+                                                                          sizeof(StageSmem<StageLarge>), s>>>(
+                           P<SplitJob>(c->bjobs), P<uint64_t>(c->recA), P<uint64_t>(c->recB), c->group_cap,
+                           P<unsigned int>(c->scur), P<unsigned int>(c->bcnt), abort)));
         XTN_LAUNCH("split_descs", k_split_slot_descs<<<b_n, 256, 0, s>>>(
                                       P<SplitJob>(c->bjobs), P<unsigned int>(c->scur), c->group_cap,
                                       P<BucketDesc>(c->bdesc), P<BucketDesc>(c->bfall), (uint32_t)desc_cap,
@@ -1146,7 +1160,7 @@ static int bucket_round(xtn_context* c, const BucketPlan& bp, int n, int d, int 
     XTN_CK(cudaGetLastError());
     uint32_t cnt[8] = {0};
     {
-        launch_split(c, bp, b_n, sub_bound, desc_cap, nullptr, s);
+        launch_split(c, bp, b_n, sub_bound, desc_cap, Vr, nullptr, s);
         XTN_CK(cudaGetLastError());
         XTN_CK(cudaMemcpyAsync(c->h_scalar, c->bcnt.p, 32, cudaMemcpyDeviceToHost, s));
         XTN_CK(cudaStreamSynchronize(s));
@@ -1821,7 +1835,7 @@ static int graph_enqueue(xtn_context* c, GraphState* g) {
     XTN_LAUNCH("bucket_plan", k_bucket_plan<<<blocks_for(nb), kThreads, 0, s>>>(
                                   bstart, nb, 0ull, c->group_cap, (uint32_t)c->split_fill, P<BucketDesc>(c->bdesc), (uint32_t)desc_cap,
                                   P<SplitJob>(c->bjobs), P<unsigned int>(c->bcnt), abort));
-    launch_split(c, bp, (uint32_t)nb, bp.sub_bound, desc_cap, abort, s);
+    launch_split(c, bp, (uint32_t)nb, bp.sub_bound, desc_cap, g->Vcap, abort, s);
     XTN_LAUNCH("set_cursor", k_set_u64<<<1, 1, 0, s>>>(P<unsigned long long>(c->counter), 0ull));
     XTN_CK(cudaMemsetAsync(P<unsigned long long>(c->counter) + 1, 0, 8, s));
     XTN_TRY(launch_group(c, 0, true, idbits, P<uint64_t>(c->pairA), g->Pcap, (uint32_t)desc_cap, s));
@@ -2873,7 +2887,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
         *ms = best;
         return XTN_SUCCESS;
     };
-    TuneShape best{4096, 4096, kMaxFirstLevelBits, 1, 1, 0, 1};
+    TuneShape best{4096, 0, kMaxFirstLevelBits, 1, 1, 0, 1};
     float best_ms = 1e30f;
     int tried = 0;
     auto consider = [&](const TuneShape& sh) -> int {
@@ -2892,7 +2906,7 @@ static int autotune(xtn_context* c, const xtn_args* args, const uint8_t* chars, 
     // stage shape and first-level bits
     for (int flat : {1, 0})
         for (int stage : {4096, 2048})
-            for (int split : {4096, 2048})
+            for (int split : {0, 2048})
                 for (int bits : {9, 10}) {
                     if (st != XTN_SUCCESS) break;
                     if (bits == 10 && stage == 2048) continue;  // 1024 first-level buckets need the large shape
@@ -3163,7 +3177,7 @@ int xtn_context_set_option(xtn_context* c, const char* name, int64_t v) {
     else if (!strcmp(name, "pair_dedup") && v >= 0 && v <= 2) c->pair_dedup = (int)v;
     else if (!strcmp(name, "key_tables") && (v == 0 || v == 1)) c->key_tables = (int)v;
     else if (!strcmp(name, "stage_chunk") && (v == 2048 || v == 4096 || v == 8192)) c->stage_chunk = (int)v;
-    else if (!strcmp(name, "split_chunk") && (v == 2048 || v == 4096)) c->split_chunk = (int)v;
+    else if (!strcmp(name, "split_chunk") && (v == 0 || v == 2048 || v == 4096 || v == 8192)) c->split_chunk = (int)v;
     else if (!strcmp(name, "split_slices") && (v == 1 || v == kSplitSlices)) c->split_slices = (int)v;
     else if (!strcmp(name, "wait_polls") && v >= 1 && v <= (int64_t)kScanPollLimit) c->wait_polls = (uint32_t)v;
     else if (!strcmp(name, "memory_budget") && v >= 0) c->memory_budget = v;
