@@ -105,3 +105,70 @@ def test_owner_ranges_cover_the_buckets_in_order():
         starts = np.concatenate([[0], np.cumsum(counts)])
         for k in range(1, K):  # rank k starts at the bucket holding record k V / K
             assert starts[b[k]] >= starts[-1] * k // K and (b[k] == 0 or starts[b[k] - 1] < starts[-1] * k // K)
+
+
+def rank_records(r, nb=40):
+    """Rank r's first-level bucket counts (some empty) and its records in bucket order, each
+    encoding (source rank, bucket, index)."""
+    rng = np.random.default_rng(100 + r)
+    counts = rng.integers(0, 30, nb)
+    counts[rng.random(nb) < 0.2] = 0
+    recs = np.concatenate([[(r << 40) | (b << 20) | i for i in range(int(c))] for b, c in enumerate(counts)] +
+                          [np.zeros(0, np.int64)]).astype(np.int64)
+    return counts, recs
+
+
+def record_worker(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.join(ROOT, "xt-neighbor_b200"))
+    import xtn
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        counts, recs = rank_records(rank)
+        t = torch.from_numpy(recs) if len(recs) else torch.zeros(1, dtype=torch.int64)
+        got, pieces, bounds = xtn.exchange_records(counts, t)
+        out.put((rank, got.numpy().copy(), pieces, bounds))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_three_rank_record_exchange_sends_each_owner_its_buckets():
+    """xtn.exchange_records (the sequence-sharded search's exchange): every owner receives the
+    records of its first-level buckets from every rank, one piece per source in rank order, with
+    the per-bucket counts that xtn_shard_search needs to gather them."""
+    sys.path.insert(0, os.path.join(ROOT, "xt-neighbor_b200"))
+    import xtn
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=record_worker, args=(r, WORLD, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    res = {r: (g, pc, b) for r, g, pc, b in (q.get(timeout=120) for _ in procs)}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    data = [rank_records(r) for r in range(WORLD)]
+    bounds = xtn.owner_ranges(sum(c for c, _ in data), WORLD)
+    total = 0
+    for k in range(WORLD):
+        got, pieces, b = res[k]
+        assert b == bounds
+        lo, hi = bounds[k], bounds[k + 1]
+        expect = np.concatenate([recs[((recs >> 20) & 0xFFFFF >= lo) & ((recs >> 20) & 0xFFFFF < hi)]
+                                 for _, recs in data])
+        assert np.array_equal(got, expect)
+        assert pieces.shape == (WORLD, hi - lo)
+        for p, (counts, _) in enumerate(data):
+            assert np.array_equal(pieces[p], counts[lo:hi].astype(np.uint64))
+        total += len(got)
+    assert total == sum(len(r) for _, r in data)

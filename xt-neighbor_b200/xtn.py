@@ -528,6 +528,33 @@ def owner_ranges(counts, n_ranks: int):
     return bounds
 
 
+def exchange_records(counts, recs, group=None):
+    """The record exchange of a sequence-sharded search: this rank's records `recs` (int64, on
+    the device the collectives use), partitioned into the search's first-level buckets with
+    counts[b] records in bucket b, go to the ranks that own their buckets. The bucket counts
+    are summed over the ranks (all-reduce), rank k owns owner_ranges(totals, K)[k:k+2], and two
+    all-to-alls send each owner its buckets' records and their per-bucket counts. Returns (the
+    records this rank received, one piece per source rank in rank order; piece_counts, a
+    K x b_n uint64 array: piece p holds piece_counts[p, j] records of this rank's j-th bucket;
+    the owner bounds)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    local = torch.from_numpy(np.asarray(counts).astype(np.int64)).to(recs.device)
+    total = local.clone()
+    dist.all_reduce(total, group=group)
+    bounds = owner_ranges(total.cpu().numpy(), world)
+    cum = np.concatenate([[0], np.cumsum(np.asarray(counts).astype(np.int64))])
+    # records: keys [cum[bounds[k]], cum[bounds[k+1]]) go to rank k
+    got = exchange_keys(recs, [int(cum[b]) for b in bounds], group)
+    # per-bucket counts of the sent pieces: counts[bounds[k]:bounds[k+1]] go to rank k
+    got_counts = exchange_keys(local, bounds, group)
+    b_n = bounds[rank + 1] - bounds[rank]
+    piece_counts = got_counts.cpu().numpy().astype(np.uint64).reshape(world, b_n)
+    return got, piece_counts, bounds
+
+
 def nn_sharded_exchange(ctx, d_chars: int, d_offsets: int, n: int, distance=1, measure=LEVENSHTEIN,
                         group=None) -> int:
     """One rank's part of a search sharded by sequences (xtn_shard_generate / xtn_shard_search):
@@ -542,19 +569,9 @@ def nn_sharded_exchange(ctx, d_chars: int, d_offsets: int, n: int, distance=1, m
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     dev = torch.device("cuda", torch.cuda.current_device())
     counts, ptr, nrec = ctx.shard_generate(d_chars, d_offsets, n, distance, measure, rank, world)
-    local = torch.from_numpy(counts.astype(np.int64)).to(dev)
-    total = local.clone()
-    dist.all_reduce(total, group=group)
-    bounds = owner_ranges(total.cpu().numpy(), world)
-    cum = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
-    # records: keys [cum[bounds[k]], cum[bounds[k+1]]) go to rank k
     recs = torch.as_tensor(_DeviceWords(ptr, nrec), device=dev) if nrec > 0 else torch.zeros(1, dtype=torch.int64,
                                                                                              device=dev)
-    got = exchange_keys(recs, [int(cum[b]) for b in bounds], group)
-    # per-bucket counts of the sent pieces: counts[bounds[k]:bounds[k+1]] go to rank k
-    got_counts = exchange_keys(local, bounds, group)
-    b_n = bounds[rank + 1] - bounds[rank]
-    piece_counts = got_counts.cpu().numpy().astype(np.uint64).reshape(world, b_n)
+    got, piece_counts, _ = exchange_records(counts, recs, group)
     m = ctx.shard_search(d_chars, d_offsets, n, distance, measure, got.data_ptr(), piece_counts)
     keys = torch.empty(max(m, 1), dtype=torch.int64, device=dev)
     starts = ctx.result_keys(n, keys.data_ptr(), keys.numel(), world)
