@@ -115,6 +115,8 @@ int hc_lev_myers(const char* a, int la, const char* b, int lb) {
     return lev_myers64((const uint8_t*)a, la, (const uint8_t*)b, lb);
 }
 
+int hc_first_bad_offset(const uint32_t* offs, int n, int threads) { return first_bad_offset(offs, n, threads); }
+
 int hc_lev_myers32(const char* a, int la, const char* b, int lb) {
     return lev_myers<uint32_t>((const uint8_t*)a, la, (const uint8_t*)b, lb);
 }

@@ -199,3 +199,36 @@ def test_hash_set_sizing(hc):
     # a rerun gets four times the slots, and never fewer than two per candidate
     assert regrow(1 << 16, 1_000_000) == 1 << 21
     assert regrow(1 << 25, 1_000_000) == 1 << 27
+
+
+def test_first_bad_offset_threaded_scan(hc):
+    """The host length check of the whole-search entry point (first_bad_offset): from 2^20
+    sequences on up to four threads scan parts of the offsets; the first bad sequence must be
+    found wherever it lies (part boundaries, the last part) and with any thread count."""
+    f = hc.hc_first_bad_offset
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    f.restype = ctypes.c_int
+    n = (1 << 21) + 7
+    lens = np.random.default_rng(12).integers(1, 40, n).astype(np.uint32)
+    good = np.zeros(n + 1, np.uint32)
+    good[1:] = np.cumsum(lens)
+    for threads in (1, 2, 4):
+        assert f(good.ctypes.data, n, threads) == -1
+    for pos in (0, n // 4 - 1, n // 4, n // 2 + 3, 3 * n // 4, n - 1):
+        for kind in ("empty", "long", "down"):
+            o = good.copy()
+            if kind == "empty":
+                o[pos + 1:] -= lens[pos]  # sequence pos has no residues
+            elif kind == "long":
+                o[pos + 1:] += 501 - lens[pos]
+            else:
+                o[pos + 1] = o[pos] - 1 if o[pos] > 0 else 0
+            for threads in (1, 2, 4):
+                assert f(o.ctypes.data, n, threads) == pos, (pos, kind, threads)
+    o = good.copy()
+    o[n - 2 + 1:] += 600  # sequence n - 2 too long
+    o[5 + 1:] -= lens[5]  # and sequence 5 empty: the first is reported
+    assert f(o.ctypes.data, n, 4) == 5
+    small = good[:1001].copy()
+    small[11] = small[10]
+    assert f(small.ctypes.data, 1000, 4) == 10

@@ -1071,46 +1071,40 @@ __global__ void __launch_bounds__(C::kThreads, stage_ctas_per_sm<C>())
                 S.sbkt[q] = (uint16_t)b;
             }
             __syncthreads();
-            for (uint32_t q = threadIdx.x; q < m; q += T) {
-                const uint16_t b = S.sbkt[q];
-                const uint32_t pos = S.gcur[b] + (q - S.lstart[b]);
-                if (pos < slot) dst[(uint64_t)b * slot + pos] = S.sorted[q];
+        } else {
+            for (uint32_t p = threadIdx.x; p < m; p += T) atomicAdd(&S.cnt[split_sub(r[p], nsub)], 1u);
+            __syncthreads();
+            {
+                uint32_t tot, loc[kFanPer], cnt[kFanPer], sum = 0;
+                const int b0 = threadIdx.x * kFanPer;
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++) {
+                    loc[k] = sum;
+                    cnt[k] = (b0 + k < (int)nsub) ? S.cnt[b0 + k] : 0u;
+                    sum += cnt[k];
+                }
+                const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
+#pragma unroll
+                for (int k = 0; k < kFanPer; k++)
+                    if (cnt[k]) {
+                        S.lstart[b0 + k] = ex + loc[k];
+                        S.cnt[b0 + k] = ex + loc[k];
+                        S.gcur[b0 + k] = atomicAdd(&cur[b0 + k], cnt[k]);  // this chunk's runs in the slot
+                    }
             }
             __syncthreads();
-            continue;
-        }
-        for (uint32_t p = threadIdx.x; p < m; p += T) atomicAdd(&S.cnt[split_sub(r[p], nsub)], 1u);
-        __syncthreads();
-        {
-            uint32_t tot, loc[kFanPer], cnt[kFanPer], sum = 0;
-            const int b0 = threadIdx.x * kFanPer;
-#pragma unroll
-            for (int k = 0; k < kFanPer; k++) {
-                loc[k] = sum;
-                cnt[k] = (b0 + k < (int)nsub) ? S.cnt[b0 + k] : 0u;
-                sum += cnt[k];
+            // (the ranks kept in registers from the counting pass, as split_partition_ranked does,
+            // measured slower here: 5.53 against 5.44 ms at 10M)
+            for (uint32_t p = threadIdx.x; p < m; p += T) {
+                const uint64_t x = r[p];
+                const uint32_t b = split_sub(x, nsub);
+                const uint32_t q = atomicAdd(&S.cnt[b], 1u);
+                S.sorted[q] = x;
+                S.sbkt[q] = (uint16_t)b;
             }
-            const uint32_t ex = block_scan_ex<uint32_t, T>(sum, &tot, S.warp_sums);
-#pragma unroll
-            for (int k = 0; k < kFanPer; k++)
-                if (cnt[k]) {
-                    S.lstart[b0 + k] = ex + loc[k];
-                    S.cnt[b0 + k] = ex + loc[k];
-                    S.gcur[b0 + k] = atomicAdd(&cur[b0 + k], cnt[k]);  // this chunk's runs in the slot
-                }
+            __syncthreads();
+            if (threadIdx.x == 0 && c0 + kChunk < size) issue(c0 + kChunk);
         }
-        __syncthreads();
-        // (the ranks kept in registers from the counting pass, as split_partition_ranked does,
-        // measured slower here: 5.53 against 5.44 ms at 10M)
-        for (uint32_t p = threadIdx.x; p < m; p += T) {
-            const uint64_t x = r[p];
-            const uint32_t b = split_sub(x, nsub);
-            const uint32_t q = atomicAdd(&S.cnt[b], 1u);
-            S.sorted[q] = x;
-            S.sbkt[q] = (uint16_t)b;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && c0 + kChunk < size) issue(c0 + kChunk);
         for (uint32_t q = threadIdx.x; q < m; q += T) {
             const uint16_t b = S.sbkt[q];
             const uint32_t pos = S.gcur[b] + (q - S.lstart[b]);

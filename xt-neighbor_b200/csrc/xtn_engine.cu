@@ -2067,43 +2067,12 @@ static int check_args(const xtn_args* a) {
     return XTN_SUCCESS;
 }
 
-// Every sequence must have 1..kMaxInputLength residues. The scan has no early exit so that the
-// compiler vectorises it; the first bad index is searched for only when one exists. From 2^20
-// sequences on, four host threads share the scan: xtn_context_perform runs it while the input
-// copies are in flight, and one thread took 5.5 ms for 10M offsets, longer than the 3.4 ms
-// copy, so the first kernel waited on it (four threads: about 1.5 ms).
-static uint32_t offsets_bad(const uint32_t* offs, int a, int b) {
-    uint32_t bad = 0;
-    for (int i = a; i < b; i++)
-        bad |= (uint32_t)(offs[i + 1] <= offs[i]) | (uint32_t)(offs[i + 1] - offs[i] > (uint32_t)kMaxInputLength);
-    return bad;
-}
-
+// Every sequence must have 1..kMaxInputLength residues (first_bad_offset: a threaded scan).
 static int check_offsets(const uint32_t* offs, int n) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = n >= (1 << 20) ? (int)std::min(4u, std::max(1u, hw)) : 1;
-    uint32_t bad = 0;
-    if (nt <= 1) {
-        bad = offsets_bad(offs, 0, n);
-    } else {
-        uint32_t part[4] = {0, 0, 0, 0};
-        std::thread th[3];
-        for (int t = 1; t < nt; t++)
-            th[t - 1] = std::thread([=, &part] {
-                part[t] = offsets_bad(offs, (int)((int64_t)n * t / nt), (int)((int64_t)n * (t + 1) / nt));
-            });
-        part[0] = offsets_bad(offs, 0, (int)((int64_t)n / nt));
-        for (int t = 1; t < nt; t++) th[t - 1].join();
-        for (int t = 0; t < nt; t++) bad |= part[t];
-    }
-    if (!bad) return XTN_SUCCESS;
-    for (int i = 0; i < n; i++) {
-        if (offs[i + 1] <= offs[i] || offs[i + 1] - offs[i] > (uint32_t)kMaxInputLength) {
-            set_err("sequence " + std::to_string(i) + " has an invalid length");
-            return XTN_ERR_ARG;
-        }
-    }
-    return XTN_SUCCESS;
+    const int i = first_bad_offset(offs, n);
+    if (i < 0) return XTN_SUCCESS;
+    set_err("sequence " + std::to_string(i) + " has an invalid length");
+    return XTN_ERR_ARG;
 }
 
 static int upload(xtn_context* c, const char* seqs, const uint32_t* offsets, int n) {
